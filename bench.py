@@ -1,0 +1,461 @@
+"""Benchmark of the geodesic hot path on B200 (one JSON line on rank 0).
+
+Workload (default): the raw-throughput case -- 2^20 photons per GPU on the
+Kerr-Schild sphere r = 30 M, directions uniform on the local sky, spin
+uniform in [-0.95, 0.95] per ray, past-directed null momenta; each step is
+2000 attempted DP5(4) steps per ray with per-ray error control (rtol 1e-8,
+atol 1e-10, h0 0.1, max_step 2) and no termination.  The product arm runs
+the mixed-precision kernel (float32 stage arithmetic, float64 state, error
+norm and step control); the plain float64 kernel runs on the same inputs and
+is reported beside it.  Synthetic data from seed 20260 (the reference's
+benchmark has no dataset).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision mixed|fp64] [--rays R] [--dp5-steps S]
+
+Timing: W untimed steps, then K steps between a barrier + synchronize on both
+sides, CUDA events on the launching stream, max over ranks; a 256 MiB buffer
+is written between timed steps to flush L2.  Multi-GPU runs give each rank
+its own 2^20 rays (weak scaling, no collective in the data path).
+
+``--impl reference`` times the CPU restatement of the reference's algorithm
+(oracle/bh_oracle.c, all host cores) on a bounded sample of the same
+workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# Algorithmic FLOPs of one attempted DP5(4) ray-step: 6 RHS evaluations
+# (first-same-as-last) x 146 + 419 for the stage combinations + 41 for the
+# error norm, every +,-,*,/,sqrt counted once, as the reference writes them
+# (geodesics.py:42-74, kerr.py:118-193, integrators.py:76-117).
+FLOPS_PER_RAY_STEP = 1336
+# Algorithmic HBM bytes per ray of one propagate launch: state in and out
+# (2 x 64), spin (8), step size in and out (2 x 8), accepted count (8).
+BYTES_PER_RAY = 160
+
+METRIC = "ray-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--precision", choices=("mixed", "fp64"), default="mixed")
+    ap.add_argument("--rays", type=int, default=1 << 20, help="rays per GPU")
+    ap.add_argument("--dp5-steps", type=int, default=2000)
+    ap.add_argument("--variant", type=int, default=-1)
+    ap.add_argument("--no-fp64", action="store_true", help="skip the float64 comparison arm")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+# --------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device_index}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------ workload
+def make_inputs(n, rank, device):
+    import torch
+
+    from blackhorizon_b200.geodesics import null_momentum_from_velocity
+    from blackhorizon_b200.kerr import KerrSpacetime
+    from blackhorizon_b200.workloads import raw_throughput_inputs
+
+    pos, d, spin = raw_throughput_inputs(n, offset=rank * n)
+
+    class _PerRay(KerrSpacetime):
+        pass
+
+    st = object.__new__(_PerRay)
+    st.mass = 1.0
+    st.spin = torch.as_tensor(spin, device=device)
+    mom = null_momentum_from_velocity(st, torch.as_tensor(pos, device=device),
+                                      torch.as_tensor(d, device=device), "past")
+    state0 = torch.empty((n, 8), dtype=torch.float64, device=device)
+    state0[:, 0] = 0.0
+    state0[:, 1:4] = torch.as_tensor(pos, device=device)
+    state0[:, 4:8] = mom
+    return state0, torch.as_tensor(spin, device=device), pos, d, spin
+
+
+def fma_peak(precision: str, device):
+    """Measured CUDA-core FMA throughput (TFLOP/s) on this GPU."""
+    import torch
+
+    from blackhorizon_b200 import _lib
+    from blackhorizon_b200.backend import stream_handle
+
+    lib = _lib.load()
+    sink = torch.zeros(1, dtype=torch.float64, device=device)
+    flops = _lib._I64(0)
+    code = _lib.PRECISION[precision]
+    iters = 4096 if precision == "mixed" else 2048
+    best = 0.0
+    for _ in range(4):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _lib.check(lib.bh_fma_peak_launch(code, iters, sink.data_ptr(), flops, stream_handle()))
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, flops.value / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    return best
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from blackhorizon_b200 import _lib
+    from blackhorizon_b200.backend import stream_handle
+    from blackhorizon_b200.integrators import make_config, propagate
+    from blackhorizon_b200.kerr import KerrSpacetime
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=device)
+    n = args.rays
+    S = args.dp5_steps
+    lib = _lib.load()
+    state0, spins, pos_h, dir_h, spin_h = make_inputs(n, rank, device)
+    work = torch.empty_like(state0)
+    h = torch.empty(n, dtype=torch.float64, device=device)
+    acc = torch.empty(n, dtype=torch.int64, device=device)
+    ws = torch.empty(lib.bh_trace_workspace_bytes(), dtype=torch.uint8, device=device)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
+    stream = stream_handle()
+
+    def barrier():
+        if world > 1:
+            dist.barrier(device_ids=[local])
+        torch.cuda.synchronize()
+
+    def one_step(precision, kev=None):
+        work.copy_(state0)
+        h.fill_(0.1)
+        cfg = make_config(1, 1e-8, 1e-10, 0.1, 2.0, 0.0, precision, "aos", 600.0,
+                          args.variant)
+        if kev is not None:
+            kev[0].record()
+        rc = lib.bh_propagate(cfg, 1.0, 0.0, spins.data_ptr(), work.data_ptr(), h.data_ptr(),
+                              acc.data_ptr(), n, S, ws.data_ptr(), stream)
+        if kev is not None:
+            kev[1].record()
+        _lib.check(rc, "bench propagate")
+
+    def timed(precision, k, w, sample_clocks=False):
+        for _ in range(w):
+            one_step(precision)
+        flush.fill_(1)
+        barrier()
+        sampler = ClockSampler(local) if sample_clocks else None
+        if sampler:
+            sampler.start()
+            time.sleep(0.5)
+        kevs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                for _ in range(k)]
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        t0.record()
+        for i in range(k):
+            one_step(precision, kevs[i])
+            if i + 1 < k:
+                flush.fill_(i & 0xFF)
+        t1.record()
+        barrier()
+        clocks = sampler.stop() if sampler else None
+        st = _lib.TraceStats()
+        _lib.check(lib.bh_trace_stats_read(ws.data_ptr(), st, stream), "bench stats")
+        if st.attempts != n * S:
+            raise RuntimeError(f"propagate did {st.attempts} attempts, expected {n * S}")
+        total_ms = t0.elapsed_time(t1)
+        kernel_ms = sum(a.elapsed_time(b) for a, b in kevs) / k
+        if world > 1:
+            tt = torch.tensor([total_ms], dtype=torch.float64, device=device)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            total_ms = float(tt.item())
+        return total_ms / k, kernel_ms, clocks
+
+    prec = args.precision
+    ms_step, kernel_ms, clocks = timed(prec, args.steps, max(args.warmup, 3), True)
+    final = work.clone()
+    value = world * n * S / (ms_step * 1e-3)
+
+    fp64 = None
+    if not args.no_fp64 and prec != "fp64":
+        ms64, k64, _ = timed("fp64", max(1, args.steps), max(args.warmup, 3))
+        final64 = work.clone()
+        fp64 = {"value": world * n * S / (ms64 * 1e-3), "ms_per_step": ms64,
+                "kernel_ms": k64}
+    else:
+        final64 = None
+
+    # ---- end to end through the public API with host (pinned) buffers
+    host_state = state0.cpu().pin_memory()
+    host_spin = torch.as_tensor(spin_h).pin_memory()
+    st_mass = KerrSpacetime(1.0, 0.0)
+    e2e_k = max(1, min(args.steps, 3))
+
+    def e2e_step():
+        s_dev = host_state.to(device, non_blocking=True)
+        sp_dev = host_spin.to(device, non_blocking=True)
+        out, _, _, _ = propagate(st_mass, s_dev, S, rtol=1e-8, atol=1e-10,
+                                 precision=prec, spins=sp_dev, in_place=True,
+                                 timeout_s=600.0, variant=args.variant, workspace=ws)
+        return out.to("cpu")
+
+    e2e_step()
+    barrier()
+    w0 = time.perf_counter()
+    for _ in range(e2e_k):
+        res = e2e_step()
+    barrier()
+    e2e_s = (time.perf_counter() - w0) / e2e_k
+    if world > 1:
+        tt = torch.tensor([e2e_s], dtype=torch.float64, device=device)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    del res
+
+    out = None
+    if rank == 0:
+        peak_name = "fp32" if prec == "mixed" else "fp64"
+        peak = fma_peak(prec, device)
+        achieved = n * S * FLOPS_PER_RAY_STEP / (kernel_ms * 1e-3) / 1e12
+        out = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "ray-steps/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": max(args.warmup, 3),
+            "ms_per_step": ms_step,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32+f64" if prec == "mixed" else "f64",
+            "data": "synthetic (seed 20260)",
+            "config": {
+                "workload": "raw-throughput: 2^20 photons/GPU on KS r=30, per-ray spin "
+                            "U[-0.95,0.95], 2000 attempted DP5(4) steps, no termination",
+                "rays_per_gpu": n, "dp5_steps_per_ray": S, "rtol": 1e-8, "atol": 1e-10,
+                "precision": prec, "l2": "flushed between timed steps (256 MiB write)",
+                "parallelism": f"weak: {n} rays per GPU, no collective",
+            },
+            "ns_per_ray_step": ms_step * 1e6 / (world * n * S),
+            "roofline": {
+                "bound": peak_name,
+                "achieved": achieved,
+                "peak": peak,
+                "unit": "TFLOP/s",
+                "frac": achieved / peak,
+                "peak_source": f"measured in this run: {peak_name} FMA loop kernel "
+                               "(bh_fma_peak_launch), FMA = 2 FLOP",
+                "flops_per_ray_step": FLOPS_PER_RAY_STEP,
+                "hbm_gbs": n * BYTES_PER_RAY / (kernel_ms * 1e-3) / 1e9,
+                "traffic": None,
+            },
+            "gpu_launches": args.steps,
+            "e2e": {
+                "value": world * n * S / e2e_s,
+                "unit": "ray-steps/s",
+                "h2d_bytes_per_step": n * 8 * 8 + n * 8,
+                "d2h_bytes_per_step": n * 8 * 8,
+            },
+            "clocks": clocks,
+        }
+        if fp64 is not None:
+            out["fp64"] = fp64
+            out["speedup_vs_fp64"] = fp64["ms_per_step"] / ms_step
+            d = final.cpu().numpy()
+            d64 = final64.cpu().numpy()
+            rel = np.max(np.abs(d - d64) / np.maximum(np.abs(d64), 1.0), axis=1)
+            out["mixed_vs_fp64_endpoint_err"] = {
+                "median": float(np.median(rel)), "p99": float(np.quantile(rel, 0.99))}
+        if not args.no_cpu:
+            out["cpu_baseline"], errs = cpu_baseline(state0, spin_h, S, args.cpu_seconds,
+                                                     final, final64)
+            out["endpoint_err_vs_oracle"] = errs
+    if world > 1:
+        dist.barrier(device_ids=[local])
+        dist.destroy_process_group()
+    return out
+
+
+def cpu_baseline(state0, spin_h, S, seconds, final, final64):
+    """The CPU oracle (oracle/bh_oracle.c, every host core) on the first rays
+    of the same workload, sized to about `seconds` of CPU time; also the
+    endpoint error of the GPU results on those rays."""
+    from oracle import oracle
+
+    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    s0 = state0.cpu().numpy()
+    probe = max(threads, 8)
+    t = time.perf_counter()
+    oracle.propagate(1.0, spin_h[:probe], s0[:probe], S, 1e-8, 1e-10, nthreads=threads)
+    rate = probe * S / max(time.perf_counter() - t, 1e-6)
+    m = int(min(s0.shape[0], max(probe, rate * seconds / S)))
+    m = max(threads, (m // threads) * threads)
+    t = time.perf_counter()
+    ref, _, _ = oracle.propagate(1.0, spin_h[:m], s0[:m], S, 1e-8, 1e-10, nthreads=threads)
+    dt = time.perf_counter() - t
+    base = {"value": m * S / dt, "unit": "ray-steps/s", "cores": threads, "kind": "port",
+            "sample": f"first {m} rays x {S} attempted DP5(4) steps of the same workload, "
+                      f"oracle/bh_oracle.c on {threads} threads, {dt:.1f} s"}
+    errs = {}
+    for name, arr in (("mixed", final), ("fp64", final64)):
+        if arr is None:
+            continue
+        got = arr[:m].cpu().numpy()
+        ok = np.all(np.isfinite(ref), axis=1)
+        rel = np.max(np.abs(got[ok] - ref[ok]) / np.maximum(np.abs(ref[ok]), 1.0), axis=1)
+        errs[name] = {"rays": int(ok.sum()), "median": float(np.median(rel)),
+                      "p90": float(np.quantile(rel, 0.9)), "max": float(np.max(rel))}
+    return base, errs
+
+
+def run_reference(args):
+    """The CPU restatement of the reference algorithm on this host's cores;
+    rank 0 only."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return None
+    from oracle import oracle
+
+    from blackhorizon_b200.workloads import raw_throughput_inputs
+
+    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    S = args.dp5_steps
+    # Initial states of the first rays, through the oracle's null momentum.
+    probe_n = max(threads, 8)
+    pos, d, spin = raw_throughput_inputs(max(probe_n, 65536))
+
+    def states(m):
+        p = np.stack([oracle.null_momentum(1.0, float(spin[i]), pos[i:i + 1], d[i:i + 1])[0]
+                      for i in range(m)])
+        s = np.zeros((m, 8))
+        s[:, 1:4] = pos[:m]
+        s[:, 4:8] = p
+        return s
+
+    t = time.perf_counter()
+    oracle.propagate(1.0, spin[:probe_n], states(probe_n), S, 1e-8, 1e-10, nthreads=threads)
+    rate = probe_n * S / max(time.perf_counter() - t, 1e-6)
+    m = int(min(65536, max(probe_n, rate * 5.0 / S)))
+    m = max(threads, (m // threads) * threads)
+    s0 = states(m)
+    for _ in range(max(args.warmup, 3) if args.warmup else 0):
+        oracle.propagate(1.0, spin[:m], s0[: max(threads, 8)], 50, 1e-8, 1e-10, nthreads=threads)
+    times = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        oracle.propagate(1.0, spin[:m], s0, S, 1e-8, 1e-10, nthreads=threads)
+        times.append(time.perf_counter() - t)
+    ms = 1e3 * sum(times) / len(times)
+    value = m * S / (ms * 1e-3)
+    return {
+        "impl": "reference",
+        "metric": METRIC, "value": value, "unit": "ray-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seed 20260)",
+        "config": {"workload": "raw-throughput (bounded sample): first rays of the 2^20-photon "
+                               "workload, 2000 attempted DP5(4) steps, per-ray spin",
+                   "rays_per_step": m, "dp5_steps_per_ray": S, "rtol": 1e-8, "atol": 1e-10},
+        "cpu_baseline": {"value": value, "unit": "ray-steps/s", "cores": threads, "kind": "port",
+                         "sample": f"{m} rays x {S} steps per step, oracle/bh_oracle.c "
+                                   f"(float64 C restatement of the reference), {threads} threads"},
+        "e2e": {"value": value, "unit": "ray-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        out = run_reference(args)
+    else:
+        out = run_ours(args)
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

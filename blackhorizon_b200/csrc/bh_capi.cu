@@ -1,0 +1,645 @@
+// bh_capi.cu -- extern "C" entry points of libbh_b200.so and the point-wise
+// kernels (geometry, RHS, Hamiltonian, velocity, null momentum, camera rays,
+// single DP5 / RK4 steps, error ratio, step factor).
+//
+// Every entry point validates its arguments on the host, launches on the
+// caller's stream and returns a bh_status; nothing here allocates device
+// memory.  The reference function each one replaces is cited in
+// include/bh_b200.h.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "bh_device.cuh"
+#include "bh_internal.h"
+
+namespace bh {
+
+static thread_local char g_last_error[512] = "";
+
+void set_error(const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
+    va_end(ap);
+}
+
+static int cuda_status(cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return BH_OK;
+    set_error("%s: %s", what, cudaGetErrorString(e));
+    return BH_ERR_CUDA;
+}
+
+static int invalid(const char *msg) {
+    set_error("%s", msg);
+    return BH_ERR_INVALID_ARGUMENT;
+}
+
+static bool kerr_ok(double mass, double spin) {
+    // kerr.py:65-71: mass > 0 and |a| <= M.
+    return mass > 0.0 && std::fabs(spin) <= mass && std::isfinite(mass) &&
+           std::isfinite(spin);
+}
+
+static constexpr int kBlock = 256;
+
+static unsigned grid_for(long long n) {
+    long long g = (n + kBlock - 1) / kBlock;
+    if (g < 1) g = 1;
+    if (g > 0x7fffffffLL) g = 0x7fffffffLL;
+    return (unsigned)g;
+}
+
+__device__ __forceinline__ long long tid() {
+    return (long long)blockIdx.x * blockDim.x + threadIdx.x;
+}
+
+// ------------------------------------------------------------ point-wise
+
+__global__ void geometry_kernel(double m, double a, const double *x,
+                                const double *y, const double *z,
+                                long long stride, long long n, double *r,
+                                double *h, double *l, double *gh, double *gl) {
+    const long long i = tid();
+    if (i >= n) return;
+    Geometry g;
+    const bool grads = gh != nullptr || gl != nullptr;
+    geometry_full(m, a, x[i * stride], y[i * stride], z[i * stride], grads, g);
+    if (r) r[i] = g.r;
+    if (h) h[i] = g.h;
+    if (l) { l[3 * i] = g.l[0]; l[3 * i + 1] = g.l[1]; l[3 * i + 2] = g.l[2]; }
+    if (gh) { gh[3 * i] = g.grad_h[0]; gh[3 * i + 1] = g.grad_h[1]; gh[3 * i + 2] = g.grad_h[2]; }
+    if (gl) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) gl[9 * i + 3 * j + k] = g.grad_l[j][k];
+    }
+}
+
+__device__ __forceinline__ RayState read_state(const double *s, long long i) {
+    const double *p = s + 8 * i;
+    RayState y;
+    y.t = p[0]; y.x = p[1]; y.y = p[2]; y.z = p[3];
+    y.pt = p[4]; y.px = p[5]; y.py = p[6]; y.pz = p[7];
+    return y;
+}
+
+__device__ __forceinline__ void write_state(double *s, long long i, const RayState &y) {
+    double *p = s + 8 * i;
+    p[0] = y.t; p[1] = y.x; p[2] = y.y; p[3] = y.z;
+    p[4] = y.pt; p[5] = y.px; p[6] = y.py; p[7] = y.pz;
+}
+
+__global__ void rhs_kernel(double m, double a, const double *state,
+                           double *deriv, long long n) {
+    const long long i = tid();
+    if (i >= n) return;
+    const RayState y = read_state(state, i);
+    const Deriv<double> d = rhs<double>(m, a, y.x, y.y, y.z, y.pt, y.px, y.py, y.pz);
+    double *o = deriv + 8 * i;
+    o[0] = -y.pt + d.thl;
+    o[1] = y.px + d.qx;
+    o[2] = y.py + d.qy;
+    o[3] = y.pz + d.qz;
+    o[4] = 0.0;
+    o[5] = d.px; o[6] = d.py; o[7] = d.pz;
+}
+
+__global__ void hamiltonian_kernel(double m, double a, const double *state,
+                                   double *out, long long n) {
+    const long long i = tid();
+    if (i >= n) return;
+    const RayState y = read_state(state, i);
+    Geometry g;
+    geometry_full(m, a, y.x, y.y, y.z, false, g);
+    const double lp = -y.pt + (g.l[0] * y.px + g.l[1] * y.py + g.l[2] * y.pz);
+    const double eta = 0.5 * (-y.pt * y.pt + (y.px * y.px + y.py * y.py + y.pz * y.pz));
+    out[i] = eta - g.h * lp * lp;
+}
+
+__global__ void velocity_kernel(double m, double a, const double *state,
+                                double *out, long long n) {
+    const long long i = tid();
+    if (i >= n) return;
+    const RayState y = read_state(state, i);
+    Geometry g;
+    geometry_full(m, a, y.x, y.y, y.z, false, g);
+    const double lp = -y.pt + (g.l[0] * y.px + g.l[1] * y.py + g.l[2] * y.pz);
+    const double thl = 2.0 * g.h * lp;
+    double *o = out + 4 * i;
+    o[0] = -y.pt + thl;
+    o[1] = y.px - thl * g.l[0];
+    o[2] = y.py - thl * g.l[1];
+    o[3] = y.pz - thl * g.l[2];
+}
+
+__global__ void null_momentum_kernel(double m, double a, const double *spins,
+                                     const double *pos, const double *dir,
+                                     long long n, int past, int normalize,
+                                     double *out) {
+    const long long i = tid();
+    if (i >= n) return;
+    const double pp[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+    const double dd[3] = {dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]};
+    double p[4];
+    null_momentum(m, spins ? spins[i] : a, pp, dd, past != 0, normalize != 0, p);
+    double *o = out + 4 * i;
+    o[0] = p[0]; o[1] = p[1]; o[2] = p[2]; o[3] = p[3];
+}
+
+__global__ void camera_states_kernel(CameraDev c, double *state, long long n) {
+    const long long i = tid();
+    if (i >= n) return;
+    double d[3], p[4];
+    pinhole_direction(c.fwd, c.right, c.up, c.half_w, c.half_h, c.width,
+                      c.height, i, d);
+    null_momentum(c.mass, c.spin, c.pos, d, true, true, p);
+    RayState y;
+    y.t = 0.0; y.x = c.pos[0]; y.y = c.pos[1]; y.z = c.pos[2];
+    y.pt = p[0]; y.px = p[1]; y.py = p[2]; y.pz = p[3];
+    write_state(state, i, y);
+}
+
+template <typename W>
+__global__ void dp5_kernel(double m, double a, const double *state,
+                           const double *h, double *out, double *err,
+                           long long n) {
+    const long long i = tid();
+    if (i >= n) return;
+    const RayState y = read_state(state, i);
+    const Stage<W> k1 = first_stage<W>(W(m), W(a), y);
+    Attempt<W> at;
+    dp5_attempt<W>(W(m), W(a), y, h[i], k1, at);
+    write_state(out, i, at.y_new);
+    double *e = err + 8 * i;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) e[j] = at.err[j];
+}
+
+__global__ void error_ratio_kernel(const double *s, const double *sn,
+                                   const double *err, double rtol, double atol,
+                                   double *out, long long n) {
+    const long long i = tid();
+    if (i >= n) return;
+    const RayState y = read_state(s, i), yn = read_state(sn, i);
+    double e[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) e[j] = err[8 * i + j];
+    out[i] = error_ratio<double>(y, yn, e, rtol, atol);
+}
+
+__global__ void step_factor_kernel(const double *ratio, double *out, long long n) {
+    const long long i = tid();
+    if (i >= n) return;
+    out[i] = step_factor<double>(ratio[i]);
+}
+
+// rk4_step (integrators.py:57-73) n_steps times with the state in registers.
+template <typename W>
+__global__ void rk4_kernel(double m, double a, const double *state,
+                           const double *hs, double *out, long long n,
+                           long long n_steps) {
+    const long long i = tid();
+    if (i >= n) return;
+    RayState y = read_state(state, i);
+    const double h = hs[i];
+    const W mw = W(m), aw = W(a), hw = W(h);
+    const W half = W(0.5) * hw;
+    for (long long s = 0; s < n_steps; ++s) {
+        // k_x = P + q in split form; the stage inputs use W arithmetic.
+        const W x = W(y.x), yy = W(y.y), z = W(y.z), pt = W(y.pt);
+        const W px = W(y.px), py = W(y.py), pz = W(y.pz);
+        const Deriv<W> d1 = rhs<W>(mw, aw, x, yy, z, pt, px, py, pz);
+        const W k1x = px + d1.qx, k1y = py + d1.qy, k1z = pz + d1.qz;
+        const Deriv<W> d2 = rhs<W>(mw, aw, x + half * k1x, yy + half * k1y,
+                                   z + half * k1z, pt, px + half * d1.px,
+                                   py + half * d1.py, pz + half * d1.pz);
+        const W p2x = px + half * d1.px, p2y = py + half * d1.py, p2z = pz + half * d1.pz;
+        const W k2x = p2x + d2.qx, k2y = p2y + d2.qy, k2z = p2z + d2.qz;
+        const Deriv<W> d3 = rhs<W>(mw, aw, x + half * k2x, yy + half * k2y,
+                                   z + half * k2z, pt, px + half * d2.px,
+                                   py + half * d2.py, pz + half * d2.pz);
+        const W p3x = px + half * d2.px, p3y = py + half * d2.py, p3z = pz + half * d2.pz;
+        const W k3x = p3x + d3.qx, k3y = p3y + d3.qy, k3z = p3z + d3.qz;
+        const Deriv<W> d4 = rhs<W>(mw, aw, x + hw * k3x, yy + hw * k3y,
+                                   z + hw * k3z, pt, px + hw * d3.px,
+                                   py + hw * d3.py, pz + hw * d3.pz);
+        const W p4x = px + hw * d3.px, p4y = py + hw * d3.py, p4z = pz + hw * d3.pz;
+        const W k4x = p4x + d4.qx, k4y = p4y + d4.qy, k4z = p4z + d4.qz;
+        const double h6 = h / 6.0;
+        y.t += h6 * double(W(-6) * pt + d1.thl + W(2) * d2.thl + W(2) * d3.thl + d4.thl);
+        y.x += h6 * double(k1x + W(2) * k2x + W(2) * k3x + k4x);
+        y.y += h6 * double(k1y + W(2) * k2y + W(2) * k3y + k4y);
+        y.z += h6 * double(k1z + W(2) * k2z + W(2) * k3z + k4z);
+        y.px += h6 * double(d1.px + W(2) * d2.px + W(2) * d3.px + d4.px);
+        y.py += h6 * double(d1.py + W(2) * d2.py + W(2) * d3.py + d4.py);
+        y.pz += h6 * double(d1.pz + W(2) * d2.pz + W(2) * d3.pz + d4.pz);
+    }
+    write_state(out, i, y);
+}
+
+static CameraDev camera_dev(const bh_camera &c, long long first_ray) {
+    CameraDev d;
+    for (int i = 0; i < 3; ++i) {
+        d.pos[i] = c.position[i];
+        d.fwd[i] = c.forward[i];
+        d.right[i] = c.right[i];
+        d.up[i] = c.up[i];
+    }
+    // camera.py:102-103; math.radians(x) is x * (pi / 180).
+    d.half_w = std::tan(c.fov_degrees * (M_PI / 180.0) / 2.0);
+    d.half_h = d.half_w * double(c.height) / double(c.width);
+    d.width = c.width;
+    d.height = c.height;
+    d.first_ray = first_ray;
+    d.mass = c.scene.mass;
+    d.spin = c.scene.spin;
+    d.capture_radius = c.scene.capture_radius;
+    d.escape_radius = c.scene.escape_radius;
+    return d;
+}
+
+static int camera_ok(const bh_camera &c) {
+    if (c.width <= 0 || c.height <= 0) return invalid("image dimensions must be positive");
+    if (!(c.fov_degrees > 0.0 && c.fov_degrees < 180.0))
+        return invalid("fov_degrees must be in (0, 180)");
+    if (!kerr_ok(c.scene.mass, c.scene.spin))
+        return invalid("Kerr bound violated or mass not positive");
+    return BH_OK;
+}
+
+static int config_ok(const bh_trace_config *c) {
+    if (!c) return invalid("config is NULL");
+    if (c->precision != BH_PRECISION_FP64 && c->precision != BH_PRECISION_MIXED)
+        return invalid("precision must be BH_PRECISION_FP64 or BH_PRECISION_MIXED");
+    if (c->layout != BH_LAYOUT_AOS && c->layout != BH_LAYOUT_SOA)
+        return invalid("layout must be BH_LAYOUT_AOS or BH_LAYOUT_SOA");
+    if (!(c->rtol >= 0.0) || !(c->atol >= 0.0) || !(c->rtol > 0.0 || c->atol > 0.0))
+        return invalid("rtol and atol must be >= 0 and not both zero");
+    if (!(c->initial_step > 0.0) || !(c->max_step > 0.0) || !(c->min_step >= 0.0))
+        return invalid("initial_step and max_step must be > 0, min_step >= 0");
+    if (c->max_steps < 1 || c->max_steps > (1LL << 60))
+        return invalid("max_steps must be in [1, 2^60]");
+    if (c->timeout_ns < 0) return invalid("timeout_ns must be >= 0");
+    return BH_OK;
+}
+
+static bool aligned(const void *p, size_t a) {
+    return (reinterpret_cast<uintptr_t>(p) % a) == 0;
+}
+
+static TraceArgs base_args(const bh_trace_config *c) {
+    TraceArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.rtol = c->rtol;
+    a.atol = c->atol;
+    a.initial_step = c->initial_step;
+    a.max_step = c->max_step;
+    a.min_step = c->min_step;
+    a.max_steps = c->max_steps;
+    a.max_attempts = 4 * c->max_steps;
+    a.timeout_ns = c->timeout_ns;
+    a.layout = c->layout;
+    return a;
+}
+
+}  // namespace bh
+
+using namespace bh;
+
+extern "C" {
+
+int bh_abi_version(void) { return BH_ABI_VERSION; }
+
+const char *bh_status_string(int status) {
+    switch (status) {
+        case BH_OK: return "ok";
+        case BH_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case BH_ERR_CUDA: return "CUDA error";
+        case BH_ERR_TIMEOUT: return "trace deadline exceeded";
+        case BH_ERR_ESCAPE_RADIUS: return "escape_radius must exceed all initial radii";
+        case BH_ERR_WORKSPACE: return "workspace missing, too small or misaligned";
+        default: return "unknown status";
+    }
+}
+
+const char *bh_last_error(void) { return g_last_error; }
+
+int bh_geometry(double mass, double spin, const double *x, const double *y,
+                const double *z, int64_t stride, int64_t n, double *r,
+                double *h, double *l, double *grad_h, double *grad_l,
+                void *stream) {
+    if (!kerr_ok(mass, spin)) return invalid("Kerr bound violated or mass not positive");
+    if (n < 0 || stride < 1) return invalid("n must be >= 0 and stride >= 1");
+    if (n == 0) return BH_OK;
+    if (!x || !y || !z) return invalid("x, y, z must not be NULL");
+    geometry_kernel<<<grid_for(n), kBlock, 0, (cudaStream_t)stream>>>(
+        mass, spin, x, y, z, stride, n, r, h, l, grad_h, grad_l);
+    return cuda_status(cudaGetLastError(), "bh_geometry launch");
+}
+
+int bh_geodesic_rhs(double mass, double spin, const double *state,
+                    double *deriv, int64_t n, void *stream) {
+    if (!kerr_ok(mass, spin)) return invalid("Kerr bound violated or mass not positive");
+    if (n < 0) return invalid("n must be >= 0");
+    if (n == 0) return BH_OK;
+    if (!state || !deriv) return invalid("state and deriv must not be NULL");
+    rhs_kernel<<<grid_for(n), kBlock, 0, (cudaStream_t)stream>>>(mass, spin, state, deriv, n);
+    return cuda_status(cudaGetLastError(), "bh_geodesic_rhs launch");
+}
+
+int bh_hamiltonian(double mass, double spin, const double *state, double *out,
+                   int64_t n, void *stream) {
+    if (!kerr_ok(mass, spin)) return invalid("Kerr bound violated or mass not positive");
+    if (n < 0) return invalid("n must be >= 0");
+    if (n == 0) return BH_OK;
+    if (!state || !out) return invalid("state and out must not be NULL");
+    hamiltonian_kernel<<<grid_for(n), kBlock, 0, (cudaStream_t)stream>>>(mass, spin, state, out, n);
+    return cuda_status(cudaGetLastError(), "bh_hamiltonian launch");
+}
+
+int bh_coordinate_velocity(double mass, double spin, const double *state,
+                           double *out, int64_t n, void *stream) {
+    if (!kerr_ok(mass, spin)) return invalid("Kerr bound violated or mass not positive");
+    if (n < 0) return invalid("n must be >= 0");
+    if (n == 0) return BH_OK;
+    if (!state || !out) return invalid("state and out must not be NULL");
+    velocity_kernel<<<grid_for(n), kBlock, 0, (cudaStream_t)stream>>>(mass, spin, state, out, n);
+    return cuda_status(cudaGetLastError(), "bh_coordinate_velocity launch");
+}
+
+int bh_null_momentum(double mass, double spin, const double *spin_of_ray,
+                     const double *positions, const double *directions,
+                     int64_t n, int32_t past, int32_t normalize,
+                     double *momenta, void *stream) {
+    if (!spin_of_ray && !kerr_ok(mass, spin))
+        return invalid("Kerr bound violated or mass not positive");
+    if (!(mass > 0.0)) return invalid("mass must be positive");
+    if (n < 0) return invalid("n must be >= 0");
+    if (n == 0) return BH_OK;
+    if (!positions || !directions || !momenta)
+        return invalid("positions, directions and momenta must not be NULL");
+    null_momentum_kernel<<<grid_for(n), kBlock, 0, (cudaStream_t)stream>>>(
+        mass, spin, spin_of_ray, positions, directions, n, past, normalize, momenta);
+    return cuda_status(cudaGetLastError(), "bh_null_momentum launch");
+}
+
+int bh_camera_states(const bh_camera *camera, double *state, void *stream) {
+    if (!camera) return invalid("camera is NULL");
+    int rc = camera_ok(*camera);
+    if (rc != BH_OK) return rc;
+    if (!state) return invalid("state must not be NULL");
+    const long long n = camera->width * camera->height;
+    camera_states_kernel<<<grid_for(n), kBlock, 0, (cudaStream_t)stream>>>(
+        camera_dev(*camera, 0), state, n);
+    return cuda_status(cudaGetLastError(), "bh_camera_states launch");
+}
+
+int bh_dp5_step(double mass, double spin, const double *state,
+                const double *h, double *new_state, double *error, int64_t n,
+                int32_t precision, void *stream) {
+    if (!kerr_ok(mass, spin)) return invalid("Kerr bound violated or mass not positive");
+    if (n < 0) return invalid("n must be >= 0");
+    if (n == 0) return BH_OK;
+    if (!state || !h || !new_state || !error) return invalid("NULL pointer argument");
+    if (precision == BH_PRECISION_FP64)
+        dp5_kernel<double><<<grid_for(n), kBlock, 0, (cudaStream_t)stream>>>(
+            mass, spin, state, h, new_state, error, n);
+    else if (precision == BH_PRECISION_MIXED)
+        dp5_kernel<float><<<grid_for(n), kBlock, 0, (cudaStream_t)stream>>>(
+            mass, spin, state, h, new_state, error, n);
+    else
+        return invalid("unknown precision");
+    return cuda_status(cudaGetLastError(), "bh_dp5_step launch");
+}
+
+int bh_error_ratio(const double *state, const double *new_state,
+                   const double *error, double rtol, double atol,
+                   double *ratio, int64_t n, void *stream) {
+    if (n < 0) return invalid("n must be >= 0");
+    if (n == 0) return BH_OK;
+    if (!state || !new_state || !error || !ratio) return invalid("NULL pointer argument");
+    error_ratio_kernel<<<grid_for(n), kBlock, 0, (cudaStream_t)stream>>>(
+        state, new_state, error, rtol, atol, ratio, n);
+    return cuda_status(cudaGetLastError(), "bh_error_ratio launch");
+}
+
+int bh_step_factor(const double *ratio, double *factor, int64_t n, void *stream) {
+    if (n < 0) return invalid("n must be >= 0");
+    if (n == 0) return BH_OK;
+    if (!ratio || !factor) return invalid("NULL pointer argument");
+    step_factor_kernel<<<grid_for(n), kBlock, 0, (cudaStream_t)stream>>>(ratio, factor, n);
+    return cuda_status(cudaGetLastError(), "bh_step_factor launch");
+}
+
+int bh_rk4(double mass, double spin, const double *state, const double *h,
+           double *new_state, int64_t n, int64_t n_steps, int32_t precision,
+           void *stream) {
+    if (!kerr_ok(mass, spin)) return invalid("Kerr bound violated or mass not positive");
+    if (n < 0 || n_steps < 0) return invalid("n and n_steps must be >= 0");
+    if (n == 0) return BH_OK;
+    if (!state || !h || !new_state) return invalid("NULL pointer argument");
+    if (precision == BH_PRECISION_FP64)
+        rk4_kernel<double><<<grid_for(n), kBlock, 0, (cudaStream_t)stream>>>(
+            mass, spin, state, h, new_state, n, n_steps);
+    else if (precision == BH_PRECISION_MIXED)
+        rk4_kernel<float><<<grid_for(n), kBlock, 0, (cudaStream_t)stream>>>(
+            mass, spin, state, h, new_state, n, n_steps);
+    else
+        return invalid("unknown precision");
+    return cuda_status(cudaGetLastError(), "bh_rk4 launch");
+}
+
+int bh_trace_variant_count(int32_t precision) { return trace_variant_count(precision); }
+
+int bh_trace_variant(int32_t precision, int32_t index, int32_t *block_threads,
+                     int32_t *min_blocks, int32_t *registers,
+                     int32_t *max_blocks_per_sm) {
+    if (precision != BH_PRECISION_FP64 && precision != BH_PRECISION_MIXED)
+        return invalid("unknown precision");
+    if (index < 0) index = trace_default_variant(precision);
+    if (index >= trace_variant_count(precision)) return invalid("variant index out of range");
+    const Variant v = trace_variant(precision, index);
+    if (block_threads) *block_threads = v.block;
+    if (min_blocks) *min_blocks = v.min_blocks;
+    int regs = 0, nb = 0;
+    if (kernel_attributes(false, precision, index, &regs, &nb) != 0)
+        return cuda_status(cudaGetLastError(), "bh_trace_variant attributes");
+    if (registers) *registers = regs;
+    if (max_blocks_per_sm) *max_blocks_per_sm = nb;
+    return BH_OK;
+}
+
+size_t bh_trace_workspace_bytes(void) { return sizeof(TraceWorkspace); }
+
+size_t bh_trace_cameras_workspace_bytes(int32_t ncameras) {
+    if (ncameras < 0) ncameras = 0;
+    const size_t bytes = sizeof(TraceWorkspace) + size_t(ncameras) * sizeof(CameraDev);
+    return (bytes + 255) / 256 * 256;
+}
+
+int bh_trace(const bh_trace_config *config, const bh_scene *scene,
+             const double *state0, double *states, int32_t *status,
+             int64_t *steps, int64_t n, void *workspace, void *stream) {
+    int rc = config_ok(config);
+    if (rc != BH_OK) return rc;
+    if (!scene) return invalid("scene is NULL");
+    if (!kerr_ok(scene->mass, scene->spin)) return invalid("Kerr bound violated or mass not positive");
+    if (n < 0) return invalid("n must be >= 0");
+    if (!workspace || !aligned(workspace, 256)) {
+        set_error("workspace must be a 256-byte aligned device buffer of bh_trace_workspace_bytes()");
+        return BH_ERR_WORKSPACE;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    rc = cuda_status(cudaMemsetAsync(workspace, 0, sizeof(TraceWorkspace), s), "bh_trace workspace reset");
+    if (rc != BH_OK || n == 0) return rc;
+    if (!state0 || !states || !status || !steps) return invalid("NULL pointer argument");
+    if (config->layout == BH_LAYOUT_AOS && (!aligned(state0, 16) || !aligned(states, 16)))
+        return invalid("state buffers must be 16-byte aligned");
+    TraceArgs a = base_args(config);
+    a.state0 = state0;
+    a.source = 0;
+    a.mass = scene->mass;
+    a.spin = scene->spin;
+    a.capture_radius = scene->capture_radius;
+    a.escape_radius = scene->escape_radius;
+    a.states = states;
+    a.status = status;
+    a.steps = steps;
+    a.n = n;
+    a.ws = reinterpret_cast<TraceWorkspace *>(workspace);
+    return cuda_status(launch_trace(a, config->precision, config->variant,
+                                    config->blocks_per_sm, s),
+                       "bh_trace launch");
+}
+
+int bh_camera_table_upload(const bh_camera *cameras, int32_t ncameras,
+                           void *workspace, size_t workspace_bytes,
+                           int64_t *n_rays, void *stream) {
+    if (ncameras < 1 || !cameras) return invalid("need at least one camera");
+    if (!workspace || !aligned(workspace, 256) ||
+        workspace_bytes < bh_trace_cameras_workspace_bytes(ncameras)) {
+        set_error("workspace must be a 256-byte aligned device buffer of bh_trace_cameras_workspace_bytes(ncameras)");
+        return BH_ERR_WORKSPACE;
+    }
+    CameraDev *table = new CameraDev[ncameras];
+    long long total = 0;
+    for (int c = 0; c < ncameras; ++c) {
+        const int rc = camera_ok(cameras[c]);
+        if (rc != BH_OK) {
+            delete[] table;
+            return rc;
+        }
+        table[c] = camera_dev(cameras[c], total);
+        total += cameras[c].width * cameras[c].height;
+    }
+    char *ws = reinterpret_cast<char *>(workspace);
+    // A copy from pageable memory returns once the runtime has staged the
+    // source, so the table can be freed right after.
+    const int rc = cuda_status(
+        cudaMemcpyAsync(ws + sizeof(TraceWorkspace), table, sizeof(CameraDev) * ncameras,
+                        cudaMemcpyHostToDevice, (cudaStream_t)stream),
+        "bh_camera_table_upload copy");
+    delete[] table;
+    if (rc == BH_OK && n_rays) *n_rays = total;
+    return rc;
+}
+
+int bh_trace_cameras(const bh_trace_config *config, int32_t ncameras,
+                     int64_t n_rays, double *states, int32_t *status,
+                     int64_t *steps, void *workspace, size_t workspace_bytes,
+                     void *stream) {
+    int rc = config_ok(config);
+    if (rc != BH_OK) return rc;
+    if (ncameras < 1) return invalid("need at least one camera");
+    if (n_rays < 0) return invalid("n_rays must be >= 0");
+    if (!workspace || !aligned(workspace, 256) ||
+        workspace_bytes < bh_trace_cameras_workspace_bytes(ncameras)) {
+        set_error("workspace must be a 256-byte aligned device buffer of bh_trace_cameras_workspace_bytes(ncameras)");
+        return BH_ERR_WORKSPACE;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    rc = cuda_status(cudaMemsetAsync(workspace, 0, sizeof(TraceWorkspace), s),
+                     "bh_trace_cameras workspace reset");
+    if (rc != BH_OK || n_rays == 0) return rc;
+    if (!states || !status || !steps) return invalid("NULL pointer argument");
+    if (config->layout == BH_LAYOUT_AOS && !aligned(states, 16))
+        return invalid("state buffers must be 16-byte aligned");
+    TraceArgs a = base_args(config);
+    a.source = 1;
+    a.cameras = reinterpret_cast<const CameraDev *>(
+        reinterpret_cast<char *>(workspace) + sizeof(TraceWorkspace));
+    a.ncameras = ncameras;
+    a.states = states;
+    a.status = status;
+    a.steps = steps;
+    a.n = n_rays;
+    a.ws = reinterpret_cast<TraceWorkspace *>(workspace);
+    return cuda_status(launch_trace(a, config->precision, config->variant,
+                                    config->blocks_per_sm, s),
+                       "bh_trace_cameras launch");
+}
+
+int bh_trace_stats_read(const void *workspace, bh_trace_stats *out, void *stream) {
+    if (!workspace || !out) return invalid("NULL pointer argument");
+    TraceWorkspace w;
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc = cuda_status(cudaMemcpyAsync(&w, workspace, sizeof(w), cudaMemcpyDeviceToHost, s),
+                         "bh_trace_stats_read copy");
+    if (rc != BH_OK) return rc;
+    rc = cuda_status(cudaStreamSynchronize(s), "bh_trace_stats_read sync");
+    if (rc != BH_OK) return rc;
+    out->iterations = w.iterations;
+    out->attempts = (int64_t)w.attempts;
+    out->accepted = (int64_t)w.accepted;
+    out->timed_out = w.timed_out;
+    out->bad_rays = w.bad_rays;
+    if (w.bad_rays) {
+        set_error("escape_radius must exceed all initial radii (%d rays)", w.bad_rays);
+        return BH_ERR_ESCAPE_RADIUS;
+    }
+    if (w.timed_out) {
+        set_error("trace deadline exceeded");
+        return BH_ERR_TIMEOUT;
+    }
+    return BH_OK;
+}
+
+int bh_propagate(const bh_trace_config *config, double mass, double spin,
+                 const double *spin_of_ray, double *states, double *h,
+                 int64_t *accepted, int64_t n, int64_t n_steps,
+                 void *workspace, void *stream) {
+    int rc = config_ok(config);
+    if (rc != BH_OK) return rc;
+    if (!(mass > 0.0)) return invalid("mass must be positive");
+    if (!spin_of_ray && !kerr_ok(mass, spin)) return invalid("Kerr bound violated");
+    if (n < 0 || n_steps < 0) return invalid("n and n_steps must be >= 0");
+    if (!workspace || !aligned(workspace, 256)) {
+        set_error("workspace must be a 256-byte aligned device buffer of bh_trace_workspace_bytes()");
+        return BH_ERR_WORKSPACE;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    rc = cuda_status(cudaMemsetAsync(workspace, 0, sizeof(TraceWorkspace), s), "bh_propagate workspace reset");
+    if (rc != BH_OK || n == 0) return rc;
+    if (!states || !h || !accepted) return invalid("NULL pointer argument");
+    if (config->layout == BH_LAYOUT_AOS && !aligned(states, 16))
+        return invalid("state buffers must be 16-byte aligned");
+    TraceArgs a = base_args(config);
+    a.state0 = states;
+    a.states = states;
+    a.mass = mass;
+    a.spin = spin;
+    a.spin_of_ray = spin_of_ray;
+    a.h_io = h;
+    a.steps = accepted;
+    a.n = n;
+    a.max_attempts = n_steps;
+    a.ws = reinterpret_cast<TraceWorkspace *>(workspace);
+    return cuda_status(launch_propagate(a, config->precision, config->variant,
+                                        config->blocks_per_sm, s),
+                       "bh_propagate launch");
+}
+
+}  // extern "C"

@@ -1,0 +1,82 @@
+// bh_internal.h -- shared declarations of the library's translation units.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/bh_b200.h"
+
+namespace bh {
+
+// Device workspace of a trace / propagate launch (the first 256 bytes of the
+// caller's workspace).  Zeroed by the launcher before every launch.
+struct alignas(256) TraceWorkspace {
+    unsigned long long queue_head;  // next unclaimed ray of the work queue
+    long long iterations;           // max attempts over rays
+    unsigned long long attempts;    // sum of attempts
+    unsigned long long accepted;    // sum of accepted steps
+    int timed_out;
+    int bad_rays;
+};
+static_assert(sizeof(TraceWorkspace) == 256, "workspace header is 256 bytes");
+
+// Device copy of a camera: the pinhole basis plus its scene, and the first
+// global ray index it owns.
+struct CameraDev {
+    double pos[3], fwd[3], right[3], up[3];
+    double half_w, half_h;
+    long long width, height;
+    long long first_ray;
+    double mass, spin, capture_radius, escape_radius;
+};
+
+struct TraceArgs {
+    // ray source: states (source == 0) or cameras (source == 1)
+    const double *state0;
+    const CameraDev *cameras;  // device copy (in the workspace)
+    int ncameras;
+    int source;
+    // single-scene parameters (source == 0)
+    double mass, spin, capture_radius, escape_radius;
+    const double *spin_of_ray;  // propagate only; may be null
+    // outputs
+    double *states;
+    int32_t *status;
+    int64_t *steps;  // accepted steps (trace) or accepted count (propagate)
+    double *h_io;    // propagate: per-ray step size in/out
+    long long n;
+    int layout;
+    // controller
+    double rtol, atol, initial_step, max_step, min_step;
+    long long max_steps;     // trace: accepted-step budget
+    long long max_attempts;  // trace: 4 * max_steps; propagate: n_steps
+    long long timeout_ns;
+    TraceWorkspace *ws;
+};
+
+// Launch-shape variants of the trace / propagate kernels: threads per block
+// and the __launch_bounds__ minimum blocks per SM, which caps registers.
+struct Variant {
+    int block;
+    int min_blocks;
+};
+
+int trace_variant_count(int precision);
+Variant trace_variant(int precision, int idx);
+int trace_default_variant(int precision);
+
+// Registers and occupancy of a compiled trace (propagate = false) or propagate
+// kernel variant; returns 0 on success.
+int kernel_attributes(bool propagate, int precision, int idx, int *regs,
+                      int *max_blocks);
+
+cudaError_t launch_trace(const TraceArgs &args, int precision, int variant,
+                         int blocks_per_sm, cudaStream_t stream);
+cudaError_t launch_propagate(const TraceArgs &args, int precision, int variant,
+                             int blocks_per_sm, cudaStream_t stream);
+
+// Records a message for bh_last_error on this host thread.
+void set_error(const char *fmt, ...);
+
+}  // namespace bh

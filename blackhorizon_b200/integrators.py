@@ -1,0 +1,189 @@
+"""Batched integrators, b200 backend.
+
+Same signatures as blackhorizon/integrators.py: ``rk4_step``,
+``dormand_prince_step``, ``error_ratio``, ``step_factor`` and
+``integrate_dense``, each a CUDA kernel.  The RHS argument must be a
+``GeodesicRhs`` (or ``functools.partial(geodesic_rhs, spacetime)``);
+any other callable raises TypeError because there is no CPU path.
+
+``propagate`` is the no-termination mode of the tracer loop (tracer.py:111-120
+without the status cascade): every ray makes exactly ``n_steps`` attempted
+DP5(4) steps with its own adaptive step size, optionally with one spin per
+ray.  It is the raw-throughput benchmark workload.
+"""
+
+from __future__ import annotations
+
+import numpy
+import torch
+
+from . import _lib
+from .backend import Array, is_device_array, out_like, ptr, stream_handle, to_device_f64
+from .geodesics import spacetime_of_rhs
+
+PRECISIONS = ("fp64", "mixed")
+
+
+def _precision_code(precision: str) -> int:
+    try:
+        return _lib.PRECISION[precision]
+    except KeyError:
+        raise ValueError(f"precision must be one of {PRECISIONS}") from None
+
+
+def _h_vector(h, n, device):
+    if is_device_array(h):
+        t = h.to(device=device, dtype=torch.float64)
+    else:
+        t = torch.as_tensor(numpy.asarray(h, dtype=numpy.float64), device=device)
+    if t.dim() == 0:
+        t = t.expand(n)
+    if t.shape != (n,):
+        raise ValueError("h must be a scalar or have shape (n,)")
+    return t.contiguous()
+
+
+def rk4_step(rhs, state: Array, h: Array, precision: str = "fp64",
+             n_steps: int = 1) -> Array:
+    """Classical RK4 (integrators.py:57-73); ``n_steps`` > 1 repeats it in
+    registers without leaving the kernel."""
+    st = spacetime_of_rhs(rhs)
+    s, host = to_device_f64(state, "state")
+    if s.dim() != 2 or s.shape[1] != 8:
+        raise ValueError("state must have shape (n, 8)")
+    hh = _h_vector(h, s.shape[0], s.device)
+    out = torch.empty_like(s)
+    _lib.check(_lib.load().bh_rk4(st.mass, st.spin, ptr(s), ptr(hh), ptr(out),
+                                  s.shape[0], int(n_steps), _precision_code(precision),
+                                  stream_handle()), "rk4_step")
+    return out_like(out, host, state)
+
+
+def dormand_prince_step(rhs, state: Array, h: Array, precision: str = "fp64"):
+    """Embedded Dormand-Prince 5(4) step (integrators.py:76-107): returns
+    (new_state, error)."""
+    st = spacetime_of_rhs(rhs)
+    s, host = to_device_f64(state, "state")
+    if s.dim() != 2 or s.shape[1] != 8:
+        raise ValueError("state must have shape (n, 8)")
+    hh = _h_vector(h, s.shape[0], s.device)
+    new = torch.empty_like(s)
+    err = torch.empty_like(s)
+    _lib.check(_lib.load().bh_dp5_step(st.mass, st.spin, ptr(s), ptr(hh), ptr(new),
+                                       ptr(err), s.shape[0], _precision_code(precision),
+                                       stream_handle()), "dormand_prince_step")
+    return out_like(new, host, state), out_like(err, host, state)
+
+
+def error_ratio(state: Array, new_state: Array, error: Array, rtol: float,
+                atol: float) -> Array:
+    """Scaled RMS error per sample (integrators.py:110-117)."""
+    s, host = to_device_f64(state, "state")
+    sn, _ = to_device_f64(new_state, "new_state")
+    e, _ = to_device_f64(error, "error")
+    if s.dim() != 2 or s.shape[1] != 8 or sn.shape != s.shape or e.shape != s.shape:
+        raise ValueError("state, new_state and error must have shape (n, 8)")
+    out = torch.empty(s.shape[0], dtype=torch.float64, device=s.device)
+    _lib.check(_lib.load().bh_error_ratio(ptr(s), ptr(sn), ptr(e), float(rtol),
+                                          float(atol), ptr(out), s.shape[0],
+                                          stream_handle()), "error_ratio")
+    return out_like(out, host, state)
+
+
+def step_factor(ratio: Array) -> Array:
+    """clip(0.9 max(ratio, 1e-16)^-0.2, 0.2, 5) (integrators.py:120-124)."""
+    r, host = to_device_f64(ratio, "ratio")
+    flat = r.reshape(-1).contiguous()
+    out = torch.empty_like(flat)
+    _lib.check(_lib.load().bh_step_factor(ptr(flat), ptr(out), flat.shape[0],
+                                          stream_handle()), "step_factor")
+    return out_like(out.reshape(r.shape), host, ratio)
+
+
+def integrate_dense(rhs, state0: Array, lambda_total: float, rtol: float = 1e-10,
+                    atol: float = 1e-12, initial_step: float = 0.05,
+                    max_step: float = 2.0, precision: str = "fp64") -> list:
+    """Lock-step adaptive integration with one step size for the batch
+    (integrators.py:127-174): returns the list of accepted states."""
+    st = spacetime_of_rhs(rhs)
+    s, host = to_device_f64(state0, "state0")
+    n = s.shape[0]
+    state = s.clone()
+    states = [state.clone()]
+    elapsed = 0.0
+    h_scalar = float(initial_step)
+    while elapsed < lambda_total:
+        h_scalar = min(h_scalar, max_step, lambda_total - elapsed)
+        h = torch.full((n,), h_scalar, dtype=torch.float64, device=s.device)
+        new_state, error = dormand_prince_step(rhs, state, h, precision)
+        ratio = float(error_ratio(state, new_state, error, rtol, atol).max())
+        if ratio <= 1.0:
+            state = new_state
+            states.append(state.clone())
+            elapsed += h_scalar
+        factor = float(min(max(0.9 * max(ratio, 1e-16) ** (-0.2), 0.2), 5.0))
+        h_scalar *= factor
+        if h_scalar < 1e-14:
+            raise RuntimeError("integrate_dense: step size underflow")
+    del st
+    return [out_like(x, host, state0) for x in states]
+
+
+def make_config(max_steps: int = 1, rtol: float = 1e-9, atol: float = 1e-12,
+                initial_step: float = 0.1, max_step: float = 2.0,
+                min_step: float = 1e-10, precision: str = "fp64",
+                layout: str = "aos", timeout_s: float = 0.0, variant: int = -1,
+                blocks_per_sm: int = 0) -> "_lib.TraceConfig":
+    if layout not in _lib.LAYOUT:
+        raise ValueError("layout must be 'aos' or 'soa'")
+    return _lib.TraceConfig(
+        int(max_steps), float(rtol), float(atol), float(initial_step),
+        float(max_step), float(min_step), _precision_code(precision),
+        _lib.LAYOUT[layout], int(max(0.0, timeout_s) * 1e9), int(variant),
+        int(blocks_per_sm))
+
+
+def propagate(spacetime, state0: Array, n_steps: int, rtol: float = 1e-8,
+              atol: float = 1e-10, initial_step: float = 0.1,
+              max_step: float = 2.0, precision: str = "fp64", spins=None,
+              h0: Array | None = None, layout: str = "aos",
+              timeout_s: float = 0.0, variant: int = -1, workspace=None,
+              in_place: bool = False):
+    """n_steps attempted DP5(4) steps per ray with per-ray accept/reject and
+    step update (tracer.py:111-120), no termination.
+
+    Returns (states, h, accepted, stats).  ``spins`` (n,) gives each ray its
+    own spin.  With ``in_place`` and a device float64 ``state0`` the states are
+    advanced in place."""
+    s, host = to_device_f64(state0, "state0")
+    n = s.shape[0] if layout == "aos" else s.shape[-1]
+    if layout == "aos" and (s.dim() != 2 or s.shape[1] != 8):
+        raise ValueError("state0 must have shape (n, 8)")
+    if layout == "soa" and (s.dim() != 2 or s.shape[0] != 8):
+        raise ValueError("state0 must have shape (8, n) for layout 'soa'")
+    states = s if (in_place and host is None and s.data_ptr() == state0.data_ptr()) else s.clone()
+    if h0 is None:
+        h = torch.full((n,), float(initial_step), dtype=torch.float64, device=s.device)
+    else:
+        h = _h_vector(h0, n, s.device).clone()
+    spin_t = None
+    if spins is not None:
+        spin_t, _ = to_device_f64(spins, "spins")
+        if spin_t.shape != (n,):
+            raise ValueError("spins must have shape (n,)")
+        if bool((spin_t.abs() > spacetime.mass).any()):
+            raise ValueError("Kerr bound violated: |spin| must be <= mass")
+    acc = torch.empty(n, dtype=torch.int64, device=s.device)
+    lib = _lib.load()
+    ws = workspace if workspace is not None else torch.empty(
+        lib.bh_trace_workspace_bytes(), dtype=torch.uint8, device=s.device)
+    cfg = make_config(1, rtol, atol, initial_step, max_step, 0.0, precision,
+                      layout, timeout_s, variant)
+    stream = stream_handle()
+    _lib.check(lib.bh_propagate(cfg, float(spacetime.mass), float(spacetime.spin),
+                                ptr(spin_t), ptr(states), ptr(h), ptr(acc), n,
+                                int(n_steps), ptr(ws), stream), "propagate")
+    stats = _lib.TraceStats()
+    _lib.check(lib.bh_trace_stats_read(ptr(ws), stats, stream), "propagate")
+    return (out_like(states, host, state0), out_like(h, host, state0),
+            acc.cpu().numpy() if host is not None else acc, stats)

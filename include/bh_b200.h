@@ -1,0 +1,245 @@
+/*
+ * bh_b200.h -- C ABI of the B200 geodesic hot path (libbh_b200.so).
+ *
+ * Plain pointers and sizes only; every device pointer is CUDA global memory
+ * owned by the caller, every stream is a cudaStream_t passed as void*.  All
+ * calls are stream-ordered and asynchronous unless the comment says
+ * otherwise.  Functions return BH_OK (0) or a negative bh_status.
+ *
+ * State layout: a batch of n geodesic states (t, x, y, z, p_t, p_x, p_y, p_z),
+ * covariant momenta, float64 -- the reference's (n, 8) row-major array
+ * (blackhorizon/geodesics.py:1-16).  Trace and propagate calls also accept
+ * the structure-of-arrays layout (8 planes of n doubles).
+ *
+ * Each entry point names the reference function it replaces
+ * (MegaKruk/BlackHorizon, path within that project, file:line).
+ */
+#ifndef BH_B200_H
+#define BH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BH_ABI_VERSION 1
+
+typedef enum {
+    BH_OK = 0,
+    BH_ERR_INVALID_ARGUMENT = -1, /* bad pointer, size, tolerance or Kerr bound */
+    BH_ERR_CUDA = -2,             /* a CUDA runtime call failed; see bh_last_error */
+    BH_ERR_TIMEOUT = -3,          /* the trace deadline passed before every ray finished */
+    BH_ERR_ESCAPE_RADIUS = -4,    /* an initial radius is >= escape_radius (tracer.py:95-99) */
+    BH_ERR_WORKSPACE = -5         /* workspace missing, too small or misaligned */
+} bh_status;
+
+/* Per-ray termination codes: blackhorizon/tracer.py:21-30 (RayStatus). */
+enum {
+    BH_RAY_IN_FLIGHT = 0,
+    BH_RAY_CAPTURED = 1,
+    BH_RAY_ESCAPED = 2,
+    BH_RAY_MAX_STEPS = 3,
+    BH_RAY_FAILED = 4
+};
+
+typedef enum {
+    BH_PRECISION_FP64 = 0,  /* every operation in float64 */
+    BH_PRECISION_MIXED = 1  /* float32 stage arithmetic, float64 state, error norm,
+                               step control and termination radius */
+} bh_precision;
+
+typedef enum {
+    BH_LAYOUT_AOS = 0, /* (n, 8) row-major, the reference's layout */
+    BH_LAYOUT_SOA = 1  /* 8 planes of n doubles */
+} bh_layout;
+
+/* Kerr spacetime and termination radii of one scene.  capture_radius is
+ * r_plus * (1 + capture_margin) (tracer.py:84); escape_radius as passed to
+ * trace_rays. */
+typedef struct {
+    double mass;
+    double spin;
+    double capture_radius;
+    double escape_radius;
+} bh_scene;
+
+/* A pinhole camera (camera.py:25-120) plus the scene it looks at.  The basis
+ * (forward, right, up) is the one camera.py:48-66 builds on the host. */
+typedef struct {
+    double position[3];
+    double forward[3];
+    double right[3];
+    double up[3];
+    double fov_degrees;
+    int64_t width;
+    int64_t height;
+    bh_scene scene;
+} bh_camera;
+
+/* Controller settings of trace_rays (tracer.py:50-61) and launch knobs. */
+typedef struct {
+    int64_t max_steps;     /* accepted-step budget per ray */
+    double rtol, atol;
+    double initial_step, max_step, min_step;
+    int32_t precision;     /* bh_precision */
+    int32_t layout;        /* bh_layout */
+    int64_t timeout_ns;    /* device deadline for the launch; 0 = none */
+    int32_t variant;       /* launch-shape variant (bh_trace_variant); -1 = default */
+    int32_t blocks_per_sm; /* resident blocks per SM; 0 = occupancy maximum */
+} bh_trace_config;
+
+/* Whole-launch counters of a trace or propagate call. */
+typedef struct {
+    int64_t iterations;    /* max attempts over rays == reference TraceResult.iterations */
+    int64_t attempts;      /* attempted DP5 steps summed over rays */
+    int64_t accepted;      /* accepted DP5 steps summed over rays */
+    int32_t timed_out;     /* nonzero when the deadline stopped the launch */
+    int32_t bad_rays;      /* rays whose initial radius is >= their escape radius */
+} bh_trace_stats;
+
+/* ------------------------------------------------------------- library */
+
+int bh_abi_version(void);
+const char *bh_status_string(int status);
+/* Message of the last failure on the calling host thread ("" if none). */
+const char *bh_last_error(void);
+
+/* ---------------------------------------------------------- pointwise
+ * One thread per point; float64. */
+
+/* KerrSpacetime.geometry (blackhorizon/kerr.py:118-193).  x, y, z are read
+ * with element stride `stride` (8 reads the columns of an (n,8) state).  Any
+ * of grad_h (n,3) / grad_l (n,3,3, grad_l[i][j] = dl_j/dx_i) may be NULL. */
+int bh_geometry(double mass, double spin, const double *x, const double *y,
+                const double *z, int64_t stride, int64_t n, double *r,
+                double *h, double *l, double *grad_h, double *grad_l,
+                void *stream);
+
+/* geodesic_rhs (blackhorizon/geodesics.py:42-74): (n,8) -> (n,8). */
+int bh_geodesic_rhs(double mass, double spin, const double *state,
+                    double *deriv, int64_t n, void *stream);
+
+/* hamiltonian (geodesics.py:77-85): (n,8) -> (n,). */
+int bh_hamiltonian(double mass, double spin, const double *state, double *out,
+                   int64_t n, void *stream);
+
+/* coordinate_velocity (geodesics.py:95-106): (n,8) -> (n,4). */
+int bh_coordinate_velocity(double mass, double spin, const double *state,
+                           double *out, int64_t n, void *stream);
+
+/* null_momentum_from_velocity (geodesics.py:109-170): positions (n,3),
+ * directions (n,3) -> momenta (n,4).  spin_of_ray (n,) overrides spin when
+ * non-NULL. */
+int bh_null_momentum(double mass, double spin, const double *spin_of_ray,
+                     const double *positions, const double *directions,
+                     int64_t n, int32_t past, int32_t normalize,
+                     double *momenta, void *stream);
+
+/* PinholeCamera.ray_directions + ray_origins (camera.py:96-120) followed by
+ * null_momentum_from_velocity(..., "past") and build_state (geodesics.py:25-39,
+ * t0 = 0): writes the (width*height, 8) initial states of a camera. */
+int bh_camera_states(const bh_camera *camera, double *state, void *stream);
+
+/* -------------------------------------------------------- integrators */
+
+/* dormand_prince_step (blackhorizon/integrators.py:76-107) with the
+ * geodesic RHS: state (n,8), h (n,) -> new_state (n,8), error (n,8). */
+int bh_dp5_step(double mass, double spin, const double *state,
+                const double *h, double *new_state, double *error, int64_t n,
+                int32_t precision, void *stream);
+
+/* error_ratio (integrators.py:110-117) for 8-component states. */
+int bh_error_ratio(const double *state, const double *new_state,
+                   const double *error, double rtol, double atol,
+                   double *ratio, int64_t n, void *stream);
+
+/* step_factor (integrators.py:120-124). */
+int bh_step_factor(const double *ratio, double *factor, int64_t n,
+                   void *stream);
+
+/* rk4_step (integrators.py:57-73) with the geodesic RHS, repeated n_steps
+ * times in registers with the fixed per-ray step h (n,).  n_steps = 1 is one
+ * rk4_step; the README benchmark (examples/benchmark.py:39-51) is h = 0.05,
+ * 50 steps. */
+int bh_rk4(double mass, double spin, const double *state, const double *h,
+           double *new_state, int64_t n, int64_t n_steps, int32_t precision,
+           void *stream);
+
+/* ------------------------------------------------------------- tracer */
+
+/* Launch-shape variants of the trace and propagate kernels for a precision:
+ * threads per block, the __launch_bounds__ minimum blocks per SM (which caps
+ * registers per thread) and the registers the compiled kernel uses.  The
+ * autotuner times them; index -1 in bh_trace_config selects the default. */
+int bh_trace_variant_count(int32_t precision);
+int bh_trace_variant(int32_t precision, int32_t index, int32_t *block_threads,
+                     int32_t *min_blocks, int32_t *registers,
+                     int32_t *max_blocks_per_sm);
+
+/* Bytes of device workspace a trace or propagate launch needs (queue head and
+ * counters), for any n; 256-byte aligned. */
+size_t bh_trace_workspace_bytes(void);
+
+/* trace_rays (blackhorizon/tracer.py:50-157) for one scene: a persistent
+ * kernel, one ray per thread, state in registers, warp-aggregated refill from
+ * a work queue held in `workspace`.  state0 and states may alias.  status (n,)
+ * int32, steps (n,) int64 = accepted steps.  Launch counters stay in the
+ * workspace until the next call; read them with bh_trace_stats_read.
+ * Rays whose initial radius is >= escape_radius are counted in bad_rays and
+ * make bh_trace_stats_read return BH_ERR_ESCAPE_RADIUS. */
+int bh_trace(const bh_trace_config *config, const bh_scene *scene,
+             const double *state0, double *states, int32_t *status,
+             int64_t *steps, int64_t n, void *workspace, void *stream);
+
+/* trace_rays for many cameras in one launch.  The pinhole ray generation of
+ * bh_camera_states is fused into the refill of the persistent kernel, each
+ * camera carries its own scene, and the rays of all cameras form one work
+ * queue: camera c owns global rays [offset_c, offset_c + width_c*height_c),
+ * offsets in table order.  bh_camera_table_upload copies the HOST camera
+ * array into the workspace (which must hold
+ * bh_trace_cameras_workspace_bytes(ncameras) bytes) and returns the total
+ * ray count; bh_trace_cameras then resets the counters and launches, and
+ * makes no host-to-device copy, so it can be captured in a CUDA graph and
+ * replayed while the table stays in the workspace. */
+size_t bh_trace_cameras_workspace_bytes(int32_t ncameras);
+int bh_camera_table_upload(const bh_camera *cameras, int32_t ncameras,
+                           void *workspace, size_t workspace_bytes,
+                           int64_t *n_rays, void *stream);
+int bh_trace_cameras(const bh_trace_config *config, int32_t ncameras,
+                     int64_t n_rays, double *states, int32_t *status,
+                     int64_t *steps, void *workspace, size_t workspace_bytes,
+                     void *stream);
+
+/* Copies the counters of the last launch on `workspace` to the host and
+ * synchronises `stream`.  Returns BH_ERR_TIMEOUT / BH_ERR_ESCAPE_RADIUS when
+ * the launch hit its deadline or met a ray outside its escape radius. */
+int bh_trace_stats_read(const void *workspace, bh_trace_stats *out,
+                        void *stream);
+
+/* Adaptive propagation without termination: n_steps attempted DP5(4) steps
+ * per ray with the accept/reject and step-size update of tracer.py:111-120.
+ * spin_of_ray (n,) gives each ray its own spin when non-NULL.  states (n,8)
+ * and h (n,) are updated in place; accepted (n,) int64 receives accepted
+ * steps.  Uses the workspace counters like bh_trace. */
+int bh_propagate(const bh_trace_config *config, double mass, double spin,
+                 const double *spin_of_ray, double *states, double *h,
+                 int64_t *accepted, int64_t n, int64_t n_steps,
+                 void *workspace, void *stream);
+
+/* ------------------------------------------------------------ diagnostics */
+
+/* Launches a vector-FMA throughput kernel (FP64 when precision is
+ * BH_PRECISION_FP64, else FP32) of sms*8 blocks x 256 threads, each running
+ * iters x 128 FMAs; *flops receives the launch's FLOP count (FMA = 2).  Timed
+ * with events by the caller, it gives the CUDA-core peak that the tracer's
+ * roofline fraction is quoted against.  sink: device buffer of >= 8 bytes.
+ * No counterpart in the reference (a measurement aid). */
+int bh_fma_peak_launch(int32_t precision, int64_t iters, void *sink,
+                       int64_t *flops, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BH_B200_H */

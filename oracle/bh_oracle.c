@@ -1,0 +1,531 @@
+/*
+ * bh_oracle.c -- CPU restatement of BlackHorizon's geodesic hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker for the CUDA library, never part of
+ * the product.  Compile with -ffp-contract=off and without -ffast-math so each
+ * expression rounds exactly like the NumPy expression it restates.  The
+ * association order of every sum and product below follows the reference
+ * expression left to right; NumPy reduces a 3-element axis sequentially and an
+ * 8-element axis pairwise ((0+1)+(2+3))+((4+5)+(6+7)); sum3 and the sum in
+ * bho_error_ratio reproduce both orders.
+ */
+#include "bh_oracle.h"
+
+#include <math.h>
+#include <pthread.h>
+#include <stdatomic.h>
+#include <string.h>
+#include <unistd.h>
+
+/* kerr.py:26 (_TINY). */
+#define BHO_TINY 1e-30
+
+/* numpy.maximum / numpy.minimum propagate NaN from either operand. */
+static inline double np_max(double a, double b) {
+    if (isnan(a) || isnan(b)) return NAN;
+    return a >= b ? a : b;
+}
+static inline double np_min(double a, double b) {
+    if (isnan(a) || isnan(b)) return NAN;
+    return a <= b ? a : b;
+}
+/* numpy.clip(x, lo, hi) == minimum(maximum(x, lo), hi). */
+static inline double np_clip(double x, double lo, double hi) {
+    return np_min(np_max(x, lo), hi);
+}
+static inline double sum3(double a, double b, double c) { return (a + b) + c; }
+
+/* ------------------------------------------------- host thread pool */
+
+/* A minimal dynamic-schedule parallel-for over [0, n) in chunks, on plain
+ * pthreads so the oracle needs no OpenMP runtime. */
+typedef void (*bho_range_fn)(void *ctx, int64_t begin, int64_t end, int64_t *acc);
+typedef struct {
+    bho_range_fn fn;
+    void *ctx;
+    int64_t n, chunk;
+    atomic_llong next;
+    int64_t acc_max;
+    pthread_mutex_t mu;
+} bho_pool_t;
+
+static void *bho_worker(void *arg) {
+    bho_pool_t *pool = (bho_pool_t *)arg;
+    int64_t local = 0;
+    for (;;) {
+        const int64_t b = (int64_t)atomic_fetch_add(&pool->next, pool->chunk);
+        if (b >= pool->n) break;
+        const int64_t e = b + pool->chunk < pool->n ? b + pool->chunk : pool->n;
+        pool->fn(pool->ctx, b, e, &local);
+    }
+    pthread_mutex_lock(&pool->mu);
+    if (local > pool->acc_max) pool->acc_max = local;
+    pthread_mutex_unlock(&pool->mu);
+    return NULL;
+}
+
+int bho_num_threads(void) {
+    const long c = sysconf(_SC_NPROCESSORS_ONLN);
+    return c > 0 ? (int)c : 1;
+}
+
+/* Runs fn over [0, n) on nthreads threads (<= 0: all online cores) and
+ * returns the maximum of the per-thread accumulators. */
+static int64_t bho_parallel_for(int64_t n, int nthreads, int64_t chunk,
+                                bho_range_fn fn, void *ctx) {
+    bho_pool_t pool;
+    pool.fn = fn;
+    pool.ctx = ctx;
+    pool.n = n;
+    pool.chunk = chunk > 0 ? chunk : 1;
+    atomic_init(&pool.next, 0);
+    pool.acc_max = 0;
+    pthread_mutex_init(&pool.mu, NULL);
+    if (nthreads <= 0) nthreads = bho_num_threads();
+    if (nthreads > 256) nthreads = 256;
+    if (nthreads == 1 || n <= pool.chunk) {
+        bho_worker(&pool);
+    } else {
+        pthread_t tid[256];
+        int started = 0;
+        for (int i = 0; i < nthreads; ++i)
+            if (pthread_create(&tid[i], NULL, bho_worker, &pool) == 0) ++started;
+        if (started == 0) bho_worker(&pool);
+        for (int i = 0; i < started; ++i) pthread_join(tid[i], NULL);
+    }
+    pthread_mutex_destroy(&pool.mu);
+    return pool.acc_max;
+}
+
+/* ---------------------------------------------------------------- kerr.py */
+
+void bho_geometry(double m, double a, double x, double y, double z,
+                  int gradients, bho_geometry_t *o) {
+    /* kerr.py:135-155 */
+    const double a2 = a * a;
+    const double rho2 = x * x + y * y + z * z;
+    const double q = rho2 - a2;
+    double s = sqrt(q * q + 4.0 * a2 * z * z);
+    s = np_max(s, BHO_TINY);
+    const double r2 = 0.5 * (q + s);
+    const double r = sqrt(np_max(r2, BHO_TINY));
+    const double r2_plus_a2 = r2 + a2;
+    const double qd = np_max(r2 * r2 + a2 * z * z, BHO_TINY);
+    const double h = m * r * r2 / qd;
+    const double inv_r2a2 = 1.0 / np_max(r2_plus_a2, BHO_TINY);
+    const double inv_r = 1.0 / r;
+    const double lx = (r * x + a * y) * inv_r2a2;
+    const double ly = (r * y - a * x) * inv_r2a2;
+    const double lz = z * inv_r;
+    o->r = r;
+    o->h = h;
+    o->l[0] = lx;
+    o->l[1] = ly;
+    o->l[2] = lz;
+    if (!gradients) return;
+
+    /* kerr.py:160-163: implicit derivative of the radius. */
+    const double inv_s = 1.0 / s;
+    const double r_x = x * r * inv_s;
+    const double r_y = y * r * inv_s;
+    const double r_z = z * r2_plus_a2 * inv_r * inv_s;
+
+    /* kerr.py:166-171: gradient of H. */
+    const double inv_qd2 = 1.0 / (qd * qd);
+    const double dh_dr = m * r2 * (3.0 * a2 * z * z - r2 * r2) * inv_qd2;
+    const double dh_dz_explicit = -2.0 * m * a2 * z * r * r2 * inv_qd2;
+    o->grad_h[0] = dh_dr * r_x;
+    o->grad_h[1] = dh_dr * r_y;
+    o->grad_h[2] = dh_dr * r_z + dh_dz_explicit;
+
+    /* kerr.py:177-191: gradients of the spatial null covector. */
+    const double two_r = 2.0 * r;
+    const double dlx_dx = (r_x * x + r) * inv_r2a2 - lx * two_r * r_x * inv_r2a2;
+    const double dlx_dy = (r_y * x + a) * inv_r2a2 - lx * two_r * r_y * inv_r2a2;
+    const double dlx_dz = r_z * x * inv_r2a2 - lx * two_r * r_z * inv_r2a2;
+    const double dly_dx = (r_x * y - a) * inv_r2a2 - ly * two_r * r_x * inv_r2a2;
+    const double dly_dy = (r_y * y + r) * inv_r2a2 - ly * two_r * r_y * inv_r2a2;
+    const double dly_dz = r_z * y * inv_r2a2 - ly * two_r * r_z * inv_r2a2;
+    const double dlz_dx = -lz * r_x * inv_r;
+    const double dlz_dy = -lz * r_y * inv_r;
+    const double dlz_dz = (1.0 - lz * r_z) * inv_r;
+    o->grad_l[0][0] = dlx_dx; o->grad_l[0][1] = dly_dx; o->grad_l[0][2] = dlz_dx;
+    o->grad_l[1][0] = dlx_dy; o->grad_l[1][1] = dly_dy; o->grad_l[1][2] = dlz_dy;
+    o->grad_l[2][0] = dlx_dz; o->grad_l[2][1] = dly_dz; o->grad_l[2][2] = dlz_dz;
+}
+
+/* ----------------------------------------------------------- geodesics.py */
+
+void bho_rhs(double m, double a, const double s[8], double d[8]) {
+    /* geodesics.py:57-74 */
+    bho_geometry_t g;
+    bho_geometry(m, a, s[1], s[2], s[3], 1, &g);
+    const double p_t = s[4];
+    const double p0 = s[5], p1 = s[6], p2 = s[7];
+    const double lp = -p_t + sum3(g.l[0] * p0, g.l[1] * p1, g.l[2] * p2);
+    const double two_h_lp = 2.0 * g.h * lp;
+    d[0] = -p_t + two_h_lp;
+    d[1] = p0 - two_h_lp * g.l[0];
+    d[2] = p1 - two_h_lp * g.l[1];
+    d[3] = p2 - two_h_lp * g.l[2];
+    d[4] = 0.0;
+    const double lp2 = lp * lp;
+    for (int i = 0; i < 3; ++i) {
+        const double c = sum3(g.grad_l[i][0] * p0, g.grad_l[i][1] * p1,
+                              g.grad_l[i][2] * p2);
+        d[5 + i] = g.grad_h[i] * lp2 + two_h_lp * c;
+    }
+}
+
+double bho_hamiltonian(double m, double a, const double s[8]) {
+    /* geodesics.py:79-85 */
+    bho_geometry_t g;
+    bho_geometry(m, a, s[1], s[2], s[3], 0, &g);
+    const double p_t = s[4];
+    const double lp = -p_t + sum3(g.l[0] * s[5], g.l[1] * s[6], g.l[2] * s[7]);
+    const double eta = 0.5 * (-p_t * p_t + sum3(s[5] * s[5], s[6] * s[6], s[7] * s[7]));
+    return eta - g.h * lp * lp;
+}
+
+void bho_coordinate_velocity(double m, double a, const double s[8], double v[4]) {
+    /* geodesics.py:97-106 */
+    bho_geometry_t g;
+    bho_geometry(m, a, s[1], s[2], s[3], 0, &g);
+    const double p_t = s[4];
+    const double lp = -p_t + sum3(g.l[0] * s[5], g.l[1] * s[6], g.l[2] * s[7]);
+    const double two_h_lp = 2.0 * g.h * lp;
+    v[0] = -p_t + two_h_lp;
+    v[1] = s[5] - two_h_lp * g.l[0];
+    v[2] = s[6] - two_h_lp * g.l[1];
+    v[3] = s[7] - two_h_lp * g.l[2];
+}
+
+void bho_null_momentum(double m, double a, const double pos[3],
+                       const double dir[3], int past, int normalize,
+                       double p[4]) {
+    /* geodesics.py:141-170 */
+    bho_geometry_t g;
+    bho_geometry(m, a, pos[0], pos[1], pos[2], 0, &g);
+    const double h = g.h;
+    const double l_dot_s = sum3(g.l[0] * dir[0], g.l[1] * dir[1], g.l[2] * dir[2]);
+    const double s_dot_s = sum3(dir[0] * dir[0], dir[1] * dir[1], dir[2] * dir[2]);
+    const double g_tt = 2.0 * h - 1.0;
+    const double b_coef = 4.0 * h * l_dot_s;
+    const double c_coef = s_dot_s + 2.0 * h * l_dot_s * l_dot_s;
+    const double disc = b_coef * b_coef - 4.0 * g_tt * c_coef;
+    const double sqrt_disc = sqrt(np_max(disc, 0.0));
+    const double root_a = (-b_coef + sqrt_disc) / (2.0 * g_tt);
+    const double root_b = (-b_coef - sqrt_disc) / (2.0 * g_tt);
+    const double k_t = past ? np_min(root_a, root_b) : np_max(root_a, root_b);
+    const double l_dot_k = k_t + l_dot_s;
+    p[0] = -k_t + 2.0 * h * l_dot_k;
+    for (int i = 0; i < 3; ++i) p[1 + i] = dir[i] + (2.0 * h * l_dot_k) * g.l[i];
+    if (normalize) {
+        const double n0 = fabs(p[0]);
+        for (int i = 0; i < 4; ++i) p[i] = p[i] / n0;
+    }
+}
+
+/* --------------------------------------------------------- integrators.py */
+
+/* integrators.py:24-54 -- Dormand-Prince 5(4) tableau, autonomous form. */
+#define A21 (1.0 / 5.0)
+#define A31 (3.0 / 40.0)
+#define A32 (9.0 / 40.0)
+#define A41 (44.0 / 45.0)
+#define A42 (-56.0 / 15.0)
+#define A43 (32.0 / 9.0)
+#define A51 (19372.0 / 6561.0)
+#define A52 (-25360.0 / 2187.0)
+#define A53 (64448.0 / 6561.0)
+#define A54 (-212.0 / 729.0)
+#define A61 (9017.0 / 3168.0)
+#define A62 (-355.0 / 33.0)
+#define A63 (46732.0 / 5247.0)
+#define A64 (49.0 / 176.0)
+#define A65 (-5103.0 / 18656.0)
+#define B1 (35.0 / 384.0)
+#define B3 (500.0 / 1113.0)
+#define B4 (125.0 / 192.0)
+#define B5 (-2187.0 / 6784.0)
+#define B6 (11.0 / 84.0)
+#define E1 (71.0 / 57600.0)
+#define E3 (-71.0 / 16695.0)
+#define E4 (71.0 / 1920.0)
+#define E5 (-17253.0 / 339200.0)
+#define E6 (22.0 / 525.0)
+#define E7 (-1.0 / 40.0)
+
+void bho_dp5_step(double m, double a, const double y[8], double h,
+                  double y_new[8], double err[8]) {
+    /* integrators.py:92-107 */
+    double k1[8], k2[8], k3[8], k4[8], k5[8], k6[8], k7[8], t[8];
+    int i;
+    bho_rhs(m, a, y, k1);
+    for (i = 0; i < 8; ++i) t[i] = y[i] + h * (A21 * k1[i]);
+    bho_rhs(m, a, t, k2);
+    for (i = 0; i < 8; ++i) t[i] = y[i] + h * (A31 * k1[i] + A32 * k2[i]);
+    bho_rhs(m, a, t, k3);
+    for (i = 0; i < 8; ++i)
+        t[i] = y[i] + h * (A41 * k1[i] + A42 * k2[i] + A43 * k3[i]);
+    bho_rhs(m, a, t, k4);
+    for (i = 0; i < 8; ++i)
+        t[i] = y[i] + h * (A51 * k1[i] + A52 * k2[i] + A53 * k3[i] + A54 * k4[i]);
+    bho_rhs(m, a, t, k5);
+    for (i = 0; i < 8; ++i)
+        t[i] = y[i] + h * (A61 * k1[i] + A62 * k2[i] + A63 * k3[i] +
+                           A64 * k4[i] + A65 * k5[i]);
+    bho_rhs(m, a, t, k6);
+    for (i = 0; i < 8; ++i) {
+        const double inc = B1 * k1[i] + B3 * k3[i] + B4 * k4[i] + B5 * k5[i] + B6 * k6[i];
+        y_new[i] = y[i] + h * inc;
+    }
+    bho_rhs(m, a, y_new, k7);
+    for (i = 0; i < 8; ++i)
+        err[i] = h * (E1 * k1[i] + E3 * k3[i] + E4 * k4[i] + E5 * k5[i] +
+                      E6 * k6[i] + E7 * k7[i]);
+}
+
+double bho_error_ratio(const double y[8], const double y_new[8],
+                       const double err[8], double rtol, double atol) {
+    /* integrators.py:113-117 */
+    double q[8];
+    for (int i = 0; i < 8; ++i) {
+        const double scale = atol + rtol * np_max(fabs(y[i]), fabs(y_new[i]));
+        const double e = err[i] / scale;
+        q[i] = e * e;
+    }
+    const double sum = ((q[0] + q[1]) + (q[2] + q[3])) + ((q[4] + q[5]) + (q[6] + q[7]));
+    const double ratio = sqrt(sum / 8.0);
+    return isfinite(ratio) ? ratio : INFINITY;
+}
+
+double bho_step_factor(double ratio) {
+    /* integrators.py:122-124 */
+    const double safe = np_max(ratio, 1e-16);
+    return np_clip(0.9 * pow(safe, -0.2), 0.2, 5.0);
+}
+
+void bho_rk4_step(double m, double a, const double y[8], double h,
+                  double y_new[8]) {
+    /* integrators.py:69-73 */
+    double k1[8], k2[8], k3[8], k4[8], t[8];
+    int i;
+    bho_rhs(m, a, y, k1);
+    for (i = 0; i < 8; ++i) t[i] = y[i] + 0.5 * h * k1[i];
+    bho_rhs(m, a, t, k2);
+    for (i = 0; i < 8; ++i) t[i] = y[i] + 0.5 * h * k2[i];
+    bho_rhs(m, a, t, k3);
+    for (i = 0; i < 8; ++i) t[i] = y[i] + h * k3[i];
+    bho_rhs(m, a, t, k4);
+    for (i = 0; i < 8; ++i)
+        y_new[i] = y[i] + (h / 6.0) * (k1[i] + 2.0 * k2[i] + 2.0 * k3[i] + k4[i]);
+}
+
+/* -------------------------------------------------------------- camera.py */
+
+void bho_pinhole_directions(const double fwd[3], const double right[3],
+                            const double up[3], double fov_degrees,
+                            int64_t width, int64_t height, double *dirs) {
+    /* camera.py:102-113; math.radians(x) is x * (pi / 180). */
+    const double half_w = tan(fov_degrees * (M_PI / 180.0) / 2.0);
+    const double half_h = half_w * (double)height / (double)width;
+    for (int64_t row = 0; row < height; ++row) {
+        const double rv = 1.0 - ((double)row + 0.5) / (double)height * 2.0;
+        const double v = rv * half_h;
+        for (int64_t col = 0; col < width; ++col) {
+            const double cu = ((double)col + 0.5) / (double)width * 2.0 - 1.0;
+            const double u = cu * half_w;
+            double d[3];
+            for (int i = 0; i < 3; ++i) d[i] = fwd[i] + u * right[i] + v * up[i];
+            const double nrm = sqrt(sum3(d[0] * d[0], d[1] * d[1], d[2] * d[2]));
+            double *o = dirs + 3 * (row * width + col);
+            for (int i = 0; i < 3; ++i) o[i] = d[i] / nrm;
+        }
+    }
+}
+
+/* -------------------------------------------------------------- tracer.py */
+
+static int64_t trace_one(const bho_trace_params_t *p, double capture_radius,
+                         double y[8], int32_t *status_out, int64_t *steps_out) {
+    /* Body of the batch loop tracer.py:103-149 for one ray: a ray that is in
+     * flight at batch iteration k has made exactly k attempts, so the
+     * batch-global cap 4*max_steps (tracer.py:101) is a per-ray attempt cap. */
+    const int64_t max_iterations = 4 * p->max_steps;
+    double h = p->initial_step;
+    int64_t steps = 0;
+    int32_t status = BHO_IN_FLIGHT;
+    int64_t it = 0;
+    while (it < max_iterations) {
+        ++it;
+        double y_new[8], err[8];
+        bho_dp5_step(p->mass, p->spin, y, h, y_new, err);
+        const double ratio = bho_error_ratio(y, y_new, err, p->rtol, p->atol);
+        const int accept = ratio <= 1.0;
+        if (accept) memcpy(y, y_new, sizeof(y_new));
+        steps += accept;
+        h = np_clip(h * bho_step_factor(ratio), 0.0, p->max_step);
+
+        bho_geometry_t g;
+        bho_geometry(p->mass, p->spin, y[1], y[2], y[3], 0, &g);
+        int finite = 1;
+        for (int i = 0; i < 8; ++i) finite &= isfinite(y[i]) ? 1 : 0;
+        int32_t st = BHO_IN_FLIGHT;
+        if (!finite) st = BHO_FAILED;
+        if (finite && g.r <= capture_radius) st = BHO_CAPTURED;
+        if (finite && g.r >= p->escape_radius) st = BHO_ESCAPED;
+        const int in_flight = st == BHO_IN_FLIGHT;
+        if (in_flight && h < p->min_step) st = BHO_FAILED;
+        if (in_flight && steps >= p->max_steps) st = BHO_MAX_STEPS;
+        status = st;
+        if (status != BHO_IN_FLIGHT) break;
+    }
+    /* tracer.py:151-154 */
+    if (status == BHO_IN_FLIGHT) status = BHO_MAX_STEPS;
+    *status_out = status;
+    *steps_out = steps;
+    return it;
+}
+
+typedef struct {
+    const bho_trace_params_t *p;
+    double capture_radius;
+    double *states;
+    int32_t *status;
+    int64_t *steps;
+} trace_ctx_t;
+
+static void trace_range(void *vctx, int64_t b, int64_t e, int64_t *acc) {
+    trace_ctx_t *c = (trace_ctx_t *)vctx;
+    for (int64_t i = b; i < e; ++i) {
+        const int64_t it = trace_one(c->p, c->capture_radius, c->states + 8 * i,
+                                     c->status + i, c->steps + i);
+        if (it > *acc) *acc = it;
+    }
+}
+
+int64_t bho_trace_batch(const bho_trace_params_t *p, double *states,
+                        int32_t *status, int64_t *steps, int64_t n,
+                        int nthreads) {
+    /* tracer.py:84 */
+    const double r_plus = p->mass + sqrt(p->mass * p->mass - p->spin * p->spin);
+    const double capture_radius = r_plus * (1.0 + p->capture_margin);
+    /* tracer.py:95-99 */
+    for (int64_t i = 0; i < n; ++i) {
+        bho_geometry_t g;
+        const double *s = states + 8 * i;
+        bho_geometry(p->mass, p->spin, s[1], s[2], s[3], 0, &g);
+        if (g.r >= p->escape_radius) return -1;
+    }
+    trace_ctx_t c = {p, capture_radius, states, status, steps};
+    return bho_parallel_for(n, nthreads, 16, trace_range, &c);
+}
+
+typedef struct {
+    double mass, spin;
+    const double *spins;
+    double *states, *h;
+    int64_t *accepted;
+    int64_t n_steps;
+    double rtol, atol, max_step;
+} prop_ctx_t;
+
+static void prop_range(void *vctx, int64_t b, int64_t e, int64_t *acc) {
+    prop_ctx_t *c = (prop_ctx_t *)vctx;
+    (void)acc;
+    for (int64_t i = b; i < e; ++i) {
+        const double a = c->spins ? c->spins[i] : c->spin;
+        double *y = c->states + 8 * i;
+        double hh = c->h[i];
+        int64_t nacc = 0;
+        for (int64_t k = 0; k < c->n_steps; ++k) {
+            double y_new[8], err[8];
+            bho_dp5_step(c->mass, a, y, hh, y_new, err);
+            const double ratio = bho_error_ratio(y, y_new, err, c->rtol, c->atol);
+            if (ratio <= 1.0) {
+                memcpy(y, y_new, sizeof(y_new));
+                ++nacc;
+            }
+            hh = np_clip(hh * bho_step_factor(ratio), 0.0, c->max_step);
+        }
+        c->h[i] = hh;
+        c->accepted[i] = nacc;
+    }
+}
+
+void bho_propagate_batch(double mass, double spin, const double *spins,
+                         double *states, double *h, int64_t *accepted,
+                         int64_t n, int64_t n_steps, double rtol, double atol,
+                         double max_step, int nthreads) {
+    /* The accept/reject and step update of tracer.py:111-120, without the
+     * termination cascade. */
+    prop_ctx_t c = {mass, spin, spins, states, h, accepted, n_steps, rtol, atol, max_step};
+    bho_parallel_for(n, nthreads, 4, prop_range, &c);
+}
+
+typedef struct {
+    double mass, spin, h;
+    double *states;
+    int64_t n_steps;
+} rk4_ctx_t;
+
+static void rk4_range(void *vctx, int64_t b, int64_t e, int64_t *acc) {
+    rk4_ctx_t *c = (rk4_ctx_t *)vctx;
+    (void)acc;
+    for (int64_t i = b; i < e; ++i) {
+        double *y = c->states + 8 * i;
+        for (int64_t k = 0; k < c->n_steps; ++k) {
+            double y_new[8];
+            bho_rk4_step(c->mass, c->spin, y, c->h, y_new);
+            memcpy(y, y_new, sizeof(y_new));
+        }
+    }
+}
+
+void bho_rk4_batch(double mass, double spin, double *states, int64_t n,
+                   int64_t n_steps, double h, int nthreads) {
+    rk4_ctx_t c = {mass, spin, h, states, n_steps};
+    bho_parallel_for(n, nthreads, 64, rk4_range, &c);
+}
+
+/* ------------------------------------------------- batched test helpers */
+
+void bho_geometry_batch(double m, double a, const double *xyz, int64_t n,
+                        double *r, double *h, double *l, double *grad_h,
+                        double *grad_l) {
+    for (int64_t i = 0; i < n; ++i) {
+        bho_geometry_t g;
+        bho_geometry(m, a, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], 1, &g);
+        r[i] = g.r;
+        h[i] = g.h;
+        for (int j = 0; j < 3; ++j) {
+            l[3 * i + j] = g.l[j];
+            grad_h[3 * i + j] = g.grad_h[j];
+            for (int k = 0; k < 3; ++k) grad_l[9 * i + 3 * j + k] = g.grad_l[j][k];
+        }
+    }
+}
+
+void bho_rhs_batch(double m, double a, const double *states, int64_t n,
+                   double *deriv) {
+    for (int64_t i = 0; i < n; ++i) bho_rhs(m, a, states + 8 * i, deriv + 8 * i);
+}
+
+void bho_dp5_batch(double m, double a, const double *states, const double *h,
+                   int64_t n, double *y_new, double *err, double *ratio,
+                   double rtol, double atol) {
+    for (int64_t i = 0; i < n; ++i) {
+        bho_dp5_step(m, a, states + 8 * i, h[i], y_new + 8 * i, err + 8 * i);
+        if (ratio)
+            ratio[i] = bho_error_ratio(states + 8 * i, y_new + 8 * i,
+                                       err + 8 * i, rtol, atol);
+    }
+}
+
+void bho_null_momentum_batch(double m, double a, const double *pos,
+                             const double *dir, int64_t n, int past,
+                             int normalize, double *p) {
+    for (int64_t i = 0; i < n; ++i)
+        bho_null_momentum(m, a, pos + 3 * i, dir + 3 * i, past, normalize, p + 4 * i);
+}

@@ -1,0 +1,134 @@
+/*
+ * bh_oracle.h -- CPU restatement of BlackHorizon's geodesic hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This header and bh_oracle.c are the oracle that
+ * the parity tests, the smoke check and the CPU-baseline leg of the benchmark
+ * compare the CUDA library against.  Nothing in the product path
+ * (blackhorizon_b200/) may include, link or call it.
+ *
+ * Every function restates one reference function operation for operation
+ * (same association order as the NumPy expressions, no FMA contraction) so
+ * that results agree with the reference to the last bit wherever libm and
+ * NumPy agree; the one known source of ulp-level difference is pow() in the
+ * step-size factor (NumPy may use a SIMD pow).  Citations are to files of the
+ * reference project (MegaKruk/BlackHorizon).
+ */
+#ifndef BH_ORACLE_H
+#define BH_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Ray status codes: blackhorizon/tracer.py:21-30 (RayStatus). */
+enum {
+    BHO_IN_FLIGHT = 0,
+    BHO_CAPTURED = 1,
+    BHO_ESCAPED = 2,
+    BHO_MAX_STEPS = 3,
+    BHO_FAILED = 4
+};
+
+/* Kerr-Schild geometry at one point: blackhorizon/kerr.py:32-49.
+ * grad_l[i][j] = d l_j / d x_i. */
+typedef struct {
+    double r, h;
+    double l[3];
+    double grad_h[3];
+    double grad_l[3][3];
+} bho_geometry_t;
+
+/* Tracer controls: keyword arguments of blackhorizon/tracer.py:50-61. */
+typedef struct {
+    double mass, spin;
+    double escape_radius;
+    int64_t max_steps;
+    double rtol, atol, initial_step, max_step, min_step, capture_margin;
+} bho_trace_params_t;
+
+/* kerr.py:118-193 (KerrSpacetime.geometry). */
+void bho_geometry(double m, double a, double x, double y, double z,
+                  int gradients, bho_geometry_t *out);
+
+/* geodesics.py:42-74 (geodesic_rhs) for one state. */
+void bho_rhs(double m, double a, const double s[8], double d[8]);
+
+/* geodesics.py:77-85 (hamiltonian). */
+double bho_hamiltonian(double m, double a, const double s[8]);
+
+/* geodesics.py:95-106 (coordinate_velocity). */
+void bho_coordinate_velocity(double m, double a, const double s[8], double v[4]);
+
+/* geodesics.py:109-170 (null_momentum_from_velocity); past != 0 selects the
+ * past-directed root. */
+void bho_null_momentum(double m, double a, const double pos[3],
+                       const double dir[3], int past, int normalize,
+                       double p[4]);
+
+/* integrators.py:76-107 (dormand_prince_step), autonomous form, k7 recomputed. */
+void bho_dp5_step(double m, double a, const double y[8], double h,
+                  double y_new[8], double err[8]);
+
+/* integrators.py:110-117 (error_ratio) for one 8-component state. */
+double bho_error_ratio(const double y[8], const double y_new[8],
+                       const double err[8], double rtol, double atol);
+
+/* integrators.py:120-124 (step_factor). */
+double bho_step_factor(double ratio);
+
+/* integrators.py:57-73 (rk4_step). */
+void bho_rk4_step(double m, double a, const double y[8], double h,
+                  double y_new[8]);
+
+/* camera.py:96-113 (PinholeCamera.ray_directions) given the basis that
+ * camera.py:48-66 builds; dirs is (height*width, 3), row-major from the
+ * top-left pixel. */
+void bho_pinhole_directions(const double forward[3], const double right[3],
+                            const double up[3], double fov_degrees,
+                            int64_t width, int64_t height, double *dirs);
+
+/* tracer.py:50-157 (trace_rays) for a batch; each ray runs the reference's
+ * per-iteration body until it leaves IN_FLIGHT or the batch-global cap of
+ * 4*max_steps iterations.  states (n,8) is updated in place.  Returns the
+ * reference's `iterations` (max attempts over rays), or -1 when an initial
+ * radius is at or beyond escape_radius (the reference raises ValueError).
+ * nthreads <= 0 uses one thread per online core. */
+int64_t bho_trace_batch(const bho_trace_params_t *p, double *states,
+                        int32_t *status, int64_t *steps, int64_t n,
+                        int nthreads);
+
+/* Lock-step adaptive propagation without termination: n_steps attempted
+ * DP5(4) steps per ray with the tracer's accept/reject and step update
+ * (tracer.py:111-120).  spin may be per ray (spins != NULL).  states (n,8)
+ * updated in place; accepted (n,) receives accepted-step counts; h (n,) holds
+ * the step size in and out. */
+void bho_propagate_batch(double mass, double spin, const double *spins,
+                         double *states, double *h, int64_t *accepted,
+                         int64_t n, int64_t n_steps, double rtol, double atol,
+                         double max_step, int nthreads);
+
+/* Fixed-step RK4 for a batch (examples/benchmark.py:39-51). */
+void bho_rk4_batch(double mass, double spin, double *states, int64_t n,
+                   int64_t n_steps, double h, int nthreads);
+
+/* Batched point-wise helpers used by the parity tests. */
+void bho_geometry_batch(double m, double a, const double *xyz, int64_t n,
+                        double *r, double *h, double *l, double *grad_h,
+                        double *grad_l);
+void bho_rhs_batch(double m, double a, const double *states, int64_t n,
+                   double *deriv);
+void bho_dp5_batch(double m, double a, const double *states, const double *h,
+                   int64_t n, double *y_new, double *err, double *ratio,
+                   double rtol, double atol);
+void bho_null_momentum_batch(double m, double a, const double *pos,
+                             const double *dir, int64_t n, int past,
+                             int normalize, double *p);
+
+int bho_num_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,201 @@
+"""ctypes front end of the CPU oracle (``oracle/bh_oracle.c``).
+
+TEST INFRASTRUCTURE ONLY.  The parity tests, ``__graft_entry__.smoke()`` and
+the CPU-baseline leg of ``bench.py`` use this module as the checker for the
+CUDA library; the product package ``blackhorizon_b200`` never imports it.
+
+Each wrapper names the reference function (MegaKruk/BlackHorizon, path within
+that project) whose behaviour the C restatement follows.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libbh_oracle.so")
+_lib = None
+
+_D = ctypes.c_double
+_I64 = ctypes.c_int64
+_P = ctypes.c_void_p
+
+
+class TraceParams(ctypes.Structure):
+    """Keyword arguments of blackhorizon/tracer.py:50-61 plus mass and spin."""
+
+    _fields_ = [
+        ("mass", _D), ("spin", _D), ("escape_radius", _D), ("max_steps", _I64),
+        ("rtol", _D), ("atol", _D), ("initial_step", _D), ("max_step", _D),
+        ("min_step", _D), ("capture_margin", _D),
+    ]
+
+
+def build(force: bool = False) -> str:
+    """Compile the oracle with its Makefile (gcc, no FMA contraction)."""
+    src = os.path.join(_HERE, "bh_oracle.c")
+    if force or not os.path.exists(_LIB_PATH) or (
+        os.path.getmtime(_LIB_PATH) < os.path.getmtime(src)
+    ):
+        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        _lib = ctypes.CDLL(_LIB_PATH)
+        _lib.bho_trace_batch.restype = _I64
+        _lib.bho_error_ratio.restype = _D
+        _lib.bho_step_factor.restype = _D
+        _lib.bho_hamiltonian.restype = _D
+        _lib.bho_step_factor.argtypes = [_D]
+        _lib.bho_num_threads.restype = ctypes.c_int
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_P)
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def num_threads() -> int:
+    return int(lib().bho_num_threads())
+
+
+def geometry(mass: float, spin: float, xyz):
+    """kerr.py:118-193 with gradients: returns r, h, l, grad_h, grad_l."""
+    xyz = _f64(xyz)
+    n = xyz.shape[0]
+    r = np.empty(n); h = np.empty(n)
+    l = np.empty((n, 3)); gh = np.empty((n, 3)); gl = np.empty((n, 3, 3))
+    lib().bho_geometry_batch(_D(mass), _D(spin), _ptr(xyz), _I64(n), _ptr(r),
+                             _ptr(h), _ptr(l), _ptr(gh), _ptr(gl))
+    return r, h, l, gh, gl
+
+
+def rhs(mass: float, spin: float, states):
+    """geodesics.py:42-74."""
+    s = _f64(states)
+    out = np.empty_like(s)
+    lib().bho_rhs_batch(_D(mass), _D(spin), _ptr(s), _I64(s.shape[0]), _ptr(out))
+    return out
+
+
+def hamiltonian(mass: float, spin: float, states):
+    """geodesics.py:77-85."""
+    s = _f64(states)
+    out = np.empty(s.shape[0])
+    f = lib().bho_hamiltonian
+    f.argtypes = [_D, _D, _P]
+    for i in range(s.shape[0]):
+        out[i] = f(mass, spin, s[i].ctypes.data_as(_P))
+    return out
+
+
+def coordinate_velocity(mass: float, spin: float, states):
+    """geodesics.py:95-106."""
+    s = _f64(states)
+    out = np.empty((s.shape[0], 4))
+    f = lib().bho_coordinate_velocity
+    for i in range(s.shape[0]):
+        f(_D(mass), _D(spin), s[i].ctypes.data_as(_P), out[i].ctypes.data_as(_P))
+    return out
+
+
+def null_momentum(mass: float, spin: float, positions, directions,
+                  past: bool = True, normalize: bool = True):
+    """geodesics.py:109-170."""
+    pos = _f64(positions); d = _f64(directions)
+    out = np.empty((pos.shape[0], 4))
+    lib().bho_null_momentum_batch(_D(mass), _D(spin), _ptr(pos), _ptr(d),
+                                  _I64(pos.shape[0]), ctypes.c_int(int(past)),
+                                  ctypes.c_int(int(normalize)), _ptr(out))
+    return out
+
+
+def dp5_step(mass: float, spin: float, states, h, rtol: float = 1e-9,
+             atol: float = 1e-12):
+    """integrators.py:76-117: returns (new_state, error, error_ratio)."""
+    s = _f64(states)
+    hh = _f64(np.broadcast_to(np.asarray(h, dtype=np.float64), (s.shape[0],)))
+    y_new = np.empty_like(s); err = np.empty_like(s); ratio = np.empty(s.shape[0])
+    lib().bho_dp5_batch(_D(mass), _D(spin), _ptr(s), _ptr(hh), _I64(s.shape[0]),
+                        _ptr(y_new), _ptr(err), _ptr(ratio), _D(rtol), _D(atol))
+    return y_new, err, ratio
+
+
+def step_factor(ratio):
+    """integrators.py:120-124."""
+    f = lib().bho_step_factor
+    return np.array([f(float(r)) for r in np.ravel(ratio)])
+
+
+def rk4(mass: float, spin: float, states, h: float, n_steps: int,
+        nthreads: int = 0):
+    """n_steps of integrators.py:57-73 per ray."""
+    s = _f64(states).copy()
+    lib().bho_rk4_batch(_D(mass), _D(spin), _ptr(s), _I64(s.shape[0]),
+                        _I64(n_steps), _D(h), ctypes.c_int(nthreads))
+    return s
+
+
+def pinhole_directions(forward, right, up, fov_degrees: float, width: int,
+                       height: int):
+    """camera.py:96-113 given the camera basis."""
+    out = np.empty((height * width, 3))
+    f = _f64(forward); r = _f64(right); u = _f64(up)
+    lib().bho_pinhole_directions(_ptr(f), _ptr(r), _ptr(u), _D(fov_degrees),
+                                 _I64(width), _I64(height), _ptr(out))
+    return out
+
+
+def trace(mass: float, spin: float, state0, escape_radius: float,
+          max_steps: int = 20000, rtol: float = 1e-9, atol: float = 1e-12,
+          initial_step: float = 0.1, max_step: float = 2.0,
+          min_step: float = 1e-10, capture_margin: float = 1e-3,
+          nthreads: int = 0):
+    """tracer.py:50-157: returns (states, status, steps, iterations)."""
+    s = _f64(state0).copy()
+    n = s.shape[0]
+    status = np.empty(n, dtype=np.int32)
+    steps = np.empty(n, dtype=np.int64)
+    p = TraceParams(mass, spin, escape_radius, max_steps, rtol, atol,
+                    initial_step, max_step, min_step, capture_margin)
+    it = lib().bho_trace_batch(ctypes.byref(p), _ptr(s), _ptr(status),
+                               _ptr(steps), _I64(n), ctypes.c_int(nthreads))
+    if it < 0:
+        raise ValueError("escape_radius must exceed all initial radii")
+    return s, status, steps, int(it)
+
+
+def propagate(mass: float, spins, state0, n_steps: int, rtol: float,
+              atol: float, initial_step: float = 0.1, max_step: float = 2.0,
+              nthreads: int = 0):
+    """n_steps attempted DP5(4) steps per ray with the tracer's accept/reject
+    and step update (tracer.py:111-120) and no termination; spins is a scalar
+    or a per-ray array.  Returns (states, h, accepted)."""
+    s = _f64(state0).copy()
+    n = s.shape[0]
+    h = np.full(n, float(initial_step))
+    acc = np.empty(n, dtype=np.int64)
+    spins_arr = None
+    spin = 0.0
+    if np.ndim(spins) == 0:
+        spin = float(spins)
+    else:
+        spins_arr = _f64(spins)
+    lib().bho_propagate_batch(_D(mass), _D(spin),
+                              _ptr(spins_arr) if spins_arr is not None else None,
+                              _ptr(s), _ptr(h), _ptr(acc), _I64(n), _I64(n_steps),
+                              _D(rtol), _D(atol), _D(max_step),
+                              ctypes.c_int(nthreads))
+    return s, h, acc

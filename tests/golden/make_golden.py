@@ -1,0 +1,352 @@
+"""Generate the golden fixtures under tests/golden/ from the reference itself.
+
+Run in a container where the reference project (MegaKruk/BlackHorizon) is
+importable; it is read from the path given by --reference (default: the
+read-only mount this build was developed against).  The fixtures are small
+.npz files; MANIFEST.json records the command, the reference files' SHA-256
+and the shapes written, so a reader can regenerate and compare.
+
+    python tests/golden/make_golden.py --reference /root/reference
+
+Every workload below is built with the reference's own functions
+(KerrSpacetime, null_momentum_from_velocity, build_state, PinholeCamera,
+trace_rays, dormand_prince_step, error_ratio, step_factor, rk4_step).  The
+raw-throughput workload (2^20 photons on the Kerr-Schild sphere r=30, per-ray
+spin in [-0.95, 0.95]) is defined in synthetic_inputs() so bench.py and the
+tests can rebuild the same rays from the seed without the reference.
+"""
+
+from __future__ import annotations
+
+import argparse
+import hashlib
+import json
+import multiprocessing as mp
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from blackhorizon_b200.workloads import (  # noqa: E402  (host-only, no GPU)
+    RAW_SEED,
+    raw_throughput_inputs,
+)
+
+REF_FILES = [
+    "blackhorizon/kerr.py",
+    "blackhorizon/geodesics.py",
+    "blackhorizon/integrators.py",
+    "blackhorizon/tracer.py",
+    "blackhorizon/camera.py",
+    "blackhorizon/examples/benchmark.py",
+    "tests/test_kerr.py",
+    "tests/test_shadow.py",
+]
+
+
+def sha256(path: str) -> str:
+    with open(path, "rb") as f:
+        return hashlib.sha256(f.read()).hexdigest()
+
+
+def random_points(n, r_min, r_max, seed):
+    """Same construction as the reference's tests/test_kerr.py:11-17."""
+    rng = np.random.default_rng(seed)
+    u = rng.normal(size=(n, 3))
+    u /= np.linalg.norm(u, axis=-1, keepdims=True)
+    radii = rng.uniform(r_min, r_max, size=(n, 1))
+    return radii * u
+
+
+def gen_geometry(ref, out):
+    KerrSpacetime = ref["KerrSpacetime"]
+    sets = {}
+    special = np.array([
+        [0.0, 0.0, 1.5], [0.0, 0.0, -7.0], [2.0, 0.0, 0.0], [11.0, 0.0, 0.0],
+        [0.5, 0.3, 0.01], [0.95, 0.0, 1e-6], [1.2, 0.9, 0.4], [0.0, 1.5, -0.2],
+        [1.44, 0.0, 0.0], [0.3, -0.2, 1.45],
+    ])
+    for tag, spin, pts in [
+        ("a09", 0.9, np.concatenate([random_points(300, 2.2, 60.0, 11), special])),
+        ("a095", 0.95, random_points(200, 2.5, 40.0, 3)),
+        ("a0", 0.0, random_points(100, 2.5, 40.0, 13)),
+        ("am0998", -0.998, random_points(200, 1.1, 30.0, 17)),
+    ]:
+        st = KerrSpacetime(1.0, spin)
+        g = st.geometry(pts[:, 0], pts[:, 1], pts[:, 2], gradients=True)
+        sets[f"{tag}_spin"] = np.float64(spin)
+        sets[f"{tag}_xyz"] = pts
+        sets[f"{tag}_r"] = g.radius
+        sets[f"{tag}_h"] = g.h
+        sets[f"{tag}_l"] = g.l
+        sets[f"{tag}_grad_h"] = g.grad_h
+        sets[f"{tag}_grad_l"] = g.grad_l
+    np.savez_compressed(os.path.join(out, "geometry.npz"), **sets)
+
+
+def photon_states(ref, spin, n, seed, r_min=2.5, r_max=40.0):
+    """Past-directed null states at random points outside the ergosphere."""
+    G = ref["geodesics"]
+    st = ref["KerrSpacetime"](1.0, spin)
+    rng = np.random.default_rng(seed)
+    pos = random_points(n, r_min, r_max, seed)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=-1, keepdims=True)
+    mom = G.null_momentum_from_velocity(st, pos, d, "past")
+    return st, G.build_state(pos, mom), pos, d
+
+
+def gen_steps(ref, out):
+    G, I = ref["geodesics"], ref["integrators"]
+    st, s0, pos, d = photon_states(ref, 0.9, 512, 21)
+    rng = np.random.default_rng(22)
+    h = np.exp(rng.uniform(np.log(1e-3), np.log(2.0), size=512))
+
+    def rhs(b):
+        return G.geodesic_rhs(st, b)
+
+    y_new, err = I.dormand_prince_step(rhs, s0, h)
+    ratio = I.error_ratio(s0, y_new, err, 1e-8, 1e-10)
+    factor = I.step_factor(ratio)
+    rk4 = I.rk4_step(rhs, s0, h)
+    np.savez_compressed(
+        os.path.join(out, "steps.npz"),
+        spin=np.float64(0.9), state=s0, h=h, rhs=G.geodesic_rhs(st, s0),
+        dp5_new=y_new, dp5_err=err, ratio=ratio, factor=factor, rk4_new=rk4,
+        hamiltonian=G.hamiltonian(st, s0),
+        velocity=G.coordinate_velocity(st, s0), rtol=1e-8, atol=1e-10,
+    )
+    # Null momenta, both time orientations, normalised and not.
+    out_nm = {"spin": np.float64(0.9), "pos": pos, "dir": d}
+    for tor in ("past", "future"):
+        for norm in (True, False):
+            out_nm[f"{tor}_{int(norm)}"] = G.null_momentum_from_velocity(
+                st, pos, d, tor, norm
+            )
+    np.savez_compressed(os.path.join(out, "null_momentum.npz"), **out_nm)
+
+
+def gen_camera(ref, out):
+    C = ref["camera"]
+    cams = {
+        "c1": C.PinholeCamera.from_orbit(50.0, 60.0, fov_degrees=30.0, width=40, height=30),
+        "c3": C.PinholeCamera.from_orbit(50.0, 80.0, fov_degrees=25.0, width=32, height=18),
+        "pole": C.PinholeCamera.from_orbit(20.0, 0.0, fov_degrees=30.0, width=8, height=6),
+        "free": C.PinholeCamera(position=(3.0, -40.0, 7.0), target=(1.0, 2.0, -1.0),
+                                up_hint=(0.2, 0.1, 1.0), fov_degrees=45.0, width=17, height=11),
+    }
+    arrs = {}
+    for k, c in cams.items():
+        arrs[f"{k}_position"] = np.asarray(c.position, dtype=np.float64)
+        arrs[f"{k}_target"] = np.asarray(c.target, dtype=np.float64)
+        arrs[f"{k}_up_hint"] = np.asarray(c.up_hint, dtype=np.float64)
+        arrs[f"{k}_fov"] = np.float64(c.fov_degrees)
+        arrs[f"{k}_wh"] = np.array([c.width, c.height], dtype=np.int64)
+        arrs[f"{k}_basis"] = np.stack([c.forward, c.right, c.up])
+        arrs[f"{k}_dirs"] = c.ray_directions()
+    np.savez_compressed(os.path.join(out, "camera.npz"), **arrs)
+
+
+def camera_state(ref, spin, distance, inc, fov, w, h):
+    C, G = ref["camera"], ref["geodesics"]
+    st = ref["KerrSpacetime"](1.0, spin)
+    cam = C.PinholeCamera.from_orbit(distance, inc, fov_degrees=fov, width=w, height=h)
+    pos = cam.ray_origins()
+    d = cam.ray_directions()
+    mom = G.null_momentum_from_velocity(st, pos, d, "past")
+    return st, G.build_state(pos, mom)
+
+
+def gen_trace_c1(ref, out):
+    T = ref["tracer"]
+    kw = dict(escape_radius=100.0, max_steps=5000, rtol=1e-8, atol=1e-10,
+              capture_margin=0.01)
+    # Full-state golden at 40x30 (same camera geometry as the 160x120 frame).
+    st, s_small = camera_state(ref, 0.9, 50.0, 60.0, 30.0, 40, 30)
+    res = T.trace_rays(st, s_small, **kw)
+    np.savez_compressed(
+        os.path.join(out, "trace_c1_40x30.npz"), state0=s_small,
+        states=res.states, status=res.status.astype(np.int8),
+        steps=res.steps.astype(np.int32), iterations=np.int64(res.iterations),
+    )
+    # Full 160x120 frame: status and steps for every ray, states for every
+    # 8th ray.
+    st, s_full = camera_state(ref, 0.9, 50.0, 60.0, 30.0, 160, 120)
+    t0 = time.perf_counter()
+    res = T.trace_rays(st, s_full, **kw)
+    dt = time.perf_counter() - t0
+    sub = np.arange(0, s_full.shape[0], 8)
+    np.savez_compressed(
+        os.path.join(out, "trace_c1_160x120.npz"),
+        status=res.status.astype(np.int8), steps=res.steps.astype(np.int16),
+        iterations=np.int64(res.iterations), sub_index=sub,
+        sub_states=res.states[sub], reference_seconds=np.float64(dt),
+    )
+
+
+def _trace_shard(args):
+    spin, state, kw = args
+    sys.path.insert(0, _REFERENCE_PATH)
+    from blackhorizon.kerr import KerrSpacetime
+    from blackhorizon.tracer import trace_rays
+
+    res = trace_rays(KerrSpacetime(1.0, spin), state, **kw)
+    return res.status.astype(np.int8), res.steps.astype(np.int16)
+
+
+def gen_trace_c3(ref, out, procs):
+    """Full-HD frame, a=0.9, 80 deg, fov 25: status for every pixel.
+
+    Rays are independent, so tracing contiguous shards in worker processes
+    gives the per-ray results of one trace_rays call."""
+    st, s = camera_state(ref, 0.9, 50.0, 80.0, 25.0, 1920, 1080)
+    kw = dict(escape_radius=100.0, max_steps=10000, rtol=1e-9, atol=1e-12,
+              capture_margin=0.01)
+    shards = np.array_split(s, procs * 8)
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(procs) as pool:
+        parts = pool.map(_trace_shard, [(0.9, x, kw) for x in shards])
+    dt = time.perf_counter() - t0
+    status = np.concatenate([p[0] for p in parts])
+    steps = np.concatenate([p[1] for p in parts])
+    np.savez_compressed(
+        os.path.join(out, "trace_c3_status.npz"), status=status, steps=steps,
+        reference_seconds=np.float64(dt), procs=np.int64(procs),
+    )
+
+
+def gen_fans(ref, out):
+    """First-round equatorial fans of the reference's tests/test_shadow.py:22-84
+    (camera at D=1000 on +x, escape 1.2 D, max_steps 60000, rtol 1e-10,
+    atol 1e-13, max_step 5)."""
+    G, T = ref["geodesics"], ref["tracer"]
+    D = 1000.0
+    arrs = {}
+    for tag, spin, lo, hi in [
+        ("a0_pos", 0.0, 4.5e-3, 6.5e-3),
+        ("a09_pro", 0.9, -4.0e-3, -2.0e-3),
+        ("a09_ret", 0.9, 5.5e-3, 8.0e-3),
+    ]:
+        st = ref["KerrSpacetime"](1.0, spin)
+        offsets = np.linspace(lo, hi, 48)
+        n = offsets.shape[0]
+        pos = np.tile(np.array([[D, 0.0, 0.0]]), (n, 1))
+        d = np.stack([-np.ones(n), offsets, np.zeros(n)], axis=-1)
+        d /= np.linalg.norm(d, axis=-1, keepdims=True)
+        mom = G.null_momentum_from_velocity(st, pos, d, "past")
+        s0 = G.build_state(pos, mom)
+        res = T.trace_rays(st, s0, escape_radius=1.2 * D, max_steps=60000,
+                           rtol=1e-10, atol=1e-13, max_step=5.0)
+        arrs[f"{tag}_spin"] = np.float64(spin)
+        arrs[f"{tag}_offsets"] = offsets
+        arrs[f"{tag}_state0"] = s0
+        arrs[f"{tag}_status"] = res.status.astype(np.int8)
+        arrs[f"{tag}_steps"] = res.steps.astype(np.int32)
+        arrs[f"{tag}_states"] = res.states
+    np.savez_compressed(os.path.join(out, "fans.npz"), **arrs)
+
+
+def gen_raw_throughput(ref, out, n=512, n_steps=2000):
+    """First n rays of the raw-throughput workload, n_steps attempted DP5(4)
+    steps each with the tracer's accept/reject and step update
+    (tracer.py:111-120) and no termination, per-ray spin."""
+    G, I = ref["geodesics"], ref["integrators"]
+    pos, d, spin = raw_throughput_inputs(n)
+    st = object.__new__(ref["KerrSpacetime"])
+    st.mass = 1.0
+    st.spin = spin
+    mom = G.null_momentum_from_velocity(st, pos, d, "past")
+    s0 = G.build_state(pos, mom)
+    y = s0.copy()
+    h = np.full(n, 0.1)
+    acc = np.zeros(n, dtype=np.int64)
+
+    def rhs(b):
+        return G.geodesic_rhs(st, b)
+
+    with np.errstate(all="ignore"):
+        for _ in range(n_steps):
+            y_new, err = I.dormand_prince_step(rhs, y, h)
+            ratio = I.error_ratio(y, y_new, err, 1e-8, 1e-10)
+            ok = ratio <= 1.0
+            y = np.where(ok[:, None], y_new, y)
+            acc += ok
+            h = np.clip(h * I.step_factor(ratio), 0.0, 2.0)
+    np.savez_compressed(
+        os.path.join(out, "raw_throughput.npz"), seed=np.int64(RAW_SEED),
+        pos=pos, dir=d, spin=spin, state0=s0, final=y, h=h, accepted=acc,
+        n_steps=np.int64(n_steps), rtol=1e-8, atol=1e-10,
+    )
+
+
+def gen_rk4(ref, out, n=256, n_steps=50):
+    """examples/benchmark.py:22-51: inward photons on r=50, a=0.9, seed 7,
+    fixed h=0.05."""
+    G, I = ref["geodesics"], ref["integrators"]
+    st = ref["KerrSpacetime"](1.0, 0.9)
+    rng = np.random.default_rng(7)
+    u = rng.normal(size=(n, 3))
+    u /= np.linalg.norm(u, axis=-1, keepdims=True)
+    pos = 50.0 * u
+    mom = G.null_momentum_from_velocity(st, pos, -u)
+    s0 = G.build_state(pos, mom)
+    y = s0.copy()
+    h = np.full(n, 0.05)
+    for _ in range(n_steps):
+        y = I.rk4_step(lambda b: G.geodesic_rhs(st, b), y, h)
+    np.savez_compressed(os.path.join(out, "rk4.npz"), state0=s0, final=y,
+                        h=np.float64(0.05), n_steps=np.int64(n_steps))
+
+
+_REFERENCE_PATH = "/root/reference"
+
+
+def main():
+    global _REFERENCE_PATH
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default=_REFERENCE_PATH)
+    ap.add_argument("--out", default=HERE)
+    ap.add_argument("--procs", type=int, default=os.cpu_count() or 1)
+    ap.add_argument("--skip-c3", action="store_true")
+    args = ap.parse_args()
+    _REFERENCE_PATH = args.reference
+    sys.path.insert(0, args.reference)
+    from blackhorizon import camera, geodesics, integrators, tracer
+    from blackhorizon.kerr import KerrSpacetime
+
+    ref = dict(KerrSpacetime=KerrSpacetime, geodesics=geodesics,
+               integrators=integrators, tracer=tracer, camera=camera)
+    steps = [
+        ("geometry", lambda: gen_geometry(ref, args.out)),
+        ("steps", lambda: gen_steps(ref, args.out)),
+        ("camera", lambda: gen_camera(ref, args.out)),
+        ("rk4", lambda: gen_rk4(ref, args.out)),
+        ("fans", lambda: gen_fans(ref, args.out)),
+        ("trace_c1", lambda: gen_trace_c1(ref, args.out)),
+        ("raw_throughput", lambda: gen_raw_throughput(ref, args.out)),
+    ]
+    if not args.skip_c3:
+        steps.append(("trace_c3", lambda: gen_trace_c3(ref, args.out, args.procs)))
+    timings = {}
+    for name, fn in steps:
+        t0 = time.perf_counter()
+        fn()
+        timings[name] = round(time.perf_counter() - t0, 2)
+        print(f"{name}: {timings[name]} s", flush=True)
+    manifest = {
+        "command": "python tests/golden/make_golden.py --reference <path>",
+        "reference_sha256": {f: sha256(os.path.join(args.reference, f)) for f in REF_FILES},
+        "numpy": np.__version__,
+        "seconds": timings,
+        "files": sorted(f for f in os.listdir(args.out) if f.endswith(".npz")),
+    }
+    with open(os.path.join(args.out, "MANIFEST.json"), "w") as f:
+        json.dump(manifest, f, indent=1)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,170 @@
+"""Point-wise kernels against the reference's golden vectors (float64).
+
+Tolerances: the kernels evaluate the reference formulas with FMA contraction
+and a regrouped gradient contraction, so results agree to a few ulps of the
+largest term: rtol 1e-12 on values, an absolute floor of 1e-14 x the largest
+magnitude in each array for terms that cancel.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+def close(a, b, rtol=1e-12, floor=1e-14):
+    a = a.detach().cpu().numpy() if isinstance(a, torch.Tensor) else np.asarray(a)
+    b = np.asarray(b)
+    atol = floor * max(np.max(np.abs(b)), 1.0)
+    np.testing.assert_allclose(a, b, rtol=rtol, atol=atol)
+
+
+def dev(a):
+    return torch.as_tensor(np.ascontiguousarray(a), device="cuda")
+
+
+def test_geometry(cuda):
+    from blackhorizon_b200.kerr import KerrSpacetime
+
+    g = golden("geometry.npz")
+    for tag in ("a09", "a095", "a0", "am0998"):
+        st = KerrSpacetime(1.0, float(g[f"{tag}_spin"]))
+        xyz = dev(g[f"{tag}_xyz"])
+        geo = st.geometry(xyz[:, 0].contiguous(), xyz[:, 1].contiguous(),
+                          xyz[:, 2].contiguous(), gradients=True)
+        close(geo.radius, g[f"{tag}_r"])
+        close(geo.h, g[f"{tag}_h"])
+        close(geo.l, g[f"{tag}_l"])
+        close(geo.grad_h, g[f"{tag}_grad_h"], rtol=1e-11)
+        close(geo.grad_l, g[f"{tag}_grad_l"], rtol=1e-11)
+
+
+def test_geometry_numpy_in_numpy_out(cuda):
+    from blackhorizon_b200.kerr import KerrSpacetime
+
+    st = KerrSpacetime(1.0, 0.8)
+    x = np.array([2.0, 5.0, 11.0])
+    r = st.kerr_schild_radius(x, np.zeros(3), np.zeros(3))
+    assert isinstance(r, np.ndarray)
+    # Reference tests/test_kerr.py:61-66: r = sqrt(x^2 - a^2) on the equator.
+    np.testing.assert_allclose(r, np.sqrt(x * x - 0.64), rtol=1e-14)
+    z = np.array([1.5, 3.0, -7.0])
+    np.testing.assert_allclose(st.kerr_schild_radius(np.zeros(3), np.zeros(3), z),
+                               np.abs(z), rtol=1e-14)
+
+
+def test_rhs_hamiltonian_velocity(cuda):
+    from blackhorizon_b200 import geodesics
+    from blackhorizon_b200.kerr import KerrSpacetime
+
+    g = golden("steps.npz")
+    st = KerrSpacetime(1.0, float(g["spin"]))
+    s = dev(g["state"])
+    close(geodesics.geodesic_rhs(st, s), g["rhs"], rtol=1e-11)
+    close(geodesics.hamiltonian(st, s), g["hamiltonian"], rtol=1e-9, floor=1e-15)
+    close(geodesics.coordinate_velocity(st, s), g["velocity"])
+
+
+@pytest.mark.parametrize("tor", ["past", "future"])
+@pytest.mark.parametrize("norm", [True, False])
+def test_null_momentum(cuda, tor, norm):
+    from blackhorizon_b200 import geodesics
+    from blackhorizon_b200.kerr import KerrSpacetime
+
+    g = golden("null_momentum.npz")
+    st = KerrSpacetime(1.0, float(g["spin"]))
+    p = geodesics.null_momentum_from_velocity(st, dev(g["pos"]), dev(g["dir"]), tor, norm)
+    close(p, g[f"{tor}_{int(norm)}"])
+
+
+def test_camera_states(cuda):
+    from blackhorizon_b200.camera import PinholeCamera
+    from blackhorizon_b200.kerr import KerrSpacetime
+
+    g = golden("trace_c1_40x30.npz")
+    cam = PinholeCamera.from_orbit(50.0, 60.0, fov_degrees=30.0, width=40, height=30)
+    s = cam.initial_states(KerrSpacetime(1.0, 0.9))
+    close(s, g["state0"])
+
+
+def test_dp5_step_fp64(cuda):
+    from blackhorizon_b200 import integrators
+    from blackhorizon_b200.geodesics import GeodesicRhs
+    from blackhorizon_b200.kerr import KerrSpacetime
+
+    g = golden("steps.npz")
+    rhs = GeodesicRhs(KerrSpacetime(1.0, float(g["spin"])))
+    s, h = dev(g["state"]), dev(g["h"])
+    new, err = integrators.dormand_prince_step(rhs, s, h)
+    close(new, g["dp5_new"])
+    # The embedded error is a difference of O(h^5) terms: compare against the
+    # magnitude of the step it estimates.
+    ref = g["dp5_err"]
+    scale = np.abs(g["h"])[:, None] * np.maximum(np.abs(g["rhs"]), 1e-3)
+    assert np.max(np.abs(err.cpu().numpy() - ref) / scale) < 1e-12
+    # error_ratio on the reference's own step outputs: same formula and
+    # NumPy's pairwise summation order.
+    ratio = integrators.error_ratio(s, dev(g["dp5_new"]), dev(g["dp5_err"]),
+                                    float(g["rtol"]), float(g["atol"]))
+    np.testing.assert_allclose(ratio.cpu().numpy(), g["ratio"], rtol=1e-15)
+    factor = integrators.step_factor(dev(g["ratio"]))
+    np.testing.assert_allclose(factor.cpu().numpy(), g["factor"], rtol=1e-15)
+
+
+def test_dp5_step_mixed(cuda):
+    """Mixed policy: float32 stage arithmetic; the update is float64, so the
+    new state differs from the reference by ~1e-7 of the step increment."""
+    from blackhorizon_b200 import integrators
+    from blackhorizon_b200.geodesics import GeodesicRhs
+    from blackhorizon_b200.kerr import KerrSpacetime
+
+    g = golden("steps.npz")
+    rhs = GeodesicRhs(KerrSpacetime(1.0, float(g["spin"])))
+    s, h = dev(g["state"]), dev(g["h"])
+    new, _ = integrators.dormand_prince_step(rhs, s, h, precision="mixed")
+    inc = np.abs(g["dp5_new"] - g["state"]) + 1e-12
+    rel = np.abs(new.cpu().numpy() - g["dp5_new"]) / inc
+    assert np.max(rel) < 2e-5
+
+
+def test_rk4_benchmark(cuda):
+    from blackhorizon_b200 import integrators
+    from blackhorizon_b200.geodesics import GeodesicRhs
+    from blackhorizon_b200.kerr import KerrSpacetime
+
+    g = golden("rk4.npz")
+    rhs = GeodesicRhs(KerrSpacetime(1.0, 0.9))
+    out = integrators.rk4_step(rhs, dev(g["state0"]), float(g["h"]), n_steps=int(g["n_steps"]))
+    close(out, g["final"], rtol=1e-11)
+    one = integrators.rk4_step(rhs, dev(g["state0"]), float(g["h"]))
+    two = integrators.rk4_step(rhs, one, float(g["h"]))
+    both = integrators.rk4_step(rhs, dev(g["state0"]), float(g["h"]), n_steps=2)
+    close(two, both.cpu().numpy(), rtol=1e-14)
+
+
+def test_empty_batches(cuda):
+    from blackhorizon_b200 import geodesics, integrators
+    from blackhorizon_b200.geodesics import GeodesicRhs
+    from blackhorizon_b200.kerr import KerrSpacetime
+
+    st = KerrSpacetime(1.0, 0.9)
+    empty = torch.empty((0, 8), dtype=torch.float64, device="cuda")
+    assert geodesics.geodesic_rhs(st, empty).shape == (0, 8)
+    new, err = integrators.dormand_prince_step(GeodesicRhs(st), empty,
+                                               torch.empty(0, dtype=torch.float64, device="cuda"))
+    assert new.shape == (0, 8) and err.shape == (0, 8)
+
+
+def test_nan_error_is_infinite_ratio(cuda):
+    """Reference tests/test_integrators.py:72-76."""
+    from blackhorizon_b200 import integrators
+
+    s = torch.zeros((1, 8), dtype=torch.float64, device="cuda")
+    s[0, 1] = 1.0
+    bad = s.clone()
+    bad[0, 1] = float("nan")
+    r = integrators.error_ratio(s, s, bad, 1e-9, 1e-12)
+    assert torch.isinf(r[0])

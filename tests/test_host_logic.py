@@ -1,0 +1,116 @@
+"""Host-side logic of the b200 backend that needs no GPU: backend dispatch,
+the Kerr radii and argument checks, the camera basis, the RHS recognition of
+the integrators and the synthetic workloads."""
+
+import functools
+import math
+
+import numpy as np
+import pytest
+
+from conftest import golden
+
+
+def test_get_xp_errors_follow_reference():
+    from blackhorizon_b200 import backend
+
+    assert backend.get_xp("cpu") is np
+    with pytest.raises(ValueError):
+        backend.get_xp("tpu")
+    if not backend.b200_available():
+        with pytest.raises(RuntimeError):
+            backend.get_xp("b200")
+
+
+def test_kerr_radii_match_reference_tests():
+    """The analytic values pinned by the reference's tests/test_kerr.py:21-49."""
+    from blackhorizon_b200.kerr import KerrSpacetime
+
+    assert KerrSpacetime(spin=0.0).outer_horizon_radius == pytest.approx(2.0)
+    assert KerrSpacetime(spin=1.0).outer_horizon_radius == pytest.approx(1.0)
+    st = KerrSpacetime(spin=0.6)
+    assert st.outer_horizon_radius == pytest.approx(1.8)
+    assert st.inner_horizon_radius == pytest.approx(0.2)
+    assert KerrSpacetime(spin=0.0).isco_radius() == pytest.approx(6.0)
+    assert KerrSpacetime(spin=1.0).isco_radius(True) == pytest.approx(1.0)
+    assert KerrSpacetime(spin=1.0).isco_radius(False) == pytest.approx(9.0)
+    assert KerrSpacetime(spin=0.0).photon_orbit_radius() == pytest.approx(3.0)
+    assert KerrSpacetime(spin=1.0).photon_orbit_radius(True) == pytest.approx(1.0)
+    assert KerrSpacetime(spin=1.0).photon_orbit_radius(False) == pytest.approx(4.0)
+    st = KerrSpacetime(spin=0.9)
+    assert st.ergosphere_radius(0.0) == pytest.approx(st.outer_horizon_radius)
+    assert st.ergosphere_radius(math.pi / 2.0) == pytest.approx(2.0)
+    with pytest.raises(ValueError):
+        KerrSpacetime(spin=1.01)
+    with pytest.raises(ValueError):
+        KerrSpacetime(mass=-1.0)
+    assert KerrSpacetime(1.0, 0.9).capture_radius(0.01) == pytest.approx(
+        (1.0 + math.sqrt(1 - 0.81)) * 1.01)
+
+
+def test_camera_basis_matches_reference():
+    from blackhorizon_b200.camera import PinholeCamera
+
+    g = golden("camera.npz")
+    for k in ("c1", "c3", "pole", "free"):
+        w, h = (int(v) for v in g[f"{k}_wh"])
+        cam = PinholeCamera(position=tuple(g[f"{k}_position"]), target=tuple(g[f"{k}_target"]),
+                            up_hint=tuple(g[f"{k}_up_hint"]), fov_degrees=float(g[f"{k}_fov"]),
+                            width=w, height=h)
+        np.testing.assert_array_equal(np.stack([cam.forward, cam.right, cam.up]), g[f"{k}_basis"])
+        np.testing.assert_array_equal(cam.ray_directions(), g[f"{k}_dirs"])
+
+
+def test_camera_argument_errors():
+    from blackhorizon_b200.camera import PinholeCamera
+
+    with pytest.raises(ValueError):
+        PinholeCamera(position=(1, 0, 0), width=0)
+    with pytest.raises(ValueError):
+        PinholeCamera(position=(1, 0, 0), fov_degrees=180.0)
+    with pytest.raises(ValueError):
+        PinholeCamera.from_orbit(0.0, 30.0)
+    with pytest.raises(ValueError):
+        PinholeCamera(position=(0, 0, 0))
+
+
+def test_integrators_reject_unknown_rhs():
+    from blackhorizon_b200 import geodesics
+    from blackhorizon_b200.kerr import KerrSpacetime
+
+    st = KerrSpacetime(1.0, 0.5)
+    assert geodesics.spacetime_of_rhs(geodesics.GeodesicRhs(st)) is st
+    assert geodesics.spacetime_of_rhs(functools.partial(geodesics.geodesic_rhs, st)) is st
+    with pytest.raises(TypeError):
+        geodesics.spacetime_of_rhs(lambda b: b)
+
+
+def test_raw_workload_prefix_and_radius():
+    from blackhorizon_b200.workloads import RAW_RADIUS, raw_throughput_inputs
+
+    pos, d, spin = raw_throughput_inputs(4096)
+    p2, d2, s2 = raw_throughput_inputs(1000)
+    np.testing.assert_array_equal(pos[:1000], p2)
+    np.testing.assert_array_equal(d[:1000], d2)
+    np.testing.assert_array_equal(spin[:1000], s2)
+    p3, d3, s3 = raw_throughput_inputs(100, offset=500)
+    np.testing.assert_array_equal(pos[500:600], p3)
+    assert np.all(np.abs(spin) <= 0.95)
+    # Kerr-Schild radius of every point is exactly RAW_RADIUS (up to rounding).
+    a2 = spin ** 2
+    q = (pos ** 2).sum(-1) - a2
+    r2 = 0.5 * (q + np.sqrt(q * q + 4 * a2 * pos[:, 2] ** 2))
+    np.testing.assert_allclose(np.sqrt(r2), RAW_RADIUS, rtol=1e-13)
+    np.testing.assert_allclose(np.linalg.norm(d, axis=-1), 1.0, rtol=1e-14)
+
+
+def test_uneven_cameras_are_deterministic():
+    from blackhorizon_b200.workloads import uneven_cameras
+
+    a = uneven_cameras()
+    b = uneven_cameras()
+    assert a == b and len(a) == 64
+    for c in a:
+        assert 64 <= c.width <= 1024 and 48 <= c.height <= 768
+        assert abs(c.spin) <= 0.998 and 0.0 <= c.inclination <= 90.0
+        assert 20.0 <= c.distance <= 200.0

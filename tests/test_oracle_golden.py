@@ -1,0 +1,161 @@
+"""Pins the CPU oracle (oracle/bh_oracle.c) to golden vectors produced by the
+reference itself (tests/golden/make_golden.py).
+
+The oracle restates the reference operation by operation without FMA
+contraction, so point-wise results must match to the last bit.  The only
+known ulp-level difference is pow() in step_factor (NumPy may use a SIMD
+pow), which can perturb step sizes after a few hundred steps; traces are
+therefore pinned exactly on status and step counts and to a tolerance on
+states.
+"""
+
+import numpy as np
+import pytest
+
+from conftest import golden
+
+
+def test_geometry_bit_exact(oracle):
+    g = golden("geometry.npz")
+    for tag in ("a09", "a095", "a0", "am0998"):
+        r, h, l, gh, gl = oracle.geometry(1.0, float(g[f"{tag}_spin"]), g[f"{tag}_xyz"])
+        np.testing.assert_array_equal(r, g[f"{tag}_r"])
+        np.testing.assert_array_equal(h, g[f"{tag}_h"])
+        np.testing.assert_array_equal(l, g[f"{tag}_l"])
+        np.testing.assert_array_equal(gh, g[f"{tag}_grad_h"])
+        np.testing.assert_array_equal(gl, g[f"{tag}_grad_l"])
+
+
+def test_rhs_dp5_rk4_bit_exact(oracle):
+    g = golden("steps.npz")
+    a = float(g["spin"])
+    s0 = g["state"]
+    np.testing.assert_array_equal(oracle.rhs(1.0, a, s0), g["rhs"])
+    y_new, err, ratio = oracle.dp5_step(1.0, a, s0, g["h"], float(g["rtol"]), float(g["atol"]))
+    np.testing.assert_array_equal(y_new, g["dp5_new"])
+    np.testing.assert_array_equal(err, g["dp5_err"])
+    np.testing.assert_array_equal(ratio, g["ratio"])
+    # pow(): libm vs NumPy may differ by an ulp.
+    np.testing.assert_allclose(oracle.step_factor(g["ratio"]), g["factor"], rtol=4e-16, atol=0)
+    np.testing.assert_array_equal(oracle.hamiltonian(1.0, a, s0), g["hamiltonian"])
+    np.testing.assert_array_equal(oracle.coordinate_velocity(1.0, a, s0), g["velocity"])
+
+
+def test_rk4_benchmark_states(oracle):
+    g = golden("rk4.npz")
+    out = oracle.rk4(1.0, 0.9, g["state0"], float(g["h"]), int(g["n_steps"]), nthreads=1)
+    np.testing.assert_array_equal(out, g["final"])
+
+
+@pytest.mark.parametrize("tor", ["past", "future"])
+@pytest.mark.parametrize("norm", [True, False])
+def test_null_momentum_bit_exact(oracle, tor, norm):
+    g = golden("null_momentum.npz")
+    p = oracle.null_momentum(1.0, float(g["spin"]), g["pos"], g["dir"], tor == "past", norm)
+    np.testing.assert_array_equal(p, g[f"{tor}_{int(norm)}"])
+
+
+def test_camera_directions_bit_exact(oracle):
+    g = golden("camera.npz")
+    for k in ("c1", "c3", "pole", "free"):
+        fwd, right, up = g[f"{k}_basis"]
+        w, h = (int(v) for v in g[f"{k}_wh"])
+        d = oracle.pinhole_directions(fwd, right, up, float(g[f"{k}_fov"]), w, h)
+        np.testing.assert_array_equal(d, g[f"{k}_dirs"])
+
+
+def test_trace_small_frame(oracle):
+    g = golden("trace_c1_40x30.npz")
+    states, status, steps, it = oracle.trace(
+        1.0, 0.9, g["state0"], 100.0, max_steps=5000, rtol=1e-8, atol=1e-10,
+        capture_margin=0.01)
+    np.testing.assert_array_equal(status, g["status"])
+    np.testing.assert_array_equal(steps, g["steps"])
+    assert it == int(g["iterations"])
+    ref = g["states"]
+    scale = np.maximum(np.abs(ref), 1.0)
+    # A one-ulp change of a step size moves the end point by the local
+    # truncation error, ~rtol.
+    assert np.max(np.abs(states - ref) / scale) < 1e-7
+
+
+def test_trace_full_small_config_status(oracle):
+    """160x120, a=0.9, 60 deg, escape 100, rtol 1e-8: every ray's status and
+    accepted steps, and the batch iteration count."""
+    from blackhorizon_b200.workloads import SHADOW_SMALL as C
+    cam = golden("camera.npz")  # noqa: F841  (camera geometry pinned separately)
+    g = golden("trace_c1_160x120.npz")
+    s0 = _camera_state0(oracle, C)
+    states, status, steps, it = oracle.trace(
+        1.0, C.spin, s0, C.escape_radius, max_steps=C.max_steps, rtol=C.rtol,
+        atol=C.atol, capture_margin=C.capture_margin)
+    np.testing.assert_array_equal(status, g["status"])
+    np.testing.assert_array_equal(steps, g["steps"])
+    assert it == int(g["iterations"])
+    sub = g["sub_index"]
+    ref = g["sub_states"]
+    assert np.max(np.abs(states[sub] - ref) / np.maximum(np.abs(ref), 1.0)) < 1e-7
+
+
+def _camera_state0(oracle, C):
+    """Initial states of a ShadowConfig frame via the reference's host camera
+    basis and the oracle's restatement of the pixel directions and null
+    momenta."""
+    from blackhorizon_b200.camera import PinholeCamera
+
+    cam = PinholeCamera.from_orbit(C.distance, C.inclination, fov_degrees=C.fov,
+                                   width=C.width, height=C.height)
+    d = oracle.pinhole_directions(cam.forward, cam.right, cam.up, C.fov, C.width, C.height)
+    pos = cam.ray_origins()
+    p = oracle.null_momentum(1.0, C.spin, pos, d, True, True)
+    s0 = np.zeros((pos.shape[0], 8))
+    s0[:, 1:4] = pos
+    s0[:, 4:8] = p
+    return s0
+
+
+def test_trace_full_hd_status_subsample(oracle):
+    """Every 97th pixel of the 1920x1080 frame (a=0.9, 80 deg, fov 25,
+    rtol 1e-9) against the reference's full-frame statuses."""
+    from blackhorizon_b200.workloads import SHADOW_FULL_HD as C
+
+    g = golden("trace_c3_status.npz")
+    s0 = _camera_state0(oracle, C)
+    idx = np.arange(0, s0.shape[0], 97)
+    _, status, steps, _ = oracle.trace(
+        1.0, C.spin, s0[idx], C.escape_radius, max_steps=C.max_steps, rtol=C.rtol,
+        atol=C.atol, capture_margin=C.capture_margin)
+    np.testing.assert_array_equal(status, g["status"][idx])
+    np.testing.assert_array_equal(steps, g["steps"][idx])
+
+
+def test_equatorial_fans(oracle):
+    g = golden("fans.npz")
+    for tag in ("a0_pos", "a09_pro", "a09_ret"):
+        states, status, steps, _ = oracle.trace(
+            1.0, float(g[f"{tag}_spin"]), g[f"{tag}_state0"], 1200.0, max_steps=60000,
+            rtol=1e-10, atol=1e-13, max_step=5.0)
+        np.testing.assert_array_equal(status, g[f"{tag}_status"])
+        np.testing.assert_array_equal(steps, g[f"{tag}_steps"])
+
+
+def test_raw_throughput_propagation(oracle):
+    """512 rays of the raw-throughput workload, 2000 attempted steps, per-ray
+    spin, no termination."""
+    from blackhorizon_b200.workloads import raw_throughput_inputs
+
+    g = golden("raw_throughput.npz")
+    pos, d, spin = raw_throughput_inputs(512)
+    np.testing.assert_array_equal(pos, g["pos"])
+    np.testing.assert_array_equal(spin, g["spin"])
+    # Initial states through the oracle with per-ray spin.
+    p = np.stack([oracle.null_momentum(1.0, float(spin[i]), pos[i:i + 1], d[i:i + 1])[0]
+                  for i in range(512)])
+    np.testing.assert_array_equal(p, g["state0"][:, 4:8])
+    states, h, acc = oracle.propagate(1.0, spin, g["state0"], int(g["n_steps"]),
+                                      float(g["rtol"]), float(g["atol"]))
+    ref = g["final"]
+    rel = np.abs(states - ref) / np.maximum(np.abs(ref), 1.0)
+    # pow() ulps move a handful of accept decisions over 2000 steps.
+    assert np.median(np.max(rel, axis=1)) < 1e-12
+    assert np.mean(acc == g["accepted"]) > 0.95
