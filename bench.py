@@ -197,6 +197,7 @@ def run_ours(args):
     state0, spins, pos_h, dir_h, spin_h = make_inputs(n, rank, device)
     work = torch.empty_like(state0)
     h = torch.empty(n, dtype=torch.float64, device=device)
+    lam = torch.empty(n, dtype=torch.float64, device=device)
     acc = torch.empty(n, dtype=torch.int64, device=device)
     ws = torch.empty(lib.bh_trace_workspace_bytes(), dtype=torch.uint8, device=device)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
@@ -210,12 +211,13 @@ def run_ours(args):
     def one_step(precision, kev=None):
         work.copy_(state0)
         h.fill_(0.1)
+        lam.zero_()
         cfg = make_config(1, 1e-8, 1e-10, 0.1, 2.0, 0.0, precision, "aos", 600.0,
                           args.variant)
         if kev is not None:
             kev[0].record()
         rc = lib.bh_propagate(cfg, 1.0, 0.0, spins.data_ptr(), work.data_ptr(), h.data_ptr(),
-                              acc.data_ptr(), n, S, ws.data_ptr(), stream)
+                              lam.data_ptr(), acc.data_ptr(), n, S, ws.data_ptr(), stream)
         if kev is not None:
             kev[1].record()
         _lib.check(rc, "bench propagate")
@@ -256,16 +258,17 @@ def run_ours(args):
     prec = args.precision
     ms_step, kernel_ms, clocks = timed(prec, args.steps, max(args.warmup, 3), True)
     final = work.clone()
+    final_lam = lam.clone()
     value = world * n * S / (ms_step * 1e-3)
 
     fp64 = None
+    final64 = lam64 = None
     if not args.no_fp64 and prec != "fp64":
         ms64, k64, _ = timed("fp64", max(1, args.steps), max(args.warmup, 3))
         final64 = work.clone()
+        lam64 = lam.clone()
         fp64 = {"value": world * n * S / (ms64 * 1e-3), "ms_per_step": ms64,
                 "kernel_ms": k64}
-    else:
-        final64 = None
 
     # ---- end to end through the public API with host (pinned) buffers
     host_state = state0.cpu().pin_memory()
@@ -276,7 +279,7 @@ def run_ours(args):
     def e2e_step():
         s_dev = host_state.to(device, non_blocking=True)
         sp_dev = host_spin.to(device, non_blocking=True)
-        out, _, _, _ = propagate(st_mass, s_dev, S, rtol=1e-8, atol=1e-10,
+        out, _, _, _, _ = propagate(st_mass, s_dev, S, rtol=1e-8, atol=1e-10,
                                  precision=prec, spins=sp_dev, in_place=True,
                                  timeout_s=600.0, variant=args.variant, workspace=ws)
         return out.to("cpu")
@@ -344,28 +347,49 @@ def run_ours(args):
         if fp64 is not None:
             out["fp64"] = fp64
             out["speedup_vs_fp64"] = fp64["ms_per_step"] / ms_step
-            d = final.cpu().numpy()
-            d64 = final64.cpu().numpy()
-            rel = np.max(np.abs(d - d64) / np.maximum(np.abs(d64), 1.0), axis=1)
-            out["mixed_vs_fp64_endpoint_err"] = {
-                "median": float(np.median(rel)), "p99": float(np.quantile(rel, 0.99))}
         if not args.no_cpu:
-            out["cpu_baseline"], errs = cpu_baseline(state0, spin_h, S, args.cpu_seconds,
-                                                     final, final64)
-            out["endpoint_err_vs_oracle"] = errs
+            out["cpu_baseline"] = cpu_baseline(state0, spin_h, S, args.cpu_seconds)
+            out["endpoint_err"] = endpoint_errors(
+                state0, spin_h, {prec: (final, final_lam), "fp64": (final64, lam64)})
     if world > 1:
         dist.barrier(device_ids=[local])
         dist.destroy_process_group()
     return out
 
 
-def cpu_baseline(state0, spin_h, S, seconds, final, final64):
-    """The CPU oracle (oracle/bh_oracle.c, every host core) on the first rays
-    of the same workload, sized to about `seconds` of CPU time; also the
-    endpoint error of the GPU results on those rays."""
+def host_threads() -> int:
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+
+
+def endpoint_errors(state0, spin_h, runs, m=4096):
+    """Endpoint error of the first m rays at equal affine parameter: the
+    oracle integrates each ray to the lambda the kernel reached (rtol 1e-12,
+    atol 1e-14, last step cut to land on it); error = max over components of
+    |y - y_ref| / max(|y_ref|, 1)."""
     from oracle import oracle
 
-    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    s0 = state0[:m].cpu().numpy()
+    out = {"rays": m, "reference": "oracle DP5(4) to the kernel's lambda, rtol 1e-12"}
+    for name, (fin, lam) in runs.items():
+        if fin is None:
+            continue
+        got = fin[:m].cpu().numpy()
+        truth, _ = oracle.propagate_to(1.0, spin_h[:m], s0, lam[:m].cpu().numpy(),
+                                       rtol=1e-12, atol=1e-14, nthreads=host_threads())
+        ok = np.all(np.isfinite(truth), axis=1) & np.all(np.isfinite(got), axis=1)
+        rel = np.max(np.abs(got[ok] - truth[ok]) / np.maximum(np.abs(truth[ok]), 1.0), axis=1)
+        out[name] = {"median": float(np.median(rel)), "p90": float(np.quantile(rel, 0.9)),
+                     "p99": float(np.quantile(rel, 0.99)), "max": float(np.max(rel)),
+                     "excluded_nonfinite": int((~ok).sum())}
+    return out
+
+
+def cpu_baseline(state0, spin_h, S, seconds):
+    """The CPU oracle (oracle/bh_oracle.c, every host core) on the first rays
+    of the same workload, sized to about `seconds` of CPU time."""
+    from oracle import oracle
+
+    threads = host_threads()
     s0 = state0.cpu().numpy()
     probe = max(threads, 8)
     t = time.perf_counter()
@@ -374,21 +398,11 @@ def cpu_baseline(state0, spin_h, S, seconds, final, final64):
     m = int(min(s0.shape[0], max(probe, rate * seconds / S)))
     m = max(threads, (m // threads) * threads)
     t = time.perf_counter()
-    ref, _, _ = oracle.propagate(1.0, spin_h[:m], s0[:m], S, 1e-8, 1e-10, nthreads=threads)
+    oracle.propagate(1.0, spin_h[:m], s0[:m], S, 1e-8, 1e-10, nthreads=threads)
     dt = time.perf_counter() - t
-    base = {"value": m * S / dt, "unit": "ray-steps/s", "cores": threads, "kind": "port",
+    return {"value": m * S / dt, "unit": "ray-steps/s", "cores": threads, "kind": "port",
             "sample": f"first {m} rays x {S} attempted DP5(4) steps of the same workload, "
-                      f"oracle/bh_oracle.c on {threads} threads, {dt:.1f} s"}
-    errs = {}
-    for name, arr in (("mixed", final), ("fp64", final64)):
-        if arr is None:
-            continue
-        got = arr[:m].cpu().numpy()
-        ok = np.all(np.isfinite(ref), axis=1)
-        rel = np.max(np.abs(got[ok] - ref[ok]) / np.maximum(np.abs(ref[ok]), 1.0), axis=1)
-        errs[name] = {"rays": int(ok.sum()), "median": float(np.median(rel)),
-                      "p90": float(np.quantile(rel, 0.9)), "max": float(np.max(rel))}
-    return base, errs
+                      f"oracle/bh_oracle.c (float64) on {threads} threads, {dt:.1f} s"}
 
 
 def run_reference(args):
@@ -401,7 +415,7 @@ def run_reference(args):
 
     from blackhorizon_b200.workloads import raw_throughput_inputs
 
-    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    threads = host_threads()
     S = args.dp5_steps
     # Initial states of the first rays, through the oracle's null momentum.
     probe_n = max(threads, 8)

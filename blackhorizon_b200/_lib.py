@@ -71,7 +71,7 @@ _SIGNATURES = {
     "bh_trace_variant_count": (ctypes.c_int, [_I32]),
     "bh_trace_variant": (ctypes.c_int, [_I32, _I32, ctypes.POINTER(_I32),
                                          ctypes.POINTER(_I32), ctypes.POINTER(_I32),
-                                         ctypes.POINTER(_I32)]),
+                                         ctypes.POINTER(_I32), ctypes.POINTER(_I32)]),
     "bh_trace_workspace_bytes": (_SZ, []),
     "bh_trace": (ctypes.c_int, [ctypes.POINTER(TraceConfig), ctypes.POINTER(Scene),
                                 _P, _P, _P, _P, _I64, _P, _P]),
@@ -82,7 +82,7 @@ _SIGNATURES = {
                                         _P, _P, _P, _SZ, _P]),
     "bh_trace_stats_read": (ctypes.c_int, [_P, ctypes.POINTER(TraceStats), _P]),
     "bh_propagate": (ctypes.c_int, [ctypes.POINTER(TraceConfig), _D, _D, _P, _P, _P,
-                                    _P, _I64, _I64, _P, _P]),
+                                    _P, _P, _I64, _I64, _P, _P]),
     "bh_fma_peak_launch": (ctypes.c_int, [_I32, _I64, _P, ctypes.POINTER(_I64), _P]),
 }
 

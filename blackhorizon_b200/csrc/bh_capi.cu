@@ -97,12 +97,15 @@ __global__ void rhs_kernel(double m, double a, const double *state,
     const long long i = tid();
     if (i >= n) return;
     const RayState y = read_state(state, i);
-    const Deriv<double> d = rhs<double>(m, a, y.x, y.y, y.z, y.pt, y.px, y.py, y.pz);
+    const KerrV<double> K = make_kerr<double>(m, a);
+    WStateV<double> yw;
+    put_work<double>(yw, 0, y);
+    const StageV<double> d = first_stage<double>(K, yw);
     double *o = deriv + 8 * i;
     o[0] = -y.pt + d.thl;
-    o[1] = y.px + d.qx;
-    o[2] = y.py + d.qy;
-    o[3] = y.pz + d.qz;
+    o[1] = y.px + d.kx;
+    o[2] = y.py + d.ky;
+    o[3] = y.pz + d.kz;
     o[4] = 0.0;
     o[5] = d.px; o[6] = d.py; o[7] = d.pz;
 }
@@ -162,80 +165,104 @@ __global__ void camera_states_kernel(CameraDev c, double *state, long long n) {
     write_state(state, i, y);
 }
 
-template <typename W>
+template <typename V>
 __global__ void dp5_kernel(double m, double a, const double *state,
                            const double *h, double *out, double *err,
                            long long n) {
+    using T = VT<V>;
     const long long i = tid();
     if (i >= n) return;
     const RayState y = read_state(state, i);
-    const Stage<W> k1 = first_stage<W>(W(m), W(a), y);
-    Attempt<W> at;
-    dp5_attempt<W>(W(m), W(a), y, h[i], k1, at);
-    write_state(out, i, at.y_new);
+    const KerrV<V> K = make_kerr<V>(T::set(m), T::set(a));
+    WStateV<V> yw;
+    put_work<V>(yw, 0, y);
+    const StageV<V> k1 = first_stage<V>(K, yw);
+    const double hh = h[i];
+    AttemptV<V> at;
+    dp5_attempt<V>(K, yw, T::set(hh), k1, at);
+    RayState yn = y;
+    commit<V>(yn, yw, at, 0, hh);
+    write_state(out, i, yn);
     double *e = err + 8 * i;
-#pragma unroll
-    for (int j = 0; j < 8; ++j) e[j] = at.err[j];
+    e[0] = hh * double(at.err[0]);
+    e[1] = hh * double(at.err[1]);
+    e[2] = hh * double(at.err[2]);
+    e[3] = hh * double(at.err[3]);
+    e[4] = 0.0;
+    e[5] = hh * double(at.err[4]);
+    e[6] = hh * double(at.err[5]);
+    e[7] = hh * double(at.err[6]);
 }
 
+// error_ratio (integrators.py:110-117) of arbitrary (n,8) arrays, float64,
+// NumPy's pairwise summation order.
 __global__ void error_ratio_kernel(const double *s, const double *sn,
                                    const double *err, double rtol, double atol,
                                    double *out, long long n) {
     const long long i = tid();
     if (i >= n) return;
-    const RayState y = read_state(s, i), yn = read_state(sn, i);
-    double e[8];
+    double q[8];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) e[j] = err[8 * i + j];
-    out[i] = error_ratio<double>(y, yn, e, rtol, atol);
+    for (int j = 0; j < 8; ++j) {
+        const double sc = atol + rtol * np_max(fabs(s[8 * i + j]), fabs(sn[8 * i + j]));
+        const double e = err[8 * i + j] / sc;
+        q[j] = e * e;
+    }
+    const double sum = ((q[0] + q[1]) + (q[2] + q[3])) + ((q[4] + q[5]) + (q[6] + q[7]));
+    const double r = ::sqrt(sum * 0.125);
+    out[i] = isfinite(r) ? r : __longlong_as_double(0x7ff0000000000000LL);
 }
 
 __global__ void step_factor_kernel(const double *ratio, double *out, long long n) {
     const long long i = tid();
     if (i >= n) return;
-    out[i] = step_factor<double>(ratio[i]);
+    out[i] = step_factor<true>(ratio[i]);
 }
 
-// rk4_step (integrators.py:57-73) n_steps times with the state in registers.
-template <typename W>
+// rk4_step (integrators.py:57-73) n_steps times with the state in registers;
+// stage arithmetic in the lane type V, the state update in double.
+template <typename V>
 __global__ void rk4_kernel(double m, double a, const double *state,
                            const double *hs, double *out, long long n,
                            long long n_steps) {
+    using T = VT<V>;
     const long long i = tid();
     if (i >= n) return;
     RayState y = read_state(state, i);
     const double h = hs[i];
-    const W mw = W(m), aw = W(a), hw = W(h);
-    const W half = W(0.5) * hw;
+    const KerrV<V> K = make_kerr<V>(T::set(m), T::set(a));
+    const V hw = T::set(h), half = T::set(0.5 * h);
+    const V zero = T::set(0.0);
     for (long long s = 0; s < n_steps; ++s) {
-        // k_x = P + q in split form; the stage inputs use W arithmetic.
-        const W x = W(y.x), yy = W(y.y), z = W(y.z), pt = W(y.pt);
-        const W px = W(y.px), py = W(y.py), pz = W(y.pz);
-        const Deriv<W> d1 = rhs<W>(mw, aw, x, yy, z, pt, px, py, pz);
-        const W k1x = px + d1.qx, k1y = py + d1.qy, k1z = pz + d1.qz;
-        const Deriv<W> d2 = rhs<W>(mw, aw, x + half * k1x, yy + half * k1y,
-                                   z + half * k1z, pt, px + half * d1.px,
-                                   py + half * d1.py, pz + half * d1.pz);
-        const W p2x = px + half * d1.px, p2y = py + half * d1.py, p2z = pz + half * d1.pz;
-        const W k2x = p2x + d2.qx, k2y = p2y + d2.qy, k2z = p2z + d2.qz;
-        const Deriv<W> d3 = rhs<W>(mw, aw, x + half * k2x, yy + half * k2y,
-                                   z + half * k2z, pt, px + half * d2.px,
-                                   py + half * d2.py, pz + half * d2.pz);
-        const W p3x = px + half * d2.px, p3y = py + half * d2.py, p3z = pz + half * d2.pz;
-        const W k3x = p3x + d3.qx, k3y = p3y + d3.qy, k3z = p3z + d3.qz;
-        const Deriv<W> d4 = rhs<W>(mw, aw, x + hw * k3x, yy + hw * k3y,
-                                   z + hw * k3z, pt, px + hw * d3.px,
-                                   py + hw * d3.py, pz + hw * d3.pz);
-        const W p4x = px + hw * d3.px, p4y = py + hw * d3.py, p4z = pz + hw * d3.pz;
-        const W k4x = p4x + d4.qx, k4y = p4y + d4.qy, k4z = p4z + d4.qz;
+        WStateV<V> w;
+        put_work<V>(w, 0, y);
+        // Full derivatives: dx = P + kappa - dP, dt = -p_t + thl, dp = pdot.
+        const StageV<V> d1 = rhs_v<V>(K, w.x, w.y, w.z, w.npt, w.px, w.py, w.pz, zero, zero, zero);
+        const V k1x = w.px + d1.kx, k1y = w.py + d1.ky, k1z = w.pz + d1.kz;
+        const V e2x = half * d1.px, e2y = half * d1.py, e2z = half * d1.pz;
+        const StageV<V> d2 = rhs_v<V>(K, T::fma(half, k1x, w.x), T::fma(half, k1y, w.y),
+                                      T::fma(half, k1z, w.z), w.npt, w.px + e2x, w.py + e2y,
+                                      w.pz + e2z, e2x, e2y, e2z);
+        const V k2x = w.px + d2.kx, k2y = w.py + d2.ky, k2z = w.pz + d2.kz;
+        const V e3x = half * d2.px, e3y = half * d2.py, e3z = half * d2.pz;
+        const StageV<V> d3 = rhs_v<V>(K, T::fma(half, k2x, w.x), T::fma(half, k2y, w.y),
+                                      T::fma(half, k2z, w.z), w.npt, w.px + e3x, w.py + e3y,
+                                      w.pz + e3z, e3x, e3y, e3z);
+        const V k3x = w.px + d3.kx, k3y = w.py + d3.ky, k3z = w.pz + d3.kz;
+        const V e4x = hw * d3.px, e4y = hw * d3.py, e4z = hw * d3.pz;
+        const StageV<V> d4 = rhs_v<V>(K, T::fma(hw, k3x, w.x), T::fma(hw, k3y, w.y),
+                                      T::fma(hw, k3z, w.z), w.npt, w.px + e4x, w.py + e4y,
+                                      w.pz + e4z, e4x, e4y, e4z);
+        const V k4x = w.px + d4.kx, k4y = w.py + d4.ky, k4z = w.pz + d4.kz;
+        const V two = T::set(2.0);
         const double h6 = h / 6.0;
-        y.t += h6 * double(W(-6) * pt + d1.thl + W(2) * d2.thl + W(2) * d3.thl + d4.thl);
-        y.x += h6 * double(k1x + W(2) * k2x + W(2) * k3x + k4x);
-        y.y += h6 * double(k1y + W(2) * k2y + W(2) * k3y + k4y);
-        y.z += h6 * double(k1z + W(2) * k2z + W(2) * k3z + k4z);
-        y.px += h6 * double(d1.px + W(2) * d2.px + W(2) * d3.px + d4.px);
-        y.py += h6 * double(d1.py + W(2) * d2.py + W(2) * d3.py + d4.py);
-        y.pz += h6 * double(d1.pz + W(2) * d2.pz + W(2) * d3.pz + d4.pz);
+        y.t += h6 * double(T::set(6.0) * w.npt + (d1.thl + two * d2.thl + two * d3.thl + d4.thl));
+        y.x += h6 * double(k1x + two * k2x + two * k3x + k4x);
+        y.y += h6 * double(k1y + two * k2y + two * k3y + k4y);
+        y.z += h6 * double(k1z + two * k2z + two * k3z + k4z);
+        y.px += h6 * double(d1.px + two * d2.px + two * d3.px + d4.px);
+        y.py += h6 * double(d1.py + two * d2.py + two * d3.py + d4.py);
+        y.pz += h6 * double(d1.pz + two * d2.pz + two * d3.pz + d4.pz);
     }
     write_state(out, i, y);
 }
@@ -455,8 +482,8 @@ int bh_rk4(double mass, double spin, const double *state, const double *h,
 int bh_trace_variant_count(int32_t precision) { return trace_variant_count(precision); }
 
 int bh_trace_variant(int32_t precision, int32_t index, int32_t *block_threads,
-                     int32_t *min_blocks, int32_t *registers,
-                     int32_t *max_blocks_per_sm) {
+                     int32_t *min_blocks, int32_t *rays_per_thread,
+                     int32_t *registers, int32_t *max_blocks_per_sm) {
     if (precision != BH_PRECISION_FP64 && precision != BH_PRECISION_MIXED)
         return invalid("unknown precision");
     if (index < 0) index = trace_default_variant(precision);
@@ -464,6 +491,7 @@ int bh_trace_variant(int32_t precision, int32_t index, int32_t *block_threads,
     const Variant v = trace_variant(precision, index);
     if (block_threads) *block_threads = v.block;
     if (min_blocks) *min_blocks = v.min_blocks;
+    if (rays_per_thread) *rays_per_thread = v.rays_per_thread;
     int regs = 0, nb = 0;
     if (kernel_attributes(false, precision, index, &regs, &nb) != 0)
         return cuda_status(cudaGetLastError(), "bh_trace_variant attributes");
@@ -609,7 +637,7 @@ int bh_trace_stats_read(const void *workspace, bh_trace_stats *out, void *stream
 
 int bh_propagate(const bh_trace_config *config, double mass, double spin,
                  const double *spin_of_ray, double *states, double *h,
-                 int64_t *accepted, int64_t n, int64_t n_steps,
+                 double *lam, int64_t *accepted, int64_t n, int64_t n_steps,
                  void *workspace, void *stream) {
     int rc = config_ok(config);
     if (rc != BH_OK) return rc;
@@ -633,6 +661,7 @@ int bh_propagate(const bh_trace_config *config, double mass, double spin,
     a.spin = spin;
     a.spin_of_ray = spin_of_ray;
     a.h_io = h;
+    a.lam_io = lam;
     a.steps = accepted;
     a.n = n;
     a.max_attempts = n_steps;

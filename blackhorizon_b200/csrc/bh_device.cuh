@@ -7,10 +7,13 @@
 // tracer.py:113-149), written for one ray per thread with the state in
 // registers.
 //
-// Precision policy: the work type W is double (BH_PRECISION_FP64) or float
-// (BH_PRECISION_MIXED).  The state y, its update, the error norm, the step
-// size and the termination radius are always double.  W carries the stage
-// arithmetic: the RHS evaluations and the stage combinations.
+// Precision policy: the lane type V is double (BH_PRECISION_FP64), float
+// (BH_PRECISION_MIXED, one ray per thread) or F2 (BH_PRECISION_MIXED, two
+// rays per thread in the two halves of packed float32x2 instructions).  The
+// state y, its update, the affine parameter, the step size with its accept
+// test and the termination radius are always double, per ray.  V carries the
+// stage arithmetic: the RHS evaluations, the stage combinations and the
+// embedded error with its norm.
 //
 // Derivative split.  With the momentum P_i of stage i, the position
 // derivative is dx/dlam = P_i - 2 H lp l and dt/dlam = -p_t + 2 H lp
@@ -35,8 +38,7 @@ namespace bh {
 constexpr double kTiny = 1e-30;
 
 // ---------------------------------------------------------------- fast math
-// Approximate float32 special functions (one MUFU instruction each, <= 2 ulp);
-// float64 uses the IEEE operations.
+// Approximate float32 special functions (one MUFU instruction each, <= 2 ulp).
 __device__ __forceinline__ float rcp_approx(float x) {
     float r;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
@@ -63,16 +65,40 @@ __device__ __forceinline__ float lg2_approx(float x) {
     return r;
 }
 
+// Reciprocal and reciprocal square root of the stage arithmetic.  float32:
+// one MUFU instruction (<= 2 ulp).  float64: the MUFU seed refined by two
+// Newton steps on the FP64 pipe (<= 2 ulp, no IEEE slow path).
+__device__ __forceinline__ double rcp_f64(double x) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    double e = fma(-x, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-x, r, 1.0);
+    return fma(r, e, r);
+}
+__device__ __forceinline__ double rsqrt_f64(double x) {
+    double r;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    // r <- r (3 - x r^2) / 2, twice.
+    double h = 0.5 * x;
+    r = r * fma(-h * r, r, 1.5);
+    r = r * fma(-h * r, r, 1.5);
+    return r;
+}
+
 template <typename W> struct Math;
 template <> struct Math<double> {
-    static __device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
-    static __device__ __forceinline__ double sqrt_(double x) { return ::sqrt(x); }
+    static __device__ __forceinline__ double rcp(double x) { return rcp_f64(x); }
+    static __device__ __forceinline__ double rsqrt(double x) { return rsqrt_f64(x); }
     static __device__ __forceinline__ double tiny() { return kTiny; }
+    static __device__ __forceinline__ double tiny2() { return kTiny * kTiny; }
 };
 template <> struct Math<float> {
     static __device__ __forceinline__ float rcp(float x) { return rcp_approx(x); }
-    static __device__ __forceinline__ float sqrt_(float x) { return sqrt_approx(x); }
+    static __device__ __forceinline__ float rsqrt(float x) { return rsqrt_approx(x); }
     static __device__ __forceinline__ float tiny() { return 1e-30f; }
+    // Smallest clamp of a squared quantity that stays a normal float.
+    static __device__ __forceinline__ float tiny2() { return 1e-37f; }
 };
 
 // numpy.maximum propagates NaN (fmax would drop it).
@@ -146,72 +172,173 @@ __device__ __forceinline__ double ks_radius2(double a, double x, double y,
     return np_max(r2, kTiny);
 }
 
-// ------------------------------------------------------------ compact RHS
-// Output of one RHS evaluation in the split form described at the top.
-template <typename W>
-struct Deriv {
-    W thl;           // 2 H lp: dt/dlam = -p_t + thl
-    W qx, qy, qz;    // -thl * l: dx/dlam = P + q
-    W px, py, pz;    // dp/dlam
+// ------------------------------------------------------------- lane types
+// F2: two rays side by side, one per half of a float2; arithmetic through the
+// packed sm_100 FFMA2 / FADD2 / FMUL2 instructions (two FP32 operations per
+// issue), special functions one MUFU per half.
+struct F2 {
+    float2 v;
+};
+__device__ __forceinline__ F2 operator+(F2 a, F2 b) { return {__fadd2_rn(a.v, b.v)}; }
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) { return {__fmul2_rn(a.v, b.v)}; }
+__device__ __forceinline__ F2 operator-(F2 a, F2 b) {
+    return {__ffma2_rn(b.v, make_float2(-1.0f, -1.0f), a.v)};
+}
+__device__ __forceinline__ F2 operator-(F2 a) {
+    return {__fmul2_rn(a.v, make_float2(-1.0f, -1.0f))};
+}
+
+// Traits of a lane type: N rays, scalar type S, broadcast, lane access and
+// the handful of operations the stage arithmetic needs.
+template <class V> struct VT;
+template <> struct VT<double> {
+    static constexpr int N = 1;
+    using S = double;
+    static __device__ __forceinline__ double set(double a) { return a; }
+    static __device__ __forceinline__ double get(double v, int) { return v; }
+    static __device__ __forceinline__ void put(double &v, int, double a) { v = a; }
+    static __device__ __forceinline__ double fma(double a, double b, double c) { return ::fma(a, b, c); }
+    static __device__ __forceinline__ double max(double a, double b) { return ::fmax(a, b); }
+    static __device__ __forceinline__ double abs(double a) { return ::fabs(a); }
+    static __device__ __forceinline__ double rcp(double a) { return rcp_f64(a); }
+    static __device__ __forceinline__ double rsqrt(double a) { return rsqrt_f64(a); }
+    static __device__ __forceinline__ double tiny() { return kTiny; }
+    static __device__ __forceinline__ double tiny2() { return kTiny * kTiny; }
+};
+template <> struct VT<float> {
+    static constexpr int N = 1;
+    using S = float;
+    static __device__ __forceinline__ float set(double a) { return float(a); }
+    static __device__ __forceinline__ float get(float v, int) { return v; }
+    static __device__ __forceinline__ void put(float &v, int, float a) { v = a; }
+    static __device__ __forceinline__ float fma(float a, float b, float c) { return fmaf(a, b, c); }
+    static __device__ __forceinline__ float max(float a, float b) { return fmaxf(a, b); }
+    static __device__ __forceinline__ float abs(float a) { return fabsf(a); }
+    static __device__ __forceinline__ float rcp(float a) { return rcp_approx(a); }
+    static __device__ __forceinline__ float rsqrt(float a) { return rsqrt_approx(a); }
+    static __device__ __forceinline__ float tiny() { return 1e-30f; }
+    // Smallest clamp of a squared quantity that stays a normal float.
+    static __device__ __forceinline__ float tiny2() { return 1e-37f; }
+};
+template <> struct VT<F2> {
+    static constexpr int N = 2;
+    using S = float;
+    static __device__ __forceinline__ F2 set(double a) {
+        const float f = float(a);
+        return {make_float2(f, f)};
+    }
+    static __device__ __forceinline__ float get(F2 v, int i) { return i == 0 ? v.v.x : v.v.y; }
+    static __device__ __forceinline__ void put(F2 &v, int i, float a) {
+        if (i == 0) v.v.x = a; else v.v.y = a;
+    }
+    static __device__ __forceinline__ F2 fma(F2 a, F2 b, F2 c) { return {__ffma2_rn(a.v, b.v, c.v)}; }
+    static __device__ __forceinline__ F2 max(F2 a, F2 b) {
+        return {make_float2(fmaxf(a.v.x, b.v.x), fmaxf(a.v.y, b.v.y))};
+    }
+    static __device__ __forceinline__ F2 abs(F2 a) {
+        return {make_float2(fabsf(a.v.x), fabsf(a.v.y))};
+    }
+    static __device__ __forceinline__ F2 rcp(F2 a) {
+        return {make_float2(rcp_approx(a.v.x), rcp_approx(a.v.y))};
+    }
+    static __device__ __forceinline__ F2 rsqrt(F2 a) {
+        return {make_float2(rsqrt_approx(a.v.x), rsqrt_approx(a.v.y))};
+    }
+    static __device__ __forceinline__ float tiny() { return 1e-30f; }
+    static __device__ __forceinline__ float tiny2() { return 1e-37f; }
 };
 
-// geodesics.py:42-74 with kerr.py:118-193 folded in.  The 3x3 gradient of l
-// is never formed: its contraction with p is
+// Per-ray Kerr constants in the lane type, formed once per ray.
+template <class V>
+struct KerrV {
+    V m, a, na, a2, a2x4, a2x3, n2ma2;
+};
+template <class V>
+__device__ __forceinline__ KerrV<V> make_kerr(V m, V a) {
+    using T = VT<V>;
+    KerrV<V> k;
+    k.m = m;
+    k.a = a;
+    k.na = -a;
+    k.a2 = a * a;
+    k.a2x4 = k.a2 * T::set(4.0);
+    k.a2x3 = k.a2 * T::set(3.0);
+    k.n2ma2 = (m * k.a2) * T::set(-2.0);
+    return k;
+}
+
+// Stage derivative in split form (see the top of this file):
+//   kx..kz = dP - 2 H lp l   (position part)   thl = 2 H lp   (time part)
+//   px..pz = dp/dlambda      (momentum part)
+template <class V>
+struct StageV {
+    V kx, ky, kz, thl, px, py, pz;
+};
+
+// ------------------------------------------------------------ compact RHS
+// geodesics.py:42-74 with kerr.py:118-193 folded in, evaluated at position
+// (x, y, z) and momentum (pt, px, py, pz); dpx..dpz is the stage's momentum
+// offset dP that the position part carries.  npt = -p_t (p_t is conserved).
+//
+// The 3x3 gradient of l is never formed: its contraction with p is
 //   c_i = r_i G + (r p_x - a p_y, r p_y + a p_x, 0)_i / (r^2+a^2) + (0,0,p_z/r)_i
 //   G   = (x p_x + y p_y - 2 r (l_x p_x + l_y p_y)) / (r^2+a^2) - z p_z / r^2
 // and with grad H = dH/dr grad r + (0, 0, dH/dz|_r) the momentum derivative is
 //   pdot_i = r_i (dH/dr lp^2 + thl G) + [thl * the explicit terms above]
 // which is the reference's grad_h * lp^2 + thl * (grad_l . p) regrouped.
-template <typename W>
-__device__ __forceinline__ Deriv<W> rhs(W m, W a, W x, W y, W z, W pt, W px,
-                                        W py, W pz) {
-    using M = Math<W>;
-    const W a2 = a * a;
-    const W z2 = z * z;
-    const W a2z2 = a2 * z2;
-    const W q = x * x + y * y + z2 - a2;
-    const W s = np_max(M::sqrt_(q * q + W(4) * a2z2), M::tiny());
-    W r2;
-    if constexpr (sizeof(W) == 8) {
-        r2 = W(0.5) * (q + s);  // kerr.py:141, as the reference computes it
-    } else {
-        r2 = q >= W(0) ? W(0.5) * (q + s) : W(2) * a2z2 * M::rcp(s - q);
-    }
-    r2 = np_max(r2, M::tiny());
-    const W r = M::sqrt_(r2);
-    const W w = r2 + a2;
-    const W qd = np_max(r2 * r2 + a2z2, M::tiny());
-    const W inv_qd = M::rcp(qd);
-    const W h = m * r * r2 * inv_qd;
-    const W inv_w = M::rcp(np_max(w, M::tiny()));
-    const W inv_r = M::rcp(r);
-    const W inv_s = M::rcp(s);
-    const W lx = (r * x + a * y) * inv_w;
-    const W ly = (r * y - a * x) * inv_w;
-    const W lz = z * inv_r;
-    const W lxy = lx * px + ly * py;
-    const W lp = -pt + (lxy + lz * pz);
-    const W thl = W(2) * h * lp;
-    Deriv<W> d;
-    d.thl = thl;
-    d.qx = -thl * lx;
-    d.qy = -thl * ly;
-    d.qz = -thl * lz;
-    const W rs = r * inv_s;
-    const W r_x = x * rs, r_y = y * rs;
-    const W r_z = z * w * inv_r * inv_s;
-    const W inv_qd2 = inv_qd * inv_qd;
-    const W lp2 = lp * lp;
-    const W dh_dr = m * r2 * (W(3) * a2z2 - r2 * r2) * inv_qd2;
-    const W dh_dz = W(-2) * m * a2 * z * r * r2 * inv_qd2;
-    const W u = x * px + y * py;
-    const W g = (u - W(2) * r * lxy) * inv_w - z * pz * inv_r * inv_r;
-    const W k = dh_dr * lp2 + thl * g;
-    const W tw = thl * inv_w;
-    d.px = r_x * k + tw * (r * px - a * py);
-    d.py = r_y * k + tw * (r * py + a * px);
-    d.pz = r_z * k + dh_dz * lp2 + thl * pz * inv_r;
-    return d;
+// The radius uses the reference's r^2 = (q + s)/2 (kerr.py:141) for every
+// lane type.
+template <class V>
+__device__ __forceinline__ StageV<V> rhs_v(const KerrV<V> &K, V x, V y, V z,
+                                           V npt, V px, V py, V pz, V dpx,
+                                           V dpy, V dpz) {
+    using T = VT<V>;
+    const V z2 = z * z;
+    const V a2z2 = K.a2 * z2;
+    const V q = T::fma(x, x, T::fma(y, y, z2 - K.a2));
+    const V s2 = T::max(T::fma(q, q, K.a2x4 * z2), T::set(T::tiny2()));
+    const V inv_s = T::rsqrt(s2);
+    const V s = s2 * inv_s;
+    const V r2 = T::max((q + s) * T::set(0.5), T::set(T::tiny()));
+    const V inv_r = T::rsqrt(r2);
+    const V r = r2 * inv_r;
+    const V w = r2 + K.a2;
+    const V r2sq = r2 * r2;
+    const V qd = T::max(r2sq + a2z2, T::set(T::tiny()));
+    const V inv_qd = T::rcp(qd);
+    const V inv_w = T::rcp(w);
+    const V r3 = r * r2;
+    const V h = (K.m * r3) * inv_qd;
+    const V lx = T::fma(r, x, K.a * y) * inv_w;
+    const V ly = T::fma(r, y, K.na * x) * inv_w;
+    const V lz = z * inv_r;
+    const V lxy = T::fma(lx, px, ly * py);
+    const V lzpz = lz * pz;
+    const V lp = (lxy + lzpz) + npt;
+    const V thl = (h + h) * lp;
+    const V nthl = -thl;
+    StageV<V> o;
+    o.thl = thl;
+    o.kx = T::fma(nthl, lx, dpx);
+    o.ky = T::fma(nthl, ly, dpy);
+    o.kz = T::fma(nthl, lz, dpz);
+    const V rs = r * inv_s;
+    const V r_x = x * rs, r_y = y * rs;
+    const V r_z = z * (w * (inv_r * inv_s));
+    const V inv_qd2 = inv_qd * inv_qd;
+    const V lp2 = lp * lp;
+    const V t3 = K.a2x3 * z2 - r2sq;
+    const V dh_dr = ((K.m * r2) * t3) * inv_qd2;
+    const V dh_dz = ((K.n2ma2 * z) * r3) * inv_qd2;
+    const V u = T::fma(x, px, y * py);
+    const V g1 = T::fma(r * T::set(-2.0), lxy, u);
+    const V g = g1 * inv_w - lzpz * inv_r;
+    const V k = T::fma(dh_dr, lp2, thl * g);
+    const V tw = thl * inv_w;
+    o.px = T::fma(r_x, k, tw * T::fma(r, px, K.na * py));
+    o.py = T::fma(r_y, k, tw * T::fma(r, py, K.a * px));
+    o.pz = T::fma(r_z, k, T::fma(dh_dz, lp2, (thl * pz) * inv_r));
+    return o;
 }
 
 // ---------------------------------------------------------------- tableau
@@ -234,157 +361,171 @@ constexpr double C2 = 1.0 / 5.0, C3 = 3.0 / 10.0, C4 = 4.0 / 5.0,
                  C5 = 8.0 / 9.0, C6 = 1.0;
 }  // namespace dp
 
-// One ray's integration state.
+// One ray's integration state (float64).
 struct RayState {
     double t, x, y, z, pt, px, py, pz;
 };
 
-// Stage derivative in the split form: kappa (position), thl (time), pd (momentum).
-template <typename W>
-struct Stage {
-    W kx, ky, kz, thl, px, py, pz;
+// The rays' states rounded to the lane type: RHS inputs of the stages and
+// magnitudes of the error scale.  npt = -p_t.
+template <class V>
+struct WStateV {
+    V t, x, y, z, npt, px, py, pz;
 };
 
-template <typename W>
-__device__ __forceinline__ Stage<W> make_stage(const Deriv<W> &d, W dpx,
-                                               W dpy, W dpz) {
-    Stage<W> s;
-    s.kx = dpx + d.qx;
-    s.ky = dpy + d.qy;
-    s.kz = dpz + d.qz;
-    s.thl = d.thl;
-    s.px = d.px;
-    s.py = d.py;
-    s.pz = d.pz;
-    return s;
+template <class V>
+__device__ __forceinline__ void put_work(WStateV<V> &w, int l, const RayState &y) {
+    using T = VT<V>;
+    using S = typename T::S;
+    T::put(w.t, l, S(y.t));
+    T::put(w.x, l, S(y.x));
+    T::put(w.y, l, S(y.y));
+    T::put(w.z, l, S(y.z));
+    T::put(w.npt, l, S(-y.pt));
+    T::put(w.px, l, S(y.px));
+    T::put(w.py, l, S(y.py));
+    T::put(w.pz, l, S(y.pz));
 }
 
-// Evaluates the RHS at stage input (X = x + h (c p + S), P = p + dP).
-template <typename W>
-__device__ __forceinline__ Stage<W> eval_stage(W m, W a, const RayState &y,
-                                               const W yw[7], double h, W hw,
-                                               double c, W sx, W sy, W sz,
-                                               W dpx, W dpy, W dpz) {
-    W X, Y, Z;
-    if constexpr (sizeof(W) == 8) {
-        X = y.x + h * (c * y.px + sx);
-        Y = y.y + h * (c * y.py + sy);
-        Z = y.z + h * (c * y.pz + sz);
-    } else {
-        const W cw = W(c);
-        X = yw[0] + hw * (cw * yw[4] + sx);
-        Y = yw[1] + hw * (cw * yw[5] + sy);
-        Z = yw[2] + hw * (cw * yw[6] + sz);
-    }
-    const Deriv<W> d = rhs<W>(m, a, X, Y, Z, yw[3], yw[4] + dpx, yw[5] + dpy,
-                              yw[6] + dpz);
-    return make_stage<W>(d, dpx, dpy, dpz);
-}
-
-#define BH_LIN2(f, c1, s1, c2, s2) (W(c1) * (s1).f + W(c2) * (s2).f)
-#define BH_LIN3(f, c1, s1, c2, s2, c3, s3) (BH_LIN2(f, c1, s1, c2, s2) + W(c3) * (s3).f)
-#define BH_LIN4(f, c1, s1, c2, s2, c3, s3, c4, s4) (BH_LIN3(f, c1, s1, c2, s2, c3, s3) + W(c4) * (s4).f)
-#define BH_LIN5(f, c1, s1, c2, s2, c3, s3, c4, s4, c5, s5) (BH_LIN4(f, c1, s1, c2, s2, c3, s3, c4, s4) + W(c5) * (s5).f)
-#define BH_LIN6(f, c1, s1, c2, s2, c3, s3, c4, s4, c5, s5, c6, s6) (BH_LIN5(f, c1, s1, c2, s2, c3, s3, c4, s4, c5, s5) + W(c6) * (s6).f)
-
-// Result of one DP5(4) attempt (integrators.py:76-107).
-template <typename W>
-struct Attempt {
-    RayState y_new;
-    double err[8];  // t x y z pt px py pz; err[4] == 0 (p_t is conserved)
-    Stage<W> k7;    // derivative at y_new, relative to y_new's momentum
+// Result of one DP5(4) attempt (integrators.py:76-107) for every lane.  The
+// float64 candidate state is not formed here: `ynw` (the candidate in the
+// lane type) feeds k7 and the error norm, and commit() adds the increments
+// to the float64 state once the step is accepted.
+template <class V>
+struct AttemptV {
+    WStateV<V> ynw;  // y_new in the lane type (the next yw if accepted)
+    V it, ix, iy, iz;        // sum_i b_i k_i of t, x, y, z without the exact parts
+    V dpx, dpy, dpz;         // momentum increments h sum_i b_i pdot_i
+    V err[7];        // sum_i e_i k_i for t x y z px py pz (the p_t error is 0)
+    StageV<V> k7;    // derivative at y_new relative to y_new's momentum
 };
 
-// One embedded Dormand-Prince 5(4) attempt from y with step h, reusing the
-// first-same-as-last derivative k1 = f(y).  Identical in exact arithmetic to
-// dormand_prince_step, which recomputes k1 every call.
-template <typename W>
-__device__ __forceinline__ void dp5_attempt(W m, W a, const RayState &y,
-                                            double h, const Stage<W> &k1,
-                                            Attempt<W> &out) {
+#define BH_LIN2(f, c1, s1, c2, s2) (T::set(c1) * (s1).f + T::set(c2) * (s2).f)
+#define BH_LIN3(f, c1, s1, c2, s2, c3, s3) (BH_LIN2(f, c1, s1, c2, s2) + T::set(c3) * (s3).f)
+#define BH_LIN4(f, c1, s1, c2, s2, c3, s3, c4, s4) (BH_LIN3(f, c1, s1, c2, s2, c3, s3) + T::set(c4) * (s4).f)
+#define BH_LIN5(f, c1, s1, c2, s2, c3, s3, c4, s4, c5, s5) (BH_LIN4(f, c1, s1, c2, s2, c3, s3, c4, s4) + T::set(c5) * (s5).f)
+#define BH_LIN6(f, c1, s1, c2, s2, c3, s3, c4, s4, c5, s5, c6, s6) (BH_LIN5(f, c1, s1, c2, s2, c3, s3, c4, s4, c5, s5) + T::set(c6) * (s6).f)
+
+// RHS at the stage input X = x + h (c p + S), P = p + dP with
+// dP = h sum_j a_ij pdot_j and S = sum_j a_ij kappa_j, formed in the lane type
+// from the rounded state (for V = double that is the state itself).
+template <class V>
+__device__ __forceinline__ StageV<V> stage_at(const KerrV<V> &K, const WStateV<V> &yw,
+                                              V hw, double c, V sx, V sy, V sz,
+                                              V spx, V spy, V spz) {
+    using T = VT<V>;
+    const V cw = T::set(c);
+    const V dpx = hw * spx, dpy = hw * spy, dpz = hw * spz;
+    return rhs_v<V>(K, T::fma(hw, T::fma(cw, yw.px, sx), yw.x),
+                    T::fma(hw, T::fma(cw, yw.py, sy), yw.y),
+                    T::fma(hw, T::fma(cw, yw.pz, sz), yw.z), yw.npt,
+                    yw.px + dpx, yw.py + dpy, yw.pz + dpz, dpx, dpy, dpz);
+}
+
+// One embedded Dormand-Prince 5(4) attempt per lane from yw with step hw,
+// reusing the first-same-as-last derivative k1 = f(y).  Identical in exact
+// arithmetic to dormand_prince_step, which recomputes k1 every call.  The
+// embedded error is h times out.err.  The time component's sums are
+// accumulated as the stages are produced (it never feeds a stage input).
+template <class V>
+__device__ __forceinline__ void dp5_attempt(const KerrV<V> &K, const WStateV<V> &yw,
+                                            V hw, const StageV<V> &k1,
+                                            AttemptV<V> &out) {
     using namespace dp;
-    const W yw[7] = {W(y.x), W(y.y), W(y.z), W(y.pt), W(y.px), W(y.py), W(y.pz)};
-    const W hw = W(h);
-    Stage<W> k2, k3, k4, k5, k6;
-    {
-        const W dpx = hw * (W(A21) * k1.px), dpy = hw * (W(A21) * k1.py),
-                dpz = hw * (W(A21) * k1.pz);
-        k2 = eval_stage<W>(m, a, y, yw, h, hw, C2, W(A21) * k1.kx,
-                           W(A21) * k1.ky, W(A21) * k1.kz, dpx, dpy, dpz);
-    }
-    {
-        const W dpx = hw * BH_LIN2(px, A31, k1, A32, k2);
-        const W dpy = hw * BH_LIN2(py, A31, k1, A32, k2);
-        const W dpz = hw * BH_LIN2(pz, A31, k1, A32, k2);
-        k3 = eval_stage<W>(m, a, y, yw, h, hw, C3, BH_LIN2(kx, A31, k1, A32, k2),
-                           BH_LIN2(ky, A31, k1, A32, k2),
-                           BH_LIN2(kz, A31, k1, A32, k2), dpx, dpy, dpz);
-    }
-    {
-        const W dpx = hw * BH_LIN3(px, A41, k1, A42, k2, A43, k3);
-        const W dpy = hw * BH_LIN3(py, A41, k1, A42, k2, A43, k3);
-        const W dpz = hw * BH_LIN3(pz, A41, k1, A42, k2, A43, k3);
-        k4 = eval_stage<W>(m, a, y, yw, h, hw, C4,
-                           BH_LIN3(kx, A41, k1, A42, k2, A43, k3),
-                           BH_LIN3(ky, A41, k1, A42, k2, A43, k3),
-                           BH_LIN3(kz, A41, k1, A42, k2, A43, k3), dpx, dpy, dpz);
-    }
-    {
-        const W dpx = hw * BH_LIN4(px, A51, k1, A52, k2, A53, k3, A54, k4);
-        const W dpy = hw * BH_LIN4(py, A51, k1, A52, k2, A53, k3, A54, k4);
-        const W dpz = hw * BH_LIN4(pz, A51, k1, A52, k2, A53, k3, A54, k4);
-        k5 = eval_stage<W>(m, a, y, yw, h, hw, C5,
-                           BH_LIN4(kx, A51, k1, A52, k2, A53, k3, A54, k4),
-                           BH_LIN4(ky, A51, k1, A52, k2, A53, k3, A54, k4),
-                           BH_LIN4(kz, A51, k1, A52, k2, A53, k3, A54, k4), dpx,
-                           dpy, dpz);
-    }
-    {
-        const W dpx = hw * BH_LIN5(px, A61, k1, A62, k2, A63, k3, A64, k4, A65, k5);
-        const W dpy = hw * BH_LIN5(py, A61, k1, A62, k2, A63, k3, A64, k4, A65, k5);
-        const W dpz = hw * BH_LIN5(pz, A61, k1, A62, k2, A63, k3, A64, k4, A65, k5);
-        k6 = eval_stage<W>(
-            m, a, y, yw, h, hw, C6,
-            BH_LIN5(kx, A61, k1, A62, k2, A63, k3, A64, k4, A65, k5),
-            BH_LIN5(ky, A61, k1, A62, k2, A63, k3, A64, k4, A65, k5),
-            BH_LIN5(kz, A61, k1, A62, k2, A63, k3, A64, k4, A65, k5), dpx, dpy,
-            dpz);
-    }
+    using T = VT<V>;
+    V it = T::set(B1) * k1.thl;
+    V et = T::set(E1) * k1.thl;
+    const StageV<V> k2 = stage_at<V>(K, yw, hw, C2, T::set(A21) * k1.kx, T::set(A21) * k1.ky,
+                                     T::set(A21) * k1.kz, T::set(A21) * k1.px,
+                                     T::set(A21) * k1.py, T::set(A21) * k1.pz);
+    const StageV<V> k3 = stage_at<V>(
+        K, yw, hw, C3, BH_LIN2(kx, A31, k1, A32, k2), BH_LIN2(ky, A31, k1, A32, k2),
+        BH_LIN2(kz, A31, k1, A32, k2), BH_LIN2(px, A31, k1, A32, k2),
+        BH_LIN2(py, A31, k1, A32, k2), BH_LIN2(pz, A31, k1, A32, k2));
+    it = T::fma(T::set(B3), k3.thl, it);
+    et = T::fma(T::set(E3), k3.thl, et);
+    const StageV<V> k4 = stage_at<V>(
+        K, yw, hw, C4, BH_LIN3(kx, A41, k1, A42, k2, A43, k3),
+        BH_LIN3(ky, A41, k1, A42, k2, A43, k3), BH_LIN3(kz, A41, k1, A42, k2, A43, k3),
+        BH_LIN3(px, A41, k1, A42, k2, A43, k3), BH_LIN3(py, A41, k1, A42, k2, A43, k3),
+        BH_LIN3(pz, A41, k1, A42, k2, A43, k3));
+    it = T::fma(T::set(B4), k4.thl, it);
+    et = T::fma(T::set(E4), k4.thl, et);
+    const StageV<V> k5 = stage_at<V>(
+        K, yw, hw, C5, BH_LIN4(kx, A51, k1, A52, k2, A53, k3, A54, k4),
+        BH_LIN4(ky, A51, k1, A52, k2, A53, k3, A54, k4),
+        BH_LIN4(kz, A51, k1, A52, k2, A53, k3, A54, k4),
+        BH_LIN4(px, A51, k1, A52, k2, A53, k3, A54, k4),
+        BH_LIN4(py, A51, k1, A52, k2, A53, k3, A54, k4),
+        BH_LIN4(pz, A51, k1, A52, k2, A53, k3, A54, k4));
+    it = T::fma(T::set(B5), k5.thl, it);
+    et = T::fma(T::set(E5), k5.thl, et);
+    const StageV<V> k6 = stage_at<V>(
+        K, yw, hw, C6, BH_LIN5(kx, A61, k1, A62, k2, A63, k3, A64, k4, A65, k5),
+        BH_LIN5(ky, A61, k1, A62, k2, A63, k3, A64, k4, A65, k5),
+        BH_LIN5(kz, A61, k1, A62, k2, A63, k3, A64, k4, A65, k5),
+        BH_LIN5(px, A61, k1, A62, k2, A63, k3, A64, k4, A65, k5),
+        BH_LIN5(py, A61, k1, A62, k2, A63, k3, A64, k4, A65, k5),
+        BH_LIN5(pz, A61, k1, A62, k2, A63, k3, A64, k4, A65, k5));
+    it = T::fma(T::set(B6), k6.thl, it);
+    et = T::fma(T::set(E6), k6.thl, et);
     // Fifth-order solution (b2 = b7 = 0).
-    const W ix = BH_LIN5(kx, B1, k1, B3, k3, B4, k4, B5, k5, B6, k6);
-    const W iy = BH_LIN5(ky, B1, k1, B3, k3, B4, k4, B5, k5, B6, k6);
-    const W iz = BH_LIN5(kz, B1, k1, B3, k3, B4, k4, B5, k5, B6, k6);
-    const W it = BH_LIN5(thl, B1, k1, B3, k3, B4, k4, B5, k5, B6, k6);
-    const W ipx = BH_LIN5(px, B1, k1, B3, k3, B4, k4, B5, k5, B6, k6);
-    const W ipy = BH_LIN5(py, B1, k1, B3, k3, B4, k4, B5, k5, B6, k6);
-    const W ipz = BH_LIN5(pz, B1, k1, B3, k3, B4, k4, B5, k5, B6, k6);
-    RayState &yn = out.y_new;
-    yn.t = y.t + h * (-y.pt + double(it));
-    yn.x = y.x + h * (y.px + double(ix));
-    yn.y = y.y + h * (y.py + double(iy));
-    yn.z = y.z + h * (y.pz + double(iz));
-    yn.pt = y.pt;
-    const W dpx7 = hw * ipx, dpy7 = hw * ipy, dpz7 = hw * ipz;
-    yn.px = y.px + double(dpx7);
-    yn.py = y.py + double(dpy7);
-    yn.pz = y.pz + double(dpz7);
-    // k7 = f(y_new), FSAL for the next step.  For W = float the momentum
-    // increment enters the error as dP_7 (its float value), so the error
-    // combination sees the same rounding as the stages.
-    const Deriv<W> d7 = rhs<W>(m, a, W(yn.x), W(yn.y), W(yn.z), yw[3],
-                               W(yn.px), W(yn.py), W(yn.pz));
-    const Stage<W> s7 = make_stage<W>(d7, dpx7, dpy7, dpz7);
-    out.k7 = make_stage<W>(d7, W(0), W(0), W(0));
-    // Embedded error (e2 = 0): the exact parts p and -p_t cancel because the
-    // weights e_i sum to zero.
-    out.err[0] = h * double(BH_LIN6(thl, E1, k1, E3, k3, E4, k4, E5, k5, E6, k6, E7, s7));
-    out.err[1] = h * double(BH_LIN6(kx, E1, k1, E3, k3, E4, k4, E5, k5, E6, k6, E7, s7));
-    out.err[2] = h * double(BH_LIN6(ky, E1, k1, E3, k3, E4, k4, E5, k5, E6, k6, E7, s7));
-    out.err[3] = h * double(BH_LIN6(kz, E1, k1, E3, k3, E4, k4, E5, k5, E6, k6, E7, s7));
-    out.err[4] = 0.0;
-    out.err[5] = h * double(BH_LIN6(px, E1, k1, E3, k3, E4, k4, E5, k5, E6, k6, E7, s7));
-    out.err[6] = h * double(BH_LIN6(py, E1, k1, E3, k3, E4, k4, E5, k5, E6, k6, E7, s7));
-    out.err[7] = h * double(BH_LIN6(pz, E1, k1, E3, k3, E4, k4, E5, k5, E6, k6, E7, s7));
+    out.it = it;
+    out.ix = BH_LIN5(kx, B1, k1, B3, k3, B4, k4, B5, k5, B6, k6);
+    out.iy = BH_LIN5(ky, B1, k1, B3, k3, B4, k4, B5, k5, B6, k6);
+    out.iz = BH_LIN5(kz, B1, k1, B3, k3, B4, k4, B5, k5, B6, k6);
+    out.dpx = hw * BH_LIN5(px, B1, k1, B3, k3, B4, k4, B5, k5, B6, k6);
+    out.dpy = hw * BH_LIN5(py, B1, k1, B3, k3, B4, k4, B5, k5, B6, k6);
+    out.dpz = hw * BH_LIN5(pz, B1, k1, B3, k3, B4, k4, B5, k5, B6, k6);
+    WStateV<V> &nw = out.ynw;
+    nw.t = T::fma(hw, yw.npt + it, yw.t);
+    nw.x = T::fma(hw, yw.px + out.ix, yw.x);
+    nw.y = T::fma(hw, yw.py + out.iy, yw.y);
+    nw.z = T::fma(hw, yw.pz + out.iz, yw.z);
+    nw.npt = yw.npt;
+    nw.px = yw.px + out.dpx;
+    nw.py = yw.py + out.dpy;
+    nw.pz = yw.pz + out.dpz;
+    // k7 = f(y_new), FSAL for the next step.  Relative to this step's base
+    // momentum its position part carries dP_7 = p_new - p.
+    const StageV<V> s7 = rhs_v<V>(K, nw.x, nw.y, nw.z, nw.npt, nw.px, nw.py, nw.pz,
+                                  out.dpx, out.dpy, out.dpz);
+    out.k7 = s7;
+    out.k7.kx = s7.kx - out.dpx;
+    out.k7.ky = s7.ky - out.dpy;
+    out.k7.kz = s7.kz - out.dpz;
+    // Embedded error / h (e2 = 0): the exact parts p and -p_t cancel because
+    // the weights e_i sum to zero.
+    out.err[0] = T::fma(T::set(E7), s7.thl, et);
+    out.err[1] = BH_LIN6(kx, E1, k1, E3, k3, E4, k4, E5, k5, E6, k6, E7, s7);
+    out.err[2] = BH_LIN6(ky, E1, k1, E3, k3, E4, k4, E5, k5, E6, k6, E7, s7);
+    out.err[3] = BH_LIN6(kz, E1, k1, E3, k3, E4, k4, E5, k5, E6, k6, E7, s7);
+    out.err[4] = BH_LIN6(px, E1, k1, E3, k3, E4, k4, E5, k5, E6, k6, E7, s7);
+    out.err[5] = BH_LIN6(py, E1, k1, E3, k3, E4, k4, E5, k5, E6, k6, E7, s7);
+    out.err[6] = BH_LIN6(pz, E1, k1, E3, k3, E4, k4, E5, k5, E6, k6, E7, s7);
+}
+
+// Accepts lane l of an attempt: the float64 state advances by the attempt's
+// increments (y + h (p + sum b k) for positions, y + dP for momenta) and the
+// lane-type copy becomes the rounded new state.  For V = double the attempt
+// already computed exactly these values in double.
+template <class V>
+__device__ __forceinline__ void commit(RayState &y, WStateV<V> &yw,
+                                       const AttemptV<V> &a, int l, double h) {
+    using T = VT<V>;
+    if constexpr (T::N == 1 && sizeof(typename T::S) == 8) {
+        y.t = a.ynw.t; y.x = a.ynw.x; y.y = a.ynw.y; y.z = a.ynw.z;
+        y.px = a.ynw.px; y.py = a.ynw.py; y.pz = a.ynw.pz;
+    } else {
+        y.t = y.t + h * (-y.pt + double(T::get(a.it, l)));
+        y.x = y.x + h * (y.px + double(T::get(a.ix, l)));
+        y.y = y.y + h * (y.py + double(T::get(a.iy, l)));
+        y.z = y.z + h * (y.pz + double(T::get(a.iz, l)));
+        y.px = y.px + double(T::get(a.dpx, l));
+        y.py = y.py + double(T::get(a.dpy, l));
+        y.pz = y.pz + double(T::get(a.dpz, l));
+    }
+    put_work<V>(yw, l, y);
 }
 
 #undef BH_LIN2
@@ -393,49 +534,61 @@ __device__ __forceinline__ void dp5_attempt(W m, W a, const RayState &y,
 #undef BH_LIN5
 #undef BH_LIN6
 
-// k1 = f(y) in the split form (dP = 0).
-template <typename W>
-__device__ __forceinline__ Stage<W> first_stage(W m, W a, const RayState &y) {
-    const Deriv<W> d = rhs<W>(m, a, W(y.x), W(y.y), W(y.z), W(y.pt), W(y.px),
-                              W(y.py), W(y.pz));
-    return make_stage<W>(d, W(0), W(0), W(0));
+// k1 = f(y) in split form (dP = 0).
+template <class V>
+__device__ __forceinline__ StageV<V> first_stage(const KerrV<V> &K, const WStateV<V> &yw) {
+    using T = VT<V>;
+    const V zero = T::set(0.0);
+    return rhs_v<V>(K, yw.x, yw.y, yw.z, yw.npt, yw.px, yw.py, yw.pz, zero, zero, zero);
 }
 
-// error_ratio (integrators.py:110-117): RMS over all 8 components of
-// err / (atol + rtol max(|y|, |y_new|)); non-finite -> +inf.  Accumulated in
-// double; for the mixed policy the division uses a float32 reciprocal of the
-// float64 scale (only ~7 digits of the ratio matter to the controller).
-template <typename W>
-__device__ __forceinline__ double error_ratio(const RayState &y,
-                                              const RayState &yn,
-                                              const double err[8], double rtol,
-                                              double atol) {
-    const double yv[8] = {y.t, y.x, y.y, y.z, y.pt, y.px, y.py, y.pz};
-    const double nv[8] = {yn.t, yn.x, yn.y, yn.z, yn.pt, yn.px, yn.py, yn.pz};
-    double q[8];
+// error_ratio (integrators.py:110-117) per lane: RMS over all 8 components of
+// h err / (atol + rtol max(|y|, |y_new|)), non-finite -> +inf, NumPy's
+// pairwise summation order.  The p_t term is exactly zero (p_t is conserved)
+// and is counted in the mean.  float64 policy: every operation in double.
+// Mixed policy: the error is a float32 combination of float32 stage
+// derivatives, so the scales and quotients are float32 too and the scale
+// reciprocal is one MUFU instruction (a float64 norm of float32 data would
+// add cost, not accuracy); the sum of squares, its square root and the
+// accept test are float64.
+template <class V>
+__device__ __forceinline__ void error_ratio_v(const WStateV<V> &y, const WStateV<V> &yn,
+                                              const V err[7], V hw, V rt, V at,
+                                              double ratio[VT<V>::N]) {
+    using T = VT<V>;
+    const V yv[7] = {y.t, y.x, y.y, y.z, y.px, y.py, y.pz};
+    const V nv[7] = {yn.t, yn.x, yn.y, yn.z, yn.px, yn.py, yn.pz};
+    V q[7];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        const double sc = atol + rtol * np_max(fabs(yv[i]), fabs(nv[i]));
-        double e;
-        if constexpr (sizeof(W) == 8) {
-            e = err[i] / sc;
+    for (int i = 0; i < 7; ++i) {
+        const V sc = T::fma(rt, T::max(T::abs(yv[i]), T::abs(nv[i])), at);
+        V e;
+        if constexpr (sizeof(V) == 8 && T::N == 1) {
+            e = (hw * err[i]) / sc;
         } else {
-            e = double(float(err[i]) * rcp_approx(float(sc)));
+            e = (hw * err[i]) * T::rcp(sc);
         }
         q[i] = e * e;
     }
-    // NumPy's pairwise order for an 8-element mean.
-    const double sum = ((q[0] + q[1]) + (q[2] + q[3])) + ((q[4] + q[5]) + (q[6] + q[7]));
-    const double ratio = ::sqrt(sum * 0.125);
-    return isfinite(ratio) ? ratio : __longlong_as_double(0x7ff0000000000000LL);
+#pragma unroll
+    for (int l = 0; l < T::N; ++l) {
+        const double g[7] = {double(T::get(q[0], l)), double(T::get(q[1], l)),
+                             double(T::get(q[2], l)), double(T::get(q[3], l)),
+                             double(T::get(q[4], l)), double(T::get(q[5], l)),
+                             double(T::get(q[6], l))};
+        // Components t x y z | p_t(=0) px py pz.
+        const double sum = ((g[0] + g[1]) + (g[2] + g[3])) + ((0.0 + g[4]) + (g[5] + g[6]));
+        const double r = ::sqrt(sum * 0.125);
+        ratio[l] = isfinite(r) ? r : __longlong_as_double(0x7ff0000000000000LL);
+    }
 }
 
 // step_factor (integrators.py:120-124): clip(0.9 max(ratio,1e-16)^-0.2, 0.2, 5).
-template <typename W>
+template <bool F64>
 __device__ __forceinline__ double step_factor(double ratio) {
     const double safe = np_max(ratio, 1e-16);
     double f;
-    if constexpr (sizeof(W) == 8) {
+    if constexpr (F64) {
         f = 0.9 * ::pow(safe, -0.2);
     } else {
         // float32 power through exp2/log2; only the step heuristic uses it.

@@ -45,6 +45,7 @@ struct TraceArgs {
     int32_t *status;
     int64_t *steps;  // accepted steps (trace) or accepted count (propagate)
     double *h_io;    // propagate: per-ray step size in/out
+    double *lam_io;  // affine parameter: propagate in/out, trace out; may be null
     long long n;
     int layout;
     // controller
@@ -60,6 +61,7 @@ struct TraceArgs {
 struct Variant {
     int block;
     int min_blocks;
+    int rays_per_thread;
 };
 
 int trace_variant_count(int precision);

@@ -8,13 +8,14 @@
 // 4*max_steps iterations (tracer.py:101) becomes a per-ray attempt cap and the
 // reference's `iterations` is the maximum attempt count over rays.
 //
-// Scheduling: one ray per thread, state in registers.  The grid is
-// persistent (blocks_per_sm x SMs); a lane whose ray terminates takes the next
-// ray from a global work queue.  Refills are warp-aggregated: __ballot_sync
-// collects the idle lanes, one lane claims that many rays with a single
-// atomicAdd and __shfl_sync hands each idle lane its index.  Every wait is
-// bounded: each ray makes at most max_attempts attempts and a %globaltimer
-// deadline ends the launch with a status flag.
+// Scheduling: N rays per thread (N = 1, or 2 in the packed float32x2 lane
+// type), states in registers.  The grid is persistent (blocks_per_sm x SMs);
+// a ray slot whose ray terminates takes the next ray from a global work queue.
+// Refills are warp-aggregated: __ballot_sync collects the idle slots of the
+// warp, one lane claims that many rays with a single atomicAdd and each idle
+// slot takes its rank.  Every wait is bounded: each ray makes at most
+// max_attempts attempts and a %globaltimer deadline ends the launch with a
+// status flag.
 #include <cstdio>
 
 #include "bh_device.cuh"
@@ -87,117 +88,240 @@ __device__ __forceinline__ double ks_radius(double a, const RayState &y) {
     return ::sqrt(ks_radius2(a, y.x, y.y, y.z));
 }
 
-template <typename W, int BLOCK, int MINB>
+// Lane-wise select of a lane-type value: dst[l] = src[l] where take[l].
+template <class V>
+__device__ __forceinline__ void take_lanes(V &dst, const V &src, const bool *take) {
+    using T = VT<V>;
+#pragma unroll
+    for (int l = 0; l < T::N; ++l)
+        if (take[l]) T::put(dst, l, T::get(src, l));
+}
+
+template <class V>
+__device__ __forceinline__ void take_stage(StageV<V> &d, const StageV<V> &s, const bool *take) {
+    take_lanes(d.kx, s.kx, take); take_lanes(d.ky, s.ky, take); take_lanes(d.kz, s.kz, take);
+    take_lanes(d.thl, s.thl, take);
+    take_lanes(d.px, s.px, take); take_lanes(d.py, s.py, take); take_lanes(d.pz, s.pz, take);
+}
+
+template <class V>
+__device__ __forceinline__ V lanes_of(const double *v) {
+    using T = VT<V>;
+    V out = T::set(0.0);
+#pragma unroll
+    for (int l = 0; l < T::N; ++l) T::put(out, l, typename T::S(v[l]));
+    return out;
+}
+
+// Where a thread keeps the float64 states of its N rays between attempts.
+// float64 lanes: in registers (they coincide with the lane-type copy).
+// float32 lanes: in shared memory, one plane per component, since the stages
+// only read the rounded copy and the float64 state is touched on accept only;
+// this frees 16 registers per ray.
+template <class V, int BLOCK>
+struct StateStore {
+    static constexpr int N = VT<V>::N;
+    static constexpr bool kShared = sizeof(typename VT<V>::S) == 4;
+    RayState reg[kShared ? 1 : N];
+    double *sh;
+    __device__ __forceinline__ explicit StateStore(double *smem) : sh(smem) {}
+    __device__ __forceinline__ RayState get(int l) const {
+        if constexpr (kShared) {
+            const double *p = sh + l * BLOCK + threadIdx.x;
+            constexpr int P = N * BLOCK;
+            return RayState{p[0], p[P], p[2 * P], p[3 * P], p[4 * P], p[5 * P], p[6 * P], p[7 * P]};
+        } else {
+            return reg[l];
+        }
+    }
+    __device__ __forceinline__ void set(int l, const RayState &y) {
+        if constexpr (kShared) {
+            double *p = sh + l * BLOCK + threadIdx.x;
+            constexpr int P = N * BLOCK;
+            p[0] = y.t; p[P] = y.x; p[2 * P] = y.y; p[3 * P] = y.z;
+            p[4 * P] = y.pt; p[5 * P] = y.px; p[6 * P] = y.py; p[7 * P] = y.pz;
+        } else {
+            reg[l] = y;
+        }
+    }
+    static constexpr size_t shared_bytes() { return kShared ? size_t(8) * N * BLOCK * 8 : 0; }
+};
+
+template <class V, int BLOCK, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args) {
+    using T = VT<V>;
+    constexpr int N = T::N;
+    constexpr bool F64 = sizeof(typename T::S) == 8;
     TraceWorkspace *ws = args.ws;
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
+    const unsigned lt_mask = (1u << lane) - 1u;
     const long long n = args.n;
     const unsigned long long t_start = global_timer_ns();
     const bool has_deadline = args.timeout_ns > 0;
     const unsigned long long deadline = t_start + (unsigned long long)args.timeout_ns;
+    const V rt = T::set(args.rtol), at = T::set(args.atol);
 
-    long long ray = -1;
-    RayState y;
-    Stage<W> k1;
-    double h = 0.0, spin = 0.0, mass = 0.0, rcap = 0.0, resc = 0.0, r = 0.0;
-    long long steps = 0, attempts = 0;
+    extern __shared__ double bh_state_smem[];
+    StateStore<V, BLOCK> ys(bh_state_smem);
+    long long ray[N], steps[N], attempts[N];
+    double h[N], mass[N], spin[N], rcap[N], resc[N], r[N], lam[N];
+    WStateV<V> yw;
+#pragma unroll
+    for (int l = 0; l < N; ++l) {
+        ray[l] = -1; steps[l] = 0; attempts[l] = 0;
+        h[l] = args.initial_step; mass[l] = 1.0; spin[l] = 0.0;
+        rcap[l] = 0.0; resc[l] = 0.0; r[l] = 0.0; lam[l] = 0.0;
+        // A benign placeholder state for idle slots (finite, far from the hole).
+        const RayState y0{0.0, 10.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0};
+        ys.set(l, y0);
+        put_work<V>(yw, l, y0);
+    }
+    KerrV<V> K = make_kerr<V>(lanes_of<V>(mass), lanes_of<V>(spin));
+    StageV<V> k1 = first_stage<V>(K, yw);
     bool queue_open = true;
     unsigned long long my_attempts = 0, my_accepted = 0;
     long long my_max_attempts = 0;
 
     for (unsigned iter = 0;; ++iter) {
-        // ---- warp-aggregated refill from the work queue
-        const bool need = ray < 0 && queue_open;
-        const unsigned mask = __ballot_sync(full, need);
-        if (mask) {
-            const int leader = __ffs(mask) - 1;
-            const int cnt = __popc(mask);
+        // ---- warp-aggregated refill of the idle ray slots
+        unsigned mask[N];
+        int total = 0;
+#pragma unroll
+        for (int l = 0; l < N; ++l) {
+            mask[l] = __ballot_sync(full, ray[l] < 0 && queue_open);
+            total += __popc(mask[l]);
+        }
+        bool fresh[N];
+#pragma unroll
+        for (int l = 0; l < N; ++l) fresh[l] = false;
+        if (total) {
+            unsigned any = 0;
+#pragma unroll
+            for (int l = 0; l < N; ++l) any |= mask[l];
+            const int leader = __ffs(any) - 1;
             unsigned long long base = 0;
-            if (lane == leader) base = atomicAdd(&ws->queue_head, (unsigned long long)cnt);
+            if (lane == leader) base = atomicAdd(&ws->queue_head, (unsigned long long)total);
             base = __shfl_sync(full, base, leader);
-            if (need) {
-                const long long idx = (long long)base + __popc(mask & ((1u << lane) - 1u));
-                if (idx < n) {
-                    ray = idx;
-                    if (args.source == 0) {
-                        load_state(args.state0, n, args.layout, idx, y);
-                        mass = args.mass; spin = args.spin;
-                        rcap = args.capture_radius; resc = args.escape_radius;
-                    } else {
-                        const int c = find_camera(args.cameras, args.ncameras, idx);
-                        const CameraDev &cam = args.cameras[c];
-                        camera_ray(cam, idx - cam.first_ray, y);
-                        mass = cam.mass; spin = cam.spin;
-                        rcap = cam.capture_radius; resc = cam.escape_radius;
-                    }
-                    h = args.initial_step;
-                    steps = 0;
-                    attempts = 0;
-                    r = ks_radius(spin, y);
-                    if (r >= resc) {
-                        // tracer.py:95-99 rejects the whole call; count and skip.
-                        atomicAdd(&ws->bad_rays, 1);
-                        store_state(args.states, n, args.layout, idx, y);
-                        args.status[idx] = BH_RAY_FAILED;
-                        args.steps[idx] = 0;
-                        ray = -1;
-                    } else {
-                        k1 = first_stage<W>(W(mass), W(spin), y);
+            int before = 0;
+#pragma unroll
+            for (int l = 0; l < N; ++l) {
+                if ((mask[l] >> lane) & 1u) {
+                    const long long idx = (long long)base + before + __popc(mask[l] & lt_mask);
+                    if (idx < n) {
+                        ray[l] = idx;
+                        RayState y0;
+                        if (args.source == 0) {
+                            load_state(args.state0, n, args.layout, idx, y0);
+                            mass[l] = args.mass; spin[l] = args.spin;
+                            rcap[l] = args.capture_radius; resc[l] = args.escape_radius;
+                        } else {
+                            const int c = find_camera(args.cameras, args.ncameras, idx);
+                            const CameraDev &cam = args.cameras[c];
+                            camera_ray(cam, idx - cam.first_ray, y0);
+                            mass[l] = cam.mass; spin[l] = cam.spin;
+                            rcap[l] = cam.capture_radius; resc[l] = cam.escape_radius;
+                        }
+                        h[l] = args.initial_step;
+                        lam[l] = 0.0;
+                        steps[l] = 0;
+                        attempts[l] = 0;
+                        r[l] = ks_radius(spin[l], y0);
+                        if (r[l] >= resc[l]) {
+                            // tracer.py:95-99 rejects the whole call; count and skip.
+                            atomicAdd(&ws->bad_rays, 1);
+                            store_state(args.states, n, args.layout, idx, y0);
+                            args.status[idx] = BH_RAY_FAILED;
+                            args.steps[idx] = 0;
+                            if (args.lam_io) args.lam_io[idx] = 0.0;
+                            ray[l] = -1;
+                        } else {
+                            fresh[l] = true;
+                            ys.set(l, y0);
+                            put_work<V>(yw, l, y0);
+                        }
                     }
                 }
+                before += __popc(mask[l]);
             }
-            if ((long long)base + cnt >= n) queue_open = false;
+            if ((long long)base + total >= n) queue_open = false;
         }
-        const bool active = ray >= 0;
+        bool any_fresh = false;
+#pragma unroll
+        for (int l = 0; l < N; ++l) any_fresh |= fresh[l];
+        if (any_fresh) {
+            K = make_kerr<V>(lanes_of<V>(mass), lanes_of<V>(spin));
+            const StageV<V> f = first_stage<V>(K, yw);
+            take_stage(k1, f, fresh);
+        }
+        bool active = false;
+#pragma unroll
+        for (int l = 0; l < N; ++l) active |= ray[l] >= 0;
         if (!__any_sync(full, active)) break;
 
         if (active) {
-            // ---- one controller iteration (tracer.py:109-149)
-            Attempt<W> at;
-            dp5_attempt<W>(W(mass), W(spin), y, h, k1, at);
-            const double ratio = error_ratio<W>(y, at.y_new, at.err, args.rtol, args.atol);
-            const bool accept = ratio <= 1.0;
-            ++attempts;
-            if (accept) {
-                y = at.y_new;
-                k1 = at.k7;
-                ++steps;
-                r = ks_radius(spin, y);
-            }
-            h = np_min(np_max(h * step_factor<W>(ratio), 0.0), args.max_step);
+            // ---- one controller iteration for every slot (tracer.py:109-149)
+            V hw = T::set(0.0);
+#pragma unroll
+            for (int l = 0; l < N; ++l) T::put(hw, l, typename T::S(h[l]));
+            AttemptV<V> a;
+            dp5_attempt<V>(K, yw, hw, k1, a);
+            double ratio[N];
+            error_ratio_v<V>(yw, a.ynw, a.err, hw, rt, at, ratio);
+            bool acc[N];
+#pragma unroll
+            for (int l = 0; l < N; ++l) {
+                acc[l] = false;
+                if (ray[l] < 0) continue;
+                acc[l] = ratio[l] <= 1.0;
+                ++attempts[l];
+                RayState yl = ys.get(l);
+                if (acc[l]) {
+                    commit<V>(yl, yw, a, l, h[l]);
+                    ys.set(l, yl);
+                    lam[l] += h[l];
+                    ++steps[l];
+                    r[l] = ks_radius(spin[l], yl);
+                }
+                h[l] = np_min(np_max(h[l] * step_factor<F64>(ratio[l]), 0.0), args.max_step);
 
-            const bool finite = all_finite(y);
-            int st = BH_RAY_IN_FLIGHT;
-            if (!finite) st = BH_RAY_FAILED;
-            if (finite && r <= rcap) st = BH_RAY_CAPTURED;
-            if (finite && r >= resc) st = BH_RAY_ESCAPED;
-            const bool in_flight = st == BH_RAY_IN_FLIGHT;
-            if (in_flight && h < args.min_step) st = BH_RAY_FAILED;
-            if (in_flight && steps >= args.max_steps) st = BH_RAY_MAX_STEPS;
-            // tracer.py:151-154: rays still in flight after the cap are MAX_STEPS.
-            if (st == BH_RAY_IN_FLIGHT && attempts >= args.max_attempts) st = BH_RAY_MAX_STEPS;
-            if (st != BH_RAY_IN_FLIGHT) {
-                store_state(args.states, n, args.layout, ray, y);
-                args.status[ray] = st;
-                args.steps[ray] = steps;
-                my_attempts += attempts;
-                my_accepted += steps;
-                if (attempts > my_max_attempts) my_max_attempts = attempts;
-                ray = -1;
+                const bool finite = all_finite(yl);
+                int st = BH_RAY_IN_FLIGHT;
+                if (!finite) st = BH_RAY_FAILED;
+                if (finite && r[l] <= rcap[l]) st = BH_RAY_CAPTURED;
+                if (finite && r[l] >= resc[l]) st = BH_RAY_ESCAPED;
+                const bool in_flight = st == BH_RAY_IN_FLIGHT;
+                if (in_flight && h[l] < args.min_step) st = BH_RAY_FAILED;
+                if (in_flight && steps[l] >= args.max_steps) st = BH_RAY_MAX_STEPS;
+                // tracer.py:151-154: rays still in flight after the cap are MAX_STEPS.
+                if (st == BH_RAY_IN_FLIGHT && attempts[l] >= args.max_attempts) st = BH_RAY_MAX_STEPS;
+                if (st != BH_RAY_IN_FLIGHT) {
+                    store_state(args.states, n, args.layout, ray[l], yl);
+                    args.status[ray[l]] = st;
+                    args.steps[ray[l]] = steps[l];
+                    if (args.lam_io) args.lam_io[ray[l]] = lam[l];
+                    my_attempts += attempts[l];
+                    my_accepted += steps[l];
+                    if (attempts[l] > my_max_attempts) my_max_attempts = attempts[l];
+                    ray[l] = -1;
+                }
             }
+            take_stage(k1, a.k7, acc);
         }
 
         // ---- bounded launch time
         if (has_deadline && (iter & 7u) == 0u) {
             const bool late = global_timer_ns() > deadline;
             if (__any_sync(full, late)) {
-                if (ray >= 0) {
-                    store_state(args.states, n, args.layout, ray, y);
-                    args.status[ray] = BH_RAY_IN_FLIGHT;
-                    args.steps[ray] = steps;
-                    my_attempts += attempts;
-                    my_accepted += steps;
+#pragma unroll
+                for (int l = 0; l < N; ++l) {
+                    if (ray[l] < 0) continue;
+                    store_state(args.states, n, args.layout, ray[l], ys.get(l));
+                    args.status[ray[l]] = BH_RAY_IN_FLIGHT;
+                    args.steps[ray[l]] = steps[l];
+                    if (args.lam_io) args.lam_io[ray[l]] = lam[l];
+                    my_attempts += attempts[l];
+                    my_accepted += steps[l];
                 }
                 if (lane == 0) atomicExch(&ws->timed_out, 1);
                 break;
@@ -219,9 +343,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args
 }
 
 // n_steps attempted DP5(4) steps per ray with the tracer's accept/reject and
-// step update (tracer.py:111-120) and no termination; grid-stride over rays.
-template <typename W, int BLOCK, int MINB>
+// step update (tracer.py:111-120) and no termination; grid-stride over groups
+// of N rays.
+template <class V, int BLOCK, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB) propagate_kernel(const TraceArgs args) {
+    using T = VT<V>;
+    constexpr int N = T::N;
+    constexpr bool F64 = sizeof(typename T::S) == 8;
     TraceWorkspace *ws = args.ws;
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -229,46 +357,80 @@ __global__ void __launch_bounds__(BLOCK, MINB) propagate_kernel(const TraceArgs 
     const unsigned long long deadline =
         global_timer_ns() + (unsigned long long)args.timeout_ns;
     const bool has_deadline = args.timeout_ns > 0;
+    const V rt = T::set(args.rtol), at = T::set(args.atol);
     unsigned long long my_attempts = 0, my_accepted = 0;
     long long my_max = 0;
     bool late = false;
+    const long long groups = (n + N - 1) / N;
     const long long stride = (long long)gridDim.x * blockDim.x;
-    // The loop trip count is uniform per warp: every lane of a warp runs
-    // ceil-aligned ray slots so the shuffles below see a full warp.
     const long long first = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long rounds = (n + stride - 1) / stride;
-    for (long long rd = 0; rd < rounds && !late; ++rd) {
-        const long long i = first + rd * stride;
-        const bool valid = i < n;
-        if (!valid) continue;
-        RayState y;
-        load_state(args.state0, n, args.layout, i, y);
-        const double spin = args.spin_of_ray ? args.spin_of_ray[i] : args.spin;
-        const W m = W(args.mass), a = W(spin);
-        double h = args.h_io[i];
-        Stage<W> k1 = first_stage<W>(m, a, y);
-        long long acc = 0, k = 0;
+    extern __shared__ double bh_state_smem[];
+    StateStore<V, BLOCK> ys(bh_state_smem);
+    for (long long g = first; g < groups && !late; g += stride) {
+        double h[N], lam[N], spin[N], mass[N];
+        long long acc[N];
+        bool valid[N];
+#pragma unroll
+        for (int l = 0; l < N; ++l) {
+            const long long i = g * N + l;
+            valid[l] = i < n;
+            // A missing last ray repeats the group's first ray; its results
+            // are not stored.
+            const long long src = valid[l] ? i : g * N;
+            RayState y0;
+            load_state(args.state0, n, args.layout, src, y0);
+            ys.set(l, y0);
+            spin[l] = args.spin_of_ray ? args.spin_of_ray[src] : args.spin;
+            mass[l] = args.mass;
+            h[l] = args.h_io[src];
+            lam[l] = args.lam_io ? args.lam_io[src] : 0.0;
+            acc[l] = 0;
+        }
+        const KerrV<V> K = make_kerr<V>(lanes_of<V>(mass), lanes_of<V>(spin));
+        WStateV<V> yw;
+#pragma unroll
+        for (int l = 0; l < N; ++l) put_work<V>(yw, l, ys.get(l));
+        StageV<V> k1 = first_stage<V>(K, yw);
+        long long k = 0;
         for (; k < args.max_attempts; ++k) {
-            Attempt<W> at;
-            dp5_attempt<W>(m, a, y, h, k1, at);
-            const double ratio = error_ratio<W>(y, at.y_new, at.err, args.rtol, args.atol);
-            if (ratio <= 1.0) {
-                y = at.y_new;
-                k1 = at.k7;
-                ++acc;
+            V hw = T::set(0.0);
+#pragma unroll
+            for (int l = 0; l < N; ++l) T::put(hw, l, typename T::S(h[l]));
+            AttemptV<V> a;
+            dp5_attempt<V>(K, yw, hw, k1, a);
+            double ratio[N];
+            error_ratio_v<V>(yw, a.ynw, a.err, hw, rt, at, ratio);
+            bool ok[N];
+#pragma unroll
+            for (int l = 0; l < N; ++l) {
+                ok[l] = ratio[l] <= 1.0;
+                if (ok[l]) {
+                    RayState yl = ys.get(l);
+                    commit<V>(yl, yw, a, l, h[l]);
+                    ys.set(l, yl);
+                    lam[l] += h[l];
+                    ++acc[l];
+                }
+                h[l] = np_min(np_max(h[l] * step_factor<F64>(ratio[l]), 0.0), args.max_step);
             }
-            h = np_min(np_max(h * step_factor<W>(ratio), 0.0), args.max_step);
+            take_stage(k1, a.k7, ok);
             if (has_deadline && (k & 63) == 63 && global_timer_ns() > deadline) {
                 late = true;
                 ++k;
                 break;
             }
         }
-        store_state(args.states, n, args.layout, i, y);
-        args.h_io[i] = h;
-        args.steps[i] = acc;
-        my_attempts += (unsigned long long)k;
-        my_accepted += (unsigned long long)acc;
+#pragma unroll
+        for (int l = 0; l < N; ++l) {
+            if (!valid[l]) continue;
+            const long long i = g * N + l;
+            store_state(args.states, n, args.layout, i, ys.get(l));
+            args.h_io[i] = h[l];
+            if (args.lam_io) args.lam_io[i] = lam[l];
+            args.steps[i] = acc[l];
+            my_attempts += (unsigned long long)k;
+            my_accepted += (unsigned long long)acc[l];
+        }
         if (k > my_max) my_max = k;
     }
     if (late) atomicExch(&ws->timed_out, 1);
@@ -286,45 +448,56 @@ __global__ void __launch_bounds__(BLOCK, MINB) propagate_kernel(const TraceArgs 
 }
 
 // ---------------------------------------------------------------- variants
-// (threads per block, __launch_bounds__ min blocks per SM).  The register cap
-// is 65536 / (block * min_blocks), rounded down to the allocation granule.
-static const Variant kVariantsF64[] = {{128, 2}, {128, 3}, {128, 4}, {256, 2}};
-static const Variant kVariantsMixed[] = {{128, 3}, {128, 4}, {128, 5}, {256, 2}};
-static constexpr int kNumVariants = 4;
+// (threads per block, __launch_bounds__ min blocks per SM, rays per thread).
+// The register cap is 65536 / (block * min_blocks), rounded down to the
+// allocation granule.  Mixed variants 4..7 run two rays per thread in packed
+// float32x2 arithmetic.
+static const Variant kVariantsF64[] = {{128, 2, 1}, {128, 3, 1}, {128, 4, 1}, {256, 2, 1}};
+static const Variant kVariantsMixed[] = {{128, 3, 1}, {128, 4, 1}, {128, 5, 1}, {256, 2, 1},
+                                         {128, 2, 2}, {128, 3, 2}, {64, 4, 2}, {256, 1, 2}};
 
-int trace_variant_count(int) { return kNumVariants; }
+int trace_variant_count(int precision) {
+    return precision == BH_PRECISION_MIXED ? 8 : 4;
+}
 Variant trace_variant(int precision, int idx) {
     return precision == BH_PRECISION_MIXED ? kVariantsMixed[idx] : kVariantsF64[idx];
 }
 int trace_default_variant(int precision) {
-    return precision == BH_PRECISION_MIXED ? 1 : 1;
+    return precision == BH_PRECISION_MIXED ? 5 : 3;
 }
 
-template <typename W, int B, int M>
-static const void *trace_fn() { return (const void *)trace_kernel<W, B, M>; }
-template <typename W, int B, int M>
-static const void *prop_fn() { return (const void *)propagate_kernel<W, B, M>; }
+template <class V, int B, int M>
+static const void *kfn(bool propagate, size_t *smem) {
+    *smem = StateStore<V, B>::shared_bytes();
+    return propagate ? (const void *)propagate_kernel<V, B, M>
+                     : (const void *)trace_kernel<V, B, M>;
+}
 
-static const void *kernel_for(bool propagate, int precision, int idx) {
+static const void *kernel_for(bool propagate, int precision, int idx, size_t *smem) {
     if (precision == BH_PRECISION_MIXED) {
         switch (idx) {
-            case 0: return propagate ? prop_fn<float, 128, 3>() : trace_fn<float, 128, 3>();
-            case 1: return propagate ? prop_fn<float, 128, 4>() : trace_fn<float, 128, 4>();
-            case 2: return propagate ? prop_fn<float, 128, 5>() : trace_fn<float, 128, 5>();
-            default: return propagate ? prop_fn<float, 256, 2>() : trace_fn<float, 256, 2>();
+            case 0: return kfn<float, 128, 3>(propagate, smem);
+            case 1: return kfn<float, 128, 4>(propagate, smem);
+            case 2: return kfn<float, 128, 5>(propagate, smem);
+            case 3: return kfn<float, 256, 2>(propagate, smem);
+            case 4: return kfn<F2, 128, 2>(propagate, smem);
+            case 5: return kfn<F2, 128, 3>(propagate, smem);
+            case 6: return kfn<F2, 64, 4>(propagate, smem);
+            default: return kfn<F2, 256, 1>(propagate, smem);
         }
     }
     switch (idx) {
-        case 0: return propagate ? prop_fn<double, 128, 2>() : trace_fn<double, 128, 2>();
-        case 1: return propagate ? prop_fn<double, 128, 3>() : trace_fn<double, 128, 3>();
-        case 2: return propagate ? prop_fn<double, 128, 4>() : trace_fn<double, 128, 4>();
-        default: return propagate ? prop_fn<double, 256, 2>() : trace_fn<double, 256, 2>();
+        case 0: return kfn<double, 128, 2>(propagate, smem);
+        case 1: return kfn<double, 128, 3>(propagate, smem);
+        case 2: return kfn<double, 128, 4>(propagate, smem);
+        default: return kfn<double, 256, 2>(propagate, smem);
     }
 }
 
 int kernel_attributes(bool propagate, int precision, int idx, int *regs,
                       int *max_blocks) {
-    const void *fn = kernel_for(propagate, precision, idx);
+    size_t smem = 0;
+    const void *fn = kernel_for(propagate, precision, idx, &smem);
     cudaFuncAttributes attr;
     cudaError_t e = cudaFuncGetAttributes(&attr, fn);
     if (e != cudaSuccess) return -1;
@@ -332,7 +505,7 @@ int kernel_attributes(bool propagate, int precision, int idx, int *regs,
     if (max_blocks) {
         int nb = 0;
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &nb, fn, trace_variant(precision, idx).block, 0);
+            &nb, fn, trace_variant(precision, idx).block, smem);
         if (e != cudaSuccess) return -1;
         *max_blocks = nb;
     }
@@ -341,28 +514,31 @@ int kernel_attributes(bool propagate, int precision, int idx, int *regs,
 
 static cudaError_t launch(bool propagate, const TraceArgs &args, int precision,
                           int variant, int blocks_per_sm, cudaStream_t stream) {
-    if (variant < 0 || variant >= kNumVariants) variant = trace_default_variant(precision);
+    if (variant < 0 || variant >= trace_variant_count(precision))
+        variant = trace_default_variant(precision);
     const Variant v = trace_variant(precision, variant);
-    const void *fn = kernel_for(propagate, precision, variant);
+    size_t smem = 0;
+    const void *fn = kernel_for(propagate, precision, variant, &smem);
     int dev = 0, sms = 0, occ = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, v.block, 0);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, v.block, smem);
     if (e != cudaSuccess) return e;
     if (occ < 1) occ = 1;
-    int per_sm = blocks_per_sm > 0 && blocks_per_sm < occ ? blocks_per_sm : occ;
+    const int per_sm = blocks_per_sm > 0 && blocks_per_sm < occ ? blocks_per_sm : occ;
     long long blocks = (long long)sms * per_sm;
     if (propagate) {
-        // Grid-stride: never more blocks than rays need.
-        const long long need = (args.n + v.block - 1) / v.block;
+        // Grid-stride: never more blocks than the ray groups need.
+        const long long groups = (args.n + v.rays_per_thread - 1) / v.rays_per_thread;
+        const long long need = (groups + v.block - 1) / v.block;
         if (blocks > need) blocks = need;
     }
     if (blocks < 1) blocks = 1;
     TraceArgs a = args;
     void *params[] = {(void *)&a};
-    return cudaLaunchKernel(fn, dim3((unsigned)blocks), dim3(v.block), params, 0, stream);
+    return cudaLaunchKernel(fn, dim3((unsigned)blocks), dim3(v.block), params, smem, stream);
 }
 
 cudaError_t launch_trace(const TraceArgs &args, int precision, int variant,

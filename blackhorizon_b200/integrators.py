@@ -152,9 +152,10 @@ def propagate(spacetime, state0: Array, n_steps: int, rtol: float = 1e-8,
     """n_steps attempted DP5(4) steps per ray with per-ray accept/reject and
     step update (tracer.py:111-120), no termination.
 
-    Returns (states, h, accepted, stats).  ``spins`` (n,) gives each ray its
-    own spin.  With ``in_place`` and a device float64 ``state0`` the states are
-    advanced in place."""
+    Returns (states, h, lam, accepted, stats): ``lam`` is the affine
+    parameter each ray advanced (sum of its accepted step sizes, float64).
+    ``spins`` (n,) gives each ray its own spin.  With ``in_place`` and a
+    device float64 ``state0`` the states are advanced in place."""
     s, host = to_device_f64(state0, "state0")
     n = s.shape[0] if layout == "aos" else s.shape[-1]
     if layout == "aos" and (s.dim() != 2 or s.shape[1] != 8):
@@ -174,6 +175,7 @@ def propagate(spacetime, state0: Array, n_steps: int, rtol: float = 1e-8,
         if bool((spin_t.abs() > spacetime.mass).any()):
             raise ValueError("Kerr bound violated: |spin| must be <= mass")
     acc = torch.empty(n, dtype=torch.int64, device=s.device)
+    lam = torch.zeros(n, dtype=torch.float64, device=s.device)
     lib = _lib.load()
     ws = workspace if workspace is not None else torch.empty(
         lib.bh_trace_workspace_bytes(), dtype=torch.uint8, device=s.device)
@@ -181,9 +183,10 @@ def propagate(spacetime, state0: Array, n_steps: int, rtol: float = 1e-8,
                       layout, timeout_s, variant)
     stream = stream_handle()
     _lib.check(lib.bh_propagate(cfg, float(spacetime.mass), float(spacetime.spin),
-                                ptr(spin_t), ptr(states), ptr(h), ptr(acc), n,
+                                ptr(spin_t), ptr(states), ptr(h), ptr(lam), ptr(acc), n,
                                 int(n_steps), ptr(ws), stream), "propagate")
     stats = _lib.TraceStats()
     _lib.check(lib.bh_trace_stats_read(ptr(ws), stats, stream), "propagate")
     return (out_like(states, host, state0), out_like(h, host, state0),
+            out_like(lam, host, state0),
             acc.cpu().numpy() if host is not None else acc, stats)

@@ -171,12 +171,14 @@ int bh_rk4(double mass, double spin, const double *state, const double *h,
 
 /* Launch-shape variants of the trace and propagate kernels for a precision:
  * threads per block, the __launch_bounds__ minimum blocks per SM (which caps
- * registers per thread) and the registers the compiled kernel uses.  The
- * autotuner times them; index -1 in bh_trace_config selects the default. */
+ * registers per thread), rays per thread (2 = two rays in the halves of
+ * packed float32x2 instructions, mixed precision only), and the registers
+ * and resident blocks per SM of the compiled trace kernel.  The autotuner
+ * times them; index -1 in bh_trace_config selects the default. */
 int bh_trace_variant_count(int32_t precision);
 int bh_trace_variant(int32_t precision, int32_t index, int32_t *block_threads,
-                     int32_t *min_blocks, int32_t *registers,
-                     int32_t *max_blocks_per_sm);
+                     int32_t *min_blocks, int32_t *rays_per_thread,
+                     int32_t *registers, int32_t *max_blocks_per_sm);
 
 /* Bytes of device workspace a trace or propagate launch needs (queue head and
  * counters), for any n; 256-byte aligned. */
@@ -221,21 +223,24 @@ int bh_trace_stats_read(const void *workspace, bh_trace_stats *out,
 /* Adaptive propagation without termination: n_steps attempted DP5(4) steps
  * per ray with the accept/reject and step-size update of tracer.py:111-120.
  * spin_of_ray (n,) gives each ray its own spin when non-NULL.  states (n,8)
- * and h (n,) are updated in place; accepted (n,) int64 receives accepted
- * steps.  Uses the workspace counters like bh_trace. */
+ * and h (n,) are updated in place; lam (n,), when non-NULL, accumulates the
+ * affine parameter of the accepted steps in float64 (in/out); accepted (n,)
+ * int64 receives accepted steps.  Uses the workspace counters like bh_trace. */
 int bh_propagate(const bh_trace_config *config, double mass, double spin,
                  const double *spin_of_ray, double *states, double *h,
-                 int64_t *accepted, int64_t n, int64_t n_steps,
+                 double *lam, int64_t *accepted, int64_t n, int64_t n_steps,
                  void *workspace, void *stream);
 
 /* ------------------------------------------------------------ diagnostics */
 
-/* Launches a vector-FMA throughput kernel (FP64 when precision is
- * BH_PRECISION_FP64, else FP32) of sms*8 blocks x 256 threads, each running
- * iters x 128 FMAs; *flops receives the launch's FLOP count (FMA = 2).  Timed
+/* Launches a vector-FMA throughput kernel of sms*8 blocks x 256 threads, each
+ * running iters x 128 FMA instructions: FP64 for BH_PRECISION_FP64, packed
+ * float32x2 (two FMAs per instruction) for BH_PEAK_F32X2, else FP32.  *flops
+ * receives the launch's FLOP count (FMA = 2).  Timed
  * with events by the caller, it gives the CUDA-core peak that the tracer's
  * roofline fraction is quoted against.  sink: device buffer of >= 8 bytes.
  * No counterpart in the reference (a measurement aid). */
+#define BH_PEAK_F32X2 2
 int bh_fma_peak_launch(int32_t precision, int64_t iters, void *sink,
                        int64_t *flops, void *stream);
 

@@ -465,6 +465,59 @@ void bho_propagate_batch(double mass, double spin, const double *spins,
 }
 
 typedef struct {
+    double mass, spin;
+    const double *spins, *target;
+    double *states;
+    int64_t *attempts;
+    double rtol, atol, initial_step, max_step;
+    int64_t max_attempts;
+} to_ctx_t;
+
+static void to_range(void *vctx, int64_t b, int64_t e, int64_t *acc) {
+    /* integrate_dense (integrators.py:155-173) for one ray: the step is cut
+     * to land on the target affine parameter; a ray whose step underflows or
+     * runs out of attempts gets NaN states. */
+    to_ctx_t *c = (to_ctx_t *)vctx;
+    (void)acc;
+    for (int64_t i = b; i < e; ++i) {
+        const double a = c->spins ? c->spins[i] : c->spin;
+        double *y = c->states + 8 * i;
+        const double total = c->target[i];
+        double elapsed = 0.0, h = c->initial_step;
+        int64_t k = 0;
+        int ok = 1;
+        while (elapsed < total) {
+            if (k++ >= c->max_attempts) { ok = 0; break; }
+            double rem = total - elapsed;
+            if (c->max_step < h) h = c->max_step;
+            if (rem < h) h = rem;
+            double y_new[8], err[8];
+            bho_dp5_step(c->mass, a, y, h, y_new, err);
+            const double ratio = bho_error_ratio(y, y_new, err, c->rtol, c->atol);
+            if (ratio <= 1.0) {
+                memcpy(y, y_new, sizeof(y_new));
+                elapsed += h;
+            }
+            h *= bho_step_factor(ratio);
+            if (h < 1e-14) { ok = 0; break; }
+        }
+        if (!ok)
+            for (int j = 0; j < 8; ++j) y[j] = NAN;
+        if (c->attempts) c->attempts[i] = k;
+    }
+}
+
+void bho_propagate_to(double mass, double spin, const double *spins,
+                      double *states, const double *lam_target,
+                      int64_t *attempts, int64_t n, double rtol, double atol,
+                      double initial_step, double max_step,
+                      int64_t max_attempts, int nthreads) {
+    to_ctx_t c = {mass, spin, spins, lam_target, states, attempts, rtol, atol,
+                  initial_step, max_step, max_attempts};
+    bho_parallel_for(n, nthreads, 2, to_range, &c);
+}
+
+typedef struct {
     double mass, spin, h;
     double *states;
     int64_t n_steps;

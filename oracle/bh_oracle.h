@@ -109,6 +109,16 @@ void bho_propagate_batch(double mass, double spin, const double *spins,
                          int64_t n, int64_t n_steps, double rtol, double atol,
                          double max_step, int nthreads);
 
+/* integrate_dense (integrators.py:127-174) per ray: adaptive DP5(4) from
+ * affine parameter 0 to lam_target[i], the last step cut to land on it.
+ * Rays that exhaust max_attempts or underflow the step get NaN states.
+ * attempts (n,) may be NULL. */
+void bho_propagate_to(double mass, double spin, const double *spins,
+                      double *states, const double *lam_target,
+                      int64_t *attempts, int64_t n, double rtol, double atol,
+                      double initial_step, double max_step,
+                      int64_t max_attempts, int nthreads);
+
 /* Fixed-step RK4 for a batch (examples/benchmark.py:39-51). */
 void bho_rk4_batch(double mass, double spin, double *states, int64_t n,
                    int64_t n_steps, double h, int nthreads);

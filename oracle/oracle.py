@@ -199,3 +199,28 @@ def propagate(mass: float, spins, state0, n_steps: int, rtol: float,
                               _D(rtol), _D(atol), _D(max_step),
                               ctypes.c_int(nthreads))
     return s, h, acc
+
+
+def propagate_to(mass: float, spins, state0, lam_target, rtol: float = 1e-12,
+                 atol: float = 1e-14, initial_step: float = 0.1,
+                 max_step: float = 2.0, max_attempts: int = 1_000_000,
+                 nthreads: int = 0):
+    """States at affine parameter lam_target (per ray), integrated with the
+    reference's DP5(4) and controller and the last step cut to land on the
+    target (integrators.py:127-174 per ray).  Returns (states, attempts)."""
+    s = _f64(state0).copy()
+    n = s.shape[0]
+    lam = _f64(np.broadcast_to(np.asarray(lam_target, dtype=np.float64), (n,)))
+    att = np.empty(n, dtype=np.int64)
+    spins_arr = None
+    spin = 0.0
+    if np.ndim(spins) == 0:
+        spin = float(spins)
+    else:
+        spins_arr = _f64(spins)
+    lib().bho_propagate_to(_D(mass), _D(spin),
+                           _ptr(spins_arr) if spins_arr is not None else None,
+                           _ptr(s), _ptr(lam), _ptr(att), _I64(n), _D(rtol), _D(atol),
+                           _D(initial_step), _D(max_step), _I64(max_attempts),
+                           ctypes.c_int(nthreads))
+    return s, att

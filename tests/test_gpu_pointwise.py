@@ -115,8 +115,9 @@ def test_dp5_step_fp64(cuda):
 
 
 def test_dp5_step_mixed(cuda):
-    """Mixed policy: float32 stage arithmetic; the update is float64, so the
-    new state differs from the reference by ~1e-7 of the step increment."""
+    """Mixed policy: float32 stage arithmetic; the update is float64, so on
+    steps the reference accepts (error ratio <= 1) the new state differs from
+    the reference by ~1e-6 of the step increment."""
     from blackhorizon_b200 import integrators
     from blackhorizon_b200.geodesics import GeodesicRhs
     from blackhorizon_b200.kerr import KerrSpacetime
@@ -125,9 +126,12 @@ def test_dp5_step_mixed(cuda):
     rhs = GeodesicRhs(KerrSpacetime(1.0, float(g["spin"])))
     s, h = dev(g["state"]), dev(g["h"])
     new, _ = integrators.dormand_prince_step(rhs, s, h, precision="mixed")
-    inc = np.abs(g["dp5_new"] - g["state"]) + 1e-12
-    rel = np.abs(new.cpu().numpy() - g["dp5_new"]) / inc
-    assert np.max(rel) < 2e-5
+    ok = g["ratio"] <= 1.0
+    assert ok.sum() > 100
+    inc = np.max(np.abs(g["dp5_new"] - g["state"]), axis=1, keepdims=True)
+    rel = np.abs(new.cpu().numpy() - g["dp5_new"])[ok] / inc[ok]
+    print("mixed dp5 step: max error / increment %.3g" % np.max(rel))
+    assert np.max(rel) < 1e-5
 
 
 def test_rk4_benchmark(cuda):

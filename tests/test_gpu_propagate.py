@@ -4,8 +4,18 @@ no termination) against the reference's end points for its first 512 rays.
 Endpoint error of a ray = max over the 8 components of
 |y - y_ref| / max(|y_ref|, 1): relative for large components, absolute for
 components near zero (momenta of order 1, p_z of an equatorial ray ~ 0).
-Float64 policy: median 1e-10, every ray 1e-6.  Mixed policy: median 1e-6;
-the target of the raw-throughput benchmark is <= 1e-6 at the median.
+
+Float64 policy: the same step sequence as the reference, so the end point
+after 2000 attempts matches it (median 1e-10, every ray 1e-6).
+
+Mixed policy: float32 rounding puts a noise floor of ~1e-3 under the error
+ratio near r = 30, so the controller's step sequence is not the float64 one
+and the end point after a fixed attempt count sits at a different affine
+parameter.  Its accuracy is therefore measured at equal affine parameter: the
+oracle integrates each ray to the lambda the kernel reached, at rtol 1e-12
+(the reference's DP5(4) and controller, last step cut to land on lambda).
+Bar: median <= 1e-6, 90th percentile <= 1e-5; the float64 kernel is held to
+the same comparison.
 """
 
 import numpy as np
@@ -21,7 +31,7 @@ def endpoint_error(got, ref):
     return np.max(np.abs(got - ref) / np.maximum(np.abs(ref), 1.0), axis=1)
 
 
-def run(precision, layout="aos"):
+def run(precision, layout="aos", variant=-1):
     from blackhorizon_b200 import propagate
     from blackhorizon_b200.kerr import KerrSpacetime
 
@@ -29,11 +39,13 @@ def run(precision, layout="aos"):
     s0 = torch.as_tensor(g["state0"], device="cuda")
     if layout == "soa":
         s0 = s0.t().contiguous()
-    states, h, acc, stats = propagate(
+    states, h, lam, acc, stats = propagate(
         KerrSpacetime(1.0, 0.0), s0, int(g["n_steps"]), rtol=float(g["rtol"]),
-        atol=float(g["atol"]), precision=precision, spins=g["spin"], layout=layout)
+        atol=float(g["atol"]), precision=precision, spins=g["spin"], layout=layout,
+        variant=variant)
     if layout == "soa":
         states = states.t()
+    run.lam = lam.cpu().numpy()
     return g, states.cpu().numpy(), acc.cpu().numpy(), stats
 
 
@@ -54,11 +66,36 @@ def test_soa_layout(cuda):
     np.testing.assert_array_equal(acc_a, acc_b)
 
 
-def test_mixed_endpoints(cuda):
-    g, got, acc, stats = run("mixed")
-    err = endpoint_error(got, g["final"])
-    print("mixed endpoint error: median %.3g p90 %.3g max %.3g; accepted %.4f of ref"
-          % (np.median(err), np.quantile(err, 0.9), np.max(err),
-             acc.sum() / g["accepted"].sum()))
-    assert np.median(err) < 1e-6
-    assert np.all(np.isfinite(got))
+def equal_lambda_error(g, got, lam):
+    from oracle import oracle
+
+    truth, _ = oracle.propagate_to(1.0, g["spin"], g["state0"], lam, rtol=1e-12, atol=1e-14)
+    ok = np.all(np.isfinite(truth), axis=1) & np.all(np.isfinite(got), axis=1)
+    return endpoint_error(got[ok], truth[ok]), int((~ok).sum())
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_endpoints_at_equal_affine_parameter(cuda, precision):
+    g, got, acc, stats = run(precision)
+    lam = run.lam
+    assert np.all(lam > 0) and np.all(np.isfinite(got))
+    err, dropped = equal_lambda_error(g, got, lam)
+    print("%s endpoint error at equal lambda: median %.3g p90 %.3g p99 %.3g max %.3g "
+          "(%d rays without a finite oracle state); accepted %.4f of ref"
+          % (precision, np.median(err), np.quantile(err, 0.9), np.quantile(err, 0.99),
+             np.max(err), dropped, acc.sum() / g["accepted"].sum()))
+    assert dropped <= 4
+    assert np.median(err) <= 1e-6
+    assert np.quantile(err, 0.9) <= 1e-5
+
+
+@pytest.mark.parametrize("variant", range(8))
+def test_mixed_variants_agree(cuda, variant):
+    """Every mixed launch shape (one ray per thread, or two per thread in
+    packed float32x2) meets the equal-lambda bar on the same rays."""
+    g, got, acc, stats = run("mixed", variant=variant)
+    assert stats.attempts == 512 * 2000
+    err, dropped = equal_lambda_error(g, got, run.lam)
+    assert dropped <= 4
+    assert np.median(err) <= 1e-6
+    assert np.quantile(err, 0.9) <= 1e-5
