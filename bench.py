@@ -126,6 +126,25 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+# ------------------------------------------------------------ sharding
+def shard_offset(rank: int, rays_per_rank: int) -> int:
+    """First ray of this rank's shard of the seeded workload (weak scaling:
+    every rank owns rays_per_rank consecutive rays)."""
+    return rank * rays_per_rank
+
+
+def max_over_ranks(value: float, world: int, device=None) -> float:
+    """The largest value over all ranks (the job's time is the slowest rank's)."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 # ------------------------------------------------------------ workload
 def make_inputs(n, rank, device):
     import torch
@@ -134,7 +153,7 @@ def make_inputs(n, rank, device):
     from blackhorizon_b200.kerr import KerrSpacetime
     from blackhorizon_b200.workloads import raw_throughput_inputs
 
-    pos, d, spin = raw_throughput_inputs(n, offset=rank * n)
+    pos, d, spin = raw_throughput_inputs(n, offset=shard_offset(rank, n))
 
     class _PerRay(KerrSpacetime):
         pass
@@ -247,12 +266,8 @@ def run_ours(args):
         _lib.check(lib.bh_trace_stats_read(ws.data_ptr(), st, stream), "bench stats")
         if st.attempts != n * S:
             raise RuntimeError(f"propagate did {st.attempts} attempts, expected {n * S}")
-        total_ms = t0.elapsed_time(t1)
+        total_ms = max_over_ranks(t0.elapsed_time(t1), world, device)
         kernel_ms = sum(a.elapsed_time(b) for a, b in kevs) / k
-        if world > 1:
-            tt = torch.tensor([total_ms], dtype=torch.float64, device=device)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            total_ms = float(tt.item())
         return total_ms / k, kernel_ms, clocks
 
     prec = args.precision
@@ -290,11 +305,7 @@ def run_ours(args):
     for _ in range(e2e_k):
         res = e2e_step()
     barrier()
-    e2e_s = (time.perf_counter() - w0) / e2e_k
-    if world > 1:
-        tt = torch.tensor([e2e_s], dtype=torch.float64, device=device)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
+    e2e_s = max_over_ranks((time.perf_counter() - w0) / e2e_k, world, device)
     del res
 
     out = None
