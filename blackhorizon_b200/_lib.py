@@ -81,6 +81,9 @@ _SIGNATURES = {
     "bh_trace_cameras": (ctypes.c_int, [ctypes.POINTER(TraceConfig), _I32, _I64, _P,
                                         _P, _P, _P, _SZ, _P]),
     "bh_trace_stats_read": (ctypes.c_int, [_P, ctypes.POINTER(TraceStats), _P]),
+    "bh_trace_cameras_noalloc": (ctypes.c_int, [ctypes.POINTER(TraceConfig),
+                                                ctypes.POINTER(Camera), _I32, _P, _P, _P,
+                                                ctypes.POINTER(TraceStats), _P]),
     "bh_propagate": (ctypes.c_int, [ctypes.POINTER(TraceConfig), _D, _D, _P, _P, _P,
                                     _P, _P, _I64, _I64, _P, _P]),
     "bh_fma_peak_launch": (ctypes.c_int, [_I32, _I64, _P, ctypes.POINTER(_I64), _P]),

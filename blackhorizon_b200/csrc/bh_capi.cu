@@ -672,3 +672,109 @@ int bh_propagate(const bh_trace_config *config, double mass, double spin,
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------ no-alloc
+// bh_trace_cameras_noalloc: the multi-camera trace for callers that cannot
+// allocate device memory themselves -- for example a host application that
+// owns every byte of GPU memory through its own fixed-size pool and hands
+// this library only its output buffers, or code that runs under a hard
+// memory budget where an extra cudaMalloc could fail or synchronise the
+// device.  Such a caller cannot supply the workspace bh_trace_cameras needs
+// (launch counters, work-queue head and camera table), so this variant keeps
+// that scratch in one static device array: kNoAllocMaxCameras cameras at
+// most, 256 + 256 * sizeof(CameraDev) bytes, resident on every GPU that loads
+// the library until the process exits.
+#include <mutex>
+
+namespace bh {
+
+constexpr int kNoAllocMaxCameras = 256;
+constexpr size_t kNoAllocBytes =
+    sizeof(TraceWorkspace) + size_t(kNoAllocMaxCameras) * sizeof(CameraDev);
+constexpr int kNoAllocMaxDevices = 64;
+
+// The scratch itself.  Host code must not use this name as a device address:
+// on the host it is only a stand-in for the symbol.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+static std::mutex g_noalloc_mu;
+static void *g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch on the current device, looked up once per
+// device with that device current.
+static int noalloc_scratch(void **out) {
+    int dev = 0;
+    int rc = cuda_status(cudaGetDevice(&dev), "bh_trace_cameras_noalloc device");
+    if (rc != BH_OK) return rc;
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return invalid("device index out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void *p = nullptr;
+        rc = cuda_status(cudaGetSymbolAddress(&p, g_noalloc_scratch),
+                         "bh_trace_cameras_noalloc scratch address");
+        if (rc != BH_OK) return rc;
+        g_noalloc_addr[dev] = p;
+    }
+    *out = g_noalloc_addr[dev];
+    return BH_OK;
+}
+
+}  // namespace bh
+
+extern "C" int bh_trace_cameras_noalloc(const bh_trace_config *config,
+                                        const bh_camera *cameras,
+                                        int32_t ncameras, double *states,
+                                        int32_t *status, int64_t *steps,
+                                        bh_trace_stats *stats, void *stream) {
+    int rc = config_ok(config);
+    if (rc != BH_OK) return rc;
+    if (ncameras < 1 || !cameras) return invalid("need at least one camera");
+    if (ncameras > kNoAllocMaxCameras) {
+        set_error("bh_trace_cameras_noalloc takes at most %d cameras (got %d); "
+                  "use bh_trace_cameras with a caller-owned workspace",
+                  kNoAllocMaxCameras, ncameras);
+        return BH_ERR_INVALID_ARGUMENT;
+    }
+    if (!states || !status || !steps) return invalid("NULL pointer argument");
+    if (config->layout == BH_LAYOUT_AOS && !aligned(states, 16))
+        return invalid("state buffers must be 16-byte aligned");
+    // The camera table is built on the host stack: no heap allocation.
+    CameraDev table[kNoAllocMaxCameras];
+    long long total = 0;
+    for (int c = 0; c < ncameras; ++c) {
+        rc = camera_ok(cameras[c]);
+        if (rc != BH_OK) return rc;
+        table[c] = camera_dev(cameras[c], total);
+        total += cameras[c].width * cameras[c].height;
+    }
+    void *scratch = nullptr;
+    rc = noalloc_scratch(&scratch);
+    if (rc != BH_OK) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    char *base = reinterpret_cast<char *>(scratch);
+    // Counters and queue head start at zero on every call; the previous
+    // call's camera table is overwritten below.
+    rc = cuda_status(cudaMemsetAsync(base, 0, sizeof(TraceWorkspace), s),
+                     "bh_trace_cameras_noalloc reset");
+    if (rc != BH_OK) return rc;
+    rc = cuda_status(cudaMemcpyAsync(base + sizeof(TraceWorkspace), table,
+                                     sizeof(CameraDev) * ncameras,
+                                     cudaMemcpyHostToDevice, s),
+                     "bh_trace_cameras_noalloc table upload");
+    if (rc != BH_OK) return rc;
+    TraceArgs a = base_args(config);
+    a.source = 1;
+    a.cameras = reinterpret_cast<const CameraDev *>(base + sizeof(TraceWorkspace));
+    a.ncameras = ncameras;
+    a.states = states;
+    a.status = status;
+    a.steps = steps;
+    a.n = total;
+    a.ws = reinterpret_cast<TraceWorkspace *>(base);
+    rc = cuda_status(launch_trace(a, config->precision, config->variant,
+                                  config->blocks_per_sm, s),
+                     "bh_trace_cameras_noalloc launch");
+    if (rc != BH_OK) return rc;
+    bh_trace_stats local;
+    return bh_trace_stats_read(scratch, stats ? stats : &local, stream);
+}

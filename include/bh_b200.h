@@ -214,6 +214,25 @@ int bh_trace_cameras(const bh_trace_config *config, int32_t ncameras,
                      int64_t *steps, void *workspace, size_t workspace_bytes,
                      void *stream);
 
+/* bh_trace_cameras without a caller-owned workspace, for callers that cannot
+ * allocate device memory (a host application that owns all GPU memory
+ * through its own fixed pool, or code under a hard memory budget).  No
+ * counterpart in the reference.  The launch counters, work-queue head and
+ * camera table live in one static device array of the library, sized for
+ * at most 256 cameras (256 + 256 x 168 = 43,264 bytes, held on every GPU that loads the library
+ * until the process exits); more cameras return BH_ERR_INVALID_ARGUMENT.
+ * cameras is a HOST array.  The call uploads the table, launches, then copies
+ * the counters into *stats (may be NULL) and synchronises `stream`; it
+ * returns what bh_trace_stats_read would.  The first call on a device looks
+ * up the array's device address, so make it before any stream capture.
+ * Every call shares the one array: calls that overlap on the GPU (on
+ * different streams or host threads) race and must be serialised by the
+ * caller.  Allocates nothing (no cudaMalloc / cudaFree, no heap). */
+int bh_trace_cameras_noalloc(const bh_trace_config *config,
+                             const bh_camera *cameras, int32_t ncameras,
+                             double *states, int32_t *status, int64_t *steps,
+                             bh_trace_stats *stats, void *stream);
+
 /* Copies the counters of the last launch on `workspace` to the host and
  * synchronises `stream`.  Returns BH_ERR_TIMEOUT / BH_ERR_ESCAPE_RADIUS when
  * the launch hit its deadline or met a ray outside its escape radius. */
