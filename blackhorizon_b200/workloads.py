@@ -117,3 +117,19 @@ def uneven_cameras(count: int = 64, seed: int = UNEVEN_SEED):
         h = int(np.clip(round(w * 3 / 4), 48, 768))
         cams.append(UnevenCamera(float(spin[k]), float(inc[k]), float(dist[k]), w, h))
     return cams
+
+
+def ks_radius_np(states, spin):
+    """Kerr-Schild radius of (n, 8) states with per-ray spin (kerr.py:135-141),
+    NumPy, for host-side bookkeeping of end points."""
+    x, y, z = states[:, 1], states[:, 2], states[:, 3]
+    a2 = np.asarray(spin, dtype=np.float64) ** 2
+    q = x * x + y * y + z * z - a2
+    with np.errstate(invalid="ignore", over="ignore"):
+        return np.sqrt(0.5 * (q + np.sqrt(q * q + 4.0 * a2 * z * z)))
+
+
+# End points inside this Kerr-Schild radius belong to rays that fell through
+# the horizon during a no-termination run; their coordinates run toward the
+# singularity and are excluded (and counted) when end points are compared.
+PLUNGE_RADIUS = 2.5

@@ -67,10 +67,15 @@ def test_soa_layout(cuda):
 
 
 def equal_lambda_error(g, got, lam):
+    """Errors of the rays that stay outside the horizon, and how many fell in
+    (their coordinates run toward the singularity: not comparable)."""
     from oracle import oracle
+
+    from blackhorizon_b200.workloads import PLUNGE_RADIUS, ks_radius_np
 
     truth, _ = oracle.propagate_to(1.0, g["spin"], g["state0"], lam, rtol=1e-12, atol=1e-14)
     ok = np.all(np.isfinite(truth), axis=1) & np.all(np.isfinite(got), axis=1)
+    ok &= np.nan_to_num(ks_radius_np(truth, g["spin"]), nan=0.0) >= PLUNGE_RADIUS
     return endpoint_error(got[ok], truth[ok]), int((~ok).sum())
 
 
@@ -84,9 +89,10 @@ def test_endpoints_at_equal_affine_parameter(cuda, precision):
           "(%d rays without a finite oracle state); accepted %.4f of ref"
           % (precision, np.median(err), np.quantile(err, 0.9), np.quantile(err, 0.99),
              np.max(err), dropped, acc.sum() / g["accepted"].sum()))
-    assert dropped <= 4
+    assert dropped <= 8
     assert np.median(err) <= 1e-6
     assert np.quantile(err, 0.9) <= 1e-5
+    assert np.quantile(err, 0.99) <= 1e-4
 
 
 @pytest.mark.parametrize("variant", range(8))
@@ -96,6 +102,7 @@ def test_mixed_variants_agree(cuda, variant):
     g, got, acc, stats = run("mixed", variant=variant)
     assert stats.attempts == 512 * 2000
     err, dropped = equal_lambda_error(g, got, run.lam)
-    assert dropped <= 4
+    assert dropped <= 8
     assert np.median(err) <= 1e-6
     assert np.quantile(err, 0.9) <= 1e-5
+    assert np.quantile(err, 0.99) <= 1e-4
