@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true", help="skip the float64 comparison arm")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-workloads", action="store_true",
+                    help="skip the full-HD frame and the 64-camera batch")
     return ap.parse_args()
 
 
@@ -369,6 +371,8 @@ def run_ours(args):
         if fp64 is not None:
             out["fp64"] = fp64
             out["speedup_vs_fp64"] = fp64["ms_per_step"] / ms_step
+        if not args.no_workloads:
+            out["workloads"] = tracer_workloads(device)
         if not args.no_cpu:
             out["cpu_baseline"] = cpu_baseline(state0, spin_h, S, args.cpu_seconds)
             out["endpoint_err"] = endpoint_errors(
@@ -376,6 +380,89 @@ def run_ours(args):
     if world > 1:
         dist.barrier(device_ids=[local])
         dist.destroy_process_group()
+    return out
+
+
+def _event_ms(fn, reps):
+    import torch
+
+    times = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    return times
+
+
+def tracer_workloads(device, warmup=2, reps=3):
+    """The tracer-shaped workloads, timed beside the headline: the full-HD
+    shadow frame (a=0.9, 80 deg, fov 25, rtol 1e-9) and the uneven batch of
+    64 cameras in one graph-captured launch, in both precision policies,
+    each with its autotuned launch shape."""
+    import torch
+
+    from blackhorizon_b200 import CameraBatch, autotune, trace_rays
+    from blackhorizon_b200.camera import PinholeCamera
+    from blackhorizon_b200.kerr import KerrSpacetime
+    from blackhorizon_b200.tracer import CameraScene
+    from blackhorizon_b200.workloads import SHADOW_FULL_HD as C
+    from blackhorizon_b200.workloads import shadow_edge, uneven_cameras
+
+    out = {"shadow_full_hd": {}, "uneven_64_cameras": {}}
+    out["shadow_full_hd"]["auto_policy"] = None
+    st = KerrSpacetime(1.0, C.spin)
+    cam = PinholeCamera.from_orbit(C.distance, C.inclination, fov_degrees=C.fov,
+                                   width=C.width, height=C.height)
+    s0 = cam.initial_states(st)
+    golden = os.path.join(ROOT, "tests", "golden", "trace_c3_status.npz")
+    ref = np.load(golden)["status"].astype(np.int32) if os.path.exists(golden) else None
+    scenes = []
+    for c in uneven_cameras():
+        ucam = PinholeCamera.from_orbit(c.distance, c.inclination, fov_degrees=c.fov,
+                                        width=c.width, height=c.height)
+        scenes.append(CameraScene(KerrSpacetime(1.0, c.spin), ucam, c.escape_radius, 0.01))
+    for prec in ("mixed", "fp64"):
+        tuned = autotune.tune_trace(st, s0, C.escape_radius, prec, C.max_steps, C.rtol, C.atol,
+                                    C.capture_margin)
+        kw = dict(max_steps=C.max_steps, rtol=C.rtol, atol=C.atol,
+                  capture_margin=C.capture_margin, precision=prec, variant=tuned["variant"])
+        for _ in range(warmup):
+            res = trace_rays(st, s0, C.escape_radius, **kw)
+        times = _event_ms(lambda: trace_rays(st, s0, C.escape_radius, **kw), reps)
+        res = trace_rays(st, s0, C.escape_radius, **kw)
+        ms = min(times)
+        entry = {"ms_per_frame": ms, "rays_per_s": C.n / (ms * 1e-3),
+                 "attempted_ray_steps_per_s": res.attempts / (ms * 1e-3),
+                 "attempts_per_ray": res.attempts / C.n, "accepted_per_ray": res.accepted / C.n,
+                 "iterations": res.iterations, "variant": tuned["variant"]}
+        if ref is not None:
+            got = res.status.cpu().numpy()
+            diff = got != ref
+            entry["status_differs_from_reference"] = float(diff.mean())
+            entry["differences_all_at_shadow_edge"] = bool(
+                np.all(shadow_edge(ref, C.width, C.height)[diff]))
+        out["shadow_full_hd"][prec] = entry
+        batch = CameraBatch(scenes, max_steps=10000, rtol=1e-8, atol=1e-10, precision=prec,
+                            variant=tuned["variant"])
+        for _ in range(warmup):
+            batch.run()
+        times = _event_ms(batch.run, reps)
+        r = batch.results()
+        ms = min(times)
+        out["uneven_64_cameras"][prec] = {
+            "rays": batch.n, "ms_per_launch": ms, "rays_per_s": batch.n / (ms * 1e-3),
+            "attempted_ray_steps_per_s": r[0].attempts / (ms * 1e-3),
+            "attempts_per_ray": r[0].attempts / batch.n,
+            "max_attempts_of_a_ray": r[0].iterations, "cuda_graph": True,
+            "variant": tuned["variant"]}
+        batch.close()
+    pick = autotune.tune_trace_policy(st, s0, C.escape_radius, C.max_steps, C.rtol, C.atol,
+                                      C.capture_margin)
+    out["shadow_full_hd"]["auto_policy"] = {"precision": pick["precision"],
+                                            "variant": pick["variant"]}
     return out
 
 

@@ -16,7 +16,7 @@ from .geodesics import (GeodesicRhs, build_state, conserved_quantities,
 from .integrators import (dormand_prince_step, error_ratio, integrate_dense,
                           propagate, rk4_step, step_factor)
 from .kerr import KerrSchildGeometry, KerrSpacetime
-from .tracer import CameraScene, RayStatus, TraceResult, trace_cameras, trace_rays
+from .tracer import CameraBatch, CameraScene, RayStatus, TraceResult, trace_cameras, trace_rays
 
 __all__ = [
     "b200_available", "get_xp", "gpu_available", "to_numpy", "xp_of",
@@ -24,6 +24,6 @@ __all__ = [
     "coordinate_velocity", "geodesic_rhs", "hamiltonian",
     "null_momentum_from_velocity", "timelike_momentum", "dormand_prince_step",
     "error_ratio", "integrate_dense", "propagate", "rk4_step", "step_factor",
-    "KerrSchildGeometry", "KerrSpacetime", "CameraScene", "RayStatus",
+    "KerrSchildGeometry", "KerrSpacetime", "CameraBatch", "CameraScene", "RayStatus",
     "TraceResult", "trace_cameras", "trace_rays",
 ]

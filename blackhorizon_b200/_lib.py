@@ -86,6 +86,10 @@ _SIGNATURES = {
                                                 ctypes.POINTER(TraceStats), _P]),
     "bh_propagate": (ctypes.c_int, [ctypes.POINTER(TraceConfig), _D, _D, _P, _P, _P,
                                     _P, _P, _I64, _I64, _P, _P]),
+    "bh_graph_trace_cameras": (ctypes.c_int, [ctypes.POINTER(TraceConfig), _I32, _I64, _P,
+                                              _P, _P, _P, _SZ, ctypes.POINTER(_P)]),
+    "bh_graph_launch": (ctypes.c_int, [_P, _P]),
+    "bh_graph_destroy": (ctypes.c_int, [_P]),
     "bh_fma_peak_launch": (ctypes.c_int, [_I32, _I64, _P, ctypes.POINTER(_I64), _P]),
 }
 

@@ -673,6 +673,68 @@ int bh_propagate(const bh_trace_config *config, double mass, double spin,
 
 }  // extern "C"
 
+// ------------------------------------------------------------ CUDA graph
+// A captured multi-camera trace: the counter reset and the persistent launch
+// of bh_trace_cameras recorded once into a CUDA graph and replayed by
+// bh_graph_launch with one call.
+
+struct bh_graph {
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+};
+
+extern "C" int bh_graph_trace_cameras(const bh_trace_config *config,
+                                      int32_t ncameras, int64_t n_rays,
+                                      double *states, int32_t *status,
+                                      int64_t *steps, void *workspace,
+                                      size_t workspace_bytes, bh_graph **out) {
+    if (!out) return invalid("out is NULL");
+    *out = nullptr;
+    cudaStream_t cap = nullptr;
+    int rc = cuda_status(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking),
+                         "bh_graph_trace_cameras stream");
+    if (rc != BH_OK) return rc;
+    rc = cuda_status(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal),
+                     "bh_graph_trace_cameras begin capture");
+    if (rc != BH_OK) {
+        cudaStreamDestroy(cap);
+        return rc;
+    }
+    const int launch_rc = bh_trace_cameras(config, ncameras, n_rays, states, status, steps,
+                                           workspace, workspace_bytes, cap);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t end = cudaStreamEndCapture(cap, &graph);
+    cudaStreamDestroy(cap);
+    if (launch_rc != BH_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return launch_rc;
+    }
+    rc = cuda_status(end, "bh_graph_trace_cameras end capture");
+    if (rc != BH_OK) return rc;
+    cudaGraphExec_t exec = nullptr;
+    rc = cuda_status(cudaGraphInstantiate(&exec, graph, 0), "bh_graph_trace_cameras instantiate");
+    if (rc != BH_OK) {
+        cudaGraphDestroy(graph);
+        return rc;
+    }
+    *out = new bh_graph{graph, exec};
+    return BH_OK;
+}
+
+extern "C" int bh_graph_launch(bh_graph *g, void *stream) {
+    if (!g) return invalid("graph is NULL");
+    return cuda_status(cudaGraphLaunch(g->exec, (cudaStream_t)stream), "bh_graph_launch");
+}
+
+extern "C" int bh_graph_destroy(bh_graph *g) {
+    if (!g) return BH_OK;
+    cudaError_t e1 = cudaGraphExecDestroy(g->exec);
+    cudaError_t e2 = cudaGraphDestroy(g->graph);
+    delete g;
+    const int rc = cuda_status(e1, "bh_graph_destroy exec");
+    return rc != BH_OK ? rc : cuda_status(e2, "bh_graph_destroy graph");
+}
+
 // ------------------------------------------------------------ no-alloc
 // bh_trace_cameras_noalloc: the multi-camera trace for callers that cannot
 // allocate device memory themselves -- for example a host application that

@@ -177,6 +177,14 @@ def propagate(spacetime, state0: Array, n_steps: int, rtol: float = 1e-8,
     acc = torch.empty(n, dtype=torch.int64, device=s.device)
     lam = torch.zeros(n, dtype=torch.float64, device=s.device)
     lib = _lib.load()
+    if variant == "auto":
+        from .autotune import tune_propagate
+
+        variant = -1
+        if n and layout == "aos":
+            variant = tune_propagate(s, spin_t, precision, min(int(n_steps), 200), rtol, atol,
+                                     float(spacetime.mass), float(spacetime.spin), max_step,
+                                     initial_step)["variant"]
     ws = workspace if workspace is not None else torch.empty(
         lib.bh_trace_workspace_bytes(), dtype=torch.uint8, device=s.device)
     cfg = make_config(1, rtol, atol, initial_step, max_step, 0.0, precision,

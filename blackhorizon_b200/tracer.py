@@ -79,7 +79,7 @@ def trace_rays(
     capture_margin: float = 1e-3,
     *,
     precision: str = "fp64",
-    variant: int = -1,
+    variant: int | str = -1,
     blocks_per_sm: int = 0,
     timeout_s: float = DEFAULT_TIMEOUT_S,
     workspace=None,
@@ -88,12 +88,28 @@ def trace_rays(
 
     The input is copied, never mutated.  Raises ValueError when an initial
     radius is at or beyond ``escape_radius`` (tracer.py:95-99) and
-    RuntimeError when the device deadline passes."""
+    RuntimeError when the device deadline passes.  ``variant="auto"`` picks
+    the launch shape with the autotuner (cached per GPU, policy and size);
+    ``precision="auto"`` picks the policy too, by timing both on a probe."""
     s, host = to_device_f64(state0, "state0")
     if s.dim() != 2 or s.shape[1] != 8:
         raise ValueError("state0 must have shape (n, 8)")
     n = s.shape[0]
     lib = _lib.load()
+    if precision == "auto":
+        from .autotune import tune_trace_policy
+
+        if n:
+            pick = tune_trace_policy(spacetime, s, escape_radius, max_steps, rtol, atol,
+                                     capture_margin, max_step)
+            precision, variant = pick["precision"], pick["variant"]
+        else:
+            precision = "fp64"
+    if variant == "auto":
+        from .autotune import tune_trace
+
+        variant = tune_trace(spacetime, s, escape_radius, precision, max_steps, rtol, atol,
+                             capture_margin, max_step)["variant"] if n else -1
     states = torch.empty_like(s)
     status = torch.empty(n, dtype=torch.int32, device=s.device)
     steps = torch.empty(n, dtype=torch.int64, device=s.device)
@@ -203,3 +219,78 @@ def trace_cameras(
         off += k
     return out
 
+
+
+class CameraBatch:
+    """Many pinhole cameras traced in one persistent launch, captured once
+    into a CUDA graph and replayed per frame.
+
+    The camera table is uploaded once into the batch's workspace and the
+    outputs are allocated once; ``run()`` replays the graph (counter reset +
+    launch) on the current stream and ``results()`` reads the counters and
+    returns one TraceResult per camera (views into the batch's buffers, which
+    the next ``run()`` overwrites)."""
+
+    def __init__(self, scenes, max_steps: int = 20000, rtol: float = 1e-9,
+                 atol: float = 1e-12, initial_step: float = 0.1, max_step: float = 2.0,
+                 min_step: float = 1e-10, *, precision: str = "fp64", variant: int = -1,
+                 blocks_per_sm: int = 0, timeout_s: float = DEFAULT_TIMEOUT_S,
+                 graph: bool = True):
+        if not scenes:
+            raise ValueError("need at least one camera")
+        self.lib = _lib.load()
+        self.scenes = list(scenes)
+        self.table = camera_table(self.scenes)
+        self.nc = len(self.scenes)
+        dev = torch.device("cuda", torch.cuda.current_device())
+        self.wsb = self.lib.bh_trace_cameras_workspace_bytes(self.nc)
+        self.ws = torch.empty(self.wsb, dtype=torch.uint8, device=dev)
+        n_rays = _lib._I64(0)
+        _lib.check(self.lib.bh_camera_table_upload(self.table, self.nc, ptr(self.ws), self.wsb,
+                                                   n_rays, stream_handle()), "CameraBatch")
+        self.n = int(n_rays.value)
+        self.states = torch.empty((self.n, 8), dtype=torch.float64, device=dev)
+        self.status = torch.empty(self.n, dtype=torch.int32, device=dev)
+        self.steps = torch.empty(self.n, dtype=torch.int64, device=dev)
+        self.cfg = make_config(max_steps, rtol, atol, initial_step, max_step, min_step,
+                               precision, "aos", timeout_s, variant, blocks_per_sm)
+        self.graph = None
+        if graph:
+            torch.cuda.current_stream().synchronize()
+            g = _lib._P()
+            _lib.check(self.lib.bh_graph_trace_cameras(
+                self.cfg, self.nc, self.n, ptr(self.states), ptr(self.status), ptr(self.steps),
+                ptr(self.ws), self.wsb, g), "CameraBatch capture")
+            self.graph = g
+
+    def run(self) -> None:
+        """Trace every camera's rays (asynchronous on the current stream)."""
+        if self.graph is not None:
+            _lib.check(self.lib.bh_graph_launch(self.graph, stream_handle()), "CameraBatch")
+        else:
+            _lib.check(self.lib.bh_trace_cameras(
+                self.cfg, self.nc, self.n, ptr(self.states), ptr(self.status), ptr(self.steps),
+                ptr(self.ws), self.wsb, stream_handle()), "CameraBatch")
+
+    def results(self):
+        st = _stats(self.lib, self.ws, stream_handle(), "CameraBatch")
+        out, off = [], 0
+        for cs in self.scenes:
+            k = int(cs.camera.width) * int(cs.camera.height)
+            out.append(TraceResult(states=self.states[off:off + k], status=self.status[off:off + k],
+                                   steps=self.steps[off:off + k], iterations=int(st.iterations),
+                                   attempts=int(st.attempts), accepted=int(st.accepted)))
+            off += k
+        return out
+
+    def close(self) -> None:
+        if self.graph is not None:
+            torch.cuda.current_stream().synchronize()
+            _lib.check(self.lib.bh_graph_destroy(self.graph), "CameraBatch")
+            self.graph = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

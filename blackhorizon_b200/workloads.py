@@ -133,3 +133,15 @@ def ks_radius_np(states, spin):
 # the horizon during a no-termination run; their coordinates run toward the
 # singularity and are excluded (and counted) when end points are compared.
 PLUNGE_RADIUS = 2.5
+
+
+def shadow_edge(status, width: int, height: int):
+    """Pixels of a row-major status image with a 4-neighbour of another status
+    (the shadow edge, where classification is chaotic)."""
+    st = np.asarray(status).reshape(height, width)
+    e = np.zeros_like(st, dtype=bool)
+    e[1:, :] |= st[1:, :] != st[:-1, :]
+    e[:-1, :] |= st[:-1, :] != st[1:, :]
+    e[:, 1:] |= st[:, 1:] != st[:, :-1]
+    e[:, :-1] |= st[:, :-1] != st[:, 1:]
+    return e.reshape(-1)

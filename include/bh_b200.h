@@ -214,6 +214,20 @@ int bh_trace_cameras(const bh_trace_config *config, int32_t ncameras,
                      int64_t *steps, void *workspace, size_t workspace_bytes,
                      void *stream);
 
+/* The counter reset and persistent launch of bh_trace_cameras captured once
+ * into a CUDA graph (camera table already uploaded to `workspace`), then
+ * replayed with one bh_graph_launch per frame; read the counters with
+ * bh_trace_stats_read after each replay.  The graph keeps the pointers it was
+ * captured with.  bh_graph_destroy releases it.  No counterpart in the
+ * reference, which launches ~60 array kernels per RHS evaluation. */
+typedef struct bh_graph bh_graph;
+int bh_graph_trace_cameras(const bh_trace_config *config, int32_t ncameras,
+                           int64_t n_rays, double *states, int32_t *status,
+                           int64_t *steps, void *workspace,
+                           size_t workspace_bytes, bh_graph **out);
+int bh_graph_launch(bh_graph *graph, void *stream);
+int bh_graph_destroy(bh_graph *graph);
+
 /* bh_trace_cameras without a caller-owned workspace, for callers that cannot
  * allocate device memory (a host application that owns all GPU memory
  * through its own fixed pool, or code under a hard memory budget).  No
