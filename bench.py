@@ -373,6 +373,7 @@ def run_ours(args):
             out["speedup_vs_fp64"] = fp64["ms_per_step"] / ms_step
         if not args.no_workloads:
             out["workloads"] = tracer_workloads(device)
+            out["workloads"]["differentiable_256x256"] = adjoint_workload(device)
         if not args.no_cpu:
             out["cpu_baseline"] = cpu_baseline(state0, spin_h, S, args.cpu_seconds)
             out["endpoint_err"] = endpoint_errors(
@@ -463,6 +464,84 @@ def tracer_workloads(device, warmup=2, reps=3):
                                       C.capture_margin)
     out["shadow_full_hd"]["auto_policy"] = {"precision": pick["precision"],
                                             "variant": pick["variant"]}
+    return out
+
+
+def adjoint_workload(device, warmup=1, reps=3):
+    """Differentiable tracing: 256x256 rays, a=0.7, inclination 60 deg,
+    r_obs=50 M, fov 30 deg, rtol 1e-9; loss = squared error of the escaped
+    rays' celestial angles against a target frame at a=0.9; gradients with
+    respect to spin, inclination, yaw and pitch through the discrete adjoint
+    (checkpoint every 64 accepted steps).  Times the plain forward trace,
+    the taped forward and the adjoint sweep, and checks the gradients against
+    frozen-sequence central differences (h = 1e-6, float64)."""
+    import torch
+
+    from blackhorizon_b200 import trace_rays
+    from blackhorizon_b200.adjoint import (adjoint, angle_loss, celestial_angles,
+                                           fly_camera_rays, orbit_look_at, pixel_grid,
+                                           replay, trace_rays_differentiable, trace_with_tape)
+    from blackhorizon_b200.kerr import KerrSpacetime
+    from blackhorizon_b200.workloads import DIFFERENTIABLE as C
+
+    t = lambda x, g=False: torch.tensor(x, dtype=torch.float64, device=device,  # noqa: E731
+                                        requires_grad=g)
+    yaw0, pitch0 = orbit_look_at(C.distance, C.inclination)
+    u, v = pixel_grid(C.width, C.height, C.fov, device)
+    kw = dict(max_steps=C.max_steps, rtol=C.rtol, atol=C.atol, capture_margin=C.capture_margin)
+    y_tgt = fly_camera_rays(t(0.9), t(C.inclination), t(yaw0), t(pitch0), C.distance, u, v)
+    tgt = trace_rays(KerrSpacetime(1.0, 0.9), y_tgt, C.escape_radius, **kw)
+    th_t, ph_t = celestial_angles(t(0.9), tgt.states)
+    out = {"rays": C.n, "checkpoint_every": 64}
+    for prec in ("fp64", "mixed"):
+        params = [t(x, True) for x in (C.spin, C.inclination, yaw0, pitch0)]
+        s0 = fly_camera_rays(*params, C.distance, u, v)
+        st = KerrSpacetime(1.0, C.spin)
+        s0d = s0.detach()
+        fwd = lambda: trace_rays(st, s0d, C.escape_radius, precision=prec, **kw)  # noqa: E731
+        for _ in range(warmup):
+            res = fwd()
+        ms_fwd = min(_event_ms(fwd, reps))
+        taped = lambda: trace_with_tape(st, s0d, C.escape_radius, precision=prec,  # noqa: E731
+                                        checkpoint_every=64, **kw)
+        states, status, steps, tape = taped()
+        ms_tape = min(_event_ms(taped, reps))
+        sv = states.detach().requires_grad_(True)
+        mask = ((status == 2) & (tgt.status == 2)).to(torch.float64)
+        th, ph = celestial_angles(t(C.spin), sv)
+        angle_loss(th, ph, th_t, ph_t, mask).backward()
+        g_states = sv.grad.detach()
+        ms_adj = min(_event_ms(lambda: adjoint(tape, g_states), reps))
+        # Full gradient through autograd (camera -> adjoint -> angles).
+        states2, status2, _ = trace_rays_differentiable(params[0], s0, C.escape_radius,
+                                                        precision=prec, checkpoint_every=64, **kw)
+        th2, ph2 = celestial_angles(params[0], states2)
+        loss = angle_loss(th2, ph2, th_t, ph_t, mask)
+        loss.backward()
+        grads = [float(p.grad) for p in params]
+        entry = {"forward_ms": ms_fwd, "taped_forward_ms": ms_tape, "adjoint_ms": ms_adj,
+                 "adjoint_over_forward": ms_adj / ms_fwd,
+                 "taped_forward_plus_adjoint_over_forward": (ms_tape + ms_adj) / ms_fwd,
+                 "accepted_steps_per_ray": float(steps.double().mean()),
+                 "loss": float(loss), "grad": dict(zip(("spin", "inclination", "yaw", "pitch"),
+                                                       grads))}
+        if prec == "fp64":
+            base = [C.spin, C.inclination, yaw0, pitch0]
+            fd = []
+            for k in range(4):
+                vals = []
+                for sgn in (1, -1):
+                    p = list(base)
+                    p[k] += sgn * 1e-6
+                    y0 = fly_camera_rays(*(t(x) for x in p), C.distance, u, v)
+                    yN = replay(tape, y0, spin=p[0])
+                    a_, b_ = celestial_angles(t(p[0]), yN)
+                    vals.append(float(angle_loss(a_, b_, th_t, ph_t, mask)))
+                fd.append((vals[0] - vals[1]) / 2e-6)
+            entry["fd_grad"] = dict(zip(("spin", "inclination", "yaw", "pitch"), fd))
+            entry["grad_rel_err_vs_fd"] = max(abs(g - f) / max(abs(f), 1e-12)
+                                              for g, f in zip(grads, fd))
+        out[prec] = entry
     return out
 
 

@@ -20,6 +20,7 @@ BH_ERR_CUDA = -2
 BH_ERR_TIMEOUT = -3
 BH_ERR_ESCAPE_RADIUS = -4
 BH_ERR_WORKSPACE = -5
+BH_ERR_TAPE = -6
 
 PRECISION = {"fp64": 0, "mixed": 1}
 LAYOUT = {"aos": 0, "soa": 1}
@@ -90,6 +91,10 @@ _SIGNATURES = {
                                               _P, _P, _P, _SZ, ctypes.POINTER(_P)]),
     "bh_graph_launch": (ctypes.c_int, [_P, _P]),
     "bh_graph_destroy": (ctypes.c_int, [_P]),
+    "bh_trace_tape": (ctypes.c_int, [ctypes.POINTER(TraceConfig), ctypes.POINTER(Scene),
+                                     _P, _P, _P, _P, _I64, _P, _P, _I64, _I32, _P, _P]),
+    "bh_adjoint": (ctypes.c_int, [_I32, _D, _D, _P, _P, _P, _I64, _I32, _P, _P, _P, _I64, _P]),
+    "bh_replay": (ctypes.c_int, [_I32, _D, _D, _P, _P, _P, _I64, _P, _I64, _P]),
     "bh_fma_peak_launch": (ctypes.c_int, [_I32, _I64, _P, ctypes.POINTER(_I64), _P]),
 }
 

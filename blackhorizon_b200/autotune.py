@@ -166,8 +166,9 @@ def tune_trace(spacetime, state0, escape_radius: float, precision: str,
     from .integrators import make_config
 
     n = state0.shape[0]
+    extra = f"rtol={rtol:.1e}"
     if not force:
-        hit = lookup("trace", precision, n)
+        hit = lookup("trace", precision, n, extra)
         if hit is not None:
             return hit
     lib = _lib.load()
@@ -192,7 +193,7 @@ def tune_trace(spacetime, state0, escape_radius: float, precision: str,
     result = {"variant": best["variant"], "blocks_per_sm": 0, "ms": best_ms,
               "probe": f"{m} of {n} rays",
               "table": [{"variant": c["variant"], "ms": round(t, 4)} for t, c in timings]}
-    store("trace", precision, n, result)
+    store("trace", precision, n, result, extra)
     return result
 
 

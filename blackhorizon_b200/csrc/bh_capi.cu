@@ -332,6 +332,49 @@ static TraceArgs base_args(const bh_trace_config *c) {
     return a;
 }
 
+
+// trace_rays for one scene, optionally recording the accepted-step tape
+// (h_tape != nullptr).
+int bh_trace_with_tape(const bh_trace_config *config, const bh_scene *scene,
+                       const double *state0, double *states, int32_t *status,
+                       int64_t *steps, int64_t n, void *workspace, void *stream,
+                       double *h_tape, double *ckpt, int64_t tape_cap, int ckpt_every) {
+    int rc = config_ok(config);
+    if (rc != BH_OK) return rc;
+    if (!scene) return invalid("scene is NULL");
+    if (!kerr_ok(scene->mass, scene->spin)) return invalid("Kerr bound violated or mass not positive");
+    if (n < 0) return invalid("n must be >= 0");
+    if (!workspace || !aligned(workspace, 256)) {
+        set_error("workspace must be a 256-byte aligned device buffer of bh_trace_workspace_bytes()");
+        return BH_ERR_WORKSPACE;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    rc = cuda_status(cudaMemsetAsync(workspace, 0, sizeof(TraceWorkspace), s), "bh_trace workspace reset");
+    if (rc != BH_OK || n == 0) return rc;
+    if (!state0 || !states || !status || !steps) return invalid("NULL pointer argument");
+    if (config->layout == BH_LAYOUT_AOS && (!aligned(state0, 16) || !aligned(states, 16)))
+        return invalid("state buffers must be 16-byte aligned");
+    TraceArgs a = base_args(config);
+    a.state0 = state0;
+    a.source = 0;
+    a.mass = scene->mass;
+    a.spin = scene->spin;
+    a.capture_radius = scene->capture_radius;
+    a.escape_radius = scene->escape_radius;
+    a.states = states;
+    a.status = status;
+    a.steps = steps;
+    a.n = n;
+    a.ws = reinterpret_cast<TraceWorkspace *>(workspace);
+    a.h_tape = h_tape;
+    a.ckpt = ckpt;
+    a.tape_cap = tape_cap;
+    a.ckpt_every = ckpt_every;
+    return cuda_status(launch_trace(a, config->precision, config->variant,
+                                    config->blocks_per_sm, s),
+                       "bh_trace launch");
+}
+
 }  // namespace bh
 
 using namespace bh;
@@ -348,6 +391,7 @@ const char *bh_status_string(int status) {
         case BH_ERR_TIMEOUT: return "trace deadline exceeded";
         case BH_ERR_ESCAPE_RADIUS: return "escape_radius must exceed all initial radii";
         case BH_ERR_WORKSPACE: return "workspace missing, too small or misaligned";
+        case BH_ERR_TAPE: return "a ray took more accepted steps than the tape holds";
         default: return "unknown status";
     }
 }
@@ -511,36 +555,8 @@ size_t bh_trace_cameras_workspace_bytes(int32_t ncameras) {
 int bh_trace(const bh_trace_config *config, const bh_scene *scene,
              const double *state0, double *states, int32_t *status,
              int64_t *steps, int64_t n, void *workspace, void *stream) {
-    int rc = config_ok(config);
-    if (rc != BH_OK) return rc;
-    if (!scene) return invalid("scene is NULL");
-    if (!kerr_ok(scene->mass, scene->spin)) return invalid("Kerr bound violated or mass not positive");
-    if (n < 0) return invalid("n must be >= 0");
-    if (!workspace || !aligned(workspace, 256)) {
-        set_error("workspace must be a 256-byte aligned device buffer of bh_trace_workspace_bytes()");
-        return BH_ERR_WORKSPACE;
-    }
-    cudaStream_t s = (cudaStream_t)stream;
-    rc = cuda_status(cudaMemsetAsync(workspace, 0, sizeof(TraceWorkspace), s), "bh_trace workspace reset");
-    if (rc != BH_OK || n == 0) return rc;
-    if (!state0 || !states || !status || !steps) return invalid("NULL pointer argument");
-    if (config->layout == BH_LAYOUT_AOS && (!aligned(state0, 16) || !aligned(states, 16)))
-        return invalid("state buffers must be 16-byte aligned");
-    TraceArgs a = base_args(config);
-    a.state0 = state0;
-    a.source = 0;
-    a.mass = scene->mass;
-    a.spin = scene->spin;
-    a.capture_radius = scene->capture_radius;
-    a.escape_radius = scene->escape_radius;
-    a.states = states;
-    a.status = status;
-    a.steps = steps;
-    a.n = n;
-    a.ws = reinterpret_cast<TraceWorkspace *>(workspace);
-    return cuda_status(launch_trace(a, config->precision, config->variant,
-                                    config->blocks_per_sm, s),
-                       "bh_trace launch");
+    return bh_trace_with_tape(config, scene, state0, states, status, steps, n, workspace,
+                              stream, nullptr, nullptr, 0, 1);
 }
 
 int bh_camera_table_upload(const bh_camera *cameras, int32_t ncameras,
@@ -631,6 +647,10 @@ int bh_trace_stats_read(const void *workspace, bh_trace_stats *out, void *stream
     if (w.timed_out) {
         set_error("trace deadline exceeded");
         return BH_ERR_TIMEOUT;
+    }
+    if (w.tape_overflow) {
+        set_error("a ray took more accepted steps than the tape capacity");
+        return BH_ERR_TAPE;
     }
     return BH_OK;
 }

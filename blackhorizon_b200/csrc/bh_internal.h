@@ -18,6 +18,7 @@ struct alignas(256) TraceWorkspace {
     unsigned long long accepted;    // sum of accepted steps
     int timed_out;
     int bad_rays;
+    int tape_overflow;  // rays with more accepted steps than the tape holds
 };
 static_assert(sizeof(TraceWorkspace) == 256, "workspace header is 256 bytes");
 
@@ -54,6 +55,13 @@ struct TraceArgs {
     long long max_attempts;  // trace: 4 * max_steps; propagate: n_steps
     long long timeout_ns;
     TraceWorkspace *ws;
+    // optional tape of the accepted steps (trace only): step sizes
+    // (n x tape_cap) and float64 states before every ckpt_every-th accepted
+    // step (n x ceil(tape_cap / ckpt_every) x 8)
+    double *h_tape;
+    double *ckpt;
+    long long tape_cap;
+    int ckpt_every;
 };
 
 // Launch-shape variants of the trace / propagate kernels: threads per block
@@ -77,6 +85,12 @@ cudaError_t launch_trace(const TraceArgs &args, int precision, int variant,
                          int blocks_per_sm, cudaStream_t stream);
 cudaError_t launch_propagate(const TraceArgs &args, int precision, int variant,
                              int blocks_per_sm, cudaStream_t stream);
+
+// bh_trace with an optional tape of the accepted steps (bh_capi.cu).
+int bh_trace_with_tape(const bh_trace_config *config, const bh_scene *scene,
+                       const double *state0, double *states, int32_t *status,
+                       int64_t *steps, int64_t n, void *workspace, void *stream,
+                       double *h_tape, double *ckpt, int64_t tape_cap, int ckpt_every);
 
 // Records a message for bh_last_error on this host thread.
 void set_error(const char *fmt, ...);

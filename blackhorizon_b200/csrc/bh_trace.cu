@@ -276,6 +276,21 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args
                 acc[l] = ratio[l] <= 1.0;
                 ++attempts[l];
                 RayState yl = ys.get(l);
+                if (acc[l] && args.h_tape) {
+                    // Tape of the accepted step sequence for the adjoint.
+                    const long long s = steps[l];
+                    if (s < args.tape_cap) {
+                        args.h_tape[ray[l] * args.tape_cap + s] = h[l];
+                        if (s % args.ckpt_every == 0) {
+                            const long long nck = (args.tape_cap + args.ckpt_every - 1) / args.ckpt_every;
+                            double *c = args.ckpt + (ray[l] * nck + s / args.ckpt_every) * 8;
+                            c[0] = yl.t; c[1] = yl.x; c[2] = yl.y; c[3] = yl.z;
+                            c[4] = yl.pt; c[5] = yl.px; c[6] = yl.py; c[7] = yl.pz;
+                        }
+                    } else {
+                        atomicExch(&ws->tape_overflow, 1);
+                    }
+                }
                 if (acc[l]) {
                     commit<V>(yl, yw, a, l, h[l]);
                     ys.set(l, yl);

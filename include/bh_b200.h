@@ -32,7 +32,8 @@ typedef enum {
     BH_ERR_CUDA = -2,             /* a CUDA runtime call failed; see bh_last_error */
     BH_ERR_TIMEOUT = -3,          /* the trace deadline passed before every ray finished */
     BH_ERR_ESCAPE_RADIUS = -4,    /* an initial radius is >= escape_radius (tracer.py:95-99) */
-    BH_ERR_WORKSPACE = -5         /* workspace missing, too small or misaligned */
+    BH_ERR_WORKSPACE = -5,        /* workspace missing, too small or misaligned */
+    BH_ERR_TAPE = -6              /* a ray took more accepted steps than the tape holds */
 } bh_status;
 
 /* Per-ray termination codes: blackhorizon/tracer.py:21-30 (RayStatus). */
@@ -263,6 +264,41 @@ int bh_propagate(const bh_trace_config *config, double mass, double spin,
                  const double *spin_of_ray, double *states, double *h,
                  double *lam, int64_t *accepted, int64_t n, int64_t n_steps,
                  void *workspace, void *stream);
+
+/* ------------------------------------------------------------ adjoint */
+
+/* bh_trace that also records, per ray, the accepted step sizes (h_tape, n x
+ * capacity doubles, ray-major) and the float64 state before every
+ * checkpoint_every-th accepted step (checkpoints, n x ceil(capacity /
+ * checkpoint_every) x 8 doubles).  checkpoint_every in [1, 64].  A ray with
+ * more than `capacity` accepted steps makes bh_trace_stats_read return
+ * BH_ERR_TAPE.  No counterpart in the reference (which differentiates
+ * nothing); the tape is the frozen step sequence its trace took. */
+int bh_trace_tape(const bh_trace_config *config, const bh_scene *scene,
+                  const double *state0, double *states, int32_t *status,
+                  int64_t *steps, int64_t n, double *h_tape, double *checkpoints,
+                  int64_t capacity, int32_t checkpoint_every, void *workspace,
+                  void *stream);
+
+/* Discrete adjoint of the taped accepted-step sequence: given dL/d(final
+ * state) (n,8), writes dL/d(initial state) (n,8) and dL/d(spin) per ray (n,)
+ * for the fifth-order DP5 map with the step sizes frozen.  Each segment of
+ * checkpoint_every steps is replayed forward from its checkpoint, then swept
+ * backward with the stages recomputed (BH_PRECISION_FP64: float64 stage
+ * arithmetic; BH_PRECISION_MIXED: float32 stage arithmetic, float64
+ * cotangents).  No counterpart in the reference. */
+int bh_adjoint(int32_t precision, double mass, double spin, const double *h_tape,
+               const double *checkpoints, const int64_t *steps, int64_t capacity,
+               int32_t checkpoint_every, const double *grad_states,
+               double *grad_state0, double *grad_spin, int64_t n, void *stream);
+
+/* The frozen-sequence map the adjoint differentiates: steps[i] accepted DP5
+ * steps of ray i from state0 with the taped sizes, no error control.  Used
+ * for finite-difference checks of the adjoint.  No counterpart in the
+ * reference. */
+int bh_replay(int32_t precision, double mass, double spin, const double *state0,
+              const double *h_tape, const int64_t *steps, int64_t capacity,
+              double *states, int64_t n, void *stream);
 
 /* ------------------------------------------------------------ diagnostics */
 
