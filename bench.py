@@ -71,7 +71,12 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-workloads", action="store_true",
-                    help="skip the full-HD frame and the 64-camera batch")
+                    help="skip the full-HD frame, the 64-camera batch and the adjoint")
+    ap.add_argument("--profile-case", choices=("trace", "adjoint"), default=None,
+                    help="run one small untimed case of that kernel (for ncu captures): "
+                         "trace = the 1920x1080 frame (2 warm-up launches, then 1); "
+                         "adjoint = the 256x256 differentiable frame with a 2000-step "
+                         "tape (1 warm-up sweep, then 1)")
     return ap.parse_args()
 
 
@@ -527,20 +532,22 @@ def adjoint_workload(device, warmup=1, reps=3):
                                                        grads))}
         if prec == "fp64":
             base = [C.spin, C.inclination, yaw0, pitch0]
-            fd = []
-            for k in range(4):
-                vals = []
-                for sgn in (1, -1):
-                    p = list(base)
-                    p[k] += sgn * 1e-6
-                    y0 = fly_camera_rays(*(t(x) for x in p), C.distance, u, v)
-                    yN = replay(tape, y0, spin=p[0])
-                    a_, b_ = celestial_angles(t(p[0]), yN)
-                    vals.append(float(angle_loss(a_, b_, th_t, ph_t, mask)))
-                fd.append((vals[0] - vals[1]) / 2e-6)
-            entry["fd_grad"] = dict(zip(("spin", "inclination", "yaw", "pitch"), fd))
-            entry["grad_rel_err_vs_fd"] = max(abs(g - f) / max(abs(f), 1e-12)
-                                              for g, f in zip(grads, fd))
+            names = ("spin", "inclination", "yaw", "pitch")
+            for step in (1e-6, 1e-7):
+                fd = []
+                for k in range(4):
+                    vals = []
+                    for sgn in (1, -1):
+                        p = list(base)
+                        p[k] += sgn * step
+                        y0 = fly_camera_rays(*(t(x) for x in p), C.distance, u, v)
+                        yN = replay(tape, y0, spin=p[0])
+                        a_, b_ = celestial_angles(t(p[0]), yN)
+                        vals.append(float(angle_loss(a_, b_, th_t, ph_t, mask)))
+                    fd.append((vals[0] - vals[1]) / (2 * step))
+                entry[f"fd_grad_h{step:.0e}"] = dict(zip(names, fd))
+                entry[f"grad_rel_err_vs_fd_h{step:.0e}"] = dict(
+                    zip(names, (abs(g - f) / max(abs(f), 1e-12) for g, f in zip(grads, fd))))
         out[prec] = entry
     return out
 
@@ -654,8 +661,51 @@ def run_reference(args):
     }
 
 
+def profile_case(args):
+    """One small invocation of a kernel for a profiler; prints nothing."""
+    import torch
+
+    from blackhorizon_b200 import trace_rays
+    from blackhorizon_b200.adjoint import (adjoint, fly_camera_rays, orbit_look_at,
+                                           pixel_grid, trace_with_tape)
+    from blackhorizon_b200.camera import PinholeCamera
+    from blackhorizon_b200.kerr import KerrSpacetime
+    from blackhorizon_b200.workloads import DIFFERENTIABLE, SHADOW_FULL_HD
+
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(0)
+    prec = args.precision
+    if args.profile_case == "trace":
+        C = SHADOW_FULL_HD
+        st = KerrSpacetime(1.0, C.spin)
+        cam = PinholeCamera.from_orbit(C.distance, C.inclination, fov_degrees=C.fov,
+                                       width=C.width, height=C.height)
+        s0 = cam.initial_states(st)
+        for _ in range(3):
+            trace_rays(st, s0, C.escape_radius, max_steps=C.max_steps, rtol=C.rtol,
+                       atol=C.atol, capture_margin=C.capture_margin, precision=prec,
+                       variant=args.variant)
+    else:
+        C = DIFFERENTIABLE
+        t = lambda x: torch.tensor(x, dtype=torch.float64, device=device)  # noqa: E731
+        yaw0, pitch0 = orbit_look_at(C.distance, C.inclination)
+        u, v = pixel_grid(C.width, C.height, C.fov, device)
+        s0 = fly_camera_rays(t(C.spin), t(C.inclination), t(yaw0), t(pitch0), C.distance, u, v)
+        _, status, _, tape = trace_with_tape(KerrSpacetime(1.0, C.spin), s0, C.escape_radius,
+                                             max_steps=2000, rtol=C.rtol, atol=C.atol,
+                                             capture_margin=C.capture_margin, precision=prec,
+                                             checkpoint_every=64)
+        g = torch.randn((C.n, 8), dtype=torch.float64, device=device) * (status == 2)[:, None]
+        for _ in range(2):
+            adjoint(tape, g)
+    torch.cuda.synchronize()
+
+
 def main():
     args = parse()
+    if args.profile_case:
+        profile_case(args)
+        return
     if args.impl == "reference":
         out = run_reference(args)
     else:
