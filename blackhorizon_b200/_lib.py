@@ -55,6 +55,12 @@ class TraceStats(ctypes.Structure):
                 ("timed_out", _I32), ("bad_rays", _I32)]
 
 
+class TileStats(ctypes.Structure):
+    _fields_ = [("iterations", _I64), ("attempts", _I64), ("accepted", _I64),
+                ("crossings", _I64), ("disk_hits", _I64), ("rounds", _I32),
+                ("timed_out", _I32)]
+
+
 _SIGNATURES = {
     "bh_abi_version": (ctypes.c_int, []),
     "bh_status_string": (ctypes.c_char_p, [ctypes.c_int]),
@@ -95,6 +101,10 @@ _SIGNATURES = {
                                      _P, _P, _P, _P, _I64, _P, _P, _I64, _I32, _P, _P]),
     "bh_adjoint": (ctypes.c_int, [_I32, _D, _D, _P, _P, _P, _I64, _I32, _P, _P, _P, _I64, _P]),
     "bh_replay": (ctypes.c_int, [_I32, _D, _D, _P, _P, _P, _I64, _P, _I64, _P]),
+    "bh_trace_tile_workspace_bytes": (_SZ, [_I64]),
+    "bh_trace_tile": (ctypes.c_int, [ctypes.POINTER(TraceConfig), ctypes.POINTER(Scene), _D, _D,
+                                     _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _SZ,
+                                     ctypes.POINTER(TileStats), _P]),
     "bh_fma_peak_launch": (ctypes.c_int, [_I32, _I64, _P, ctypes.POINTER(_I64), _P]),
 }
 

@@ -92,6 +92,67 @@ int bh_trace_with_tape(const bh_trace_config *config, const bh_scene *scene,
                        int64_t *steps, int64_t n, void *workspace, void *stream,
                        double *h_tape, double *ckpt, int64_t tape_cap, int ckpt_every);
 
+// ------------------------------------------------------------ tile tracer
+// A ray parked at an accepted step whose z changed sign, for refinement.
+struct TileCrossing {
+    double y0[8];        // state before the step
+    double y1[8];        // state after the step
+    double h;            // the step's size
+    double h_next;       // controller step size after the step
+    long long steps;     // accepted steps before the step
+    long long attempts;  // attempts including the step
+    long long ray;
+};
+static_assert(sizeof(TileCrossing) == 168, "crossing record is 168 bytes");
+
+// A ray that continues after a crossing outside the disk.
+struct TileResume {
+    double y[8];
+    double h;
+    long long steps, attempts, ray;
+};
+static_assert(sizeof(TileResume) == 96, "resume record is 96 bytes");
+
+// Counters of a tile trace.  Round r uses the parity-(r & 1) queue head and
+// crossing count and reads the parity-(r & 1) resume count (written by the
+// refinement of round r - 1); round r's tracing kernel zeroes the other
+// parity's counters before round r's refinement and round r + 1 use them.
+struct alignas(256) TileWorkspace {
+    unsigned long long queue_head[2];
+    unsigned long long n_cross[2];
+    unsigned long long n_resume[2];
+    long long iterations;  // max attempts over finalised rays
+    unsigned long long attempts, accepted, crossings, disk_hits;
+    int timed_out;
+};
+static_assert(sizeof(TileWorkspace) == 256, "tile workspace header is 256 bytes");
+
+struct TileArgs {
+    const double *state0;
+    long long n;
+    int layout;
+    int round;  // 0: rays from state0; r > 0: resume records of parity r & 1
+    int flush;  // finalise every ray in flight as IN_FLIGHT without stepping
+    double mass, spin, capture_radius, escape_radius;
+    double disk_inner, disk_outer;  // disk_outer <= 0: no crossing tests
+    double rtol, atol, initial_step, max_step;
+    long long max_steps, max_attempts, saturate_steps;
+    long long timeout_ns;
+    TileCrossing *cross;  // capacity n
+    TileResume *resume;   // capacity n
+    double *states;
+    int32_t *status;
+    int64_t *steps;
+    double *hit_pos, *hit_mom, *escape_dir;
+    int8_t *saturated;
+    TileWorkspace *ws;
+};
+
+int tile_default_variant(int precision);
+cudaError_t launch_tile(const TileArgs &args, int precision, int variant,
+                        int blocks_per_sm, cudaStream_t stream);
+cudaError_t launch_refine(const TileArgs &args, cudaStream_t stream);
+
 // Records a message for bh_last_error on this host thread.
 void set_error(const char *fmt, ...);
 

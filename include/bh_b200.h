@@ -42,7 +42,8 @@ enum {
     BH_RAY_CAPTURED = 1,
     BH_RAY_ESCAPED = 2,
     BH_RAY_MAX_STEPS = 3,
-    BH_RAY_FAILED = 4
+    BH_RAY_FAILED = 4,
+    BH_RAY_DISK = 5  /* ended on the equatorial disk (bh_trace_tile only) */
 };
 
 typedef enum {
@@ -299,6 +300,50 @@ int bh_adjoint(int32_t precision, double mass, double spin, const double *h_tape
 int bh_replay(int32_t precision, double mass, double spin, const double *state0,
               const double *h_tape, const int64_t *steps, int64_t capacity,
               double *states, int64_t n, void *stream);
+
+/* ------------------------------------------------------------ offline tile */
+
+/* Counters of one bh_trace_tile call. */
+typedef struct {
+    int64_t iterations; /* max attempts over rays */
+    int64_t attempts;   /* sum of attempts */
+    int64_t accepted;   /* sum of accepted steps */
+    int64_t crossings;  /* equatorial crossings refined */
+    int64_t disk_hits;  /* rays ended on the disk */
+    int32_t rounds;     /* trace + refine rounds */
+    int32_t timed_out;  /* 1: rays were left BH_RAY_IN_FLIGHT at the deadline */
+} bh_tile_stats;
+
+/* Device workspace of bh_trace_tile for n rays: a 256-byte header, n
+ * crossing records (168 B) and n resume records (96 B). */
+size_t bh_trace_tile_workspace_bytes(int64_t n);
+
+/* blackhorizon/offline/render.py:184-309 (_trace_tile, exterior cameras)
+ * with the crossing refinement of render.py:312-349 (_refine_crossings).
+ * Per ray, before each attempt: captured (r <= scene->capture_radius),
+ * escaped (r >= scene->escape_radius) or out of budget (steps >=
+ * config->max_steps, BH_RAY_MAX_STEPS); then one DP5(4) attempt with
+ * config->rtol and config->atol (the reference passes atol = rtol * 1e-3);
+ * an accepted step whose z changes sign is located on the RK4 substep from
+ * the pre-step state at the reference's bisection resolution (fraction
+ * (L + 1/2) 2^-40 of the step), and a crossing radius in [disk_inner,
+ * disk_outer] ends the ray with BH_RAY_DISK, its state left before the step.
+ * disk_outer <= 0 disables crossings.  Rays in flight after 4 max_steps
+ * attempts stay BH_RAY_IN_FLIGHT (render.py:223).  config->min_step is not
+ * used.  Outputs per ray (device buffers): states (n, 8) in config->layout,
+ * status, accepted steps, hit_positions / hit_momenta (n, 3; zero unless
+ * DISK), escape_directions (n, 3; render.py:164-181, zero unless ESCAPED),
+ * saturated (render.py:289-291: MAX_STEPS or steps >= floor(0.85
+ * max_steps)).  The float64 refinement runs between rounds of the
+ * persistent tracer, so the call synchronises `stream` once per round and
+ * returns when the tile is done; stats may be NULL. */
+int bh_trace_tile(const bh_trace_config *config, const bh_scene *scene,
+                  double disk_inner, double disk_outer, const double *state0,
+                  int64_t n, double *states, int32_t *status, int64_t *steps,
+                  double *hit_positions, double *hit_momenta,
+                  double *escape_directions, int8_t *saturated,
+                  void *workspace, size_t workspace_bytes,
+                  bh_tile_stats *stats, void *stream);
 
 /* ------------------------------------------------------------ diagnostics */
 

@@ -517,6 +517,109 @@ void bho_propagate_to(double mass, double spin, const double *spins,
     bho_parallel_for(n, nthreads, 2, to_range, &c);
 }
 
+/* render.py:312-349 (_refine_crossings) for one ray: 40 bisections of the
+ * fraction of the step at which an RK4 substep from y0 crosses z = 0. */
+static int refine_crossing(double m, double a, const double y0[8], double h_full,
+                           double r_in, double r_out, double y_cross[8]) {
+    double low = 0.0, high = 1.0;
+    for (int it = 0; it < 40; ++it) {
+        const double mid = 0.5 * (low + high);
+        double ym[8];
+        bho_rk4_step(m, a, y0, h_full * mid, ym);
+        const int same_side = ym[3] * y0[3] > 0.0;
+        if (same_side) low = mid; else high = mid;
+    }
+    bho_rk4_step(m, a, y0, h_full * (0.5 * (low + high)), y_cross);
+    bho_geometry_t g;
+    bho_geometry(m, a, y_cross[1], y_cross[2], y_cross[3], 0, &g);
+    return g.r >= r_in && g.r <= r_out;
+}
+
+typedef struct {
+    const bho_trace_params_t *p;
+    double capture_radius, r_in, r_out;
+    double *states, *hit_pos, *hit_mom, *escape_dir;
+    int32_t *status, *saturated;
+    int64_t *steps;
+} tile_ctx_t;
+
+static void tile_range(void *vctx, int64_t b, int64_t e, int64_t *acc) {
+    tile_ctx_t *c = (tile_ctx_t *)vctx;
+    const bho_trace_params_t *p = c->p;
+    (void)acc;
+    for (int64_t i = b; i < e; ++i) {
+        double *y = c->states + 8 * i;
+        double h = 0.1;  /* render.py:221 */
+        int64_t steps = 0;
+        int32_t status = BHO_IN_FLIGHT;
+        for (int k = 0; k < 3; ++k) {
+            c->hit_pos[3 * i + k] = 0.0;
+            c->hit_mom[3 * i + k] = 0.0;
+            c->escape_dir[3 * i + k] = 0.0;
+        }
+        for (int64_t it = 0; it < 4 * p->max_steps; ++it) {
+            /* render.py:231-260: termination before the step. */
+            bho_geometry_t g;
+            bho_geometry(p->mass, p->spin, y[1], y[2], y[3], 0, &g);
+            const int captured = g.r <= c->capture_radius;
+            const int escaped = !captured && g.r >= p->escape_radius;
+            const int exhausted = steps >= p->max_steps;
+            if (captured) { status = BHO_CAPTURED; break; }
+            if (escaped) { status = BHO_ESCAPED; break; }
+            if (exhausted) { status = BHO_MAX_STEPS; break; }
+            /* render.py:264-266 */
+            double y_new[8], err[8];
+            bho_dp5_step(p->mass, p->spin, y, h, y_new, err);
+            const double ratio = bho_error_ratio(y, y_new, err, p->rtol, p->rtol * 1e-3);
+            const int accept = ratio <= 1.0;
+            /* render.py:268-281 */
+            if (c->r_out > 0.0 && accept && y[3] * y_new[3] < 0.0) {
+                double yc[8];
+                if (refine_crossing(p->mass, p->spin, y, h, c->r_in, c->r_out, yc)) {
+                    status = BHO_DISK;
+                    for (int k = 0; k < 3; ++k) {
+                        c->hit_pos[3 * i + k] = yc[1 + k];
+                        c->hit_mom[3 * i + k] = yc[5 + k];
+                    }
+                }
+            }
+            /* render.py:283-287 */
+            const int still = status == BHO_IN_FLIGHT;
+            if (accept && still) {
+                memcpy(y, y_new, sizeof(y_new));
+                ++steps;
+            }
+            h = np_clip(h * bho_step_factor(ratio), 0.0, p->max_step);
+            if (!still) break;
+        }
+        c->status[i] = status;
+        c->steps[i] = steps;
+        /* render.py:289-291 */
+        c->saturated[i] = status == BHO_MAX_STEPS || steps >= (int64_t)(0.85 * (double)p->max_steps);
+        if (status == BHO_ESCAPED) {
+            /* render.py:164-181 with the ray's own p_t as the energy. */
+            bho_geometry_t g;
+            bho_geometry(p->mass, p->spin, y[1], y[2], y[3], 0, &g);
+            const double lp = -y[4] + sum3(g.l[0] * y[5], g.l[1] * y[6], g.l[2] * y[7]);
+            double d[3];
+            for (int k = 0; k < 3; ++k) d[k] = y[5 + k] - 2.0 * (g.h * lp) * g.l[k];
+            const double nrm = sqrt(sum3(d[0] * d[0], d[1] * d[1], d[2] * d[2]));
+            for (int k = 0; k < 3; ++k) c->escape_dir[3 * i + k] = d[k] / nrm;
+        }
+    }
+}
+
+void bho_trace_tile(const bho_trace_params_t *p, double disk_inner,
+                    double disk_outer, double *states, int32_t *status,
+                    int64_t *steps, double *hit_pos, double *hit_mom,
+                    double *escape_dir, int32_t *saturated, int64_t n,
+                    int nthreads) {
+    const double r_plus = p->mass + sqrt(p->mass * p->mass - p->spin * p->spin);
+    tile_ctx_t c = {p, r_plus * (1.0 + p->capture_margin), disk_inner, disk_outer,
+                    states, hit_pos, hit_mom, escape_dir, status, saturated, steps};
+    bho_parallel_for(n, nthreads, 4, tile_range, &c);
+}
+
 typedef struct {
     double mass, spin, h;
     double *states;

@@ -43,6 +43,9 @@ REF_FILES = [
     "blackhorizon/tracer.py",
     "blackhorizon/camera.py",
     "blackhorizon/examples/benchmark.py",
+    "blackhorizon/offline/render.py",
+    "blackhorizon/realtime/fly_camera.py",
+    "blackhorizon/emission/novikov_thorne.py",
     "tests/test_kerr.py",
     "tests/test_shadow.py",
 ]
@@ -302,6 +305,80 @@ def gen_rk4(ref, out, n=256, n_steps=50):
                         h=np.float64(0.05), n_steps=np.int64(n_steps))
 
 
+def _offline_modules(reference):
+    """The offline renderer's module without the real-time package's GL
+    initialisation: blackhorizon.realtime is registered as a bare package so
+    that only fly_camera (pure NumPy) is imported from it."""
+    import types
+
+    if "blackhorizon.realtime" not in sys.modules:
+        pkg = types.ModuleType("blackhorizon.realtime")
+        pkg.__path__ = [os.path.join(reference, "blackhorizon", "realtime")]
+        sys.modules["blackhorizon.realtime"] = pkg
+    from blackhorizon.emission.novikov_thorne import disk_inner_radius
+    from blackhorizon.offline import render
+    from blackhorizon.realtime.fly_camera import FlyCamera
+
+    return render, FlyCamera, disk_inner_radius
+
+
+def tile_camera_states(ref, render, FlyCamera, spin, distance, inc, az, w, h, fov, ss):
+    """render.py:555-599: subpixel directions of a FlyCamera and the
+    past-directed null states at its position."""
+    G = ref["geodesics"]
+    st = ref["KerrSpacetime"](1.0, spin)
+    cam = FlyCamera.from_orbit(distance, inc, az)
+    d = render.subpixel_directions(cam, w, h, fov, ss)
+    pos = np.tile(cam.position[None, :], (d.shape[0], 1))
+    mom = G.null_momentum_from_velocity(st, pos, d, time_orientation="past")
+    return st, cam, d, G.build_state(pos, mom)
+
+
+def gen_offline_tile(ref, out):
+    """render.py:184-349 on a 32x20 tile of the offline renderer's default
+    view (a=0.9, FlyCamera at D=26, inclination 82, fov 70, disk from the
+    ISCO to 18 M, escape at 1.3 max(D, 18)): first pass at rtol 1e-9 with
+    12000 steps, then the photon-shell pass (render.py:613-630) of the
+    saturated non-disk rays at rtol 1e-11 with 48000 steps.  A second tile
+    at a=-0.7 (retrograde ISCO) with a 200-step budget makes the
+    saturation branch common."""
+    render, FlyCamera, disk_inner_radius = _offline_modules(_REFERENCE_PATH)
+    arrs = {}
+    for tag, spin, inc, az, max_steps in [("a09", 0.9, 82.0, 0.0, 12000),
+                                          ("am07", -0.7, 75.0, 40.0, 200)]:
+        settings = render.OfflineSettings(spin=spin)
+        st, cam, d, s0 = tile_camera_states(ref, render, FlyCamera, spin, 26.0, inc, az,
+                                            32, 20, settings.fov_degrees, 1)
+        r_in = float(disk_inner_radius(st))
+        r_out = max(settings.disk_outer_radius, r_in + 1.0)
+        esc = 1.3 * max(cam.distance_from_origin, r_out)
+        res = render._trace_tile(st, s0, esc, settings, (r_in, r_out), settings.rtol, max_steps)
+        retrace = res.saturated & (res.status != 5)
+        idx = np.nonzero(retrace)[0]
+        if idx.size:
+            ref2 = render._trace_tile(st, s0[idx], esc, settings, (r_in, r_out),
+                                      settings.refine_rtol, max_steps * 4)
+        arrs[f"{tag}_spin"] = np.float64(spin)
+        arrs[f"{tag}_position"] = cam.position
+        arrs[f"{tag}_directions"] = d
+        arrs[f"{tag}_state0"] = s0
+        arrs[f"{tag}_disk"] = np.array([r_in, r_out])
+        arrs[f"{tag}_escape_radius"] = np.float64(esc)
+        arrs[f"{tag}_max_steps"] = np.int64(max_steps)
+        arrs[f"{tag}_status"] = res.status.astype(np.int8)
+        arrs[f"{tag}_escape_directions"] = res.escape_directions
+        arrs[f"{tag}_hit_positions"] = res.hit_positions
+        arrs[f"{tag}_hit_momenta"] = res.hit_momenta
+        arrs[f"{tag}_saturated"] = res.saturated.astype(np.int8)
+        arrs[f"{tag}_retrace_index"] = idx
+        if idx.size:
+            arrs[f"{tag}_retrace_status"] = ref2.status.astype(np.int8)
+            arrs[f"{tag}_retrace_escape_directions"] = ref2.escape_directions
+            arrs[f"{tag}_retrace_hit_positions"] = ref2.hit_positions
+            arrs[f"{tag}_retrace_hit_momenta"] = ref2.hit_momenta
+    np.savez_compressed(os.path.join(out, "offline_tile.npz"), **arrs)
+
+
 _REFERENCE_PATH = "/root/reference"
 
 
@@ -312,6 +389,7 @@ def main():
     ap.add_argument("--out", default=HERE)
     ap.add_argument("--procs", type=int, default=os.cpu_count() or 1)
     ap.add_argument("--skip-c3", action="store_true")
+    ap.add_argument("--only", default="", help="comma-separated step names to regenerate")
     args = ap.parse_args()
     _REFERENCE_PATH = args.reference
     sys.path.insert(0, args.reference)
@@ -328,10 +406,18 @@ def main():
         ("fans", lambda: gen_fans(ref, args.out)),
         ("trace_c1", lambda: gen_trace_c1(ref, args.out)),
         ("raw_throughput", lambda: gen_raw_throughput(ref, args.out)),
+        ("offline_tile", lambda: gen_offline_tile(ref, args.out)),
     ]
     if not args.skip_c3:
         steps.append(("trace_c3", lambda: gen_trace_c3(ref, args.out, args.procs)))
+    if args.only:
+        keep = set(args.only.split(","))
+        steps = [s for s in steps if s[0] in keep]
     timings = {}
+    mpath = os.path.join(args.out, "MANIFEST.json")
+    if args.only and os.path.exists(mpath):
+        with open(mpath) as f:
+            timings = json.load(f).get("seconds", {})
     for name, fn in steps:
         t0 = time.perf_counter()
         fn()

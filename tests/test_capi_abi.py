@@ -45,6 +45,7 @@ def test_struct_layouts_match_header(tmp_path):
         'printf("%zu %zu %zu %zu\\n", offsetof(bh_trace_config, precision),'
         " offsetof(bh_trace_config, timeout_ns), offsetof(bh_camera, scene),"
         " offsetof(bh_trace_stats, bad_rays));\n"
+        'printf("%zu %zu\\n", sizeof(bh_tile_stats), offsetof(bh_tile_stats, rounds));\n'
         "return 0;}\n"
     )
     exe = tmp_path / "probe"
@@ -57,6 +58,8 @@ def test_struct_layouts_match_header(tmp_path):
                      ctypes.sizeof(_lib.Scene), ctypes.sizeof(_lib.TraceStats)]
     assert offs == [_lib.TraceConfig.precision.offset, _lib.TraceConfig.timeout_ns.offset,
                     _lib.Camera.scene.offset, _lib.TraceStats.bad_rays.offset]
+    tile = [int(v) for v in lines[2].split()]
+    assert tile == [ctypes.sizeof(_lib.TileStats), _lib.TileStats.rounds.offset]
 
 
 def test_status_strings(bhlib):
@@ -87,6 +90,34 @@ def test_trace_argument_validation(bhlib):
     cfg = _lib.TraceConfig(10, 1e-8, 1e-10, 0.1, 2.0, 1e-10, 0, 0, 0, -1, 0)
     # No workspace: reported before any CUDA call.
     assert bhlib.bh_trace(cfg, scene, None, None, None, None, 1, None, None) == -5
+
+
+def test_trace_tile_argument_validation(bhlib):
+    """bh_trace_tile rejects malformed calls before any CUDA call."""
+    import ctypes as C
+
+    from blackhorizon_b200 import _lib
+
+    scene = _lib.Scene(1.0, 0.9, 1.44, 34.0)
+    cfg = _lib.TraceConfig(12000, 1e-9, 1e-12, 0.1, 2.0, 0.0, 0, 0, 0, -1, 0)
+    st = _lib.TileStats()
+    fake = C.c_void_p(0x10000)  # never dereferenced: validation fails first
+    args = [fake] * 8
+
+    def call(cfg, r_in, r_out, n, ws=None, wsb=0):
+        return bhlib.bh_trace_tile(cfg, scene, r_in, r_out, fake, n, *args[:7], ws, wsb, st,
+                                   None)
+
+    assert call(None, 2.3, 18.0, 4) == -1
+    bad = _lib.TraceConfig(0, 1e-9, 1e-12, 0.1, 2.0, 0.0, 0, 0, 0, -1, 0)
+    assert call(bad, 2.3, 18.0, 4) == -1
+    assert call(cfg, 20.0, 18.0, 4) == -1  # inner > outer
+    assert b"disk" in bhlib.bh_last_error()
+    assert call(cfg, 2.3, 18.0, -1) == -1
+    assert call(cfg, 2.3, 18.0, 0) == 0  # empty tile: nothing to do
+    assert call(cfg, 2.3, 18.0, 4) == -5  # no workspace
+    assert call(cfg, 2.3, 18.0, 4, C.c_void_p(0x10000), 100) == -5  # too small
+    assert bhlib.bh_trace_tile_workspace_bytes(10) == 256 + 10 * (168 + 96)
 
 
 def test_check_maps_status_to_reference_exceptions(bhlib):

@@ -159,3 +159,27 @@ def test_raw_throughput_propagation(oracle):
     # pow() ulps move a handful of accept decisions over 2000 steps.
     assert np.median(np.max(rel, axis=1)) < 1e-12
     assert np.mean(acc == g["accepted"]) > 0.95
+
+
+@pytest.mark.parametrize("tag", ["a09", "am07"])
+def test_offline_tile_with_disk(oracle, tag):
+    """Offline renderer's tile tracer (render.py:184-349): disk crossings
+    refined by bisection, pre-step termination, saturation flags, and the
+    photon-shell retrace of the saturated rays at rtol 1e-11."""
+    g = golden("offline_tile.npz")
+    spin, esc, ms = float(g[f"{tag}_spin"]), float(g[f"{tag}_escape_radius"]), int(g[f"{tag}_max_steps"])
+    disk = tuple(g[f"{tag}_disk"])
+    o = oracle.trace_tile(1.0, spin, g[f"{tag}_state0"], esc, disk, rtol=1e-9, max_steps=ms)
+    np.testing.assert_array_equal(o["status"], g[f"{tag}_status"])
+    np.testing.assert_array_equal(o["saturated"], g[f"{tag}_saturated"])
+    for k in ("escape_directions", "hit_positions", "hit_momenta"):
+        np.testing.assert_allclose(o[k], g[f"{tag}_{k}"], rtol=0, atol=1e-9)
+    assert (o["status"] == 5).sum() > 300
+    idx = g[f"{tag}_retrace_index"]
+    np.testing.assert_array_equal(np.nonzero(o["saturated"] & (o["status"] != 5))[0], idx)
+    if idx.size:
+        o2 = oracle.trace_tile(1.0, spin, g[f"{tag}_state0"][idx], esc, disk, rtol=1e-11,
+                               max_steps=4 * ms)
+        np.testing.assert_array_equal(o2["status"], g[f"{tag}_retrace_status"])
+        for k in ("escape_directions", "hit_positions", "hit_momenta"):
+            np.testing.assert_allclose(o2[k], g[f"{tag}_retrace_{k}"], rtol=0, atol=1e-9)
