@@ -72,11 +72,12 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-workloads", action="store_true",
                     help="skip the full-HD frame, the 64-camera batch and the adjoint")
-    ap.add_argument("--profile-case", choices=("trace", "adjoint"), default=None,
+    ap.add_argument("--profile-case", choices=("trace", "adjoint", "tile"), default=None,
                     help="run one small untimed case of that kernel (for ncu captures): "
                          "trace = the 1920x1080 frame (2 warm-up launches, then 1); "
                          "adjoint = the 256x256 differentiable frame with a 2000-step "
-                         "tape (1 warm-up sweep, then 1)")
+                         "tape (1 warm-up sweep, then 1); tile = the offline frame at "
+                         "640x400 supersample 2 (1,024,000 rays), first pass only, twice")
     return ap.parse_args()
 
 
@@ -379,6 +380,7 @@ def run_ours(args):
         if not args.no_workloads:
             out["workloads"] = tracer_workloads(device)
             out["workloads"]["differentiable_256x256"] = adjoint_workload(device)
+            out["workloads"]["offline_frame"] = offline_workload(device, not args.no_cpu)
         if not args.no_cpu:
             out["cpu_baseline"] = cpu_baseline(state0, spin_h, S, args.cpu_seconds)
             out["endpoint_err"] = endpoint_errors(
@@ -469,6 +471,75 @@ def tracer_workloads(device, warmup=2, reps=3):
                                       C.capture_margin)
     out["shadow_full_hd"]["auto_policy"] = {"precision": pick["precision"],
                                             "variant": pick["variant"]}
+    return out
+
+
+def offline_workload(device, with_cpu=True, warmup=1, reps=3, cpu_stride=16):
+    """The offline renderer's default frame (1280x800, supersample 2, a=0.9,
+    D=26, inclination 82, fov 70, disk ISCO..18 M) traced as render_hdr does:
+    first pass at rtol 1e-9 / 12000 steps, saturated non-disk rays again at
+    rtol 1e-11 / 48000 steps; both precision policies.  The CPU leg runs the
+    oracle's tile tracer (same two passes) on every cpu_stride-th ray, which
+    also gives a status-parity sample of the whole frame."""
+    import torch
+
+    from blackhorizon_b200.kerr import KerrSpacetime
+    from blackhorizon_b200.offline import (FlyCamera, OfflineSettings, camera_states,
+                                           disk_radii, trace_frame)
+    from blackhorizon_b200.workloads import OFFLINE_FRAME as F
+
+    settings = OfflineSettings(spin=F.spin, supersample=F.supersample, max_steps=F.max_steps)
+    cam = FlyCamera.from_orbit(F.distance, F.inclination, F.azimuth)
+    st = KerrSpacetime(1.0, F.spin)
+    s0 = camera_states(cam, st, F.width, F.height, settings)
+    out = {"config": F.name, "rays": F.n}
+    frames = {}
+    for prec in ("mixed", "fp64"):
+        for _ in range(warmup):
+            trace_frame(cam, F.width, F.height, settings, precision=prec, state0=s0)
+        times = _event_ms(lambda: trace_frame(cam, F.width, F.height, settings, precision=prec,
+                                              state0=s0), reps)
+        fr = trace_frame(cam, F.width, F.height, settings, precision=prec, state0=s0)
+        frames[prec] = fr
+        ms = min(times)
+        first, second = fr.stats["first"], fr.stats.get("retrace", {})
+        out[prec] = {"ms_per_frame": ms, "rays_per_s": F.n / (ms * 1e-3),
+                     "attempts_per_ray": (first["attempts"] + second.get("attempts", 0)) / F.n,
+                     "attempted_ray_steps_per_s":
+                         (first["attempts"] + second.get("attempts", 0)) / (ms * 1e-3),
+                     "crossings": first["crossings"] + second.get("crossings", 0),
+                     "disk_hits": int((fr.status == 5).sum()),
+                     "escaped": int((fr.status == 2).sum()),
+                     "captured": int((fr.status == 1).sum()),
+                     "retraced": int(fr.retraced.sum()),
+                     "max_attempts_of_a_ray": max(first["iterations"],
+                                                  second.get("iterations", 0))}
+    out["mixed_status_agreement_with_fp64"] = float(
+        (frames["mixed"].status == frames["fp64"].status).double().mean())
+    if with_cpu:
+        from oracle import oracle
+
+        threads = host_threads()
+        idx = np.arange(0, F.n, cpu_stride)
+        s0n = s0[idx].cpu().numpy()
+        radii = disk_radii(st, settings)
+        esc = frames["fp64"].escape_radius
+        t = time.perf_counter()
+        o = oracle.trace_tile(1.0, F.spin, s0n, esc, radii, rtol=settings.rtol,
+                              max_steps=settings.max_steps, nthreads=threads)
+        re = np.nonzero((o["saturated"] != 0) & (o["status"] != 5))[0]
+        if re.size:
+            o2 = oracle.trace_tile(1.0, F.spin, s0n[re], esc, radii, rtol=settings.refine_rtol,
+                                   max_steps=4 * settings.max_steps, nthreads=threads)
+            o["status"][re] = o2["status"]
+        dt = time.perf_counter() - t
+        got = frames["fp64"].status[torch.as_tensor(idx, device=s0.device)].cpu().numpy()
+        out["cpu_baseline"] = {
+            "value": idx.size / dt, "unit": "rays/s", "cores": threads, "kind": "port",
+            "sample": f"every {cpu_stride}th ray of the frame ({idx.size} rays), both passes, "
+                      f"oracle/bh_oracle.c tile tracer (float64) on {threads} threads, "
+                      f"{dt:.1f} s"}
+        out["fp64_status_agreement_with_oracle"] = float(np.mean(got == o["status"]))
     return out
 
 
@@ -685,6 +756,21 @@ def profile_case(args):
             trace_rays(st, s0, C.escape_radius, max_steps=C.max_steps, rtol=C.rtol,
                        atol=C.atol, capture_margin=C.capture_margin, precision=prec,
                        variant=args.variant)
+    elif args.profile_case == "tile":
+        from blackhorizon_b200.offline import (FlyCamera, OfflineSettings, camera_states,
+                                               disk_radii, trace_tile)
+        from blackhorizon_b200.workloads import OFFLINE_FRAME as F
+
+        settings = OfflineSettings(spin=F.spin, supersample=F.supersample,
+                                   max_steps=F.max_steps)
+        cam = FlyCamera.from_orbit(F.distance, F.inclination, F.azimuth)
+        st = KerrSpacetime(1.0, F.spin)
+        s0 = camera_states(cam, st, F.width // 2, F.height // 2, settings)
+        radii = disk_radii(st, settings)
+        esc = 1.3 * max(cam.distance_from_origin, radii[1])
+        for _ in range(2):
+            trace_tile(st, s0, esc, settings, radii, settings.rtol, settings.max_steps,
+                       precision=prec, variant=args.variant)
     else:
         C = DIFFERENTIABLE
         t = lambda x: torch.tensor(x, dtype=torch.float64, device=device)  # noqa: E731

@@ -16,8 +16,14 @@
 // crossing record and its slot takes the next ray from the work queue.  A
 // second kernel refines all parked crossings in float64, one per thread, in
 // lock step; a hit finalises the ray, a miss writes a resume record, and the
-// next round of the tracer takes the resumed rays from its queue.  Rounds
-// repeat until no ray is left (the host reads one counter per round).
+// second round of the tracer takes the resumed rays from its queue.  The
+// second round refines its crossings in place: it holds the minority of rays
+// that cross more than once (photon-ring orbits), whose tail is bound by the
+// latency of a lone ray's attempts, and parking them again would add one
+// latency-bound tail per crossing.  So a tile takes two rounds; the host
+// reads one counter per round.  (Claiming parked crossings from inside one
+// persistent launch instead, once its queue drains, was measured ten times
+// slower: every idle warp contends for the same claim counter.)
 //
 // Refinement.  The reference bisects the step fraction 40 times
 // (render.py:332-339): it ends on the dyadic cell (L, L + 2^-40) with L the
@@ -77,198 +83,6 @@ __device__ __forceinline__ void tile_finalize(const TileArgs &a, long long ray,
         ed[0] = d0 / nrm; ed[1] = d1 / nrm; ed[2] = d2 / nrm;
     } else {
         ed[0] = ed[1] = ed[2] = 0.0;
-    }
-}
-
-template <class V, int BLOCK, int MINB>
-__global__ void __launch_bounds__(BLOCK, MINB) tile_kernel(const TileArgs args) {
-    using T = VT<V>;
-    constexpr int N = T::N;
-    constexpr bool F64 = sizeof(typename T::S) == 8;
-    TileWorkspace *ws = args.ws;
-    const int par = args.round & 1;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        // Counters of the other parity: used next by this round's refinement
-        // (n_resume) and by the next round (queue head, crossing count).
-        ws->queue_head[par ^ 1] = 0;
-        ws->n_cross[par ^ 1] = 0;
-        ws->n_resume[par ^ 1] = 0;
-    }
-    const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    const unsigned lt_mask = (1u << lane) - 1u;
-    const long long n_in = args.round == 0 ? args.n : (long long)ws->n_resume[par];
-    bool flush = args.flush != 0 || ws->timed_out != 0;
-    const bool disk = args.disk_outer > 0.0;
-    const unsigned long long deadline = global_timer_ns() + (unsigned long long)args.timeout_ns;
-    const bool has_deadline = args.timeout_ns > 0;
-    const V rt = T::set(args.rtol), at = T::set(args.atol);
-    const KerrV<V> K = make_kerr<V>(T::set(args.mass), T::set(args.spin));
-
-    extern __shared__ double bh_state_smem[];
-    StateStore<V, BLOCK> ys(bh_state_smem);
-    long long ray[N], steps[N], attempts[N];
-    double h[N];
-    WStateV<V> yw;
-#pragma unroll
-    for (int l = 0; l < N; ++l) {
-        ray[l] = -1; steps[l] = 0; attempts[l] = 0; h[l] = args.initial_step;
-        const RayState y0{0.0, 10.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0};
-        ys.set(l, y0);
-        put_work<V>(yw, l, y0);
-    }
-    StageV<V> k1 = first_stage<V>(K, yw);
-    bool queue_open = true;
-    unsigned long long my_attempts = 0, my_accepted = 0;
-    long long my_max_attempts = 0;
-
-    auto finish = [&](int l, const RayState &y, int st) {
-        tile_finalize(args, ray[l], y, st, steps[l], nullptr);
-        my_attempts += attempts[l];
-        my_accepted += steps[l];
-        if (attempts[l] > my_max_attempts) my_max_attempts = attempts[l];
-        ray[l] = -1;
-    };
-
-    for (unsigned iter = 0;; ++iter) {
-        // ---- warp-aggregated refill of the idle slots
-        unsigned mask[N];
-        int total = 0;
-#pragma unroll
-        for (int l = 0; l < N; ++l) {
-            mask[l] = __ballot_sync(full, ray[l] < 0 && queue_open);
-            total += __popc(mask[l]);
-        }
-        bool fresh[N];
-#pragma unroll
-        for (int l = 0; l < N; ++l) fresh[l] = false;
-        if (total) {
-            unsigned any = 0;
-#pragma unroll
-            for (int l = 0; l < N; ++l) any |= mask[l];
-            const int leader = __ffs(any) - 1;
-            unsigned long long base = 0;
-            if (lane == leader) base = atomicAdd(&ws->queue_head[par], (unsigned long long)total);
-            base = __shfl_sync(full, base, leader);
-            int before = 0;
-#pragma unroll
-            for (int l = 0; l < N; ++l) {
-                if ((mask[l] >> lane) & 1u) {
-                    const long long idx = (long long)base + before + __popc(mask[l] & lt_mask);
-                    if (idx < n_in) {
-                        RayState y0;
-                        if (args.round == 0) {
-                            load_state(args.state0, args.n, args.layout, idx, y0);
-                            ray[l] = idx; steps[l] = 0; attempts[l] = 0;
-                            h[l] = args.initial_step;
-                        } else {
-                            const TileResume &r = args.resume[idx];
-                            y0 = RayState{r.y[0], r.y[1], r.y[2], r.y[3],
-                                          r.y[4], r.y[5], r.y[6], r.y[7]};
-                            ray[l] = r.ray; steps[l] = r.steps; attempts[l] = r.attempts;
-                            h[l] = r.h;
-                        }
-                        const int st = flush ? BH_RAY_IN_FLIGHT
-                                             : tile_check(args, y0, steps[l], attempts[l]);
-                        if (st >= 0) {
-                            finish(l, y0, st);
-                        } else {
-                            fresh[l] = true;
-                            ys.set(l, y0);
-                            put_work<V>(yw, l, y0);
-                        }
-                    }
-                }
-                before += __popc(mask[l]);
-            }
-            if ((long long)base + total >= n_in) queue_open = false;
-        }
-        bool any_fresh = false;
-#pragma unroll
-        for (int l = 0; l < N; ++l) any_fresh |= fresh[l];
-        if (any_fresh) {
-            const StageV<V> f = first_stage<V>(K, yw);
-            take_stage(k1, f, fresh);
-        }
-        bool active = false;
-#pragma unroll
-        for (int l = 0; l < N; ++l) active |= ray[l] >= 0;
-        if (!__any_sync(full, active || queue_open)) break;
-
-        if (active) {
-            // ---- one iteration of render.py:262-287 for every slot
-            V hw = T::set(0.0);
-#pragma unroll
-            for (int l = 0; l < N; ++l) T::put(hw, l, typename T::S(h[l]));
-            AttemptV<V> a;
-            dp5_attempt<V>(K, yw, hw, k1, a);
-            double ratio[N];
-            error_ratio_v<V>(yw, a.ynw, a.err, hw, rt, at, ratio);
-            bool acc[N];
-#pragma unroll
-            for (int l = 0; l < N; ++l) {
-                acc[l] = false;
-                if (ray[l] < 0) continue;
-                acc[l] = ratio[l] <= 1.0;
-                ++attempts[l];
-                const double h_next =
-                    np_min(np_max(h[l] * step_factor<F64>(ratio[l]), 0.0), args.max_step);
-                if (acc[l]) {
-                    const RayState y0 = ys.get(l);
-                    RayState y1 = y0;
-                    commit<V>(y1, yw, a, l, h[l]);
-                    if (disk && y0.z * y1.z < 0.0) {
-                        // render.py:268-281: park for refinement.
-                        const unsigned long long k = atomicAdd(&ws->n_cross[par], 1ull);
-                        TileCrossing &c = args.cross[k];
-                        c.y0[0] = y0.t; c.y0[1] = y0.x; c.y0[2] = y0.y; c.y0[3] = y0.z;
-                        c.y0[4] = y0.pt; c.y0[5] = y0.px; c.y0[6] = y0.py; c.y0[7] = y0.pz;
-                        c.y1[0] = y1.t; c.y1[1] = y1.x; c.y1[2] = y1.y; c.y1[3] = y1.z;
-                        c.y1[4] = y1.pt; c.y1[5] = y1.px; c.y1[6] = y1.py; c.y1[7] = y1.pz;
-                        c.h = h[l];
-                        c.h_next = h_next;
-                        c.steps = steps[l];
-                        c.attempts = attempts[l];
-                        c.ray = ray[l];
-                        ray[l] = -1;
-                        acc[l] = false;
-                        continue;
-                    }
-                    ys.set(l, y1);
-                    ++steps[l];
-                }
-                h[l] = h_next;
-                int st = -1;
-                if (attempts[l] >= args.max_attempts) st = BH_RAY_IN_FLIGHT;
-                else if (acc[l]) st = tile_check(args, ys.get(l), steps[l], attempts[l]);
-                if (st >= 0) finish(l, ys.get(l), st);
-            }
-            take_stage(k1, a.k7, acc);
-        }
-
-        // ---- bounded launch time: past the deadline every ray in flight,
-        // and every ray still queued, is finalised as IN_FLIGHT.
-        if (has_deadline && !flush && (iter & 7u) == 0u) {
-            const bool late = global_timer_ns() > deadline;
-            if (__any_sync(full, late)) {
-                flush = true;
-#pragma unroll
-                for (int l = 0; l < N; ++l)
-                    if (ray[l] >= 0) finish(l, ys.get(l), BH_RAY_IN_FLIGHT);
-                if (lane == 0) atomicExch(&ws->timed_out, 1);
-            }
-        }
-    }
-    for (int off = 16; off > 0; off >>= 1) {
-        my_attempts += __shfl_down_sync(full, my_attempts, off);
-        my_accepted += __shfl_down_sync(full, my_accepted, off);
-        const long long o = __shfl_down_sync(full, my_max_attempts, off);
-        my_max_attempts = o > my_max_attempts ? o : my_max_attempts;
-    }
-    if (lane == 0) {
-        atomicAdd(&ws->attempts, my_attempts);
-        atomicAdd(&ws->accepted, my_accepted);
-        atomicMax(&ws->iterations, my_max_attempts);
     }
 }
 
@@ -370,6 +184,230 @@ __device__ __forceinline__ double crossing_fraction(const Rk4From &rk, const Ray
     return (kl + 0.5) * kCell;
 }
 
+// Refines one crossing step (render.py:312-349): the crossing state on the
+// RK4 substep at the reference's bisection point, and whether its radius is
+// on the disk.
+__device__ __forceinline__ bool refine_hit(double m, double a, double r_in, double r_out,
+                                           const RayState &y0, double h, RayState &yc) {
+    const Rk4From rk(m, a, y0);
+    const double th = crossing_fraction(rk, y0, h);
+    rk.step(y0, h * th, true, yc);
+    const double r = ks_radius(a, yc);
+    return r >= r_in && r <= r_out;
+}
+
+// INLINE = false (the first round): every crossing is parked for the
+// refinement kernel.  INLINE = true (resumed rays): crossings are refined in
+// place, so no ray needs a third round.
+template <class V, int BLOCK, int MINB, bool INLINE>
+__global__ void __launch_bounds__(BLOCK, MINB) tile_kernel(const TileArgs args) {
+    using T = VT<V>;
+    constexpr int N = T::N;
+    constexpr bool F64 = sizeof(typename T::S) == 8;
+    TileWorkspace *ws = args.ws;
+    const int par = args.round & 1;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        // Counters of the other parity: used next by this round's refinement
+        // (n_resume) and by the next round (queue head, crossing count).
+        ws->queue_head[par ^ 1] = 0;
+        ws->n_cross[par ^ 1] = 0;
+        ws->n_resume[par ^ 1] = 0;
+    }
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    const long long n_in = args.round == 0 ? args.n : (long long)ws->n_resume[par];
+    bool flush = args.flush != 0 || ws->timed_out != 0;
+    const bool disk = args.disk_outer > 0.0;
+    const unsigned long long deadline = global_timer_ns() + (unsigned long long)args.timeout_ns;
+    const bool has_deadline = args.timeout_ns > 0;
+    const V rt = T::set(args.rtol), at = T::set(args.atol);
+    const KerrV<V> K = make_kerr<V>(T::set(args.mass), T::set(args.spin));
+
+    extern __shared__ double bh_state_smem[];
+    StateStore<V, BLOCK> ys(bh_state_smem);
+    long long ray[N], steps[N], attempts[N];
+    double h[N];
+    WStateV<V> yw;
+#pragma unroll
+    for (int l = 0; l < N; ++l) {
+        ray[l] = -1; steps[l] = 0; attempts[l] = 0; h[l] = args.initial_step;
+        const RayState y0{0.0, 10.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0};
+        ys.set(l, y0);
+        put_work<V>(yw, l, y0);
+    }
+    StageV<V> k1 = first_stage<V>(K, yw);
+    bool queue_open = true;
+    unsigned long long my_attempts = 0, my_accepted = 0;
+    long long my_max_attempts = 0;
+
+    unsigned long long my_cross = 0, my_hits = 0;
+    auto finish = [&](int l, const RayState &y, int st, const RayState *hit) {
+        tile_finalize(args, ray[l], y, st, steps[l], hit);
+        my_attempts += attempts[l];
+        my_accepted += steps[l];
+        if (attempts[l] > my_max_attempts) my_max_attempts = attempts[l];
+        ray[l] = -1;
+    };
+
+    for (unsigned iter = 0;; ++iter) {
+        // ---- warp-aggregated refill of the idle slots
+        unsigned mask[N];
+        int total = 0;
+#pragma unroll
+        for (int l = 0; l < N; ++l) {
+            mask[l] = __ballot_sync(full, ray[l] < 0 && queue_open);
+            total += __popc(mask[l]);
+        }
+        bool fresh[N];
+#pragma unroll
+        for (int l = 0; l < N; ++l) fresh[l] = false;
+        if (total) {
+            unsigned any = 0;
+#pragma unroll
+            for (int l = 0; l < N; ++l) any |= mask[l];
+            const int leader = __ffs(any) - 1;
+            unsigned long long base = 0;
+            if (lane == leader) base = atomicAdd(&ws->queue_head[par], (unsigned long long)total);
+            base = __shfl_sync(full, base, leader);
+            int before = 0;
+#pragma unroll
+            for (int l = 0; l < N; ++l) {
+                if ((mask[l] >> lane) & 1u) {
+                    const long long idx = (long long)base + before + __popc(mask[l] & lt_mask);
+                    if (idx < n_in) {
+                        RayState y0;
+                        if (args.round == 0) {
+                            load_state(args.state0, args.n, args.layout, idx, y0);
+                            ray[l] = idx; steps[l] = 0; attempts[l] = 0;
+                            h[l] = args.initial_step;
+                        } else {
+                            const TileResume &r = args.resume[idx];
+                            y0 = RayState{r.y[0], r.y[1], r.y[2], r.y[3],
+                                          r.y[4], r.y[5], r.y[6], r.y[7]};
+                            ray[l] = r.ray; steps[l] = r.steps; attempts[l] = r.attempts;
+                            h[l] = r.h;
+                        }
+                        const int st = flush ? BH_RAY_IN_FLIGHT
+                                             : tile_check(args, y0, steps[l], attempts[l]);
+                        if (st >= 0) {
+                            finish(l, y0, st, nullptr);
+                        } else {
+                            fresh[l] = true;
+                            ys.set(l, y0);
+                            put_work<V>(yw, l, y0);
+                        }
+                    }
+                }
+                before += __popc(mask[l]);
+            }
+            if ((long long)base + total >= n_in) queue_open = false;
+        }
+        bool any_fresh = false;
+#pragma unroll
+        for (int l = 0; l < N; ++l) any_fresh |= fresh[l];
+        if (any_fresh) {
+            const StageV<V> f = first_stage<V>(K, yw);
+            take_stage(k1, f, fresh);
+        }
+        bool active = false;
+#pragma unroll
+        for (int l = 0; l < N; ++l) active |= ray[l] >= 0;
+        if (!__any_sync(full, active || queue_open)) break;
+
+        if (active) {
+            // ---- one iteration of render.py:262-287 for every slot
+            V hw = T::set(0.0);
+#pragma unroll
+            for (int l = 0; l < N; ++l) T::put(hw, l, typename T::S(h[l]));
+            AttemptV<V> a;
+            dp5_attempt<V>(K, yw, hw, k1, a);
+            double ratio[N];
+            error_ratio_v<V>(yw, a.ynw, a.err, hw, rt, at, ratio);
+            bool acc[N];
+#pragma unroll
+            for (int l = 0; l < N; ++l) {
+                acc[l] = false;
+                if (ray[l] < 0) continue;
+                acc[l] = ratio[l] <= 1.0;
+                ++attempts[l];
+                const double h_next =
+                    np_min(np_max(h[l] * step_factor<F64>(ratio[l]), 0.0), args.max_step);
+                if (acc[l]) {
+                    const RayState y0 = ys.get(l);
+                    RayState y1 = y0;
+                    commit<V>(y1, yw, a, l, h[l]);
+                    if (INLINE && disk && y0.z * y1.z < 0.0) {
+                        RayState yc;
+                        ++my_cross;
+                        if (refine_hit(args.mass, args.spin, args.disk_inner, args.disk_outer,
+                                       y0, h[l], yc)) {
+                            ++my_hits;
+                            finish(l, y0, BH_RAY_DISK, &yc);
+                            acc[l] = false;
+                            continue;
+                        }
+                    } else if (disk && y0.z * y1.z < 0.0) {
+                        // render.py:268-281: park for refinement.
+                        const unsigned long long k = atomicAdd(&ws->n_cross[par], 1ull);
+                        TileCrossing &c = args.cross[k];
+                        c.y0[0] = y0.t; c.y0[1] = y0.x; c.y0[2] = y0.y; c.y0[3] = y0.z;
+                        c.y0[4] = y0.pt; c.y0[5] = y0.px; c.y0[6] = y0.py; c.y0[7] = y0.pz;
+                        c.y1[0] = y1.t; c.y1[1] = y1.x; c.y1[2] = y1.y; c.y1[3] = y1.z;
+                        c.y1[4] = y1.pt; c.y1[5] = y1.px; c.y1[6] = y1.py; c.y1[7] = y1.pz;
+                        c.h = h[l];
+                        c.h_next = h_next;
+                        c.steps = steps[l];
+                        c.attempts = attempts[l];
+                        c.ray = ray[l];
+                        ray[l] = -1;
+                        acc[l] = false;
+                        continue;
+                    }
+                    ys.set(l, y1);
+                    ++steps[l];
+                }
+                h[l] = h_next;
+                int st = -1;
+                if (attempts[l] >= args.max_attempts) st = BH_RAY_IN_FLIGHT;
+                else if (acc[l]) st = tile_check(args, ys.get(l), steps[l], attempts[l]);
+                if (st >= 0) finish(l, ys.get(l), st, nullptr);
+            }
+            take_stage(k1, a.k7, acc);
+        }
+
+        // ---- bounded launch time: past the deadline every ray in flight,
+        // and every ray still queued, is finalised as IN_FLIGHT.
+        if (has_deadline && !flush && (iter & 7u) == 0u) {
+            const bool late = global_timer_ns() > deadline;
+            if (__any_sync(full, late)) {
+                flush = true;
+#pragma unroll
+                for (int l = 0; l < N; ++l)
+                    if (ray[l] >= 0) finish(l, ys.get(l), BH_RAY_IN_FLIGHT, nullptr);
+                if (lane == 0) atomicExch(&ws->timed_out, 1);
+            }
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        my_attempts += __shfl_down_sync(full, my_attempts, off);
+        my_accepted += __shfl_down_sync(full, my_accepted, off);
+        my_cross += __shfl_down_sync(full, my_cross, off);
+        my_hits += __shfl_down_sync(full, my_hits, off);
+        const long long o = __shfl_down_sync(full, my_max_attempts, off);
+        my_max_attempts = o > my_max_attempts ? o : my_max_attempts;
+    }
+    if (lane == 0) {
+        atomicAdd(&ws->attempts, my_attempts);
+        atomicAdd(&ws->accepted, my_accepted);
+        atomicMax(&ws->iterations, my_max_attempts);
+        if (my_cross) {
+            atomicAdd(&ws->crossings, my_cross);
+            atomicAdd(&ws->disk_hits, my_hits);
+        }
+    }
+}
+
 __global__ void __launch_bounds__(128) refine_kernel(const TileArgs args) {
     TileWorkspace *ws = args.ws;
     const int par = args.round & 1;
@@ -388,13 +426,10 @@ __global__ void __launch_bounds__(128) refine_kernel(const TileArgs args) {
             c = args.cross[i];
             const RayState y0{c.y0[0], c.y0[1], c.y0[2], c.y0[3],
                               c.y0[4], c.y0[5], c.y0[6], c.y0[7]};
-            const Rk4From rk(args.mass, args.spin, y0);
-            const double th = crossing_fraction(rk, y0, c.h);
             RayState yc;
-            rk.step(y0, c.h * th, true, yc);
-            const double r = ks_radius(args.spin, yc);
             ++my_cross;
-            if (r >= args.disk_inner && r <= args.disk_outer) {
+            if (refine_hit(args.mass, args.spin, args.disk_inner, args.disk_outer, y0, c.h,
+                           yc)) {
                 // render.py:278-281 and 283-286: DISK, state and steps as
                 // before the step.
                 tile_finalize(args, c.ray, y0, BH_RAY_DISK, c.steps, &yc);
@@ -444,30 +479,31 @@ __global__ void __launch_bounds__(128) refine_kernel(const TileArgs args) {
 // ------------------------------------------------------------ launches
 
 template <class V, int B, int M>
-static const void *tile_fn(size_t *smem) {
+static const void *tile_fn(bool inl, size_t *smem) {
     *smem = StateStore<V, B>::shared_bytes();
-    return (const void *)tile_kernel<V, B, M>;
+    return inl ? (const void *)tile_kernel<V, B, M, true>
+               : (const void *)tile_kernel<V, B, M, false>;
 }
 
 // Same launch shapes as the tracer's variants (bh_trace.cu).
-static const void *tile_kernel_for(int precision, int idx, size_t *smem) {
+static const void *tile_kernel_for(int precision, int idx, bool inl, size_t *smem) {
     if (precision == BH_PRECISION_MIXED) {
         switch (idx) {
-            case 0: return tile_fn<float, 128, 3>(smem);
-            case 1: return tile_fn<float, 128, 4>(smem);
-            case 2: return tile_fn<float, 128, 5>(smem);
-            case 3: return tile_fn<float, 256, 2>(smem);
-            case 4: return tile_fn<F2, 128, 2>(smem);
-            case 5: return tile_fn<F2, 128, 3>(smem);
-            case 6: return tile_fn<F2, 64, 4>(smem);
-            default: return tile_fn<F2, 256, 1>(smem);
+            case 0: return tile_fn<float, 128, 3>(inl, smem);
+            case 1: return tile_fn<float, 128, 4>(inl, smem);
+            case 2: return tile_fn<float, 128, 5>(inl, smem);
+            case 3: return tile_fn<float, 256, 2>(inl, smem);
+            case 4: return tile_fn<F2, 128, 2>(inl, smem);
+            case 5: return tile_fn<F2, 128, 3>(inl, smem);
+            case 6: return tile_fn<F2, 64, 4>(inl, smem);
+            default: return tile_fn<F2, 256, 1>(inl, smem);
         }
     }
     switch (idx) {
-        case 0: return tile_fn<double, 128, 2>(smem);
-        case 1: return tile_fn<double, 128, 3>(smem);
-        case 2: return tile_fn<double, 128, 4>(smem);
-        default: return tile_fn<double, 256, 2>(smem);
+        case 0: return tile_fn<double, 128, 2>(inl, smem);
+        case 1: return tile_fn<double, 128, 3>(inl, smem);
+        case 2: return tile_fn<double, 128, 4>(inl, smem);
+        default: return tile_fn<double, 256, 2>(inl, smem);
     }
 }
 
@@ -483,7 +519,7 @@ cudaError_t launch_tile(const TileArgs &args, int precision, int variant,
         variant = tile_default_variant(precision);
     const Variant v = trace_variant(precision, variant);
     size_t smem = 0;
-    const void *fn = tile_kernel_for(precision, variant, &smem);
+    const void *fn = tile_kernel_for(precision, variant, args.round > 0, &smem);
     int dev = 0, sms = 0, occ = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;

@@ -89,6 +89,33 @@ DIFFERENTIABLE = ShadowConfig(
 
 
 @dataclass(frozen=True)
+class OfflineFrameConfig:
+    """An offline-renderer frame: FlyCamera on the orbit sphere looking at
+    the hole, subpixel rays traced with disk crossings (two passes)."""
+
+    name: str
+    spin: float
+    distance: float
+    inclination: float
+    azimuth: float
+    width: int
+    height: int
+    supersample: int
+    max_steps: int
+
+    @property
+    def n(self) -> int:
+        return self.width * self.height * self.supersample ** 2
+
+
+# The offline renderer's command-line defaults (render.py:684-707):
+# 1280x800, supersample 2 (4,096,000 rays), a=0.9, D=26 M, inclination 82,
+# fov 70, disk from the ISCO to 18 M, rtol 1e-9 then 1e-11, 12000 steps.
+OFFLINE_FRAME = OfflineFrameConfig("offline-1280x800-ss2-a0.9-i82", 0.9, 26.0, 82.0, 0.0,
+                                   1280, 800, 2, 12000)
+
+
+@dataclass(frozen=True)
 class UnevenCamera:
     spin: float
     inclination: float
