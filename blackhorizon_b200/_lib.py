@@ -47,7 +47,8 @@ class TraceConfig(ctypes.Structure):
     _fields_ = [("max_steps", _I64), ("rtol", _D), ("atol", _D),
                 ("initial_step", _D), ("max_step", _D), ("min_step", _D),
                 ("precision", _I32), ("layout", _I32), ("timeout_ns", _I64),
-                ("variant", _I32), ("blocks_per_sm", _I32)]
+                ("variant", _I32), ("blocks_per_sm", _I32), ("project_every", _I32),
+                ("reserved", _I32)]
 
 
 class TraceStats(ctypes.Structure):

@@ -310,6 +310,7 @@ static int config_ok(const bh_trace_config *c) {
     if (c->max_steps < 1 || c->max_steps > (1LL << 60))
         return invalid("max_steps must be in [1, 2^60]");
     if (c->timeout_ns < 0) return invalid("timeout_ns must be >= 0");
+    if (c->project_every < 0) return invalid("project_every must be >= 0");
     return BH_OK;
 }
 
@@ -329,6 +330,7 @@ static TraceArgs base_args(const bh_trace_config *c) {
     a.max_attempts = 4 * c->max_steps;
     a.timeout_ns = c->timeout_ns;
     a.layout = c->layout;
+    a.project_every = c->project_every;
     return a;
 }
 
@@ -341,6 +343,8 @@ int bh_trace_with_tape(const bh_trace_config *config, const bh_scene *scene,
                        double *h_tape, double *ckpt, int64_t tape_cap, int ckpt_every) {
     int rc = config_ok(config);
     if (rc != BH_OK) return rc;
+    if (h_tape && config->project_every > 0)
+        return invalid("a taped trace cannot project: the adjoint replays unprojected steps");
     if (!scene) return invalid("scene is NULL");
     if (!kerr_ok(scene->mass, scene->spin)) return invalid("Kerr bound violated or mass not positive");
     if (n < 0) return invalid("n must be >= 0");

@@ -583,6 +583,29 @@ __device__ __forceinline__ void error_ratio_v(const WStateV<V> &y, const WStateV
     }
 }
 
+// Projection onto the null constraint, float64.  The super-Hamiltonian
+// H(x, p) = 1/2 (-p_t^2 + |p|^2) - H_ks lp^2 (geodesics.py:77-95) vanishes on
+// null geodesics; integration error drifts it.  One Newton step along the
+// spatial gradient dH/dp_i = p_i - 2 H_ks lp l_i (the coordinate velocity,
+// geodesics.py:98-106) moves p back: p_i -= H v_i / |v|^2, leaving p_t, hence
+// the energy, unchanged.  The residual after the step is O(H^2).  Not part of
+// the reference, which never projects.
+__device__ __forceinline__ void project_null(double m, double a, RayState &y) {
+    Geometry g;
+    geometry_full(m, a, y.x, y.y, y.z, false, g);
+    const double lp = -y.pt + ((g.l[0] * y.px + g.l[1] * y.py) + g.l[2] * y.pz);
+    const double ham = 0.5 * (-y.pt * y.pt + ((y.px * y.px + y.py * y.py) + y.pz * y.pz)) -
+                       g.h * lp * lp;
+    const double c = 2.0 * g.h * lp;
+    const double vx = y.px - c * g.l[0], vy = y.py - c * g.l[1], vz = y.pz - c * g.l[2];
+    const double v2 = (vx * vx + vy * vy) + vz * vz;
+    if (!(v2 > 0.0)) return;
+    const double s = ham / v2;
+    y.px -= s * vx;
+    y.py -= s * vy;
+    y.pz -= s * vz;
+}
+
 // step_factor (integrators.py:120-124): clip(0.9 max(ratio,1e-16)^-0.2, 0.2, 5).
 template <bool F64>
 __device__ __forceinline__ double step_factor(double ratio) {

@@ -54,6 +54,7 @@ struct TraceArgs {
     long long max_steps;     // trace: accepted-step budget
     long long max_attempts;  // trace: 4 * max_steps; propagate: n_steps
     long long timeout_ns;
+    int project_every;       // null-constraint projection period (iterations); 0 = off
     TraceWorkspace *ws;
     // optional tape of the accepted steps (trace only): step sizes
     // (n x tape_cap) and float64 states before every ckpt_every-th accepted

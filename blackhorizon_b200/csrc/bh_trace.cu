@@ -23,7 +23,10 @@
 
 namespace bh {
 
-template <class V, int BLOCK, int MINB>
+// PROJECT: every project_every controller iterations, each ray in flight is
+// projected onto the null constraint in float64 (project_null) and its FSAL
+// derivative recomputed; warp-uniform, so the warp pays one RHS per period.
+template <class V, int BLOCK, int MINB, bool PROJECT>
 __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args) {
     using T = VT<V>;
     constexpr int N = T::N;
@@ -187,6 +190,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args
                 // tracer.py:151-154: rays still in flight after the cap are MAX_STEPS.
                 if (st == BH_RAY_IN_FLIGHT && attempts[l] >= args.max_attempts) st = BH_RAY_MAX_STEPS;
                 if (st != BH_RAY_IN_FLIGHT) {
+                    // Returned states lie on the constraint too (p only: r
+                    // and so the classification are unchanged).
+                    if constexpr (PROJECT) project_null(mass[l], spin[l], yl);
                     store_state(args.states, n, args.layout, ray[l], yl);
                     args.status[ray[l]] = st;
                     args.steps[ray[l]] = steps[l];
@@ -198,6 +204,23 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args
                 }
             }
             take_stage(k1, a.k7, acc);
+            if constexpr (PROJECT) {
+                if (iter % (unsigned)args.project_every == 0u) {
+                    bool proj[N];
+#pragma unroll
+                    for (int l = 0; l < N; ++l) {
+                        proj[l] = ray[l] >= 0;
+                        if (proj[l]) {
+                            RayState yl = ys.get(l);
+                            project_null(mass[l], spin[l], yl);
+                            ys.set(l, yl);
+                            put_work<V>(yw, l, yl);
+                        }
+                    }
+                    const StageV<V> f = first_stage<V>(K, yw);
+                    take_stage(k1, f, proj);
+                }
+            }
         }
 
         // ---- bounded launch time
@@ -236,7 +259,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args
 // n_steps attempted DP5(4) steps per ray with the tracer's accept/reject and
 // step update (tracer.py:111-120) and no termination; grid-stride over groups
 // of N rays.
-template <class V, int BLOCK, int MINB>
+template <class V, int BLOCK, int MINB, bool PROJECT>
 __global__ void __launch_bounds__(BLOCK, MINB) propagate_kernel(const TraceArgs args) {
     using T = VT<V>;
     constexpr int N = T::N;
@@ -305,6 +328,21 @@ __global__ void __launch_bounds__(BLOCK, MINB) propagate_kernel(const TraceArgs 
                 h[l] = np_min(np_max(h[l] * step_factor<F64>(ratio[l]), 0.0), args.max_step);
             }
             take_stage(k1, a.k7, ok);
+            if constexpr (PROJECT) {
+                if ((k + 1) % args.project_every == 0) {
+                    bool proj[N];
+#pragma unroll
+                    for (int l = 0; l < N; ++l) {
+                        proj[l] = true;
+                        RayState yl = ys.get(l);
+                        project_null(mass[l], spin[l], yl);
+                        ys.set(l, yl);
+                        put_work<V>(yw, l, yl);
+                    }
+                    const StageV<V> f = first_stage<V>(K, yw);
+                    take_stage(k1, f, proj);
+                }
+            }
             if (has_deadline && (k & 63) == 63 && global_timer_ns() > deadline) {
                 late = true;
                 ++k;
@@ -315,7 +353,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) propagate_kernel(const TraceArgs 
         for (int l = 0; l < N; ++l) {
             if (!valid[l]) continue;
             const long long i = g * N + l;
-            store_state(args.states, n, args.layout, i, ys.get(l));
+            RayState yl = ys.get(l);
+            if constexpr (PROJECT) project_null(mass[l], spin[l], yl);
+            store_state(args.states, n, args.layout, i, yl);
             args.h_io[i] = h[l];
             if (args.lam_io) args.lam_io[i] = lam[l];
             args.steps[i] = acc[l];
@@ -357,14 +397,20 @@ int trace_default_variant(int precision) {
     return precision == BH_PRECISION_MIXED ? 5 : 3;
 }
 
-template <class V, int B, int M>
+template <class V, int B, int M, bool P = false>
 static const void *kfn(bool propagate, size_t *smem) {
     *smem = StateStore<V, B>::shared_bytes();
-    return propagate ? (const void *)propagate_kernel<V, B, M>
-                     : (const void *)trace_kernel<V, B, M>;
+    return propagate ? (const void *)propagate_kernel<V, B, M, P>
+                     : (const void *)trace_kernel<V, B, M, P>;
 }
 
-static const void *kernel_for(bool propagate, int precision, int idx, size_t *smem) {
+// project: the null-constraint projection is compiled for the default launch
+// shapes only (the launcher switches to them).
+static const void *kernel_for(bool propagate, int precision, int idx, bool project,
+                              size_t *smem) {
+    if (project)
+        return precision == BH_PRECISION_MIXED ? kfn<F2, 128, 3, true>(propagate, smem)
+                                               : kfn<double, 256, 2, true>(propagate, smem);
     if (precision == BH_PRECISION_MIXED) {
         switch (idx) {
             case 0: return kfn<float, 128, 3>(propagate, smem);
@@ -388,7 +434,7 @@ static const void *kernel_for(bool propagate, int precision, int idx, size_t *sm
 int kernel_attributes(bool propagate, int precision, int idx, int *regs,
                       int *max_blocks) {
     size_t smem = 0;
-    const void *fn = kernel_for(propagate, precision, idx, &smem);
+    const void *fn = kernel_for(propagate, precision, idx, false, &smem);
     cudaFuncAttributes attr;
     cudaError_t e = cudaFuncGetAttributes(&attr, fn);
     if (e != cudaSuccess) return -1;
@@ -405,11 +451,12 @@ int kernel_attributes(bool propagate, int precision, int idx, int *regs,
 
 static cudaError_t launch(bool propagate, const TraceArgs &args, int precision,
                           int variant, int blocks_per_sm, cudaStream_t stream) {
-    if (variant < 0 || variant >= trace_variant_count(precision))
+    const bool project = args.project_every > 0;
+    if (project || variant < 0 || variant >= trace_variant_count(precision))
         variant = trace_default_variant(precision);
     const Variant v = trace_variant(precision, variant);
     size_t smem = 0;
-    const void *fn = kernel_for(propagate, precision, variant, &smem);
+    const void *fn = kernel_for(propagate, precision, variant, project, &smem);
     int dev = 0, sms = 0, occ = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;

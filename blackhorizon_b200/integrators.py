@@ -133,14 +133,16 @@ def make_config(max_steps: int = 1, rtol: float = 1e-9, atol: float = 1e-12,
                 initial_step: float = 0.1, max_step: float = 2.0,
                 min_step: float = 1e-10, precision: str = "fp64",
                 layout: str = "aos", timeout_s: float = 0.0, variant: int = -1,
-                blocks_per_sm: int = 0) -> "_lib.TraceConfig":
+                blocks_per_sm: int = 0, project_every: int = 0) -> "_lib.TraceConfig":
     if layout not in _lib.LAYOUT:
         raise ValueError("layout must be 'aos' or 'soa'")
+    if int(project_every) < 0:
+        raise ValueError("project_every must be >= 0")
     return _lib.TraceConfig(
         int(max_steps), float(rtol), float(atol), float(initial_step),
         float(max_step), float(min_step), _precision_code(precision),
         _lib.LAYOUT[layout], int(max(0.0, timeout_s) * 1e9), int(variant),
-        int(blocks_per_sm))
+        int(blocks_per_sm), int(project_every), 0)
 
 
 def propagate(spacetime, state0: Array, n_steps: int, rtol: float = 1e-8,
@@ -148,14 +150,16 @@ def propagate(spacetime, state0: Array, n_steps: int, rtol: float = 1e-8,
               max_step: float = 2.0, precision: str = "fp64", spins=None,
               h0: Array | None = None, layout: str = "aos",
               timeout_s: float = 0.0, variant: int = -1, workspace=None,
-              in_place: bool = False):
+              in_place: bool = False, project_every: int = 0):
     """n_steps attempted DP5(4) steps per ray with per-ray accept/reject and
     step update (tracer.py:111-120), no termination.
 
     Returns (states, h, lam, accepted, stats): ``lam`` is the affine
     parameter each ray advanced (sum of its accepted step sizes, float64).
     ``spins`` (n,) gives each ray its own spin.  With ``in_place`` and a
-    device float64 ``state0`` the states are advanced in place."""
+    device float64 ``state0`` the states are advanced in place.
+    ``project_every`` K > 0 projects every ray onto the null constraint in
+    float64 after every K-th attempt (not in the reference; off by default)."""
     s, host = to_device_f64(state0, "state0")
     n = s.shape[0] if layout == "aos" else s.shape[-1]
     if layout == "aos" and (s.dim() != 2 or s.shape[1] != 8):
@@ -188,7 +192,7 @@ def propagate(spacetime, state0: Array, n_steps: int, rtol: float = 1e-8,
     ws = workspace if workspace is not None else torch.empty(
         lib.bh_trace_workspace_bytes(), dtype=torch.uint8, device=s.device)
     cfg = make_config(1, rtol, atol, initial_step, max_step, 0.0, precision,
-                      layout, timeout_s, variant)
+                      layout, timeout_s, variant, 0, project_every)
     stream = stream_handle()
     _lib.check(lib.bh_propagate(cfg, float(spacetime.mass), float(spacetime.spin),
                                 ptr(spin_t), ptr(states), ptr(h), ptr(lam), ptr(acc), n,

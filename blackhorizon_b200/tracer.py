@@ -83,6 +83,7 @@ def trace_rays(
     blocks_per_sm: int = 0,
     timeout_s: float = DEFAULT_TIMEOUT_S,
     workspace=None,
+    project_every: int = 0,
 ) -> TraceResult:
     """Trace a batch of geodesics to termination (tracer.py:50-157).
 
@@ -90,7 +91,11 @@ def trace_rays(
     radius is at or beyond ``escape_radius`` (tracer.py:95-99) and
     RuntimeError when the device deadline passes.  ``variant="auto"`` picks
     the launch shape with the autotuner (cached per GPU, policy and size);
-    ``precision="auto"`` picks the policy too, by timing both on a probe."""
+    ``precision="auto"`` picks the policy too, by timing both on a probe.
+    ``project_every`` K > 0 projects every ray in flight onto the null
+    constraint H = 0 in float64 every K controller iterations (one Newton
+    step on the spatial momentum, p_t kept); the reference never projects,
+    so it is off by default and runs on the default launch shape."""
     s, host = to_device_f64(state0, "state0")
     if s.dim() != 2 or s.shape[1] != 8:
         raise ValueError("state0 must have shape (n, 8)")
@@ -118,7 +123,7 @@ def trace_rays(
     scene = _lib.Scene(spacetime.mass, spacetime.spin,
                        spacetime.capture_radius(capture_margin), float(escape_radius))
     cfg = make_config(max_steps, rtol, atol, initial_step, max_step, min_step,
-                      precision, "aos", timeout_s, variant, blocks_per_sm)
+                      precision, "aos", timeout_s, variant, blocks_per_sm, project_every)
     stream = stream_handle()
     _lib.check(lib.bh_trace(cfg, scene, ptr(s), ptr(states), ptr(status), ptr(steps),
                             n, ptr(ws), stream), "trace_rays")
@@ -182,6 +187,7 @@ def trace_cameras(
     variant: int = -1,
     blocks_per_sm: int = 0,
     timeout_s: float = DEFAULT_TIMEOUT_S,
+    project_every: int = 0,
 ):
     """Trace every pixel of every camera in one persistent launch.
 
@@ -205,7 +211,7 @@ def trace_cameras(
     status = torch.empty(n, dtype=torch.int32, device=dev)
     steps = torch.empty(n, dtype=torch.int64, device=dev)
     cfg = make_config(max_steps, rtol, atol, initial_step, max_step, min_step,
-                      precision, "aos", timeout_s, variant, blocks_per_sm)
+                      precision, "aos", timeout_s, variant, blocks_per_sm, project_every)
     _lib.check(lib.bh_trace_cameras(cfg, nc, n, ptr(states), ptr(status), ptr(steps),
                                     ptr(ws), wsb, stream), "trace_cameras")
     st = _stats(lib, ws, stream, "trace_cameras")
@@ -235,7 +241,7 @@ class CameraBatch:
                  atol: float = 1e-12, initial_step: float = 0.1, max_step: float = 2.0,
                  min_step: float = 1e-10, *, precision: str = "fp64", variant: int = -1,
                  blocks_per_sm: int = 0, timeout_s: float = DEFAULT_TIMEOUT_S,
-                 graph: bool = True):
+                 graph: bool = True, project_every: int = 0):
         if not scenes:
             raise ValueError("need at least one camera")
         self.lib = _lib.load()
@@ -253,7 +259,8 @@ class CameraBatch:
         self.status = torch.empty(self.n, dtype=torch.int32, device=dev)
         self.steps = torch.empty(self.n, dtype=torch.int64, device=dev)
         self.cfg = make_config(max_steps, rtol, atol, initial_step, max_step, min_step,
-                               precision, "aos", timeout_s, variant, blocks_per_sm)
+                               precision, "aos", timeout_s, variant, blocks_per_sm,
+                               project_every)
         self.graph = None
         if graph:
             torch.cuda.current_stream().synchronize()

@@ -24,7 +24,7 @@
 extern "C" {
 #endif
 
-#define BH_ABI_VERSION 1
+#define BH_ABI_VERSION 2
 
 typedef enum {
     BH_OK = 0,
@@ -90,6 +90,9 @@ typedef struct {
     int64_t timeout_ns;    /* device deadline for the launch; 0 = none */
     int32_t variant;       /* launch-shape variant (bh_trace_variant); -1 = default */
     int32_t blocks_per_sm; /* resident blocks per SM; 0 = occupancy maximum */
+    int32_t project_every; /* Hamiltonian-constraint projection every K controller
+                              iterations, 0 = off (the reference never projects) */
+    int32_t reserved;      /* 0 */
 } bh_trace_config;
 
 /* Whole-launch counters of a trace or propagate call. */

@@ -63,7 +63,7 @@ def test_struct_layouts_match_header(tmp_path):
 
 
 def test_status_strings(bhlib):
-    assert bhlib.bh_abi_version() == 1
+    assert bhlib.bh_abi_version() == 2
     assert bhlib.bh_status_string(0) == b"ok"
     assert b"escape_radius" in bhlib.bh_status_string(-4)
     assert bhlib.bh_trace_workspace_bytes() == 256
@@ -90,6 +90,24 @@ def test_trace_argument_validation(bhlib):
     cfg = _lib.TraceConfig(10, 1e-8, 1e-10, 0.1, 2.0, 1e-10, 0, 0, 0, -1, 0)
     # No workspace: reported before any CUDA call.
     assert bhlib.bh_trace(cfg, scene, None, None, None, None, 1, None, None) == -5
+
+
+def test_projection_config_validation(bhlib):
+    """A negative projection period, and projection on a taped trace (the
+    adjoint replays unprojected steps), are rejected before any CUDA call."""
+    import ctypes as C
+
+    from blackhorizon_b200 import _lib
+
+    scene = _lib.Scene(1.0, 0.9, 1.45, 100.0)
+    cfg = _lib.TraceConfig(5000, 1e-8, 1e-10, 0.1, 2.0, 1e-10, 0, 0, 0, -1, 0, -1, 0)
+    assert bhlib.bh_trace(cfg, scene, None, None, None, None, 1, None, None) == -1
+    assert b"project_every" in bhlib.bh_last_error()
+    cfg.project_every = 4
+    fake = C.c_void_p(0x10000)
+    assert bhlib.bh_trace_tape(cfg, scene, fake, fake, fake, fake, 1, fake, fake, 16, 8,
+                               fake, None) == -1
+    assert b"taped" in bhlib.bh_last_error()
 
 
 def test_trace_tile_argument_validation(bhlib):
