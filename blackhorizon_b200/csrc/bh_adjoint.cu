@@ -51,8 +51,13 @@ __device__ __forceinline__ RayState replay_steps(double m, double a, RayState y,
     return y;
 }
 
+// Four warps per block, three blocks per SM (a 170-register cap, which the
+// float64 sweep fits without spilling).  Two-warp blocks were measured
+// slower for float64.
+constexpr int kAdjointBlock = 128;
+
 template <class V, typename W>
-__global__ void __launch_bounds__(128) adjoint_kernel(
+__global__ void __launch_bounds__(kAdjointBlock, 3) adjoint_kernel(
     double m, double a, const double *h_tape, const double *ckpt,
     const int64_t *steps, long long cap, int every, const double *grad_states,
     double *grad_state0, double *grad_spin, long long n) {
@@ -74,8 +79,21 @@ __global__ void __launch_bounds__(128) adjoint_kernel(
             const long long len = (N - k0 < every) ? (N - k0) : every;
             const RayState y0 = read8(ckpt + (i * nck + seg) * 8);
             replay_steps<V>(m, a, y0, h + k0, len, seg_states);
-            for (long long k = len - 1; k >= 0; --k)
-                dp5_step_vjp<W>(W(m), W(a), seg_states[k], h[k0 + k], lam, ga);
+            // The next step's state and size are loaded before this step's
+            // vector-Jacobian product, which hides their latency.
+            RayState cur = seg_states[len - 1];
+            double hc = h[k0 + len - 1];
+            for (long long k = len - 1; k >= 0; --k) {
+                RayState nxt = cur;
+                double hn = hc;
+                if (k > 0) {
+                    nxt = seg_states[k - 1];
+                    hn = h[k0 + k - 1];
+                }
+                dp5_step_vjp<W>(W(m), W(a), cur, hc, lam, ga);
+                cur = nxt;
+                hc = hn;
+            }
         }
     }
     double *o = grad_state0 + 8 * i;
@@ -103,6 +121,11 @@ using namespace bh;
 
 static unsigned grid128(long long n) {
     long long g = (n + 127) / 128;
+    return (unsigned)(g < 1 ? 1 : g);
+}
+
+static unsigned grid_adjoint(long long n) {
+    long long g = (n + kAdjointBlock - 1) / kAdjointBlock;
     return (unsigned)(g < 1 ? 1 : g);
 }
 
@@ -146,11 +169,11 @@ extern "C" int bh_adjoint(int32_t precision, double mass, double spin,
     }
     cudaStream_t s = (cudaStream_t)stream;
     if (precision == BH_PRECISION_FP64)
-        adjoint_kernel<double, double><<<grid128(n), 128, 0, s>>>(
+        adjoint_kernel<double, double><<<grid_adjoint(n), kAdjointBlock, 0, s>>>(
             mass, spin, h_tape, checkpoints, steps, capacity, checkpoint_every, grad_states,
             grad_state0, grad_spin, n);
     else if (precision == BH_PRECISION_MIXED)
-        adjoint_kernel<float, float><<<grid128(n), 128, 0, s>>>(
+        adjoint_kernel<float, float><<<grid_adjoint(n), kAdjointBlock, 0, s>>>(
             mass, spin, h_tape, checkpoints, steps, capacity, checkpoint_every, grad_states,
             grad_state0, grad_spin, n);
     else {
