@@ -100,7 +100,8 @@ _SIGNATURES = {
     "bh_graph_destroy": (ctypes.c_int, [_P]),
     "bh_trace_tape": (ctypes.c_int, [ctypes.POINTER(TraceConfig), ctypes.POINTER(Scene),
                                      _P, _P, _P, _P, _I64, _P, _P, _I64, _I32, _P, _P]),
-    "bh_adjoint": (ctypes.c_int, [_I32, _D, _D, _P, _P, _P, _I64, _I32, _P, _P, _P, _I64, _P]),
+    "bh_adjoint": (ctypes.c_int, [_I32, _D, _D, _P, _P, _P, _I64, _I32, _P, _P, _P, _P, _I64,
+                                  _P]),
     "bh_replay": (ctypes.c_int, [_I32, _D, _D, _P, _P, _P, _I64, _P, _I64, _P]),
     "bh_trace_tile_workspace_bytes": (_SZ, [_I64]),
     "bh_trace_tile": (ctypes.c_int, [ctypes.POINTER(TraceConfig), ctypes.POINTER(Scene), _D, _D,

@@ -85,16 +85,25 @@ def trace_with_tape(spacetime: KerrSpacetime, state0: torch.Tensor, escape_radiu
     return states, status, steps, tape
 
 
-def adjoint(tape: Tape, grad_states: torch.Tensor, precision: str | None = None):
-    """(dL/d state0 (n,8), dL/d spin per ray (n,)) for dL/d final states."""
+def adjoint(tape: Tape, grad_states: torch.Tensor, precision: str | None = None,
+            sort: bool = True):
+    """(dL/d state0 (n,8), dL/d spin per ray (n,)) for dL/d final states.
+
+    With ``sort`` the threads take the rays in order of decreasing accepted
+    steps, rays without a cotangent last, so that the lanes of a warp sweep
+    segments of equal length together; the results do not depend on it."""
     g = grad_states.detach().to(torch.float64).contiguous()
     n = g.shape[0]
     out = torch.empty_like(g)
     gspin = torch.empty(n, dtype=torch.float64, device=g.device)
+    order = None
+    if sort and n:
+        key = tape.steps.clamp(max=tape.capacity) * (g != 0).any(dim=1)
+        order = torch.argsort(key, descending=True, stable=True).contiguous()
     _lib.check(_lib.load().bh_adjoint(
         _lib.PRECISION[precision or tape.precision], tape.mass, tape.spin, ptr(tape.h),
         ptr(tape.checkpoints), ptr(tape.steps), tape.capacity, tape.every, ptr(g), ptr(out),
-        ptr(gspin), n, stream_handle()), "adjoint")
+        ptr(gspin), ptr(order), n, stream_handle()), "adjoint")
     return out, gspin
 
 

@@ -60,9 +60,10 @@ template <class V, typename W>
 __global__ void __launch_bounds__(kAdjointBlock, 3) adjoint_kernel(
     double m, double a, const double *h_tape, const double *ckpt,
     const int64_t *steps, long long cap, int every, const double *grad_states,
-    double *grad_state0, double *grad_spin, long long n) {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    double *grad_state0, double *grad_spin, const int64_t *order, long long n) {
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= n) return;
+    const long long i = order ? (long long)order[tid] : tid;
     const double *g = grad_states + 8 * i;
     Vec8<double> lam{g[0], g[1], g[2], g[3], g[4], g[5], g[6], g[7]};
     double ga = 0.0;
@@ -150,8 +151,8 @@ extern "C" int bh_adjoint(int32_t precision, double mass, double spin,
                           const double *h_tape, const double *checkpoints,
                           const int64_t *steps, int64_t capacity,
                           int32_t checkpoint_every, const double *grad_states,
-                          double *grad_state0, double *grad_spin, int64_t n,
-                          void *stream) {
+                          double *grad_state0, double *grad_spin, const int64_t *order,
+                          int64_t n, void *stream) {
     if (!(mass > 0.0) || !(fabs(spin) <= mass)) {
         set_error("Kerr bound violated or mass not positive");
         return BH_ERR_INVALID_ARGUMENT;
@@ -171,11 +172,11 @@ extern "C" int bh_adjoint(int32_t precision, double mass, double spin,
     if (precision == BH_PRECISION_FP64)
         adjoint_kernel<double, double><<<grid_adjoint(n), kAdjointBlock, 0, s>>>(
             mass, spin, h_tape, checkpoints, steps, capacity, checkpoint_every, grad_states,
-            grad_state0, grad_spin, n);
+            grad_state0, grad_spin, order, n);
     else if (precision == BH_PRECISION_MIXED)
         adjoint_kernel<float, float><<<grid_adjoint(n), kAdjointBlock, 0, s>>>(
             mass, spin, h_tape, checkpoints, steps, capacity, checkpoint_every, grad_states,
-            grad_state0, grad_spin, n);
+            grad_state0, grad_spin, order, n);
     else {
         set_error("unknown precision");
         return BH_ERR_INVALID_ARGUMENT;

@@ -290,11 +290,15 @@ int bh_trace_tape(const bh_trace_config *config, const bh_scene *scene,
  * checkpoint_every steps is replayed forward from its checkpoint, then swept
  * backward with the stages recomputed (BH_PRECISION_FP64: float64 stage
  * arithmetic; BH_PRECISION_MIXED: float32 stage arithmetic, float64
- * cotangents).  No counterpart in the reference. */
+ * cotangents).  order (device, n, nullable): a permutation of the rays in
+ * the order the threads take them; rays sorted by decreasing accepted steps
+ * (zero cotangents last) keep each warp's lanes in step.  The results are
+ * the same for any order.  No counterpart in the reference. */
 int bh_adjoint(int32_t precision, double mass, double spin, const double *h_tape,
                const double *checkpoints, const int64_t *steps, int64_t capacity,
                int32_t checkpoint_every, const double *grad_states,
-               double *grad_state0, double *grad_spin, int64_t n, void *stream);
+               double *grad_state0, double *grad_spin, const int64_t *order, int64_t n,
+               void *stream);
 
 /* The frozen-sequence map the adjoint differentiates: steps[i] accepted DP5
  * steps of ray i from state0 with the taped sizes, no error control.  Used

@@ -162,3 +162,20 @@ def test_workload_gradients_mixed_policy(cuda):
     rel = np.abs(grads - fd) / np.maximum(np.abs(fd), 1e-8)
     print("mixed loss %.6g grads %s fd %s rel %s" % (loss, grads, fd, rel))
     assert np.all(rel < 1e-2)
+
+
+def test_ray_order_does_not_change_results(cuda):
+    """The sweep's thread order (sorted by accepted steps, or identity) only
+    schedules the rays: results are bit-identical."""
+    from blackhorizon_b200.adjoint import adjoint, trace_with_tape
+    from blackhorizon_b200.kerr import KerrSpacetime
+
+    s0, _ = small_frame()
+    _, status, _, tape = trace_with_tape(KerrSpacetime(1.0, 0.7), s0, 100.0, max_steps=5000,
+                                         rtol=1e-9, capture_margin=0.01, checkpoint_every=16)
+    rng = np.random.default_rng(3)
+    g = torch.as_tensor(rng.normal(size=(s0.shape[0], 8)), device="cuda") * (status == 2)[:, None]
+    for prec in ("fp64", "mixed"):
+        a0, as0 = adjoint(tape, g, precision=prec, sort=False)
+        a1, as1 = adjoint(tape, g, precision=prec, sort=True)
+        assert torch.equal(a0, a1) and torch.equal(as0, as1)
