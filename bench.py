@@ -613,7 +613,7 @@ def adjoint_workload(device, warmup=1, reps=3):
                  "adjoint_over_forward": ms_adj / ms_fwd,
                  "taped_forward_plus_adjoint_over_forward": (ms_tape + ms_adj) / ms_fwd,
                  "accepted_steps_per_ray": float(steps.double().mean()),
-                 "loss": float(loss), "grad": dict(zip(("spin", "inclination", "yaw", "pitch"),
+                 "loss": float(loss.detach()), "grad": dict(zip(("spin", "inclination", "yaw", "pitch"),
                                                        grads))}
         if prec == "fp64":
             base = [C.spin, C.inclination, yaw0, pitch0]

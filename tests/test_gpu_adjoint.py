@@ -144,7 +144,7 @@ def _workload_loss_and_fd(precision):
             t, f = celestial_angles(pt[0], yN)
             vals.append(float(angle_loss(t, f, th_t, ph_t, mask)))
         fd.append((vals[0] - vals[1]) / (2 * eps))
-    return grads, np.array(fd), float(loss)
+    return grads, np.array(fd), float(loss.detach())
 
 
 def test_workload_gradients_against_finite_differences_fp64(cuda):
