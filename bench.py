@@ -460,6 +460,14 @@ def tracer_workloads(device, warmup=2, reps=3):
                  "attempted_ray_steps_per_s": res.attempts / (ms * 1e-3),
                  "attempts_per_ray": res.attempts / C.n, "accepted_per_ray": res.accepted / C.n,
                  "iterations": res.iterations, "variant": tuned["variant"]}
+        # Shading on the device (imaging.py:53-91): only the pixels cross to
+        # the host, 3 bytes per ray against 76 for state, status and steps.
+        from blackhorizon_b200.imaging import render_image_device
+
+        render_image_device(st, res, C.width, C.height)
+        entry["shade_ms"] = min(_event_ms(lambda: render_image_device(st, res, C.width,
+                                                                      C.height), reps))
+        entry["d2h_bytes_image_vs_states"] = [3 * C.n, (64 + 4 + 8) * C.n]
         if ref is not None:
             got = res.status.cpu().numpy()
             diff = got != ref

@@ -103,6 +103,8 @@ _SIGNATURES = {
     "bh_adjoint": (ctypes.c_int, [_I32, _D, _D, _P, _P, _P, _I64, _I32, _P, _P, _P, _P, _I64,
                                   _P]),
     "bh_replay": (ctypes.c_int, [_I32, _D, _D, _P, _P, _P, _I64, _P, _I64, _P]),
+    "bh_celestial_checkerboard": (ctypes.c_int, [_P, _I64, _I32, _P, _P]),
+    "bh_render_image": (ctypes.c_int, [_D, _D, _P, _P, _P, _I64, _I32, _P, _P]),
     "bh_trace_tile_workspace_bytes": (_SZ, [_I64]),
     "bh_trace_tile": (ctypes.c_int, [ctypes.POINTER(TraceConfig), ctypes.POINTER(Scene), _D, _D,
                                      _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _SZ,

@@ -290,6 +290,22 @@ class CameraBatch:
             off += k
         return out
 
+    def images(self, cells: int = 12):
+        """One (height, width, 3) uint8 device image per camera, shaded on the
+        device from the last run (imaging.py:53-91); only these pixels need
+        to cross to the host."""
+        from .imaging import render_image_device
+
+        out, off = [], 0
+        for cs in self.scenes:
+            w, h = int(cs.camera.width), int(cs.camera.height)
+            k = w * h
+            res = TraceResult(states=self.states[off:off + k], status=self.status[off:off + k],
+                              steps=self.steps[off:off + k], iterations=0)
+            out.append(render_image_device(cs.spacetime, res, w, h, cells))
+            off += k
+        return out
+
     def close(self) -> None:
         if self.graph is not None:
             torch.cuda.current_stream().synchronize()

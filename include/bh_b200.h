@@ -308,6 +308,24 @@ int bh_replay(int32_t precision, double mass, double spin, const double *state0,
               const double *h_tape, const int64_t *steps, int64_t capacity,
               double *states, int64_t n, void *stream);
 
+/* ------------------------------------------------------------ shading */
+
+/* imaging.py:27-50 (celestial_checkerboard): RGB (n, 3) uint8 of the checker
+ * cell of each unit direction (n, 3), `cells` cells over the polar angle and
+ * 2 cells over the azimuth (the reference's default is 12). */
+int bh_celestial_checkerboard(const double *directions, int64_t n, int32_t cells,
+                              uint8_t *rgb, void *stream);
+
+/* imaging.py:53-91 (render_image): RGB (n, 3) uint8 per traced ray.
+ * Captured rays are black; escaped rays take the checkerboard colour of
+ * their final spatial coordinate velocity (geodesics.py:98-106), normalised;
+ * rays at the step budget are (120, 32, 32); any other status (200, 0, 200).
+ * states (n, 8) AoS, 16-byte aligned; spin_of_ray (n,) or NULL for `spin`.
+ * For a (height, width) frame in row-major pixel order, rgb is the image. */
+int bh_render_image(double mass, double spin, const double *spin_of_ray,
+                    const double *states, const int32_t *status, int64_t n,
+                    int32_t cells, uint8_t *rgb, void *stream);
+
 /* ------------------------------------------------------------ offline tile */
 
 /* Counters of one bh_trace_tile call. */

@@ -685,3 +685,50 @@ void bho_null_momentum_batch(double m, double a, const double *pos,
     for (int64_t i = 0; i < n; ++i)
         bho_null_momentum(m, a, pos + 3 * i, dir + 3 * i, past, normalize, p + 4 * i);
 }
+
+/* ------------------------------------------------------------ imaging.py */
+
+static void checker_rgb(const double d[3], int cells, uint8_t rgb[3]) {
+    /* imaging.py:38-50, NumPy's evaluation order. */
+    static const uint8_t dark[3] = {24, 30, 52}, light[3] = {104, 128, 178};
+    const double z = np_clip(d[2], -1.0, 1.0);
+    const double theta = acos(z);
+    const double phi = atan2(d[1], d[0]);
+    const int64_t i_theta = (int64_t)floor(theta / M_PI * (double)cells);
+    const int64_t i_phi = (int64_t)floor((phi + M_PI) / (2.0 * M_PI) * 2.0 * (double)cells);
+    const uint8_t *c = ((i_theta + i_phi) % 2) ? light : dark;
+    rgb[0] = c[0]; rgb[1] = c[1]; rgb[2] = c[2];
+}
+
+void bho_celestial_checkerboard(const double *dirs, int64_t n, int cells,
+                                uint8_t *rgb) {
+    for (int64_t i = 0; i < n; ++i) checker_rgb(dirs + 3 * i, cells, rgb + 3 * i);
+}
+
+void bho_render_image(double m, double a, const double *states,
+                      const int32_t *status, int64_t n, int cells, uint8_t *rgb) {
+    for (int64_t i = 0; i < n; ++i) {
+        uint8_t *o = rgb + 3 * i;
+        const int32_t st = status[i];
+        if (st == BHO_CAPTURED) {
+            o[0] = o[1] = o[2] = 0;
+        } else if (st == BHO_ESCAPED) {
+            /* geodesics.py:98-106: spatial coordinate velocity. */
+            const double *y = states + 8 * i;
+            bho_geometry_t g;
+            bho_geometry(m, a, y[1], y[2], y[3], 0, &g);
+            const double lp = -y[4] + sum3(g.l[0] * y[5], g.l[1] * y[6], g.l[2] * y[7]);
+            const double two_h_lp = 2.0 * g.h * lp;
+            double v[3];
+            for (int k = 0; k < 3; ++k) v[k] = y[5 + k] - two_h_lp * g.l[k];
+            double nrm = sqrt(sum3(v[0] * v[0], v[1] * v[1], v[2] * v[2]));
+            if (nrm == 0.0) nrm = 1.0;
+            const double d[3] = {v[0] / nrm, v[1] / nrm, v[2] / nrm};
+            checker_rgb(d, cells, o);
+        } else if (st == BHO_MAX_STEPS) {
+            o[0] = 120; o[1] = 32; o[2] = 32;
+        } else {
+            o[0] = 200; o[1] = 0; o[2] = 200;
+        }
+    }
+}

@@ -129,6 +129,17 @@ void bho_trace_tile(const bho_trace_params_t *p, double disk_inner,
                     double *escape_dir, int32_t *saturated, int64_t n,
                     int nthreads);
 
+/* imaging.py:27-50 (celestial_checkerboard): RGB of the checker cell of each
+ * unit direction (n,3), `cells` cells over the polar angle. */
+void bho_celestial_checkerboard(const double *dirs, int64_t n, int cells,
+                                uint8_t *rgb);
+
+/* imaging.py:53-91 (render_image): per ray, black if captured, the
+ * checkerboard colour of the final coordinate-velocity direction if
+ * escaped, dark red at the step budget, magenta otherwise; rgb (n,3). */
+void bho_render_image(double m, double a, const double *states,
+                      const int32_t *status, int64_t n, int cells, uint8_t *rgb);
+
 /* integrate_dense (integrators.py:127-174) per ray: adaptive DP5(4) from
  * affine parameter 0 to lam_target[i], the last step cut to land on it.
  * Rays that exhaust max_attempts or underflow the step get NaN states.

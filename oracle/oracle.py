@@ -245,3 +245,25 @@ def trace_tile(mass: float, spin: float, state0, escape_radius: float,
                          _ptr(out["saturated"]), _I64(n), ctypes.c_int(nthreads))
     out["states"] = s
     return out
+
+
+def celestial_checkerboard(directions, cells: int = 12):
+    """imaging.py:27-50."""
+    d = _f64(directions)
+    out = np.empty((d.shape[0], 3), dtype=np.uint8)
+    lib().bho_celestial_checkerboard(_ptr(d), _I64(d.shape[0]), ctypes.c_int(cells), _ptr(out))
+    return out
+
+
+def render_image(mass: float, spin: float, states, status, width: int, height: int,
+                 cells: int = 12):
+    """imaging.py:53-91: (height, width, 3) uint8."""
+    s = _f64(states)
+    st = np.ascontiguousarray(status, dtype=np.int32)
+    n = width * height
+    if s.shape[0] != n or st.shape[0] != n:
+        raise ValueError("result size does not match image dimensions")
+    out = np.empty((n, 3), dtype=np.uint8)
+    lib().bho_render_image(_D(mass), _D(spin), _ptr(s), _ptr(st), _I64(n), ctypes.c_int(cells),
+                           _ptr(out))
+    return out.reshape(height, width, 3)

@@ -42,6 +42,7 @@ REF_FILES = [
     "blackhorizon/integrators.py",
     "blackhorizon/tracer.py",
     "blackhorizon/camera.py",
+    "blackhorizon/imaging.py",
     "blackhorizon/examples/benchmark.py",
     "blackhorizon/offline/render.py",
     "blackhorizon/realtime/fly_camera.py",
@@ -379,6 +380,51 @@ def gen_offline_tile(ref, out):
     np.savez_compressed(os.path.join(out, "offline_tile.npz"), **arrs)
 
 
+def gen_images(ref, out):
+    """imaging.py:27-91 on the reference's own traces.
+
+    - render_image of the 40x30 and 160x120 frames of the small config;
+    - celestial_checkerboard of random directions, directions on cell
+      boundaries, and the poles;
+    - render_image of random states with every status code (0-5), so that
+      each status's colour is pinned."""
+    from blackhorizon import imaging
+
+    T = ref["tracer"]
+    kw = dict(escape_radius=100.0, max_steps=5000, rtol=1e-8, atol=1e-10,
+              capture_margin=0.01)
+    arrs = {}
+    for w, h in ((40, 30), (160, 120)):
+        st, s0 = camera_state(ref, 0.9, 50.0, 60.0, 30.0, w, h)
+        res = T.trace_rays(st, s0, **kw)
+        arrs[f"image_{w}x{h}"] = imaging.render_image(st, res, w, h)
+        if w == 40:
+            arrs["states_40x30"] = res.states
+            arrs["status_40x30"] = res.status.astype(np.int32)
+    rng = np.random.default_rng(31)
+    d = rng.normal(size=(4000, 3))
+    d /= np.linalg.norm(d, axis=-1, keepdims=True)
+    # Cell boundaries: polar angles k pi / 12 and azimuths k pi / 12 - pi.
+    k = np.arange(0, 25)
+    th = np.repeat(k * np.pi / 12.0, 25)
+    ph = np.tile(k * np.pi / 12.0 - np.pi, 25)
+    edge = np.stack([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)], axis=-1)
+    poles = np.array([[0.0, 0.0, 1.0], [0.0, 0.0, -1.0], [1.0, 0.0, 0.0], [-1.0, 0.0, 0.0],
+                      [0.0, 1.0, 0.0], [0.0, -1.0, 0.0], [-1.0, -0.0, 0.0]])
+    dirs = np.concatenate([d, edge, poles])
+    arrs["checker_directions"] = dirs
+    arrs["checker_colors_12"] = imaging.celestial_checkerboard(dirs)
+    arrs["checker_colors_7"] = imaging.celestial_checkerboard(dirs, cells=7)
+    st, s0, _, _ = photon_states(ref, 0.9, 600, 41)
+    status = np.arange(600, dtype=np.int32) % 6
+    res = T.TraceResult(states=s0, status=status, steps=np.zeros(600, dtype=np.int64),
+                        iterations=0)
+    arrs["mixed_states"] = s0
+    arrs["mixed_status"] = status
+    arrs["mixed_image"] = imaging.render_image(st, res, 30, 20)
+    np.savez_compressed(os.path.join(out, "images.npz"), **arrs)
+
+
 _REFERENCE_PATH = "/root/reference"
 
 
@@ -407,6 +453,7 @@ def main():
         ("trace_c1", lambda: gen_trace_c1(ref, args.out)),
         ("raw_throughput", lambda: gen_raw_throughput(ref, args.out)),
         ("offline_tile", lambda: gen_offline_tile(ref, args.out)),
+        ("images", lambda: gen_images(ref, args.out)),
     ]
     if not args.skip_c3:
         steps.append(("trace_c3", lambda: gen_trace_c3(ref, args.out, args.procs)))

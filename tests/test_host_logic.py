@@ -114,3 +114,16 @@ def test_uneven_cameras_are_deterministic():
         assert 64 <= c.width <= 1024 and 48 <= c.height <= 768
         assert abs(c.spin) <= 0.998 and 0.0 <= c.inclination <= 90.0
         assert 20.0 <= c.distance <= 200.0
+
+
+def test_save_png_roundtrip(tmp_path):
+    """imaging.save_png writes the RGB array (imaging.py:94-96)."""
+    import numpy as np
+    from PIL import Image
+
+    from blackhorizon_b200.imaging import save_png
+
+    img = (np.arange(4 * 5 * 3) % 251).astype(np.uint8).reshape(4, 5, 3)
+    path = tmp_path / "frame.png"
+    save_png(img, str(path))
+    np.testing.assert_array_equal(np.asarray(Image.open(path).convert("RGB")), img)

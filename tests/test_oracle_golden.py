@@ -183,3 +183,20 @@ def test_offline_tile_with_disk(oracle, tag):
         np.testing.assert_array_equal(o2["status"], g[f"{tag}_retrace_status"])
         for k in ("escape_directions", "hit_positions", "hit_momenta"):
             np.testing.assert_allclose(o2[k], g[f"{tag}_retrace_{k}"], rtol=0, atol=1e-9)
+
+
+def test_imaging_bit_exact(oracle):
+    """imaging.py:27-91: checkerboard colours (random, cell-boundary and pole
+    directions, 12 and 7 cells) and render_image (a traced 40x30 frame, and
+    every status code) equal the reference's pixels."""
+    g = golden("images.npz")
+    for cells in (12, 7):
+        np.testing.assert_array_equal(
+            oracle.celestial_checkerboard(g["checker_directions"], cells),
+            g[f"checker_colors_{cells}"])
+    np.testing.assert_array_equal(
+        oracle.render_image(1.0, 0.9, g["states_40x30"], g["status_40x30"], 40, 30),
+        g["image_40x30"])
+    np.testing.assert_array_equal(
+        oracle.render_image(1.0, 0.9, g["mixed_states"], g["mixed_status"], 30, 20),
+        g["mixed_image"])
