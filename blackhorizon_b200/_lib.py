@@ -62,6 +62,13 @@ class TileStats(ctypes.Structure):
                 ("timed_out", _I32)]
 
 
+class RealtimeConfig(ctypes.Structure):
+    _fields_ = [("max_steps", _I64), ("step_scale", _D), ("min_step", _D), ("max_step", _D),
+                ("capture_margin", _D), ("momentum_bailout", _D), ("escape_radius", _D),
+                ("disk_inner", _D), ("disk_outer", _D), ("interior_stop", _D),
+                ("precision", _I32), ("reserved", _I32)]
+
+
 _SIGNATURES = {
     "bh_abi_version": (ctypes.c_int, []),
     "bh_status_string": (ctypes.c_char_p, [ctypes.c_int]),
@@ -105,6 +112,8 @@ _SIGNATURES = {
     "bh_replay": (ctypes.c_int, [_I32, _D, _D, _P, _P, _P, _I64, _P, _I64, _P]),
     "bh_celestial_checkerboard": (ctypes.c_int, [_P, _I64, _I32, _P, _P]),
     "bh_render_image": (ctypes.c_int, [_D, _D, _P, _P, _P, _I64, _I32, _P, _P]),
+    "bh_trace_realtime": (ctypes.c_int, [ctypes.POINTER(RealtimeConfig), _D, _D, _P, _P, _P,
+                                         _P, _P, _P, _I64, _P, _P]),
     "bh_trace_tile_workspace_bytes": (_SZ, [_I64]),
     "bh_trace_tile": (ctypes.c_int, [ctypes.POINTER(TraceConfig), ctypes.POINTER(Scene), _D, _D,
                                      _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _SZ,

@@ -583,6 +583,44 @@ __device__ __forceinline__ void error_ratio_v(const WStateV<V> &y, const WStateV
     }
 }
 
+// One classical RK4 step (integrators.py:57-73) of size h: stage arithmetic
+// in the lane type V (lane 0), the state update in double.  The derivatives
+// use the split form: dx = p + kappa, dt = -p_t + thl, dp = pdot.
+template <class V>
+__device__ __forceinline__ void rk4_advance(const KerrV<V> &K, RayState &y, double h) {
+    using T = VT<V>;
+    const V hw = T::set(h), half = T::set(0.5 * h);
+    const V zero = T::set(0.0);
+    WStateV<V> w;
+    put_work<V>(w, 0, y);
+    const StageV<V> d1 = rhs_v<V>(K, w.x, w.y, w.z, w.npt, w.px, w.py, w.pz, zero, zero, zero);
+    const V k1x = w.px + d1.kx, k1y = w.py + d1.ky, k1z = w.pz + d1.kz;
+    const V e2x = half * d1.px, e2y = half * d1.py, e2z = half * d1.pz;
+    const StageV<V> d2 = rhs_v<V>(K, T::fma(half, k1x, w.x), T::fma(half, k1y, w.y),
+                                  T::fma(half, k1z, w.z), w.npt, w.px + e2x, w.py + e2y,
+                                  w.pz + e2z, e2x, e2y, e2z);
+    const V k2x = w.px + d2.kx, k2y = w.py + d2.ky, k2z = w.pz + d2.kz;
+    const V e3x = half * d2.px, e3y = half * d2.py, e3z = half * d2.pz;
+    const StageV<V> d3 = rhs_v<V>(K, T::fma(half, k2x, w.x), T::fma(half, k2y, w.y),
+                                  T::fma(half, k2z, w.z), w.npt, w.px + e3x, w.py + e3y,
+                                  w.pz + e3z, e3x, e3y, e3z);
+    const V k3x = w.px + d3.kx, k3y = w.py + d3.ky, k3z = w.pz + d3.kz;
+    const V e4x = hw * d3.px, e4y = hw * d3.py, e4z = hw * d3.pz;
+    const StageV<V> d4 = rhs_v<V>(K, T::fma(hw, k3x, w.x), T::fma(hw, k3y, w.y),
+                                  T::fma(hw, k3z, w.z), w.npt, w.px + e4x, w.py + e4y,
+                                  w.pz + e4z, e4x, e4y, e4z);
+    const V k4x = w.px + d4.kx, k4y = w.py + d4.ky, k4z = w.pz + d4.kz;
+    const V two = T::set(2.0);
+    const double h6 = h / 6.0;
+    y.t += h6 * double(T::set(6.0) * w.npt + (d1.thl + two * d2.thl + two * d3.thl + d4.thl));
+    y.x += h6 * double(k1x + two * k2x + two * k3x + k4x);
+    y.y += h6 * double(k1y + two * k2y + two * k3y + k4y);
+    y.z += h6 * double(k1z + two * k2z + two * k3z + k4z);
+    y.px += h6 * double(d1.px + two * d2.px + two * d3.px + d4.px);
+    y.py += h6 * double(d1.py + two * d2.py + two * d3.py + d4.py);
+    y.pz += h6 * double(d1.pz + two * d2.pz + two * d3.pz + d4.pz);
+}
+
 // Projection onto the null constraint, float64.  The super-Hamiltonian
 // H(x, p) = 1/2 (-p_t^2 + |p|^2) - H_ks lp^2 (geodesics.py:77-95) vanishes on
 // null geodesics; integration error drifts it.  One Newton step along the

@@ -43,7 +43,8 @@ enum {
     BH_RAY_ESCAPED = 2,
     BH_RAY_MAX_STEPS = 3,
     BH_RAY_FAILED = 4,
-    BH_RAY_DISK = 5  /* ended on the equatorial disk (bh_trace_tile only) */
+    BH_RAY_DISK = 5,      /* ended on the equatorial disk (tile and real-time tracers) */
+    BH_RAY_TERMINATED = 6 /* reached the interior stop radius (real-time tracer) */
 };
 
 typedef enum {
@@ -325,6 +326,39 @@ int bh_celestial_checkerboard(const double *directions, int64_t n, int32_t cells
 int bh_render_image(double mass, double spin, const double *spin_of_ray,
                     const double *states, const int32_t *status, int64_t n,
                     int32_t cells, uint8_t *rgb, void *stream);
+
+/* ------------------------------------------------------------ real-time */
+
+/* Controls of the real-time shader algorithm: realtime/settings.py:70-120
+ * (RenderSettings) plus the escape radius and disk of one frame. */
+typedef struct {
+    int64_t max_steps;       /* fixed-step budget, 1..4096 (interior: capped at 1024) */
+    double step_scale;       /* step heuristic gain */
+    double min_step, max_step;
+    double capture_margin;   /* capture at r <= r_plus (1 + margin) */
+    double momentum_bailout; /* |p| at which a ray counts as captured */
+    double escape_radius;
+    double disk_inner, disk_outer; /* disk_outer <= 0: no disk */
+    double interior_stop;    /* > 0: interior camera, rays end at this radius */
+    int32_t precision;       /* bh_precision: RK4 stage arithmetic */
+    int32_t reserved;        /* 0 */
+} bh_realtime_config;
+
+/* realtime/reference.py:41-188 (trace_like_shader): fixed RK4 steps with
+ * h = clip(step_scale (r - r_plus), min_step, max_step) (interior cameras:
+ * a length min(max(|r - r_plus|, 0.15 r), 0.5 r)), capped at 1/max(1, |p|);
+ * capture at the capture radius or when |p| >= momentum_bailout, escape at
+ * escape_radius; a step crossing z = 0 is interpolated linearly and ends the
+ * ray on the disk when the crossing radius is in [disk_inner, disk_outer].
+ * Rays alive after the budget are BH_RAY_MAX_STEPS.  Outputs per ray
+ * (device): final states (n, 8) AoS, status, and for DISK rays the crossing
+ * radius, position (n, 3) and momentum (n, 4), NaN otherwise.  workspace:
+ * bh_trace_workspace_bytes(); bh_trace_stats_read gives the steps taken
+ * (attempts = accepted = total, iterations = the longest ray). */
+int bh_trace_realtime(const bh_realtime_config *config, double mass, double spin,
+                      const double *state0, double *states, int32_t *status,
+                      double *hit_radius, double *hit_positions, double *hit_momenta,
+                      int64_t n, void *workspace, void *stream);
 
 /* ------------------------------------------------------------ offline tile */
 

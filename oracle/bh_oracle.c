@@ -732,3 +732,76 @@ void bho_render_image(double m, double a, const double *states,
         }
     }
 }
+
+/* ------------------------------------------------------- realtime/reference.py */
+
+typedef struct {
+    const bho_realtime_params_t *p;
+    double *states, *hit_radius, *hit_pos, *hit_mom;
+    int32_t *status;
+} realtime_ctx_t;
+
+static void realtime_range(void *vctx, int64_t b, int64_t e, int64_t *acc) {
+    realtime_ctx_t *c = (realtime_ctx_t *)vctx;
+    const bho_realtime_params_t *p = c->p;
+    (void)acc;
+    const double m = p->mass, a = p->spin;
+    const double r_plus = m + sqrt(m * m - a * a);
+    const int interior = p->interior_stop > 0.0;
+    const double capture_radius = interior ? p->interior_stop : r_plus * (1.0 + p->capture_margin);
+    const int32_t capture_status = interior ? BHO_TERMINATED : BHO_CAPTURED;
+    const int64_t max_steps = interior && p->max_steps > 1024 ? 1024 : p->max_steps;
+    const double bail2 = p->momentum_bailout * p->momentum_bailout;
+    for (int64_t i = b; i < e; ++i) {
+        double *y = c->states + 8 * i;
+        int32_t st = BHO_MAX_STEPS;
+        c->hit_radius[i] = NAN;
+        for (int k = 0; k < 3; ++k) c->hit_pos[3 * i + k] = NAN;
+        for (int k = 0; k < 4; ++k) c->hit_mom[4 * i + k] = NAN;
+        for (int64_t it = 0; it < max_steps; ++it) {
+            /* reference.py:107-133 */
+            bho_geometry_t g;
+            bho_geometry(m, a, y[1], y[2], y[3], 0, &g);
+            const double r = g.r;
+            const double mom2 = sum3(y[5] * y[5], y[6] * y[6], y[7] * y[7]);
+            int captured = (r <= capture_radius) || (mom2 >= bail2);
+            if (interior) captured = captured || ((r <= capture_radius * 1.002) && (mom2 > 2500.0));
+            const int escaped = !captured && (r >= p->escape_radius);
+            if (captured) { st = capture_status; break; }
+            if (escaped) { st = BHO_ESCAPED; break; }
+            /* reference.py:135-154 */
+            double scale;
+            if (!interior) scale = r - r_plus;
+            else scale = np_min(np_max(fabs(r - r_plus), 0.15 * r), 0.5 * r);
+            double h = np_clip(p->step_scale * scale, p->min_step, p->max_step);
+            h = np_min(h, 1.0 / np_max(1.0, sqrt(mom2)));
+            double y_new[8];
+            bho_rk4_step(m, a, y, h, y_new);
+            int hit = 0;
+            /* reference.py:162-184 */
+            if (p->disk_outer > 0.0 && y[3] * y_new[3] < 0.0) {
+                const double t = y[3] / (y[3] - y_new[3]);
+                double q[8];
+                for (int k = 0; k < 8; ++k) q[k] = y[k] + t * (y_new[k] - y[k]);
+                bho_geometry_t gh;
+                bho_geometry(m, a, q[1], q[2], q[3], 0, &gh);
+                if (gh.r >= p->disk_inner && gh.r <= p->disk_outer) {
+                    hit = 1;
+                    c->hit_radius[i] = gh.r;
+                    for (int k = 0; k < 3; ++k) c->hit_pos[3 * i + k] = q[1 + k];
+                    for (int k = 0; k < 4; ++k) c->hit_mom[4 * i + k] = q[4 + k];
+                }
+            }
+            memcpy(y, y_new, sizeof(y_new));
+            if (hit) { st = BHO_DISK; break; }
+        }
+        c->status[i] = st;
+    }
+}
+
+void bho_trace_realtime(const bho_realtime_params_t *p, double *states,
+                        int32_t *status, double *hit_radius, double *hit_pos,
+                        double *hit_mom, int64_t n, int nthreads) {
+    realtime_ctx_t c = {p, states, hit_radius, hit_pos, hit_mom, status};
+    bho_parallel_for(n, nthreads, 4, realtime_range, &c);
+}

@@ -140,6 +140,27 @@ void bho_celestial_checkerboard(const double *dirs, int64_t n, int cells,
 void bho_render_image(double m, double a, const double *states,
                       const int32_t *status, int64_t n, int cells, uint8_t *rgb);
 
+/* Controls of the real-time shader algorithm (realtime/settings.py:70-120). */
+typedef struct {
+    double mass, spin, escape_radius;
+    int64_t max_steps;
+    double step_scale, min_step, max_step, capture_margin, momentum_bailout;
+    double disk_inner, disk_outer; /* disk_outer <= 0: no disk */
+    double interior_stop;          /* > 0: interior camera mode */
+} bho_realtime_params_t;
+
+/* Status of a ray that reached the interior stop radius: tracer.py:29. */
+#define BHO_TERMINATED 6
+
+/* realtime/reference.py:41-188 (trace_like_shader) per ray: fixed RK4 steps
+ * with the distance heuristic, momentum bail-out, linear disk crossings.
+ * states (n,8) in/out (final states; DISK rays keep the crossing step's end
+ * state), status (n,), hit radius (n,) and hit position (n,3) / momentum
+ * (n,4) (NaN unless DISK). */
+void bho_trace_realtime(const bho_realtime_params_t *p, double *states,
+                        int32_t *status, double *hit_radius, double *hit_pos,
+                        double *hit_mom, int64_t n, int nthreads);
+
 /* integrate_dense (integrators.py:127-174) per ray: adaptive DP5(4) from
  * affine parameter 0 to lam_target[i], the last step cut to land on it.
  * Rays that exhaust max_attempts or underflow the step get NaN states.

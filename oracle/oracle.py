@@ -267,3 +267,33 @@ def render_image(mass: float, spin: float, states, status, width: int, height: i
     lib().bho_render_image(_D(mass), _D(spin), _ptr(s), _ptr(st), _I64(n), ctypes.c_int(cells),
                            _ptr(out))
     return out.reshape(height, width, 3)
+
+
+class RealtimeParams(ctypes.Structure):
+    """bho_realtime_params_t: realtime/settings.py controls of one trace."""
+    _fields_ = [("mass", _D), ("spin", _D), ("escape_radius", _D), ("max_steps", _I64),
+                ("step_scale", _D), ("min_step", _D), ("max_step", _D),
+                ("capture_margin", _D), ("momentum_bailout", _D), ("disk_inner", _D),
+                ("disk_outer", _D), ("interior_stop", _D)]
+
+
+def trace_realtime(mass: float, spin: float, state0, escape_radius: float, max_steps: int,
+                   step_scale: float, min_step: float = 1e-4, max_step: float = 4.0,
+                   capture_margin: float = 2e-2, momentum_bailout: float = 1e3,
+                   disk_radii=None, interior_stop=None, nthreads: int = 0):
+    """realtime/reference.py:41-188 (trace_like_shader)."""
+    s = _f64(state0).copy()
+    n = s.shape[0]
+    r_in, r_out = (0.0, 0.0) if disk_radii is None else disk_radii
+    p = RealtimeParams(mass, spin, escape_radius, max_steps, step_scale, min_step, max_step,
+                       capture_margin, momentum_bailout, r_in, r_out,
+                       0.0 if interior_stop is None else interior_stop)
+    out = {"status": np.empty(n, dtype=np.int32), "hit_radii": np.empty(n),
+           "hit_positions": np.empty((n, 3)), "hit_momenta": np.empty((n, 4))}
+    lib().bho_trace_realtime(ctypes.byref(p), _ptr(s), _ptr(out["status"]),
+                             _ptr(out["hit_radii"]), _ptr(out["hit_positions"]),
+                             _ptr(out["hit_momenta"]), _I64(n), ctypes.c_int(nthreads))
+    out["states"] = s
+    out["positions"] = s[:, 1:4].copy()
+    out["momenta"] = s[:, 4:8].copy()
+    return out

@@ -46,6 +46,9 @@ REF_FILES = [
     "blackhorizon/examples/benchmark.py",
     "blackhorizon/offline/render.py",
     "blackhorizon/realtime/fly_camera.py",
+    "blackhorizon/realtime/reference.py",
+    "blackhorizon/realtime/settings.py",
+    "blackhorizon/frames.py",
     "blackhorizon/emission/novikov_thorne.py",
     "tests/test_kerr.py",
     "tests/test_shadow.py",
@@ -425,6 +428,101 @@ def gen_images(ref, out):
     np.savez_compressed(os.path.join(out, "images.npz"), **arrs)
 
 
+def _fibonacci_sphere(n):
+    """Nearly uniform unit directions (the construction of the reference's
+    tests/test_interior.py:26-39)."""
+    i = np.arange(n, dtype=float) + 0.5
+    polar = np.arccos(1.0 - 2.0 * i / n)
+    az = np.pi * (1.0 + 5.0 ** 0.5) * i
+    return np.stack([np.cos(az) * np.sin(polar), np.sin(az) * np.sin(polar), np.cos(polar)],
+                    axis=-1)
+
+
+def gen_realtime(ref, out):
+    """realtime/reference.py:41-188 (trace_like_shader), the CPU mirror of the
+    real-time fragment shader, on:
+
+    - the equatorial fans of tests/test_realtime_reference.py at D = 30, with
+      every quality preset at a = 0.9, MEDIUM at a = 0, HIGH and LOW at
+      a = 0.998, and the adaptive tracer's statuses at rtol 1e-10;
+    - a 48x36 pinhole frame with the disk (a = 0.9, D = 30, inclination 80);
+    - interior rain-observer cameras (frames.py:102-218; the views of
+      tests/test_interior.py) at r = 1.9 and 0.5 (a = 0) and inside a = 0.6."""
+    _offline_modules(_REFERENCE_PATH)  # registers the bare realtime package
+    from blackhorizon import frames
+    from blackhorizon.emission.novikov_thorne import disk_inner_radius
+    from blackhorizon.realtime.reference import trace_like_shader
+    from blackhorizon.realtime.settings import QualityPreset, RenderSettings
+
+    G, T, C = ref["geodesics"], ref["tracer"], ref["camera"]
+    K = ref["KerrSpacetime"]
+    arrs = {}
+
+    def store(tag, res, state0, settings, esc, extra=None):
+        arrs[f"{tag}_state0"] = state0
+        arrs[f"{tag}_settings"] = np.array([settings.max_steps, settings.step_scale,
+                                            settings.min_step, settings.max_step,
+                                            settings.capture_margin, settings.momentum_bailout,
+                                            esc])
+        arrs[f"{tag}_status"] = res.status.astype(np.int8)
+        arrs[f"{tag}_positions"] = res.positions
+        arrs[f"{tag}_momenta"] = res.momenta
+        if res.hit_radii is not None:
+            arrs[f"{tag}_hit_radii"] = res.hit_radii
+            arrs[f"{tag}_hit_positions"] = res.hit_positions
+            arrs[f"{tag}_hit_momenta"] = res.hit_momenta
+        for k, v in (extra or {}).items():
+            arrs[f"{tag}_{k}"] = v
+
+    def fan(st, offsets):
+        n = offsets.shape[0]
+        pos = np.tile([[30.0, 0.0, 0.0]], (n, 1))
+        d = np.stack([-np.ones(n), offsets, np.zeros(n)], axis=-1)
+        d /= np.linalg.norm(d, axis=-1, keepdims=True)
+        return G.build_state(pos, G.null_momentum_from_velocity(st, pos, d, "past"))
+
+    wide = np.linspace(0.03, 0.40, 300)
+    wide = np.concatenate([wide, -wide])
+    for spin, offsets, presets, tag in (
+            (0.9, wide, list(QualityPreset), "a09"),
+            (0.0, np.linspace(0.10, 0.25, 600), [QualityPreset.MEDIUM], "a0"),
+            (0.998, wide, [QualityPreset.HIGH], "a0998"),
+            (0.998, np.linspace(0.001, 0.15, 200), [QualityPreset.LOW], "plunge")):
+        st = K(spin=spin)
+        s0 = fan(st, offsets)
+        truth = T.trace_rays(st, s0, escape_radius=60.0, rtol=1e-10)
+        for preset in presets:
+            settings = RenderSettings(spin=spin).apply_preset(preset)
+            res = trace_like_shader(st, s0, settings, escape_radius=60.0)
+            store(f"fan_{tag}_{preset.value}", res, s0, settings, 60.0,
+                  {"spin": np.float64(spin), "truth_status": truth.status.astype(np.int8)})
+    # Disk frame.
+    st = K(spin=0.9)
+    cam = C.PinholeCamera.from_orbit(30.0, 80.0, fov_degrees=40.0, width=48, height=36)
+    pos = cam.ray_origins()
+    s0 = G.build_state(pos, G.null_momentum_from_velocity(st, pos, cam.ray_directions(), "past"))
+    settings = RenderSettings(spin=0.9).apply_preset(QualityPreset.MEDIUM)
+    radii = (float(disk_inner_radius(st)), 18.0)
+    res = trace_like_shader(st, s0, settings, escape_radius=100.0, disk_radii=radii)
+    store("disk", res, s0, settings, 100.0, {"spin": np.float64(0.9), "disk": np.array(radii)})
+    # Interior rain observers.
+    for tag, spin, position in (("in19", 0.0, [1.9, 0.0, 0.0]), ("in05", 0.0, [0.5, 0.0, 0.0]),
+                                ("in_a06", 0.6, [1.2, 0.3, 0.4])):
+        st = K(spin=spin)
+        p = np.array(position)
+        u = frames.rain_four_velocity(st, p[None, :])[0]
+        tetrad = frames.build_tetrad(st, p, u, -p / np.linalg.norm(p), np.array([0.0, 0.0, 1.0]))
+        dirs = _fibonacci_sphere(400)
+        mom = frames.tetrad_ray_momenta(st, p, tetrad, dirs)
+        s0 = G.build_state(np.tile(p[None, :], (400, 1)), mom)
+        settings = RenderSettings(spin=spin, disk_enabled=False).apply_preset(QualityPreset.HIGH)
+        res = trace_like_shader(st, s0, settings, escape_radius=400.0, interior_stop=0.02)
+        store(tag, res, s0, settings, 400.0,
+              {"spin": np.float64(spin), "position": p, "four_velocity": u, "tetrad": tetrad,
+               "directions": dirs})
+    np.savez_compressed(os.path.join(out, "realtime.npz"), **arrs)
+
+
 _REFERENCE_PATH = "/root/reference"
 
 
@@ -454,6 +552,7 @@ def main():
         ("raw_throughput", lambda: gen_raw_throughput(ref, args.out)),
         ("offline_tile", lambda: gen_offline_tile(ref, args.out)),
         ("images", lambda: gen_images(ref, args.out)),
+        ("realtime", lambda: gen_realtime(ref, args.out)),
     ]
     if not args.skip_c3:
         steps.append(("trace_c3", lambda: gen_trace_c3(ref, args.out, args.procs)))

@@ -200,3 +200,33 @@ def test_imaging_bit_exact(oracle):
     np.testing.assert_array_equal(
         oracle.render_image(1.0, 0.9, g["mixed_states"], g["mixed_status"], 30, 20),
         g["mixed_image"])
+
+
+def _realtime_cases(g):
+    tags = sorted({k.rsplit("_", 1)[0] for k in g.files
+                   if k.endswith("_status") and not k.endswith("truth_status")})
+    for t in tags:
+        ms, sc, mn, mx, cm, bo, esc = g[f"{t}_settings"]
+        kw = dict(max_steps=int(ms), step_scale=sc, min_step=mn, max_step=mx,
+                  capture_margin=cm, momentum_bailout=bo)
+        disk = tuple(g[f"{t}_disk"]) if f"{t}_disk" in g.files else None
+        interior = 0.02 if t.startswith("in") else None
+        yield t, float(g[f"{t}_spin"]), float(esc), kw, disk, interior
+
+
+def test_realtime_shader_algorithm_bit_exact(oracle):
+    """realtime/reference.py:41-188 on the reference's own cases: fans at
+    every preset, a disk frame, interior rain-observer views."""
+    g = golden("realtime.npz")
+    n = 0
+    for t, spin, esc, kw, disk, interior in _realtime_cases(g):
+        o = oracle.trace_realtime(1.0, spin, g[f"{t}_state0"], esc, disk_radii=disk,
+                                  interior_stop=interior, **kw)
+        np.testing.assert_array_equal(o["status"], g[f"{t}_status"])
+        np.testing.assert_array_equal(o["positions"], g[f"{t}_positions"])
+        np.testing.assert_array_equal(o["momenta"], g[f"{t}_momenta"])
+        if disk is not None:
+            np.testing.assert_array_equal(o["hit_positions"], g[f"{t}_hit_positions"])
+            np.testing.assert_array_equal(o["hit_momenta"], g[f"{t}_hit_momenta"])
+        n += 1
+    assert n == 11
