@@ -72,12 +72,14 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-workloads", action="store_true",
                     help="skip the full-HD frame, the 64-camera batch and the adjoint")
-    ap.add_argument("--profile-case", choices=("trace", "adjoint", "tile"), default=None,
+    ap.add_argument("--profile-case", choices=("trace", "adjoint", "tile", "realtime"),
+                    default=None,
                     help="run one small untimed case of that kernel (for ncu captures): "
                          "trace = the 1920x1080 frame (2 warm-up launches, then 1); "
                          "adjoint = the 256x256 differentiable frame with a 2000-step "
                          "tape (1 warm-up sweep, then 1); tile = the offline frame at "
-                         "640x400 supersample 2 (1,024,000 rays), first pass only, twice")
+                         "640x400 supersample 2 (1,024,000 rays), first pass only, twice; "
+                         "realtime = the 1280x720 real-time frame, three launches")
     return ap.parse_args()
 
 
@@ -394,6 +396,7 @@ def run_ours(args):
             out["workloads"] = tracer_workloads(device)
             out["workloads"]["differentiable_256x256"] = adjoint_workload(device)
             out["workloads"]["offline_frame"] = offline_workload(device, not args.no_cpu)
+            out["workloads"]["realtime_frame"] = realtime_workload(device, not args.no_cpu)
         if not args.no_cpu:
             out["cpu_baseline"] = cpu_baseline(state0, spin_h, S, args.cpu_seconds)
             out["endpoint_err"] = endpoint_errors(
@@ -561,6 +564,64 @@ def offline_workload(device, with_cpu=True, warmup=1, reps=3, cpu_stride=16):
             "sample": f"every {cpu_stride}th ray of the frame ({idx.size} rays), both passes, "
                       f"oracle/bh_oracle.c tile tracer (float64) on {threads} threads, "
                       f"{dt:.1f} s"}
+        out["fp64_status_agreement_with_oracle"] = float(np.mean(got == o["status"]))
+    return out
+
+
+def realtime_workload(device, with_cpu=True, warmup=2, reps=5, cpu_stride=8):
+    """The real-time viewer's frame (1280x720, MEDIUM preset, a=0.9, r=30 M,
+    inclination 80, fov 60, disk ISCO..18 M) traced with the shader
+    algorithm, both precision policies; frames per second of the tracing
+    kernel alone (initial states resident), and the CPU oracle on every
+    cpu_stride-th ray."""
+    import torch
+
+    from blackhorizon_b200.camera import PinholeCamera
+    from blackhorizon_b200.kerr import KerrSpacetime
+    from blackhorizon_b200.offline import disk_inner_radius
+    from blackhorizon_b200.realtime import QualityPreset, RenderSettings, trace_like_shader
+    from blackhorizon_b200.workloads import REALTIME_FRAME as F
+
+    st = KerrSpacetime(1.0, F.spin)
+    cam = PinholeCamera.from_orbit(F.distance, F.inclination, fov_degrees=F.fov,
+                                   width=F.width, height=F.height)
+    s0 = cam.initial_states(st)
+    settings = RenderSettings(spin=F.spin).apply_preset(QualityPreset(F.preset))
+    radii = (disk_inner_radius(st), settings.disk_outer_radius)
+    out = {"config": F.name, "rays": F.n, "max_steps": settings.max_steps}
+    res = {}
+    for prec in ("mixed", "fp64"):
+        run = lambda: trace_like_shader(st, s0, settings, F.escape_radius,  # noqa: E731
+                                        disk_radii=radii, precision=prec)
+        for _ in range(warmup):
+            r = run()
+        ms = min(_event_ms(run, reps))
+        r = run()
+        res[prec] = r
+        out[prec] = {"ms_per_frame": ms, "frames_per_s": 1e3 / ms, "rays_per_s": F.n / (ms * 1e-3),
+                     "rk4_steps_per_ray": r.steps / F.n,
+                     "rk4_ray_steps_per_s": r.steps / (ms * 1e-3),
+                     "disk": int((r.status == 5).sum()), "escaped": int((r.status == 2).sum()),
+                     "captured": int((r.status == 1).sum())}
+    out["mixed_status_agreement_with_fp64"] = float(
+        (res["mixed"].status == res["fp64"].status).double().mean())
+    if with_cpu:
+        from oracle import oracle
+
+        threads = host_threads()
+        idx = np.arange(0, F.n, cpu_stride)
+        t = time.perf_counter()
+        o = oracle.trace_realtime(1.0, F.spin, s0[idx].cpu().numpy(), F.escape_radius,
+                                  settings.max_steps, settings.step_scale, settings.min_step,
+                                  settings.max_step, settings.capture_margin,
+                                  settings.momentum_bailout, disk_radii=radii, nthreads=threads)
+        dt = time.perf_counter() - t
+        out["cpu_baseline"] = {
+            "value": idx.size / dt, "unit": "rays/s", "cores": threads, "kind": "port",
+            "sample": f"every {cpu_stride}th ray of the frame ({idx.size} rays), "
+                      f"oracle/bh_oracle.c shader algorithm (float64) on {threads} threads, "
+                      f"{dt:.1f} s"}
+        got = res["fp64"].status[torch.as_tensor(idx, device=s0.device)].cpu().numpy()
         out["fp64_status_agreement_with_oracle"] = float(np.mean(got == o["status"]))
     return out
 
@@ -778,6 +839,20 @@ def profile_case(args):
             trace_rays(st, s0, C.escape_radius, max_steps=C.max_steps, rtol=C.rtol,
                        atol=C.atol, capture_margin=C.capture_margin, precision=prec,
                        variant=args.variant)
+    elif args.profile_case == "realtime":
+        from blackhorizon_b200.offline import disk_inner_radius
+        from blackhorizon_b200.realtime import QualityPreset, RenderSettings, trace_like_shader
+        from blackhorizon_b200.workloads import REALTIME_FRAME as F
+
+        st = KerrSpacetime(1.0, F.spin)
+        cam = PinholeCamera.from_orbit(F.distance, F.inclination, fov_degrees=F.fov,
+                                       width=F.width, height=F.height)
+        s0 = cam.initial_states(st)
+        settings = RenderSettings(spin=F.spin).apply_preset(QualityPreset(F.preset))
+        radii = (disk_inner_radius(st), settings.disk_outer_radius)
+        for _ in range(3):
+            trace_like_shader(st, s0, settings, F.escape_radius, disk_radii=radii,
+                              precision=prec)
     elif args.profile_case == "tile":
         from blackhorizon_b200.offline import (FlyCamera, OfflineSettings, camera_states,
                                                disk_radii, trace_tile)

@@ -116,6 +116,36 @@ OFFLINE_FRAME = OfflineFrameConfig("offline-1280x800-ss2-a0.9-i82", 0.9, 26.0, 8
 
 
 @dataclass(frozen=True)
+class RealtimeFrameConfig:
+    """A real-time viewer frame: pinhole camera on the orbit sphere, the
+    shader algorithm at a quality preset, disk from the ISCO to 18 M."""
+
+    name: str
+    spin: float
+    distance: float
+    inclination: float
+    fov: float
+    width: int
+    height: int
+    preset: str
+
+    @property
+    def n(self) -> int:
+        return self.width * self.height
+
+    @property
+    def escape_radius(self) -> float:
+        # realtime/settings.py:166-173 (effective_escape_radius)
+        return max(2.0 * self.distance, 100.0)
+
+
+# A 1280x720 frame at the MEDIUM preset (512 steps), a=0.9, r=30 M,
+# inclination 80 deg, fov 60 deg (the real-time defaults).
+REALTIME_FRAME = RealtimeFrameConfig("realtime-1280x720-medium-a0.9-i80", 0.9, 30.0, 80.0,
+                                     60.0, 1280, 720, "medium")
+
+
+@dataclass(frozen=True)
 class UnevenCamera:
     spin: float
     inclination: float
