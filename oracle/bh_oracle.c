@@ -805,3 +805,204 @@ void bho_trace_realtime(const bho_realtime_params_t *p, double *states,
     realtime_ctx_t c = {p, states, hit_radius, hit_pos, hit_mom, status};
     bho_parallel_for(n, nthreads, 4, realtime_range, &c);
 }
+
+/* ------------------------------------------------------------ vaidya.py */
+
+/* vaidya.py:153-159 */
+static double vd_m1(const bho_vaidya_t *p, double v) {
+    const double vs = np_max(v, p->tail_start);
+    return p->mass - p->tail_mass * pow(p->tail_start / vs, p->tail_power - 1.0);
+}
+
+/* vaidya.py:161-171 */
+static double vd_rate(const bho_vaidya_t *p, double v) {
+    if (!(v >= p->tail_start)) return 0.0;
+    return p->tail_mass * (p->tail_power - 1.0) * pow(p->tail_start, p->tail_power - 1.0) /
+           pow(np_max(v, p->tail_start), p->tail_power);
+}
+
+static double vd_f(const bho_vaidya_t *p, double m, double r) {
+    return 1.0 - 2.0 * m / r + pow(p->charge, 2.0) / pow(r, 2.0);
+}
+
+int64_t bho_vaidya_shell(const bho_vaidya_t *p, double *vs, double *rs, double *m2s,
+                         int64_t capacity) {
+    double v = p->shell_start_v, radius = p->shell_start_radius;
+    double m2 = vd_m1(p, v) + p->shell_energy;
+    int64_t k = 0;
+    if (k < capacity) { vs[k] = v; rs[k] = radius; m2s[k] = m2; }
+    ++k;
+    const double step = 0.01;
+    for (int64_t it = 0; it < 4000000; ++it) {
+        const double m1 = vd_m1(p, v), lum = vd_rate(p, v);
+        const double f1 = vd_f(p, m1, radius), f2 = vd_f(p, m2, radius);
+        if (m2 >= p->mass_cap || fabs(f1) < 1e-300) break;
+        const double r_half = radius + 0.25 * step * f1;
+        const double m2_half = m2 + 0.5 * step * lum * f2 / f1;
+        const double v_half = v + 0.5 * step;
+        const double m1_half = vd_m1(p, v_half), lum_half = vd_rate(p, v_half);
+        const double f1_half = vd_f(p, m1_half, r_half), f2_half = vd_f(p, m2_half, r_half);
+        radius += 0.5 * step * f1_half;
+        m2 += step * lum_half * f2_half / f1_half;
+        if (p->mass_cap < m2) m2 = p->mass_cap; /* Python min(m2, cap) */
+        v += step;
+        if (k < capacity) { vs[k] = v; rs[k] = radius; m2s[k] = m2; }
+        ++k;
+    }
+    return k;
+}
+
+/* numpy.interp for increasing xp (NumPy's compiled interpolation). */
+static double np_interp(double x, const double *xp, const double *fp, int64_t n) {
+    if (isnan(x)) return x;
+    if (x < xp[0]) return fp[0];
+    if (x > xp[n - 1]) return fp[n - 1];
+    if (x == xp[n - 1]) return fp[n - 1];
+    int64_t lo = 0, hi = n - 1; /* xp[lo] <= x < xp[hi] */
+    while (hi - lo > 1) {
+        const int64_t mid = (lo + hi) / 2;
+        if (xp[mid] <= x) lo = mid; else hi = mid;
+    }
+    if (xp[lo] == x) return fp[lo];
+    const double slope = (fp[lo + 1] - fp[lo]) / (xp[lo + 1] - xp[lo]);
+    double r = slope * (x - xp[lo]) + fp[lo];
+    if (isnan(r)) {
+        r = slope * (x - xp[lo + 1]) + fp[lo + 1];
+        if (isnan(r) && fp[lo] == fp[lo + 1]) r = fp[lo];
+    }
+    return r;
+}
+
+/* vaidya.py:244-269 */
+double bho_vaidya_mass(const bho_vaidya_t *p, double v, double r) {
+    const double shell_r = np_interp(v, p->shell_v, p->shell_r, p->n_shell);
+    const double t = np_clip((shell_r - r) / p->shell_width + 0.5, 0.0, 1.0);
+    const double blend = t * t * (3.0 - 2.0 * t);
+    double inc = 0.0;
+    if (!(v < p->shell_start_v)) {
+        const double m2 = np_interp(v, p->shell_v, p->shell_m2, p->n_shell);
+        inc = np_clip(m2 - vd_m1(p, v), 0.0, p->mass_cap);
+    }
+    return vd_m1(p, v) + blend * inc;
+}
+
+double bho_vaidya_misner_sharp(const bho_vaidya_t *p, double v, double r) {
+    return bho_vaidya_mass(p, v, r) - pow(p->charge, 2.0) / (2.0 * r);
+}
+
+void bho_vaidya_geometry(const bho_vaidya_t *p, double t, double x, double y, double z,
+                         double *h, double l[3], double *hs, double *ht, double *radius) {
+    const double r = np_max(sqrt(sum3(x * x, y * y, z * z)), 1e-9);
+    l[0] = x / r; l[1] = y / r; l[2] = z / r;
+    const double v = t + r, eps = 1e-4;
+    const double m0 = bho_vaidya_mass(p, v, r);
+    const double m_v = (bho_vaidya_mass(p, v + eps, r) - bho_vaidya_mass(p, v - eps, r)) / (2.0 * eps);
+    const double m_r = (bho_vaidya_mass(p, v, r + eps) - bho_vaidya_mass(p, v, r - eps)) / (2.0 * eps);
+    const double q2 = pow(p->charge, 2.0);
+    *h = m0 / r - q2 / (2.0 * pow(r, 2.0));
+    const double h_v = m_v / r;
+    const double h_r = m_r / r - m0 / pow(r, 2.0) + q2 / pow(r, 3.0);
+    *hs = h_v + h_r;
+    *ht = h_v;
+    *radius = r;
+}
+
+void bho_vaidya_rhs(const bho_vaidya_t *p, const double y[8], double out[8]) {
+    double h, l[3], hs, ht, r;
+    bho_vaidya_geometry(p, y[0], y[1], y[2], y[3], &h, l, &hs, &ht, &r);
+    const double l_dot_p = sum3(l[0] * y[5], l[1] * y[6], l[2] * y[7]);
+    const double lp = -y[4] + l_dot_p;
+    const double lp2 = lp * lp;
+    out[0] = -y[4] + 2.0 * h * lp;
+    const double c = 2.0 * h * lp;
+    for (int k = 0; k < 3; ++k) out[1 + k] = y[5 + k] - c * l[k];
+    out[4] = ht * lp2;
+    const double g = c / r;
+    for (int k = 0; k < 3; ++k)
+        out[5 + k] = (hs * l[k]) * lp2 + g * (y[5 + k] - l_dot_p * l[k]);
+}
+
+static void vd_rk4_step(const bho_vaidya_t *p, const double y[8], double h, double out[8]) {
+    double k1[8], k2[8], k3[8], k4[8], tmp[8];
+    bho_vaidya_rhs(p, y, k1);
+    for (int i = 0; i < 8; ++i) tmp[i] = y[i] + 0.5 * h * k1[i];
+    bho_vaidya_rhs(p, tmp, k2);
+    for (int i = 0; i < 8; ++i) tmp[i] = y[i] + 0.5 * h * k2[i];
+    bho_vaidya_rhs(p, tmp, k3);
+    for (int i = 0; i < 8; ++i) tmp[i] = y[i] + h * k3[i];
+    bho_vaidya_rhs(p, tmp, k4);
+    const double h6 = h / 6.0;
+    for (int i = 0; i < 8; ++i) out[i] = y[i] + h6 * (k1[i] + 2.0 * k2[i] + 2.0 * k3[i] + k4[i]);
+}
+
+void bho_vaidya_rk4(const bho_vaidya_t *p, double *states, int64_t n, int64_t n_steps,
+                    double h) {
+    for (int64_t i = 0; i < n; ++i)
+        for (int64_t s = 0; s < n_steps; ++s) {
+            double out[8];
+            vd_rk4_step(p, states + 8 * i, h, out);
+            memcpy(states + 8 * i, out, sizeof(out));
+        }
+}
+
+typedef struct {
+    const bho_vaidya_t *p;
+    double *states, *escape_dir, *end_mass, *v_end;
+    double esc, stop;
+    int64_t max_steps;
+    int32_t *status;
+} vd_trace_ctx_t;
+
+static void vd_trace_range(void *vctx, int64_t b, int64_t e, int64_t *acc) {
+    vd_trace_ctx_t *c = (vd_trace_ctx_t *)vctx;
+    const bho_vaidya_t *p = c->p;
+    (void)acc;
+    const double r_plus = p->mass + sqrt(pow(p->mass, 2.0) - pow(p->charge, 2.0));
+    for (int64_t i = b; i < e; ++i) {
+        double *y = c->states + 8 * i;
+        int32_t st = -1;
+        c->escape_dir[3 * i] = c->escape_dir[3 * i + 1] = c->escape_dir[3 * i + 2] = 0.0;
+        c->end_mass[i] = 0.0;
+        for (int64_t it = 0; it < c->max_steps; ++it) {
+            /* inflation.py:197-232 */
+            const double r = sqrt(sum3(y[1] * y[1], y[2] * y[2], y[3] * y[3]));
+            const double mom2 = sum3(y[5] * y[5], y[6] * y[6], y[7] * y[7]);
+            const int captured = (r <= c->stop) || ((r <= c->stop * 1.08) && (mom2 > 400.0)) ||
+                                 (mom2 > 1.0e6);
+            const int escaped = !captured && (r >= c->esc);
+            if (captured) {
+                c->end_mass[i] = bho_vaidya_misner_sharp(p, y[0] + r, r);
+                st = 1;
+                break;
+            }
+            if (escaped) {
+                double h, l[3], hs, ht, rr;
+                bho_vaidya_geometry(p, 0.0, y[1], y[2], y[3], &h, l, &hs, &ht, &rr);
+                const double lp = -y[4] + sum3(l[0] * y[5], l[1] * y[6], l[2] * y[7]);
+                double d[3];
+                for (int k = 0; k < 3; ++k) d[k] = y[5 + k] - 2.0 * h * lp * l[k];
+                const double nrm = sqrt(sum3(d[0] * d[0], d[1] * d[1], d[2] * d[2]));
+                for (int k = 0; k < 3; ++k) c->escape_dir[3 * i + k] = d[k] / nrm;
+                st = 0;
+                break;
+            }
+            /* inflation.py:233-239 */
+            const double scale = r > r_plus ? r - r_plus : 0.5 * r;
+            const double hstep = np_clip(0.15 * scale, 3e-3, 0.08);
+            double out[8];
+            vd_rk4_step(p, y, hstep, out);
+            memcpy(y, out, sizeof(out));
+        }
+        c->status[i] = st == -1 ? 2 : st;
+        c->v_end[i] = y[0] + sqrt(sum3(y[1] * y[1], y[2] * y[2], y[3] * y[3]));
+    }
+}
+
+void bho_vaidya_trace(const bho_vaidya_t *p, double *states, int64_t n,
+                      double escape_radius, double stop_radius, int64_t max_steps,
+                      int32_t *status, double *escape_dir, double *end_mass,
+                      double *v_end, int nthreads) {
+    vd_trace_ctx_t c = {p, states, escape_dir, end_mass, v_end, escape_radius, stop_radius,
+                        max_steps, status};
+    bho_parallel_for(n, nthreads, 2, vd_trace_range, &c);
+}

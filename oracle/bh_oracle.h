@@ -161,6 +161,45 @@ void bho_trace_realtime(const bho_realtime_params_t *p, double *states,
                         int32_t *status, double *hit_radius, double *hit_pos,
                         double *hit_mom, int64_t n, int nthreads);
 
+/* ------------------------------------------------------------ vaidya.py */
+
+/* The charged-Vaidya/Ori surrogate (vaidya.py:87-330): parameters and its
+ * co-integrated shell table (v, R, m2). */
+typedef struct {
+    double mass, charge, tail_mass, tail_start, tail_power, shell_energy,
+        shell_start_v, shell_start_radius, shell_width, mass_cap;
+    const double *shell_v, *shell_r, *shell_m2;
+    int64_t n_shell;
+} bho_vaidya_t;
+
+/* vaidya.py:181-237 (_integrate_shell): writes up to `capacity` table rows
+ * and returns the row count. */
+int64_t bho_vaidya_shell(const bho_vaidya_t *p, double *v, double *r, double *m2,
+                         int64_t capacity);
+
+/* vaidya.py:260-278: mass function m(v, r) and Misner-Sharp mass. */
+double bho_vaidya_mass(const bho_vaidya_t *p, double v, double r);
+double bho_vaidya_misner_sharp(const bho_vaidya_t *p, double v, double r);
+
+/* vaidya.py:285-325 (geometry_t): H, l, dH/dx_i = hs l_i, dH/dt, radius. */
+void bho_vaidya_geometry(const bho_vaidya_t *p, double t, double x, double y, double z,
+                         double *h, double l[3], double *hs, double *ht, double *radius);
+
+/* vaidya.py:356-394 (vaidya_geodesic_rhs). */
+void bho_vaidya_rhs(const bho_vaidya_t *p, const double y[8], double out[8]);
+
+/* n_steps of rk4_step (integrators.py:57-73) with the surrogate's RHS, fixed h. */
+void bho_vaidya_rk4(const bho_vaidya_t *p, double *states, int64_t n, int64_t n_steps,
+                    double h);
+
+/* offline/inflation.py:165-240 (_trace_vaidya_tile) per ray: status 0 escaped,
+ * 1 terminal surface, 2 budget; escape direction (n,3), Misner-Sharp mass at
+ * the terminal point, advanced time v = t + r of the final state. */
+void bho_vaidya_trace(const bho_vaidya_t *p, double *states, int64_t n,
+                      double escape_radius, double stop_radius, int64_t max_steps,
+                      int32_t *status, double *escape_dir, double *end_mass,
+                      double *v_end, int nthreads);
+
 /* integrate_dense (integrators.py:127-174) per ray: adaptive DP5(4) from
  * affine parameter 0 to lam_target[i], the last step cut to land on it.
  * Rays that exhaust max_attempts or underflow the step get NaN states.

@@ -297,3 +297,79 @@ def trace_realtime(mass: float, spin: float, state0, escape_radius: float, max_s
     out["positions"] = s[:, 1:4].copy()
     out["momenta"] = s[:, 4:8].copy()
     return out
+
+
+class VaidyaParams(ctypes.Structure):
+    """bho_vaidya_t: ChargedVaidyaSpacetime fields and its shell table."""
+    _fields_ = [("mass", _D), ("charge", _D), ("tail_mass", _D), ("tail_start", _D),
+                ("tail_power", _D), ("shell_energy", _D), ("shell_start_v", _D),
+                ("shell_start_radius", _D), ("shell_width", _D), ("mass_cap", _D),
+                ("shell_v", _P), ("shell_r", _P), ("shell_m2", _P), ("n_shell", _I64)]
+
+
+class Vaidya:
+    """The charged-Vaidya/Ori surrogate (vaidya.py:87-330) with its shell
+    table integrated by the C restatement."""
+
+    def __init__(self, mass=1.0, charge=0.9, tail_mass=0.01, tail_start=12.0, tail_power=12.0,
+                 shell_energy=1e-3, shell_start_v=14.0, shell_start_radius=1.0,
+                 shell_width=0.02, mass_cap=1e7):
+        self.p = VaidyaParams(mass, charge, tail_mass, tail_start, tail_power, shell_energy,
+                              shell_start_v, shell_start_radius, shell_width, mass_cap,
+                              None, None, None, 0)
+        cap = 4000002
+        v, r, m2 = np.empty(cap), np.empty(cap), np.empty(cap)
+        k = lib().bho_vaidya_shell(ctypes.byref(self.p), _ptr(v), _ptr(r), _ptr(m2), _I64(cap))
+        self.shell_v, self.shell_r, self.shell_m2 = v[:k].copy(), r[:k].copy(), m2[:k].copy()
+        self.p.shell_v, self.p.shell_r = _ptr(self.shell_v), _ptr(self.shell_r)
+        self.p.shell_m2, self.p.n_shell = _ptr(self.shell_m2), k
+
+    def geometry_t(self, states):
+        s = _f64(states)
+        n = s.shape[0]
+        out = {k: np.empty(n) for k in ("h", "hs", "ht", "radius")}
+        out["l"] = np.empty((n, 3))
+        f = lib().bho_vaidya_geometry
+        for i in range(n):
+            h, hs, ht, r = _D(), _D(), _D(), _D()
+            l3 = (_D * 3)()
+            f(ctypes.byref(self.p), _D(s[i, 0]), _D(s[i, 1]), _D(s[i, 2]), _D(s[i, 3]),
+              ctypes.byref(h), l3, ctypes.byref(hs), ctypes.byref(ht), ctypes.byref(r))
+            out["h"][i], out["hs"][i], out["ht"][i], out["radius"][i] = h.value, hs.value, \
+                ht.value, r.value
+            out["l"][i] = list(l3)
+        return out
+
+    def mass(self, v, r):
+        f = lib().bho_vaidya_mass
+        f.restype = _D
+        g = lib().bho_vaidya_misner_sharp
+        g.restype = _D
+        m = np.array([f(ctypes.byref(self.p), _D(a), _D(b)) for a, b in zip(v, r)])
+        ms = np.array([g(ctypes.byref(self.p), _D(a), _D(b)) for a, b in zip(v, r)])
+        return m, ms
+
+    def rhs(self, states):
+        s = _f64(states)
+        out = np.empty_like(s)
+        for i in range(s.shape[0]):
+            lib().bho_vaidya_rhs(ctypes.byref(self.p), s[i].ctypes.data_as(_P),
+                                 out[i].ctypes.data_as(_P))
+        return out
+
+    def rk4(self, states, n_steps, h):
+        s = _f64(states).copy()
+        lib().bho_vaidya_rk4(ctypes.byref(self.p), _ptr(s), _I64(s.shape[0]), _I64(n_steps),
+                             _D(h))
+        return s
+
+    def trace(self, state0, escape_radius, stop_radius, max_steps=900, nthreads=0):
+        """offline/inflation.py:165-240: (status, escape_dir, end_mass, v_end)."""
+        s = _f64(state0).copy()
+        n = s.shape[0]
+        status = np.empty(n, dtype=np.int32)
+        edir, mass, v_end = np.empty((n, 3)), np.empty(n), np.empty(n)
+        lib().bho_vaidya_trace(ctypes.byref(self.p), _ptr(s), _I64(n), _D(escape_radius),
+                               _D(stop_radius), _I64(max_steps), _ptr(status), _ptr(edir),
+                               _ptr(mass), _ptr(v_end), ctypes.c_int(nthreads))
+        return status, edir, mass, v_end

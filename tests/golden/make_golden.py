@@ -49,6 +49,8 @@ REF_FILES = [
     "blackhorizon/realtime/reference.py",
     "blackhorizon/realtime/settings.py",
     "blackhorizon/frames.py",
+    "blackhorizon/vaidya.py",
+    "blackhorizon/offline/inflation.py",
     "blackhorizon/emission/novikov_thorne.py",
     "tests/test_kerr.py",
     "tests/test_shadow.py",
@@ -523,6 +525,100 @@ def gen_realtime(ref, out):
     np.savez_compressed(os.path.join(out, "realtime.npz"), **arrs)
 
 
+def gen_vaidya(ref, out):
+    """vaidya.py (the charged-Vaidya/Ori surrogate) and the tracing loop of
+    the mass-inflation renderer (offline/inflation.py:165-240):
+
+    - the shell tables of three spacetimes: the default (q = 0.9), the
+      flythrough one of tests/test_vaidya.py (shell at v = 6, R = 1.2) and
+      the static limit (no tail, no shell);
+    - geometry_t, mass_function / misner_sharp_mass and vaidya_geodesic_rhs
+      at random points around the layer;
+    - 3000 RK4 steps (h = 0.002) of the two rays of tests/test_vaidya.py;
+    - two tiles of flythrough camera rays (rain observer at r = 1.3, v = 6 and
+      at r = 0.8 inside the layer) traced by _trace_vaidya_tile."""
+    _offline_modules(_REFERENCE_PATH)
+    from blackhorizon import frames
+    from blackhorizon.offline import inflation
+    from blackhorizon.vaidya import ChargedVaidyaSpacetime, vaidya_geodesic_rhs
+
+    I = ref["integrators"]
+    arrs = {}
+    specs = {"default": {}, "fly": {"shell_start_v": 6.0, "shell_start_radius": 1.2},
+             "static": {"tail_mass": 0.0, "shell_energy": 0.0}}
+    spaces = {}
+    for tag, kw in specs.items():
+        st = ChargedVaidyaSpacetime(charge=0.9, **kw)
+        spaces[tag] = st
+        arrs[f"{tag}_params"] = np.array([st.mass, st.charge, st.tail_mass, st.tail_start,
+                                          st.tail_power, st.shell_energy, st.shell_start_v,
+                                          st.shell_start_radius, st.shell_width, st.mass_cap])
+        if st._shell_v.size <= 100000:
+            arrs[f"{tag}_shell_v"] = st._shell_v
+            arrs[f"{tag}_shell_r"] = st._shell_r
+            arrs[f"{tag}_shell_m2"] = st._shell_m2
+        else:
+            # The static limit never reaches the mass cap and runs the full
+            # 4e6 steps; its increment is zero, so keep the ends only.
+            arrs[f"{tag}_shell_size"] = np.int64(st._shell_v.size)
+            for k, a in (("v", st._shell_v), ("r", st._shell_r), ("m2", st._shell_m2)):
+                arrs[f"{tag}_shell_{k}_ends"] = np.concatenate([a[:50], a[-50:]])
+    rng = np.random.default_rng(51)
+    n = 2000
+    t = rng.uniform(0.0, 40.0, n)
+    u = rng.normal(size=(n, 3))
+    u /= np.linalg.norm(u, axis=-1, keepdims=True)
+    pts = u * np.exp(rng.uniform(np.log(0.3), np.log(30.0), n))[:, None]
+    p = rng.normal(size=(n, 4))
+    states = np.concatenate([t[:, None], pts, p], axis=1)
+    states = np.concatenate([states, np.array([[20.0, 0.9, 0.3, 0.2, -1.1, 0.4, -0.7, 0.5]])])
+    arrs["sample_states"] = states
+    for tag, st in spaces.items():
+        g = st.geometry_t(states[:, 0], states[:, 1], states[:, 2], states[:, 3])
+        arrs[f"{tag}_geo_h"] = g.h
+        arrs[f"{tag}_geo_l"] = g.l
+        arrs[f"{tag}_geo_hs"] = g.h_spatial_scale
+        arrs[f"{tag}_geo_ht"] = g.h_t
+        arrs[f"{tag}_geo_r"] = g.radius
+        v = states[:, 0] + np.linalg.norm(states[:, 1:4], axis=-1)
+        r = np.linalg.norm(states[:, 1:4], axis=-1)
+        arrs[f"{tag}_mass"] = st.mass_function(v, r)
+        arrs[f"{tag}_misner_sharp"] = st.misner_sharp_mass(v, r)
+        arrs[f"{tag}_rhs"] = vaidya_geodesic_rhs(st, states)
+    for tag, st, y0 in (("static", spaces["static"],
+                         [[0.0, 5.0, 0.0, 0.0, 1.0, 0.0, 0.55, 0.0]]),
+                        ("default", spaces["default"],
+                         [[13.0, 3.0, 0.0, 0.5, 1.0, -0.9, 0.2, 0.1]])):
+        y = np.array(y0)
+        for _ in range(3000):
+            y = I.rk4_step(lambda b, st=st: vaidya_geodesic_rhs(st, b), y, np.array([0.002]))
+        arrs[f"{tag}_rk4_state0"] = np.array(y0)
+        arrs[f"{tag}_rk4_final"] = y
+    st = spaces["fly"]
+    for tag, radius, time_ in (("tile_out", 1.3, 6.0), ("tile_in", 0.8, 9.0)):
+        state = inflation.rain_state(st, np.array([radius, 0.0, 0.0]), time_)
+        velocity = inflation.camera_four_velocity(st, state)
+        slice_geo = st.frozen(float(state[0, 0]))
+        pos = state[0, 1:4]
+        outward = pos / np.linalg.norm(pos)
+        tetrad = frames.build_tetrad(slice_geo, pos, velocity, outward,
+                                     np.array([0.0, 0.0, 1.0]))
+        dirs = _fibonacci_sphere(300)
+        mom = frames.tetrad_ray_momenta(slice_geo, pos, tetrad, dirs)
+        s0 = np.concatenate([np.full((300, 1), float(state[0, 0])), np.tile(pos, (300, 1)), mom],
+                            axis=1)
+        esc = max(12.0, 2.5 * radius)
+        stop = st.inner_horizon_radius * 1.001
+        status, edir, mass, v_end = inflation._trace_vaidya_tile(st, s0, esc, stop)
+        arrs[f"{tag}_state0"] = s0
+        arrs[f"{tag}_radii"] = np.array([esc, stop])
+        arrs[f"{tag}_status"] = status.astype(np.int8)
+        arrs[f"{tag}_escape_dir"] = edir
+        arrs[f"{tag}_end_mass"] = mass
+        arrs[f"{tag}_v_end"] = v_end
+    np.savez_compressed(os.path.join(out, "vaidya.npz"), **arrs)
+
+
 _REFERENCE_PATH = "/root/reference"
 
 
@@ -553,6 +649,7 @@ def main():
         ("offline_tile", lambda: gen_offline_tile(ref, args.out)),
         ("images", lambda: gen_images(ref, args.out)),
         ("realtime", lambda: gen_realtime(ref, args.out)),
+        ("vaidya", lambda: gen_vaidya(ref, args.out)),
     ]
     if not args.skip_c3:
         steps.append(("trace_c3", lambda: gen_trace_c3(ref, args.out, args.procs)))
