@@ -69,6 +69,13 @@ class RealtimeConfig(ctypes.Structure):
                 ("precision", _I32), ("reserved", _I32)]
 
 
+class Vaidya(ctypes.Structure):
+    _fields_ = [("mass", _D), ("charge", _D), ("tail_mass", _D), ("tail_start", _D),
+                ("tail_power", _D), ("shell_energy", _D), ("shell_start_v", _D),
+                ("shell_start_radius", _D), ("shell_width", _D), ("mass_cap", _D),
+                ("shell_v", _P), ("shell_r", _P), ("shell_m2", _P), ("n_shell", _I64)]
+
+
 _SIGNATURES = {
     "bh_abi_version": (ctypes.c_int, []),
     "bh_status_string": (ctypes.c_char_p, [ctypes.c_int]),
@@ -114,6 +121,14 @@ _SIGNATURES = {
     "bh_render_image": (ctypes.c_int, [_D, _D, _P, _P, _P, _I64, _I32, _P, _P]),
     "bh_trace_realtime": (ctypes.c_int, [ctypes.POINTER(RealtimeConfig), _D, _D, _P, _P, _P,
                                          _P, _P, _P, _I64, _P, _P]),
+    "bh_vaidya_shell_table": (_I64, [ctypes.POINTER(Vaidya), _P, _P, _P, _I64]),
+    "bh_vaidya_geometry": (ctypes.c_int, [ctypes.POINTER(Vaidya), _P, _P, _P, _P, _I64, _P, _P,
+                                          _P, _P, _P, _P]),
+    "bh_vaidya_mass": (ctypes.c_int, [ctypes.POINTER(Vaidya), _P, _P, _I64, _P, _P, _P]),
+    "bh_vaidya_rhs": (ctypes.c_int, [ctypes.POINTER(Vaidya), _P, _P, _I64, _P]),
+    "bh_vaidya_rk4": (ctypes.c_int, [ctypes.POINTER(Vaidya), _P, _P, _P, _I64, _I64, _P]),
+    "bh_vaidya_trace": (ctypes.c_int, [ctypes.POINTER(Vaidya), _P, _I64, _D, _D, _I64, _P, _P,
+                                       _P, _P, _P, _P, _P]),
     "bh_trace_tile_workspace_bytes": (_SZ, [_I64]),
     "bh_trace_tile": (ctypes.c_int, [ctypes.POINTER(TraceConfig), ctypes.POINTER(Scene), _D, _D,
                                      _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _SZ,

@@ -360,6 +360,60 @@ int bh_trace_realtime(const bh_realtime_config *config, double mass, double spin
                       double *hit_radius, double *hit_positions, double *hit_momenta,
                       int64_t n, void *workspace, void *stream);
 
+/* ------------------------------------------------------------ Vaidya surrogate */
+
+/* The charged-Vaidya/Ori mass-inflation surrogate (vaidya.py:87-135): the
+ * ChargedVaidyaSpacetime fields and its shell table (advanced time v,
+ * shell radius R, inflated mass m2; n_shell rows, v increasing), which
+ * bh_vaidya_shell_table integrates on the host and the caller copies to
+ * device memory for the device functions below. */
+typedef struct {
+    double mass, charge, tail_mass, tail_start, tail_power, shell_energy;
+    double shell_start_v, shell_start_radius, shell_width, mass_cap;
+    const double *shell_v, *shell_r, *shell_m2; /* device, n_shell rows */
+    int64_t n_shell;
+} bh_vaidya;
+
+/* vaidya.py:181-237 (_integrate_shell): the shell table into HOST arrays of
+ * `capacity` rows; returns the number of rows the table has (call with
+ * capacity 0 to size it; at most 4,000,001), or -1. */
+int64_t bh_vaidya_shell_table(const bh_vaidya *spacetime, double *v, double *r,
+                              double *m2, int64_t capacity);
+
+/* vaidya.py:285-325 (geometry_t): per point (t, x, y, z) the potential H,
+ * l (n, 3), dH/dx_i = h_spatial_scale l_i, dH/dt and the radius. */
+int bh_vaidya_geometry(const bh_vaidya *spacetime, const double *t, const double *x,
+                       const double *y, const double *z, int64_t n, double *h,
+                       double *l, double *h_spatial_scale, double *h_t,
+                       double *radius, void *stream);
+
+/* vaidya.py:260-278: mass function m(v, r) and Misner-Sharp mass
+ * m - q^2/(2r); either output may be NULL. */
+int bh_vaidya_mass(const bh_vaidya *spacetime, const double *v, const double *r,
+                   int64_t n, double *mass, double *misner_sharp, void *stream);
+
+/* vaidya.py:356-394 (vaidya_geodesic_rhs): d(state)/d(lambda), (n, 8). */
+int bh_vaidya_rhs(const bh_vaidya *spacetime, const double *states, double *deriv,
+                  int64_t n, void *stream);
+
+/* n_steps of rk4_step (integrators.py:57-73) with the surrogate's RHS and a
+ * per-ray step h (n,). */
+int bh_vaidya_rk4(const bh_vaidya *spacetime, const double *states, const double *h,
+                  double *out, int64_t n, int64_t n_steps, void *stream);
+
+/* offline/inflation.py:165-240 (_trace_vaidya_tile): fixed RK4 steps of
+ * clip(0.15 L, 3e-3, 0.08) (L = r - r_plus outside, r/2 inside) until the
+ * terminal surface (status 1: r <= stop_radius, or r <= 1.08 stop_radius with
+ * |p|^2 > 400, or |p|^2 > 1e6; Misner-Sharp mass there in end_mass), escape
+ * (status 0: r >= escape_radius; unit direction of p - 2 H lp l on the t = 0
+ * slice in escape_dir (n, 3)) or the budget (status 2).  Also the final
+ * states and v_end = t + r of every ray.  workspace:
+ * bh_trace_workspace_bytes(). */
+int bh_vaidya_trace(const bh_vaidya *spacetime, const double *state0, int64_t n,
+                    double escape_radius, double stop_radius, int64_t max_steps,
+                    double *states, int32_t *status, double *escape_dir,
+                    double *end_mass, double *v_end, void *workspace, void *stream);
+
 /* ------------------------------------------------------------ offline tile */
 
 /* Counters of one bh_trace_tile call. */
