@@ -397,6 +397,7 @@ def run_ours(args):
             out["workloads"]["differentiable_256x256"] = adjoint_workload(device)
             out["workloads"]["offline_frame"] = offline_workload(device, not args.no_cpu)
             out["workloads"]["realtime_frame"] = realtime_workload(device, not args.no_cpu)
+            out["workloads"]["inflation_tile"] = inflation_workload(device, not args.no_cpu)
         if not args.no_cpu:
             out["cpu_baseline"] = cpu_baseline(state0, spin_h, S, args.cpu_seconds)
             out["endpoint_err"] = endpoint_errors(
@@ -623,6 +624,60 @@ def realtime_workload(device, with_cpu=True, warmup=2, reps=5, cpu_stride=8):
                       f"{dt:.1f} s"}
         got = res["fp64"].status[torch.as_tensor(idx, device=s0.device)].cpu().numpy()
         out["fp64_status_agreement_with_oracle"] = float(np.mean(got == o["status"]))
+    return out
+
+
+def inflation_workload(device, with_cpu=True, warmup=1, reps=3, side=256, cpu_stride=4):
+    """The mass-inflation renderer's tracing (offline/inflation.py:165-240):
+    a rain observer at r = 1.3 M, v = 6 in the flythrough surrogate (q = 0.9,
+    Ori shell launched at v = 6, R = 1.2) looking inward (toward the
+    layer), side x side tetrad rays, fixed RK4 through the time-dependent
+    geometry."""
+    import math as _m
+
+    import torch
+
+    from blackhorizon_b200.frames import build_tetrad, tetrad_ray_momenta
+    from blackhorizon_b200.vaidya import (ChargedVaidyaSpacetime, camera_four_velocity,
+                                          rain_state, trace_vaidya_tile)
+
+    st = ChargedVaidyaSpacetime(charge=0.9, shell_start_v=6.0, shell_start_radius=1.2)
+    state = rain_state(st, np.array([1.3, 0.0, 0.0]), 6.0)
+    u = camera_four_velocity(st, state)
+    pos = state[0, 1:4]
+    tet = build_tetrad(st.frozen(6.0), pos, u, -pos / np.linalg.norm(pos),
+                       np.array([0.0, 0.0, 1.0]))
+    tan_half = _m.tan(_m.radians(70.0) / 2.0)
+    g = (np.arange(side) + 0.5) / side * 2.0 - 1.0
+    uu, vv = np.meshgrid(g, -g)
+    local = np.stack([np.ones(side * side), uu.ravel() * tan_half, vv.ravel() * tan_half], -1)
+    local /= np.linalg.norm(local, axis=-1, keepdims=True)
+    mom = tetrad_ray_momenta(st.frozen(6.0), pos, tet, local)
+    s0 = np.concatenate([np.full((side * side, 1), 6.0), np.tile(pos, (side * side, 1)), mom], 1)
+    s0d = torch.as_tensor(s0, device=device)
+    esc, stop = max(12.0, 2.5 * 1.3), st.inner_horizon_radius * 1.001
+    run = lambda: trace_vaidya_tile(st, s0d, esc, stop)  # noqa: E731
+    for _ in range(warmup):
+        status, _, _, _ = run()
+    ms = min(_event_ms(run, reps))
+    status = run()[0].cpu().numpy()
+    out = {"rays": side * side, "ms_per_tile": ms, "rays_per_s": side * side / (ms * 1e-3),
+           "escaped": int((status == 0).sum()), "terminal": int((status == 1).sum()),
+           "budget": int((status == 2).sum())}
+    if with_cpu:
+        from oracle import oracle
+
+        threads = host_threads()
+        ov = oracle.Vaidya(charge=0.9, shell_start_v=6.0, shell_start_radius=1.2)
+        idx = np.arange(0, side * side, cpu_stride)
+        t = time.perf_counter()
+        o_status, _, _, _ = ov.trace(s0[idx], esc, stop, nthreads=threads)
+        dt = time.perf_counter() - t
+        out["cpu_baseline"] = {
+            "value": idx.size / dt, "unit": "rays/s", "cores": threads, "kind": "port",
+            "sample": f"every {cpu_stride}th ray ({idx.size}), oracle/bh_oracle.c surrogate "
+                      f"(float64) on {threads} threads, {dt:.1f} s"}
+        out["status_agreement_with_oracle"] = float(np.mean(status[idx] == o_status))
     return out
 
 
