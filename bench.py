@@ -316,6 +316,7 @@ def run_ours(args):
     # ---- end to end through the public API with host (pinned) buffers
     host_state = state0.cpu().pin_memory()
     host_spin = torch.as_tensor(spin_h).pin_memory()
+    host_out = torch.empty_like(host_state).pin_memory()
     st_mass = KerrSpacetime(1.0, 0.0)
     e2e_k = max(1, min(args.steps, 3))
 
@@ -325,7 +326,10 @@ def run_ours(args):
         out, _, _, _, _ = propagate(st_mass, s_dev, S, rtol=1e-8, atol=1e-10,
                                  precision=prec, spins=sp_dev, in_place=True,
                                  timeout_s=600.0, variant=args.variant, workspace=ws)
-        return out.to("cpu")
+        # The end states into a pinned host buffer (the caller's result).
+        host_out.copy_(out, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return host_out
 
     e2e_step()
     barrier()
