@@ -387,6 +387,20 @@ __device__ __forceinline__ void put_work(WStateV<V> &w, int l, const RayState &y
     T::put(w.pz, l, S(y.pz));
 }
 
+// put_work after a step: p_t is conserved, so its rounded copy stays.
+template <class V>
+__device__ __forceinline__ void put_work_moved(WStateV<V> &w, int l, const RayState &y) {
+    using T = VT<V>;
+    using S = typename T::S;
+    T::put(w.t, l, S(y.t));
+    T::put(w.x, l, S(y.x));
+    T::put(w.y, l, S(y.y));
+    T::put(w.z, l, S(y.z));
+    T::put(w.px, l, S(y.px));
+    T::put(w.py, l, S(y.py));
+    T::put(w.pz, l, S(y.pz));
+}
+
 // Result of one DP5(4) attempt (integrators.py:76-107) for every lane.  The
 // float64 candidate state is not formed here: `ynw` (the candidate in the
 // lane type) feeds k7 and the error norm, and commit() adds the increments
@@ -525,7 +539,7 @@ __device__ __forceinline__ void commit(RayState &y, WStateV<V> &yw,
         y.py = y.py + double(T::get(a.dpy, l));
         y.pz = y.pz + double(T::get(a.dpz, l));
     }
-    put_work<V>(yw, l, y);
+    put_work_moved<V>(yw, l, y);
 }
 
 #undef BH_LIN2
