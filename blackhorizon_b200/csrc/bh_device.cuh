@@ -597,16 +597,16 @@ __device__ __forceinline__ void error_ratio_v(const WStateV<V> &y, const WStateV
     }
 }
 
-// One classical RK4 step (integrators.py:57-73) of size h: stage arithmetic
-// in the lane type V (lane 0), the state update in double.  The derivatives
-// use the split form: dx = p + kappa, dt = -p_t + thl, dp = pdot.
+// Stage sums of one classical RK4 step (integrators.py:57-73) from the
+// rounded state w with a step hw per lane: S = k1 + 2 k2 + 2 k3 + k4 for t,
+// x, y, z, p_x, p_y, p_z, in the lane type.  The derivatives use the split
+// form: dx = p + kappa, dt = -p_t + thl, dp = pdot.
 template <class V>
-__device__ __forceinline__ void rk4_advance(const KerrV<V> &K, RayState &y, double h) {
+__device__ __forceinline__ void rk4_sums(const KerrV<V> &K, const WStateV<V> &w, V hw,
+                                         V S[7]) {
     using T = VT<V>;
-    const V hw = T::set(h), half = T::set(0.5 * h);
+    const V half = hw * T::set(0.5);
     const V zero = T::set(0.0);
-    WStateV<V> w;
-    put_work<V>(w, 0, y);
     const StageV<V> d1 = rhs_v<V>(K, w.x, w.y, w.z, w.npt, w.px, w.py, w.pz, zero, zero, zero);
     const V k1x = w.px + d1.kx, k1y = w.py + d1.ky, k1z = w.pz + d1.kz;
     const V e2x = half * d1.px, e2y = half * d1.py, e2z = half * d1.pz;
@@ -625,14 +625,39 @@ __device__ __forceinline__ void rk4_advance(const KerrV<V> &K, RayState &y, doub
                                   w.pz + e4z, e4x, e4y, e4z);
     const V k4x = w.px + d4.kx, k4y = w.py + d4.ky, k4z = w.pz + d4.kz;
     const V two = T::set(2.0);
+    S[0] = T::set(6.0) * w.npt + (d1.thl + two * d2.thl + two * d3.thl + d4.thl);
+    S[1] = k1x + two * k2x + two * k3x + k4x;
+    S[2] = k1y + two * k2y + two * k3y + k4y;
+    S[3] = k1z + two * k2z + two * k3z + k4z;
+    S[4] = d1.px + two * d2.px + two * d3.px + d4.px;
+    S[5] = d1.py + two * d2.py + two * d3.py + d4.py;
+    S[6] = d1.pz + two * d2.pz + two * d3.pz + d4.pz;
+}
+
+// Lane l's float64 state after an RK4 step of size h with stage sums S.
+template <class V>
+__device__ __forceinline__ void rk4_update(RayState &y, const V S[7], int l, double h) {
+    using T = VT<V>;
     const double h6 = h / 6.0;
-    y.t += h6 * double(T::set(6.0) * w.npt + (d1.thl + two * d2.thl + two * d3.thl + d4.thl));
-    y.x += h6 * double(k1x + two * k2x + two * k3x + k4x);
-    y.y += h6 * double(k1y + two * k2y + two * k3y + k4y);
-    y.z += h6 * double(k1z + two * k2z + two * k3z + k4z);
-    y.px += h6 * double(d1.px + two * d2.px + two * d3.px + d4.px);
-    y.py += h6 * double(d1.py + two * d2.py + two * d3.py + d4.py);
-    y.pz += h6 * double(d1.pz + two * d2.pz + two * d3.pz + d4.pz);
+    y.t += h6 * double(T::get(S[0], l));
+    y.x += h6 * double(T::get(S[1], l));
+    y.y += h6 * double(T::get(S[2], l));
+    y.z += h6 * double(T::get(S[3], l));
+    y.px += h6 * double(T::get(S[4], l));
+    y.py += h6 * double(T::get(S[5], l));
+    y.pz += h6 * double(T::get(S[6], l));
+}
+
+// One classical RK4 step of size h for a single ray (lane type with one
+// lane): stage arithmetic in V, the state update in double.
+template <class V>
+__device__ __forceinline__ void rk4_advance(const KerrV<V> &K, RayState &y, double h) {
+    using T = VT<V>;
+    WStateV<V> w;
+    put_work<V>(w, 0, y);
+    V S[7];
+    rk4_sums<V>(K, w, T::set(h), S);
+    rk4_update<V>(y, S, 0, h);
 }
 
 // Projection onto the null constraint, float64.  The super-Hamiltonian
