@@ -76,6 +76,7 @@ struct Variant {
 int trace_variant_count(int precision);
 Variant trace_variant(int precision, int idx);
 int trace_default_variant(int precision);
+int propagate_default_variant(int precision);
 
 // Registers and occupancy of a compiled trace (propagate = false) or propagate
 // kernel variant; returns 0 on success.

@@ -507,14 +507,16 @@ static const void *tile_kernel_for(int precision, int idx, bool inl, size_t *sme
     }
 }
 
+// Measured on the offline renderer's 1280x800 supersample-2 frame: mixed
+// 37.9 ms with one float ray per thread at 128 x 3 (54.4 ms packed two per
+// thread: the parking and refill work does not pack); float64 36.3 ms at
+// 256 x 2 (37.4 ms at 128 x 3).
 int tile_default_variant(int precision) {
-    return precision == BH_PRECISION_MIXED ? 5 : 1;
+    return precision == BH_PRECISION_MIXED ? 0 : 3;
 }
 
 cudaError_t launch_tile(const TileArgs &args, int precision, int variant,
                         int blocks_per_sm, cudaStream_t stream) {
-    // Defaults: float64 128 x 3 (the 128-register shapes spill here), mixed
-    // packed float32x2 128 x 3.
     if (variant < 0 || variant >= trace_variant_count(precision))
         variant = tile_default_variant(precision);
     const Variant v = trace_variant(precision, variant);

@@ -393,7 +393,14 @@ int trace_variant_count(int precision) {
 Variant trace_variant(int precision, int idx) {
     return precision == BH_PRECISION_MIXED ? kVariantsMixed[idx] : kVariantsF64[idx];
 }
+// Defaults measured on the raw-throughput and full-HD workloads: float64
+// 256 x 2 for both kernels; mixed: two rays per thread (packed float32x2,
+// 128 x 3) for the propagator, one ray per thread (128 x 5) for the tracer,
+// whose per-ray termination and refill work does not pack.
 int trace_default_variant(int precision) {
+    return precision == BH_PRECISION_MIXED ? 2 : 3;
+}
+int propagate_default_variant(int precision) {
     return precision == BH_PRECISION_MIXED ? 5 : 3;
 }
 
@@ -408,9 +415,11 @@ static const void *kfn(bool propagate, size_t *smem) {
 // shapes only (the launcher switches to them).
 static const void *kernel_for(bool propagate, int precision, int idx, bool project,
                               size_t *smem) {
-    if (project)
-        return precision == BH_PRECISION_MIXED ? kfn<F2, 128, 3, true>(propagate, smem)
-                                               : kfn<double, 256, 2, true>(propagate, smem);
+    if (project) {
+        if (precision != BH_PRECISION_MIXED) return kfn<double, 256, 2, true>(propagate, smem);
+        return propagate ? kfn<F2, 128, 3, true>(propagate, smem)
+                         : kfn<float, 128, 5, true>(propagate, smem);
+    }
     if (precision == BH_PRECISION_MIXED) {
         switch (idx) {
             case 0: return kfn<float, 128, 3>(propagate, smem);
@@ -453,7 +462,8 @@ static cudaError_t launch(bool propagate, const TraceArgs &args, int precision,
                           int variant, int blocks_per_sm, cudaStream_t stream) {
     const bool project = args.project_every > 0;
     if (project || variant < 0 || variant >= trace_variant_count(precision))
-        variant = trace_default_variant(precision);
+        variant = propagate ? propagate_default_variant(precision)
+                            : trace_default_variant(precision);
     const Variant v = trace_variant(precision, variant);
     size_t smem = 0;
     const void *fn = kernel_for(propagate, precision, variant, project, &smem);

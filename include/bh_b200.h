@@ -180,7 +180,8 @@ int bh_rk4(double mass, double spin, const double *state, const double *h,
  * registers per thread), rays per thread (2 = two rays in the halves of
  * packed float32x2 instructions, mixed precision only), and the registers
  * and resident blocks per SM of the compiled trace kernel.  The autotuner
- * times them; index -1 in bh_trace_config selects the default. */
+ * times them; index -1 in bh_trace_config selects the default (here: the
+ * tracer's; the propagator's mixed default is the packed 128 x 3 shape). */
 int bh_trace_variant_count(int32_t precision);
 int bh_trace_variant(int32_t precision, int32_t index, int32_t *block_threads,
                      int32_t *min_blocks, int32_t *rays_per_thread,
