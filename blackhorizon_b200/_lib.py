@@ -24,6 +24,7 @@ BH_ERR_TAPE = -6
 
 PRECISION = {"fp64": 0, "mixed": 1}
 LAYOUT = {"aos": 0, "soa": 1}
+TRACE_INTERIOR = 1  # bh_trace_flag BH_TRACE_INTERIOR
 
 _D = ctypes.c_double
 _I32 = ctypes.c_int32
@@ -48,7 +49,7 @@ class TraceConfig(ctypes.Structure):
                 ("initial_step", _D), ("max_step", _D), ("min_step", _D),
                 ("precision", _I32), ("layout", _I32), ("timeout_ns", _I64),
                 ("variant", _I32), ("blocks_per_sm", _I32), ("project_every", _I32),
-                ("reserved", _I32)]
+                ("flags", _I32)]
 
 
 class TraceStats(ctypes.Structure):

@@ -279,6 +279,7 @@ static int config_ok(const bh_trace_config *c) {
         return invalid("max_steps must be in [1, 2^60]");
     if (c->timeout_ns < 0) return invalid("timeout_ns must be >= 0");
     if (c->project_every < 0) return invalid("project_every must be >= 0");
+    if (c->flags != 0) return invalid("config flags are accepted by bh_trace_tile only");
     return BH_OK;
 }
 

@@ -135,6 +135,7 @@ struct TileArgs {
     int layout;
     int round;  // 0: rays from state0; r > 0: resume records of parity r & 1
     int flush;  // finalise every ray in flight as IN_FLIGHT without stepping
+    int interior;  // interior camera: capture_radius is the stop radius
     double mass, spin, capture_radius, escape_radius;
     double disk_inner, disk_outer;  // disk_outer <= 0: no crossing tests
     double rtol, atol, initial_step, max_step;

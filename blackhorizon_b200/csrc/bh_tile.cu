@@ -48,7 +48,17 @@ __device__ __forceinline__ int tile_check(const TileArgs &a, const RayState &y,
     // render.py:223: the loop ends after 4 max_steps iterations.
     if (attempts >= a.max_attempts) return BH_RAY_IN_FLIGHT;
     const double r = ks_radius(a.spin, y);
-    if (r <= a.capture_radius) return BH_RAY_CAPTURED;
+    if (a.interior) {
+        // render.py:234-248: diverging spatial momentum ends the ray on the
+        // terminal surface.
+        // Rounded as NumPy does it: ((px^2 + py^2) + pz^2), no contraction.
+        const double pn = ::sqrt(__dadd_rn(__dadd_rn(__dmul_rn(y.px, y.px), __dmul_rn(y.py, y.py)),
+                                           __dmul_rn(y.pz, y.pz)));
+        if (r <= a.capture_radius || pn > 1.0e3 || (r <= a.capture_radius * 1.002 && pn > 50.0))
+            return BH_RAY_TERMINATED;
+    } else if (r <= a.capture_radius) {
+        return BH_RAY_CAPTURED;
+    }
     if (r >= a.escape_radius) return BH_RAY_ESCAPED;
     if (steps >= a.max_steps) return BH_RAY_MAX_STEPS;
     return -1;
@@ -588,6 +598,9 @@ extern "C" int bh_trace_tile(const bh_trace_config *config, const bh_scene *scen
     if (c.max_steps < 1 || c.max_steps > (1LL << 60))
         return tile_invalid("max_steps must be in [1, 2^60]");
     if (c.timeout_ns < 0) return tile_invalid("timeout_ns must be >= 0");
+    if (c.flags & ~BH_TRACE_INTERIOR) return tile_invalid("unknown config flags");
+    if ((c.flags & BH_TRACE_INTERIOR) && !(scene->capture_radius > 0.0))
+        return tile_invalid("an interior camera needs a stop radius > 0");
     if (!(scene->mass > 0.0) || !(std::fabs(scene->spin) <= scene->mass))
         return tile_invalid("Kerr bound violated or mass not positive");
     if (disk_outer > 0.0 && !(disk_inner >= 0.0 && disk_inner <= disk_outer))
@@ -615,6 +628,7 @@ extern "C" int bh_trace_tile(const bh_trace_config *config, const bh_scene *scen
     a.mass = scene->mass;
     a.spin = scene->spin;
     a.capture_radius = scene->capture_radius;
+    a.interior = (c.flags & BH_TRACE_INTERIOR) ? 1 : 0;
     a.escape_radius = scene->escape_radius;
     a.disk_inner = disk_inner;
     a.disk_outer = disk_outer;

@@ -133,7 +133,8 @@ def make_config(max_steps: int = 1, rtol: float = 1e-9, atol: float = 1e-12,
                 initial_step: float = 0.1, max_step: float = 2.0,
                 min_step: float = 1e-10, precision: str = "fp64",
                 layout: str = "aos", timeout_s: float = 0.0, variant: int = -1,
-                blocks_per_sm: int = 0, project_every: int = 0) -> "_lib.TraceConfig":
+                blocks_per_sm: int = 0, project_every: int = 0,
+                flags: int = 0) -> "_lib.TraceConfig":
     if layout not in _lib.LAYOUT:
         raise ValueError("layout must be 'aos' or 'soa'")
     if int(project_every) < 0:
@@ -142,7 +143,7 @@ def make_config(max_steps: int = 1, rtol: float = 1e-9, atol: float = 1e-12,
         int(max_steps), float(rtol), float(atol), float(initial_step),
         float(max_step), float(min_step), _precision_code(precision),
         _lib.LAYOUT[layout], int(max(0.0, timeout_s) * 1e9), int(variant),
-        int(blocks_per_sm), int(project_every), 0)
+        int(blocks_per_sm), int(project_every), int(flags))
 
 
 def propagate(spacetime, state0: Array, n_steps: int, rtol: float = 1e-8,

@@ -24,7 +24,7 @@
 extern "C" {
 #endif
 
-#define BH_ABI_VERSION 2
+#define BH_ABI_VERSION 3
 
 typedef enum {
     BH_OK = 0,
@@ -93,8 +93,18 @@ typedef struct {
     int32_t blocks_per_sm; /* resident blocks per SM; 0 = occupancy maximum */
     int32_t project_every; /* Hamiltonian-constraint projection every K controller
                               iterations, 0 = off (the reference never projects) */
-    int32_t reserved;      /* 0 */
+    int32_t flags;         /* bh_trace_flag bits; 0 for every call but bh_trace_tile */
 } bh_trace_config;
+
+/* Bits of bh_trace_config.flags. */
+typedef enum {
+    /* bh_trace_tile: interior camera (offline/render.py:203-248).  The
+     * scene's capture_radius is the interior stop radius; a ray ends with
+     * BH_RAY_TERMINATED at r <= stop, when the norm of its spatial momentum
+     * (p_x, p_y, p_z) exceeds 1e3, or at r <= 1.002 stop with a norm above
+     * 50. */
+    BH_TRACE_INTERIOR = 1
+} bh_trace_flag;
 
 /* Whole-launch counters of a trace or propagate call. */
 typedef struct {
@@ -432,9 +442,10 @@ typedef struct {
  * crossing records (168 B) and n resume records (96 B). */
 size_t bh_trace_tile_workspace_bytes(int64_t n);
 
-/* blackhorizon/offline/render.py:184-309 (_trace_tile, exterior cameras)
- * with the crossing refinement of render.py:312-349 (_refine_crossings).
- * Per ray, before each attempt: captured (r <= scene->capture_radius),
+/* blackhorizon/offline/render.py:184-309 (_trace_tile) with the crossing
+ * refinement of render.py:312-349 (_refine_crossings).  Per ray, before each
+ * attempt: captured (r <= scene->capture_radius; BH_TRACE_INTERIOR in
+ * config->flags selects the interior-camera rules of that flag),
  * escaped (r >= scene->escape_radius) or out of budget (steps >=
  * config->max_steps, BH_RAY_MAX_STEPS); then one DP5(4) attempt with
  * config->rtol and config->atol (the reference passes atol = rtol * 1e-3);

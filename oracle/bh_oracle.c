@@ -538,6 +538,7 @@ static int refine_crossing(double m, double a, const double y0[8], double h_full
 typedef struct {
     const bho_trace_params_t *p;
     double capture_radius, r_in, r_out;
+    int interior;  /* interior camera: capture_radius is the interior stop */
     double *states, *hit_pos, *hit_mom, *escape_dir;
     int32_t *status, *saturated;
     int64_t *steps;
@@ -561,10 +562,17 @@ static void tile_range(void *vctx, int64_t b, int64_t e, int64_t *acc) {
             /* render.py:231-260: termination before the step. */
             bho_geometry_t g;
             bho_geometry(p->mass, p->spin, y[1], y[2], y[3], 0, &g);
-            const int captured = g.r <= c->capture_radius;
+            int captured = g.r <= c->capture_radius;
+            if (c->interior) {
+                /* render.py:234-248: a diverging spatial momentum ends the
+                 * ray on the terminal surface. */
+                const double pn = sqrt(sum3(y[5] * y[5], y[6] * y[6], y[7] * y[7]));
+                captured = captured || pn > 1.0e3 ||
+                           (g.r <= c->capture_radius * 1.002 && pn > 50.0);
+            }
             const int escaped = !captured && g.r >= p->escape_radius;
             const int exhausted = steps >= p->max_steps;
-            if (captured) { status = BHO_CAPTURED; break; }
+            if (captured) { status = c->interior ? BHO_TERMINATED : BHO_CAPTURED; break; }
             if (escaped) { status = BHO_ESCAPED; break; }
             if (exhausted) { status = BHO_MAX_STEPS; break; }
             /* render.py:264-266 */
@@ -610,12 +618,15 @@ static void tile_range(void *vctx, int64_t b, int64_t e, int64_t *acc) {
 }
 
 void bho_trace_tile(const bho_trace_params_t *p, double disk_inner,
-                    double disk_outer, double *states, int32_t *status,
-                    int64_t *steps, double *hit_pos, double *hit_mom,
-                    double *escape_dir, int32_t *saturated, int64_t n,
-                    int nthreads) {
+                    double disk_outer, double interior_stop, double *states,
+                    int32_t *status, int64_t *steps, double *hit_pos,
+                    double *hit_mom, double *escape_dir, int32_t *saturated,
+                    int64_t n, int nthreads) {
     const double r_plus = p->mass + sqrt(p->mass * p->mass - p->spin * p->spin);
-    tile_ctx_t c = {p, r_plus * (1.0 + p->capture_margin), disk_inner, disk_outer,
+    /* render.py:203-213 */
+    const int interior = interior_stop > 0.0;
+    tile_ctx_t c = {p, interior ? interior_stop : r_plus * (1.0 + p->capture_margin),
+                    disk_inner, disk_outer, interior,
                     states, hit_pos, hit_mom, escape_dir, status, saturated, steps};
     bho_parallel_for(n, nthreads, 4, tile_range, &c);
 }

@@ -112,22 +112,26 @@ void bho_propagate_batch(double mass, double spin, const double *spins,
 /* Status of a ray that hit the accretion disk: tracer.py:28 (RayStatus.DISK). */
 #define BHO_DISK 5
 
-/* offline/render.py:184-309 (_trace_tile) for exterior cameras, with the
+/* offline/render.py:184-309 (_trace_tile), with the
  * equatorial-disk refinement of render.py:312-349 (_refine_crossings): the
  * termination test comes before each step, the error scale uses atol =
  * rtol * 1e-3, and an accepted step whose z changes sign is bisected 40
  * times along RK4 substeps; a crossing radius in [disk_inner, disk_outer]
- * ends the ray with BHO_DISK.  disk_outer <= 0 disables the disk.  Rays still
+ * ends the ray with BHO_DISK.  disk_outer <= 0 disables the disk.
+ * interior_stop > 0 selects the interior-camera mode (render.py:203-248):
+ * rays end with BHO_TERMINATED at r <= interior_stop, when the spatial
+ * momentum norm exceeds 1e3, or at r <= 1.002 interior_stop with a norm
+ * above 50; else capture is at r_plus (1 + capture_margin).  Rays still
  * in flight after 4*max_steps iterations keep BHO_IN_FLIGHT.  Outputs per
  * ray: status, accepted steps, final state (n,8; the pre-crossing state for
  * disk hits), hit position/momentum (n,3 each, zero unless DISK), escape
  * direction (n,3, render.py:164-181, zero unless ESCAPED) and the
  * saturation flag (MAX_STEPS or steps >= int(0.85 max_steps)). */
 void bho_trace_tile(const bho_trace_params_t *p, double disk_inner,
-                    double disk_outer, double *states, int32_t *status,
-                    int64_t *steps, double *hit_pos, double *hit_mom,
-                    double *escape_dir, int32_t *saturated, int64_t n,
-                    int nthreads);
+                    double disk_outer, double interior_stop, double *states,
+                    int32_t *status, int64_t *steps, double *hit_pos,
+                    double *hit_mom, double *escape_dir, int32_t *saturated,
+                    int64_t n, int nthreads);
 
 /* imaging.py:27-50 (celestial_checkerboard): RGB of the checker cell of each
  * unit direction (n,3), `cells` cells over the polar angle. */

@@ -228,9 +228,11 @@ def propagate_to(mass: float, spins, state0, lam_target, rtol: float = 1e-12,
 
 def trace_tile(mass: float, spin: float, state0, escape_radius: float,
                disk_radii=None, rtol: float = 1e-9, max_steps: int = 12000,
-               max_step: float = 2.0, capture_margin: float = 1e-3, nthreads: int = 0):
-    """offline/render.py:184-349 (_trace_tile with _refine_crossings),
-    exterior cameras.  Returns a dict of per-ray arrays."""
+               max_step: float = 2.0, capture_margin: float = 1e-3, nthreads: int = 0,
+               interior_stop: float | None = None):
+    """offline/render.py:184-349 (_trace_tile with _refine_crossings);
+    ``interior_stop`` selects the interior-camera termination of
+    render.py:203-248.  Returns a dict of per-ray arrays."""
     s = _f64(state0).copy()
     n = s.shape[0]
     out = {"status": np.empty(n, dtype=np.int32), "steps": np.empty(n, dtype=np.int64),
@@ -239,7 +241,11 @@ def trace_tile(mass: float, spin: float, state0, escape_radius: float,
     p = TraceParams(mass, spin, escape_radius, max_steps, rtol, rtol * 1e-3, 0.1, max_step,
                     0.0, capture_margin)
     r_in, r_out = (0.0, 0.0) if disk_radii is None else disk_radii
-    lib().bho_trace_tile(ctypes.byref(p), _D(r_in), _D(r_out), _ptr(s), _ptr(out["status"]),
+    stop = 0.0 if interior_stop is None else float(interior_stop)
+    if interior_stop is not None and not stop > 0.0:
+        raise ValueError("interior_stop must be > 0")
+    lib().bho_trace_tile(ctypes.byref(p), _D(r_in), _D(r_out), _D(stop), _ptr(s),
+                         _ptr(out["status"]),
                          _ptr(out["steps"]), _ptr(out["hit_positions"]),
                          _ptr(out["hit_momenta"]), _ptr(out["escape_directions"]),
                          _ptr(out["saturated"]), _I64(n), ctypes.c_int(nthreads))

@@ -54,6 +54,7 @@ REF_FILES = [
     "blackhorizon/emission/novikov_thorne.py",
     "tests/test_kerr.py",
     "tests/test_shadow.py",
+    "tests/test_bluesheet.py",
 ]
 
 
@@ -385,6 +386,62 @@ def gen_offline_tile(ref, out):
     np.savez_compressed(os.path.join(out, "offline_tile.npz"), **arrs)
 
 
+# Interior cameras of render_hdr (render.py:520-550 with camera_tetrad): the
+# rain observer's tetrad, pinhole directions, tetrad momenta, escape radius
+# max(100, 1.3 disk_outer).  (tag, spin, position, forward, up, stop, disk);
+# stop None is the realistic terminal surface 1.02 r_minus.
+INTERIOR_CASES = [
+    ("sheet", 0.9, (0.03, 0.03, 0.68), (0.0, 0.0, -1.0), (0.0, 1.0, 0.0), None, False),
+    ("ideal", 0.9, (0.03, 0.03, 1.2), (0.0, 0.0, -1.0), (0.0, 1.0, 0.0), 0.02, False),
+    ("disk", 0.6, (0.6, 0.3, 1.0), (0.0, 1.0, 0.0), (0.0, 0.0, 1.0), None, True),
+    ("schw", 0.0, (0.0, 0.0, 1.5), (0.0, 0.0, -1.0), (0.0, 1.0, 0.0), 0.05, True),
+]
+
+
+def gen_offline_interior(ref, out):
+    """render.py:184-309 in interior-camera mode (interior_stop) on 32x24
+    tetrad tiles (fov 80, supersample 1) of cameras inside the horizon,
+    as tests/test_bluesheet.py:86-130 sets them up."""
+    render, _, disk_inner_radius = _offline_modules(_REFERENCE_PATH)
+    from blackhorizon.frames import build_tetrad, rain_four_velocity, tetrad_ray_momenta
+
+    G = ref["geodesics"]
+    arrs = {}
+    for tag, spin, pos, fwd, up, stop, disk in INTERIOR_CASES:
+        st = ref["KerrSpacetime"](1.0, spin)
+        stop = st.inner_horizon_radius * 1.02 if stop is None else stop
+        pos = np.array(pos)
+        vel = rain_four_velocity(st, pos[None, :])[0]
+        tet = build_tetrad(st, pos, vel, np.array(fwd), np.array(up))
+        settings = render.OfflineSettings(spin=spin, supersample=1, fov_degrees=80.0,
+                                          disk_enabled=disk)
+        d = render.pinhole_grid(32, 24, settings.fov_degrees, 1)
+        mom = tetrad_ray_momenta(st, pos, tet, d)
+        s0 = G.build_state(np.tile(pos[None, :], (d.shape[0], 1)), mom)
+        r_in = float(disk_inner_radius(st))
+        r_out = max(settings.disk_outer_radius, r_in + 1.0)
+        esc = max(100.0, 1.3 * r_out)
+        radii = (r_in, r_out) if disk else None
+        res = render._trace_tile(st, s0, esc, settings, radii, settings.rtol,
+                                 settings.max_steps, interior_stop=stop)
+        arrs[f"{tag}_spin"] = np.float64(spin)
+        arrs[f"{tag}_position"] = pos
+        arrs[f"{tag}_forward"] = np.array(fwd)
+        arrs[f"{tag}_up"] = np.array(up)
+        arrs[f"{tag}_velocity"] = vel
+        arrs[f"{tag}_tetrad"] = tet
+        arrs[f"{tag}_stop"] = np.float64(stop)
+        arrs[f"{tag}_disk"] = np.array([r_in, r_out] if disk else [0.0, 0.0])
+        arrs[f"{tag}_escape_radius"] = np.float64(esc)
+        arrs[f"{tag}_state0"] = s0
+        arrs[f"{tag}_status"] = res.status.astype(np.int8)
+        arrs[f"{tag}_escape_directions"] = res.escape_directions
+        arrs[f"{tag}_hit_positions"] = res.hit_positions
+        arrs[f"{tag}_hit_momenta"] = res.hit_momenta
+        arrs[f"{tag}_saturated"] = res.saturated.astype(np.int8)
+    np.savez_compressed(os.path.join(out, "offline_interior.npz"), **arrs)
+
+
 def gen_images(ref, out):
     """imaging.py:27-91 on the reference's own traces.
 
@@ -647,6 +704,7 @@ def main():
         ("trace_c1", lambda: gen_trace_c1(ref, args.out)),
         ("raw_throughput", lambda: gen_raw_throughput(ref, args.out)),
         ("offline_tile", lambda: gen_offline_tile(ref, args.out)),
+        ("offline_interior", lambda: gen_offline_interior(ref, args.out)),
         ("images", lambda: gen_images(ref, args.out)),
         ("realtime", lambda: gen_realtime(ref, args.out)),
         ("vaidya", lambda: gen_vaidya(ref, args.out)),

@@ -63,7 +63,7 @@ def test_struct_layouts_match_header(tmp_path):
 
 
 def test_status_strings(bhlib):
-    assert bhlib.bh_abi_version() == 2
+    assert bhlib.bh_abi_version() == 3
     assert bhlib.bh_status_string(0) == b"ok"
     assert b"escape_radius" in bhlib.bh_status_string(-4)
     assert bhlib.bh_trace_workspace_bytes() == 256
@@ -136,6 +136,19 @@ def test_trace_tile_argument_validation(bhlib):
     assert call(cfg, 2.3, 18.0, 4) == -5  # no workspace
     assert call(cfg, 2.3, 18.0, 4, C.c_void_p(0x10000), 100) == -5  # too small
     assert bhlib.bh_trace_tile_workspace_bytes(10) == 256 + 10 * (168 + 96)
+    # Config flags: BH_TRACE_INTERIOR only, and only with a stop radius > 0.
+    cfg.flags = 2
+    assert call(cfg, 2.3, 18.0, 4) == -1
+    assert b"flags" in bhlib.bh_last_error()
+    cfg.flags = _lib.TRACE_INTERIOR
+    scene.capture_radius = 0.0
+    assert call(cfg, 2.3, 18.0, 4) == -1
+    assert b"stop" in bhlib.bh_last_error()
+    scene.capture_radius = 0.02
+    assert call(cfg, 2.3, 18.0, 4) == -5  # valid interior call: workspace next
+    # The other tracers take no flags.
+    assert bhlib.bh_trace(cfg, scene, None, None, None, None, 1, None, None) == -1
+    assert b"flags" in bhlib.bh_last_error()
 
 
 def test_check_maps_status_to_reference_exceptions(bhlib):

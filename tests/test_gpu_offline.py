@@ -162,3 +162,90 @@ def test_deadline_leaves_rays_in_flight(cuda):
     out = trace_tile(st, s0[:8], float(g["a09_escape_radius"]), OfflineSettings(), (2.3, 18.0),
                      1e-9, 12000)
     assert (out.status.cpu().numpy() > 0).all()
+
+
+INTERIOR_TAGS = ["sheet", "ideal", "disk", "schw"]
+
+
+def _interior(tag, precision="fp64"):
+    from blackhorizon_b200.kerr import KerrSpacetime
+    from blackhorizon_b200.offline import OfflineSettings, trace_tile
+
+    g = golden("offline_interior.npz")
+    spin = float(g[f"{tag}_spin"])
+    disk = tuple(float(x) for x in g[f"{tag}_disk"]) if g[f"{tag}_disk"][1] > 0 else None
+    settings = OfflineSettings(spin=spin, supersample=1, fov_degrees=80.0,
+                               disk_enabled=disk is not None)
+    s0 = torch.as_tensor(g[f"{tag}_state0"], device="cuda")
+    out = trace_tile(KerrSpacetime(1.0, spin), s0, float(g[f"{tag}_escape_radius"]), settings,
+                     disk, settings.rtol, settings.max_steps, float(g[f"{tag}_stop"]),
+                     precision=precision)
+    return g, out
+
+
+@pytest.mark.parametrize("tag", INTERIOR_TAGS)
+def test_interior_tile_matches_reference(cuda, tag):
+    """Interior cameras (render.py:203-248): tetrad rays from inside the
+    horizon cross it backwards in time, end TERMINATED at the stop radius or
+    on diverging momentum, escape, or hit the disk; statuses equal the
+    reference's, escape directions (with each ray's own energy) and hits
+    within 1e-6."""
+    g, out = _interior(tag)
+    same = _compare(out, g, f"{tag}_", 1e-6)
+    assert same.all(), np.nonzero(~same)
+    np.testing.assert_array_equal(out.saturated.cpu().numpy().astype(np.int8),
+                                  g[f"{tag}_saturated"])
+    status = out.status.cpu().numpy()
+    assert (status == 1).sum() == 0  # interior rays are never CAPTURED
+    if tag != "disk":
+        assert (status == 6).sum() > 400
+    # A TERMINATED ray ends at the stop or with a large spatial momentum.
+    st = out.states[out.status == 6]
+    if st.shape[0]:
+        from blackhorizon_b200.kerr import KerrSpacetime
+
+        r = KerrSpacetime(1.0, float(g[f"{tag}_spin"])).kerr_schild_radius(
+            st[:, 1].contiguous(), st[:, 2].contiguous(), st[:, 3].contiguous())
+        pn = torch.linalg.norm(st[:, 5:8], dim=-1)
+        stop = float(g[f"{tag}_stop"])
+        assert bool(((r <= stop * 1.002) | (pn > 1e3)).all())
+
+
+def test_interior_tile_mixed_policy(cuda):
+    for tag in INTERIOR_TAGS:
+        g, out = _interior(tag, precision="mixed")
+        agree = float(np.mean(out.status.cpu().numpy() == g[f"{tag}_status"]))
+        print(f"{tag} mixed status agreement {agree:.4f}")
+        assert agree >= 0.97
+
+
+def test_tetrad_frame_matches_reference(cuda):
+    """trace_frame with a camera tetrad (render.py:520-630): the rain
+    observer's tetrad and the tetrad ray momenta built by the b200 frames
+    module equal the reference's, and the frame's statuses equal its tile."""
+    from blackhorizon_b200.frames import build_tetrad, rain_four_velocity
+    from blackhorizon_b200.kerr import KerrSpacetime
+    from blackhorizon_b200.offline import (FlyCamera, OfflineSettings, tetrad_camera_states,
+                                           trace_frame)
+
+    g = golden("offline_interior.npz")
+    for tag in ("disk", "sheet"):
+        spin = float(g[f"{tag}_spin"])
+        st = KerrSpacetime(1.0, spin)
+        pos = g[f"{tag}_position"]
+        vel = rain_four_velocity(st, pos[None, :])[0]
+        np.testing.assert_allclose(vel, g[f"{tag}_velocity"], rtol=1e-13, atol=1e-13)
+        tet = build_tetrad(st, pos, vel, g[f"{tag}_forward"], g[f"{tag}_up"])
+        np.testing.assert_allclose(tet, g[f"{tag}_tetrad"], rtol=1e-12, atol=1e-12)
+        settings = OfflineSettings(spin=spin, supersample=1, fov_degrees=80.0,
+                                   disk_enabled=bool(g[f"{tag}_disk"][1] > 0))
+        cam = FlyCamera(position=pos.copy(), yaw=0.0, pitch=0.0)
+        s0 = tetrad_camera_states(cam, st, tet, 32, 24, settings)
+        np.testing.assert_allclose(s0.cpu().numpy(), g[f"{tag}_state0"], rtol=1e-12,
+                                   atol=1e-12)
+        fr = trace_frame(cam, 32, 24, settings, camera_tetrad=tet,
+                         interior_stop=float(g[f"{tag}_stop"]))
+        assert fr.escape_radius == float(g[f"{tag}_escape_radius"])
+        agree = float(np.mean(fr.status.cpu().numpy() == g[f"{tag}_status"]))
+        print(f"{tag} tetrad frame status agreement {agree:.4f}")
+        assert agree >= 0.99

@@ -185,6 +185,26 @@ def test_offline_tile_with_disk(oracle, tag):
             np.testing.assert_allclose(o2[k], g[f"{tag}_retrace_{k}"], rtol=0, atol=1e-9)
 
 
+INTERIOR_TAGS = ["sheet", "ideal", "disk", "schw"]
+
+
+@pytest.mark.parametrize("tag", INTERIOR_TAGS)
+def test_offline_tile_interior(oracle, tag):
+    """Interior cameras (render.py:203-248): tetrad rays from inside the
+    horizon end TERMINATED at the stop radius or on diverging momentum."""
+    g = golden("offline_interior.npz")
+    disk = tuple(g[f"{tag}_disk"]) if g[f"{tag}_disk"][1] > 0 else None
+    o = oracle.trace_tile(1.0, float(g[f"{tag}_spin"]), g[f"{tag}_state0"],
+                          float(g[f"{tag}_escape_radius"]), disk, rtol=1e-9, max_steps=12000,
+                          interior_stop=float(g[f"{tag}_stop"]))
+    np.testing.assert_array_equal(o["status"], g[f"{tag}_status"])
+    np.testing.assert_array_equal(o["saturated"], g[f"{tag}_saturated"])
+    for k in ("escape_directions", "hit_positions", "hit_momenta"):
+        np.testing.assert_allclose(o[k], g[f"{tag}_{k}"], rtol=0, atol=1e-9)
+    if tag in ("sheet", "ideal", "schw"):
+        assert (o["status"] == 6).sum() > 400
+
+
 def test_imaging_bit_exact(oracle):
     """imaging.py:27-91: checkerboard colours (random, cell-boundary and pole
     directions, 12 and 7 cells) and render_image (a traced 40x30 frame, and
