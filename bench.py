@@ -808,11 +808,18 @@ def cpu_baseline(state0, spin_h, S, seconds):
     t = time.perf_counter()
     oracle.propagate(1.0, spin_h[:probe], s0[:probe], S, 1e-8, 1e-10, nthreads=threads)
     rate = probe * S / max(time.perf_counter() - t, 1e-6)
-    m = int(min(s0.shape[0], max(probe, rate * seconds / S)))
-    m = max(threads, (m // threads) * threads)
-    t = time.perf_counter()
-    oracle.propagate(1.0, spin_h[:m], s0[:m], S, 1e-8, 1e-10, nthreads=threads)
-    dt = time.perf_counter() - t
+    # A probe of one ray per thread underestimates the rate (the slowest ray
+    # sets its time), so a sample that ends well short of `seconds` is
+    # resized from its own rate and timed again.
+    for _ in range(3):
+        m = int(min(s0.shape[0], max(probe, rate * seconds / S)))
+        m = max(threads, (m // threads) * threads)
+        t = time.perf_counter()
+        oracle.propagate(1.0, spin_h[:m], s0[:m], S, 1e-8, 1e-10, nthreads=threads)
+        dt = time.perf_counter() - t
+        rate = m * S / max(dt, 1e-6)
+        if dt >= 0.6 * seconds or m >= s0.shape[0]:
+            break
     return {"value": m * S / dt, "unit": "ray-steps/s", "cores": threads, "kind": "port",
             "sample": f"first {m} rays x {S} attempted DP5(4) steps of the same workload, "
                       f"oracle/bh_oracle.c (float64) on {threads} threads, {dt:.1f} s"}

@@ -411,19 +411,24 @@ struct AttemptV {
     V it, ix, iy, iz;        // sum_i b_i k_i of t, x, y, z without the exact parts
     V dpx, dpy, dpz;         // momentum increments h sum_i b_i pdot_i
     V err[7];        // sum_i e_i k_i for t x y z px py pz (the p_t error is 0)
-    V nse[7];        // float lanes: u sum_i |e_i| |k_i|, the rounding floor of err
     StageV<V> k7;    // derivative at y_new relative to y_new's momentum
 };
 
-// Rounding floor of the mixed policy's error scale: the embedded error
-// sum_i e_i k_i of float32 stage derivatives carries rounding noise of about
-// u sum_i |e_i| |k_i| (u = 2^-24, one unit roundoff per term) that, unlike
+// Rounding floor of the mixed policy's error scale.  The embedded error
+// h sum_i e_i k_i of float32 stage derivatives carries rounding noise of
+// about u h sum_i |e_i| |k_i| (u = 2^-24 per rounding) that, unlike
 // truncation error, shrinks only linearly with h, so no step size removes
 // it.  Counting it as error made the controller take 2.5x the attempts of
-// the float64 policy at rtol 1e-9 with no gain in accuracy; the mixed policy
-// adds h times this floor to each component's scale atol + rtol max(|y|,
-// |y_new|), and then takes about the float64 policy's step sequence.
-constexpr double kMixedNoise = 0x1p-24;
+// the float64 policy at rtol 1e-9 with no gain in accuracy.  The mixed
+// policy's scale for each component is therefore the larger of atol + rtol
+// max(|y|, |y_new|) and this floor, estimated from the step's own increment
+// as 2 u (sum_i |e_i|) |h sum_i b_i k_i| (two roundings per term; the
+// increment matches the |k_i| weighting when k varies little across the
+// step and is smaller, so stricter, when it changes sign).  Where the
+// tolerance is the larger, the float64 scale is unchanged.  With it the mixed
+// controller takes about the float64 policy's step sequence.
+constexpr double kMixedNoise =
+    2.0 * (dp::E1 - dp::E3 + dp::E4 - dp::E5 + dp::E6 - dp::E7) * 0x1p-24;
 
 #define BH_LIN2(f, c1, s1, c2, s2) (T::set(c1) * (s1).f + T::set(c2) * (s2).f)
 #define BH_LIN3(f, c1, s1, c2, s2, c3, s3) (BH_LIN2(f, c1, s1, c2, s2) + T::set(c3) * (s3).f)
@@ -528,20 +533,6 @@ __device__ __forceinline__ void dp5_attempt(const KerrV<V> &K, const WStateV<V> 
     out.err[4] = BH_LIN6(px, E1, k1, E3, k3, E4, k4, E5, k5, E6, k6, E7, s7);
     out.err[5] = BH_LIN6(py, E1, k1, E3, k3, E4, k4, E5, k5, E6, k6, E7, s7);
     out.err[6] = BH_LIN6(pz, E1, k1, E3, k3, E4, k4, E5, k5, E6, k6, E7, s7);
-    if constexpr (sizeof(typename T::S) == 4) {
-#define BH_ABS6(f) \
-    (T::set(kMixedNoise * E1) * T::abs(k1.f) + T::set(kMixedNoise * -E3) * T::abs(k3.f) + \
-     T::set(kMixedNoise * E4) * T::abs(k4.f) + T::set(kMixedNoise * -E5) * T::abs(k5.f) + \
-     T::set(kMixedNoise * E6) * T::abs(k6.f) + T::set(kMixedNoise * -E7) * T::abs(s7.f))
-        out.nse[0] = BH_ABS6(thl);
-        out.nse[1] = BH_ABS6(kx);
-        out.nse[2] = BH_ABS6(ky);
-        out.nse[3] = BH_ABS6(kz);
-        out.nse[4] = BH_ABS6(px);
-        out.nse[5] = BH_ABS6(py);
-        out.nse[6] = BH_ABS6(pz);
-#undef BH_ABS6
-    }
 }
 
 // Accepts lane l of an attempt: the float64 state advances by the attempt's
@@ -588,21 +579,27 @@ __device__ __forceinline__ StageV<V> first_stage(const KerrV<V> &K, const WState
 // Mixed policy: the error is a float32 combination of float32 stage
 // derivatives, so the scales and quotients are float32 too and the scale
 // reciprocal is one MUFU instruction (a float64 norm of float32 data would
-// add cost, not accuracy); each scale also carries the rounding floor h nse
-// (kMixedNoise); the sum of squares, its square root and the accept test are
-// float64.
+// add cost, not accuracy); each scale is at least the rounding floor
+// kMixedNoise |increment|; the sum of squares, its square root and the
+// accept test are float64.
 template <class V>
-__device__ __forceinline__ void error_ratio_v(const WStateV<V> &y, const WStateV<V> &yn,
-                                              const V err[7], const V nse[7], V hw, V rt,
-                                              V at, double ratio[VT<V>::N]) {
+__device__ __forceinline__ void error_ratio_v(const WStateV<V> &y, const AttemptV<V> &a,
+                                              V hw, V rt, V at, double ratio[VT<V>::N]) {
     using T = VT<V>;
+    const WStateV<V> &yn = a.ynw;
+    const V *err = a.err;
     const V yv[7] = {y.t, y.x, y.y, y.z, y.px, y.py, y.pz};
     const V nv[7] = {yn.t, yn.x, yn.y, yn.z, yn.px, yn.py, yn.pz};
+    // Step increments without the exact parts: h sum b k for t x y z (the
+    // first four carry the factor h in hn), dP for the momenta.
+    const V inc[7] = {a.it, a.ix, a.iy, a.iz, a.dpx, a.dpy, a.dpz};
+    const V hn = hw * T::set(kMixedNoise);
     V q[7];
 #pragma unroll
     for (int i = 0; i < 7; ++i) {
         V sc = T::fma(rt, T::max(T::abs(yv[i]), T::abs(nv[i])), at);
-        if constexpr (sizeof(typename T::S) == 4) sc = T::fma(hw, nse[i], sc);
+        if constexpr (sizeof(typename T::S) == 4)
+            sc = T::max(sc, (i < 4 ? hn : T::set(kMixedNoise)) * T::abs(inc[i]));
         V e;
         if constexpr (sizeof(V) == 8 && T::N == 1) {
             e = (hw * err[i]) / sc;

@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args
             AttemptV<V> a;
             dp5_attempt<V>(K, yw, hw, k1, a);
             double ratio[N];
-            error_ratio_v<V>(yw, a.ynw, a.err, a.nse, hw, rt, at, ratio);
+            error_ratio_v<V>(yw, a, hw, rt, at, ratio);
             bool acc[N];
 #pragma unroll
             for (int l = 0; l < N; ++l) {
@@ -313,7 +313,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) propagate_kernel(const TraceArgs 
             AttemptV<V> a;
             dp5_attempt<V>(K, yw, hw, k1, a);
             double ratio[N];
-            error_ratio_v<V>(yw, a.ynw, a.err, a.nse, hw, rt, at, ratio);
+            error_ratio_v<V>(yw, a, hw, rt, at, ratio);
             bool ok[N];
 #pragma unroll
             for (int l = 0; l < N; ++l) {
