@@ -70,6 +70,13 @@ class RealtimeConfig(ctypes.Structure):
                 ("precision", _I32), ("reserved", _I32)]
 
 
+class EmissionConfig(ctypes.Structure):
+    _fields_ = [("mass", _D), ("spin", _D), ("disk_inner", _D), ("disk_temperature", _D),
+                ("disk_detail", _D), ("observer_lapse", _D), ("bb_log_min", _D),
+                ("bb_log_max", _D), ("sheet_rgb", _D * 3), ("temperature_size", _I32),
+                ("blackbody_size", _I32), ("supersample", _I32), ("reserved", _I32)]
+
+
 class Vaidya(ctypes.Structure):
     _fields_ = [("mass", _D), ("charge", _D), ("tail_mass", _D), ("tail_start", _D),
                 ("tail_power", _D), ("shell_energy", _D), ("shell_start_v", _D),
@@ -134,6 +141,10 @@ _SIGNATURES = {
     "bh_trace_tile": (ctypes.c_int, [ctypes.POINTER(TraceConfig), ctypes.POINTER(Scene), _D, _D,
                                      _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _SZ,
                                      ctypes.POINTER(TileStats), _P]),
+    "bh_offline_radiance": (ctypes.c_int, [ctypes.POINTER(EmissionConfig), _P, _P, _P, _P, _P,
+                                           _I64, _I64, _P, _P, _P, _P, _P]),
+    "bh_develop_workspace_bytes": (_SZ, [_I64, _I64]),
+    "bh_develop": (ctypes.c_int, [_P, _I64, _I64, _D, _D, _D, _P, _I32, _P, _P, _SZ, _P]),
     "bh_fma_peak_launch": (ctypes.c_int, [_I32, _I64, _P, ctypes.POINTER(_I64), _P]),
 }
 

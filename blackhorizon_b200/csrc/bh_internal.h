@@ -151,6 +151,21 @@ struct TileArgs {
     TileWorkspace *ws;
 };
 
+// Arguments of the offline radiance kernel (bh_emission.cu).
+struct EmissionArgs {
+    double mass, spin, disk_inner, disk_temperature, disk_detail, observer_lapse;
+    double bb_log_min, bb_log_max;
+    double sheet_rgb[3];
+    int temperature_size, bb_size, supersample;
+    long long pixels;
+    const int32_t *status;
+    const double *escape_dir, *hit_pos, *hit_mom, *energy;
+    const float *temperature;
+    const double *lut_radii;
+    const float *bb_table;
+    float *hdr;
+};
+
 int tile_default_variant(int precision);
 cudaError_t launch_tile(const TileArgs &args, int precision, int variant,
                         int blocks_per_sm, cudaStream_t stream);

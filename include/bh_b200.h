@@ -470,6 +470,53 @@ int bh_trace_tile(const bh_trace_config *config, const bh_scene *scene,
                   void *workspace, size_t workspace_bytes,
                   bh_tile_stats *stats, void *stream);
 
+/* ------------------------------------------------------- offline emission */
+
+/* Shading constants of one offline frame (offline/render.py:487-560). */
+typedef struct {
+    double mass, spin;
+    double disk_inner;        /* ISCO: start of the temperature table, origin of the detail pattern */
+    double disk_temperature;  /* OfflineSettings.disk_temperature, K */
+    double disk_detail;       /* OfflineSettings.disk_detail */
+    double observer_lapse;    /* frequency factor of the camera (static lapse or blue-sheet B) */
+    double bb_log_min, bb_log_max; /* log-temperature range of the blackbody table */
+    double sheet_rgb[3];      /* radiance of BH_RAY_TERMINATED rays (zero: black) */
+    int32_t temperature_size; /* entries of the temperature table (>= 2) */
+    int32_t blackbody_size;   /* rows of the blackbody table (>= 2) */
+    int32_t supersample;      /* rays per pixel = supersample^2, consecutive */
+    int32_t reserved;         /* 0 */
+} bh_emission_config;
+
+/* The radiance half of render_hdr (render.py:352-484, 630-680): escaped rays
+ * sample the hashed HDR starfield by their escape direction (shifted by
+ * observer_lapse / energy[i] when energy, the rays' initial p_t, is given:
+ * tetrad cameras); BH_RAY_DISK rays take the redshifted blackbody of the
+ * Novikov-Thorne disk at their hit (temperature_table on the radii
+ * lut_radii, blackbody_table (blackbody_size, 3) on log temperature);
+ * BH_RAY_TERMINATED rays take sheet_rgb; the rest are black.  The
+ * supersample^2 rays of each pixel are averaged into hdr (height, width, 3)
+ * float32.  Ray arrays are (width height supersample^2[, 3]) in pixel-major
+ * order, as bh_trace_tile returns them.  float64 arithmetic in NumPy's order. */
+int bh_offline_radiance(const bh_emission_config *config, const int32_t *status,
+                        const double *escape_directions, const double *hit_positions,
+                        const double *hit_momenta, const double *energy, int64_t width,
+                        int64_t height, const float *temperature_table,
+                        const double *lut_radii, const float *blackbody_table, float *hdr,
+                        void *stream);
+
+/* Device workspace of bh_develop with bloom: two float32 images. */
+size_t bh_develop_workspace_bytes(int64_t width, int64_t height);
+
+/* offline/post.py:88-106 (develop): hdr * exposure, bloom (bright pass above
+ * bloom_threshold, separable Gaussian blur with edge padding by
+ * blur_weights[2 radius + 1], added with bloom_strength; skipped when
+ * bloom_strength <= 0), ACES filmic curve, sRGB encoding to out (height,
+ * width, 3) uint8.  float32 arithmetic in NumPy's order. */
+int bh_develop(const float *hdr, int64_t width, int64_t height, double exposure,
+               double bloom_threshold, double bloom_strength, const double *blur_weights,
+               int32_t blur_radius, uint8_t *out, void *workspace, size_t workspace_bytes,
+               void *stream);
+
 /* ------------------------------------------------------------ diagnostics */
 
 /* Launches a vector-FMA throughput kernel of sms*8 blocks x 256 threads, each

@@ -14,6 +14,7 @@
 #include <math.h>
 #include <pthread.h>
 #include <stdatomic.h>
+#include <stdlib.h>
 #include <string.h>
 #include <unistd.h>
 
@@ -1016,4 +1017,233 @@ void bho_vaidya_trace(const bho_vaidya_t *p, double *states, int64_t n,
     vd_trace_ctx_t c = {p, states, escape_dir, end_mass, v_end, escape_radius, stop_radius,
                         max_steps, status};
     bho_parallel_for(n, nthreads, 2, vd_trace_range, &c);
+}
+
+/* ------------------------------------------------- offline/render.py emission */
+
+/* render.py:368-370 */
+static double hash01(double a, double b, double salt) {
+    const double v = sin(a * 127.1 + b * 311.7 + salt * 74.7) * 43758.5453;
+    return v - floor(v);
+}
+
+static void starfield_one(const double *d, double shift, int shifted, double *c) {
+    /* render.py:366-419 */
+    const double phi = atan2(d[1], d[0]);
+    const double theta = acos(np_clip(d[2], -1.0, 1.0));
+    static const double cells_of[2] = {160.0, 420.0}, density_of[2] = {0.10, 0.05},
+                        bright_of[2] = {3.0, 0.9};
+    c[0] = c[1] = c[2] = 0.0;
+    for (int layer = 0; layer < 2; ++layer) {
+        const double cells = cells_of[layer];
+        const double cu = phi / (2.0 * M_PI) * cells;
+        const double cv = theta / M_PI * cells;
+        const double iu = floor(cu), iv = floor(cv);
+        const int present = hash01(iu, iv, 1.0) < density_of[layer];
+        const double su = iu + 0.15 + 0.7 * hash01(iu, iv, 2.0);
+        const double sv = iv + 0.15 + 0.7 * hash01(iu, iv, 3.0);
+        const double dist2 = (cu - su) * (cu - su) + (cv - sv) * (cv - sv);
+        const double magnitude = hash01(iu, iv, 4.0);
+        double amplitude = bright_of[layer] * (0.15 + pow(magnitude, 4.0));
+        const double point = exp(-dist2 / 0.006);
+        double warmth = hash01(iu, iv, 5.0);
+        if (shifted) {
+            amplitude = amplitude * pow(shift, 4.0);
+            warmth = np_clip(warmth - 0.6 * log(np_max(shift, 1e-6)), 0.0, 1.0);
+        }
+        const double tint[3] = {0.75 + 0.35 * warmth, 0.85 + 0.10 * warmth, 1.05 - 0.35 * warmth};
+        const double w = (present ? amplitude : 0.0) * point;
+        for (int k = 0; k < 3; ++k) c[k] = c[k] + w * tint[k];
+    }
+    const double zz = d[2] / 0.30;
+    const double band = 0.035 * exp(-(zz * zz));
+    const double band_rgb[3] = {1.0, 0.92, 0.80};
+    for (int k = 0; k < 3; ++k) {
+        double b = band * band_rgb[k];
+        if (shifted) {
+            const double slide = np_clip(0.35 * log(np_max(shift, 1e-6)), -0.6, 0.6);
+            const double tint = k == 0 ? 1.0 - slide : (k == 1 ? 1.0 : 1.0 + slide);
+            b = b * pow(shift, 4.0) * tint;
+        }
+        c[k] = c[k] + b;
+    }
+}
+
+void bho_starfield(const double *dirs, const double *shift, int64_t n, double *rgb) {
+    for (int64_t i = 0; i < n; ++i)
+        starfield_one(dirs + 3 * i, shift ? shift[i] : 0.0, shift != NULL, rgb + 3 * i);
+}
+
+static double interp_f32(double x, const double *xp, const float *fp, int64_t n) {
+    double buf0 = fp[0], buf1;
+    if (isnan(x)) return x;
+    if (x < xp[0]) return buf0;
+    if (x >= xp[n - 1]) return (double)fp[n - 1];
+    int64_t lo = 0, hi = n - 1;
+    while (hi - lo > 1) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (xp[mid] <= x) lo = mid; else hi = mid;
+    }
+    buf0 = fp[lo];
+    if (xp[lo] == x) return buf0;
+    buf1 = fp[lo + 1];
+    const double slope = (buf1 - buf0) / (xp[lo + 1] - xp[lo]);
+    return slope * (x - xp[lo]) + buf0;
+}
+
+static void disk_one(const bho_emission_params_t *p, const double *pos, const double *mom,
+                     const float *temperature, const double *lut_radii, const float *bb,
+                     double *c) {
+    bho_geometry_t g;
+    bho_geometry(p->mass, p->spin, pos[0], pos[1], pos[2], 0, &g);
+    const double r = g.r;
+    const double t_norm = interp_f32(r, lut_radii, temperature, p->temperature_size);
+    /* emission/redshift.py:19-116 with p_t = 1 */
+    const double omega = 1.0 / (pow(r, 1.5) + p->spin);
+    const double v[3] = {-omega * pos[1], omega * pos[0], 0.0};
+    const double ldv = 1.0 + sum3(g.l[0] * v[0], g.l[1] * v[1], g.l[2] * v[2]);
+    const double norm2 = -1.0 + sum3(v[0] * v[0], v[1] * v[1], v[2] * v[2]) +
+                         2.0 * g.h * ldv * ldv;
+    const double u_t = 1.0 / sqrt(-norm2);
+    const double u[3] = {u_t * v[0], u_t * v[1], u_t * v[2]};
+    const double freq = 1.0 * u_t + sum3(mom[0] * u[0], mom[1] * u[1], mom[2] * u[2]);
+    const double shift = p->observer_lapse / freq;
+    const double t_obs = np_max(shift * t_norm * p->disk_temperature, 1.0);
+    const double log_t = np_clip(log(t_obs), p->bb_log_min, p->bb_log_max);
+    const double lut_u = (log_t - p->bb_log_min) / (p->bb_log_max - p->bb_log_min) *
+                         (double)(p->blackbody_size - 1);
+    const double phi = atan2(pos[1], pos[0]);
+    const double detail = 1.0 + p->disk_detail * (0.18 * sin(9.0 * phi + 2.2 * r) +
+                                                   0.12 * sin(23.0 * phi - 5.0 * r) +
+                                                   0.15 * sin(3.5 * (r - p->disk_inner)));
+    const double brightness = pow(t_obs / 6500.0, 4.0) * np_max(detail, 0.2);
+    const int64_t nb = p->blackbody_size;
+    for (int k = 0; k < 3; ++k) {
+        double tint;
+        if (isnan(lut_u)) {
+            tint = lut_u;
+        } else if (lut_u < 0.0) {
+            tint = bb[k];
+        } else if (lut_u >= (double)(nb - 1)) {
+            tint = bb[3 * (nb - 1) + k];
+        } else {
+            const int64_t lo = (int64_t)floor(lut_u);
+            const double f0 = bb[3 * lo + k];
+            tint = ((double)lo == lut_u) ? f0 : (bb[3 * (lo + 1) + k] - f0) * (lut_u - (double)lo) + f0;
+        }
+        c[k] = tint * brightness;
+    }
+}
+
+void bho_disk_radiance(const bho_emission_params_t *p, const double *pos,
+                       const double *mom, int64_t n, const float *temperature,
+                       const double *lut_radii, const float *bb_table, double *rgb) {
+    for (int64_t i = 0; i < n; ++i)
+        disk_one(p, pos + 3 * i, mom + 3 * i, temperature, lut_radii, bb_table, rgb + 3 * i);
+}
+
+typedef struct {
+    const bho_emission_params_t *p;
+    const int32_t *status;
+    const double *escape_dir, *hit_pos, *hit_mom, *energy, *lut_radii;
+    const float *temperature, *bb;
+    float *hdr;
+} radiance_ctx_t;
+
+static void radiance_range(void *vctx, int64_t b, int64_t e, int64_t *acc) {
+    radiance_ctx_t *c = (radiance_ctx_t *)vctx;
+    const bho_emission_params_t *p = c->p;
+    const int ss2 = p->supersample * p->supersample;
+    (void)acc;
+    for (int64_t px = b; px < e; ++px) {
+        double sum[3] = {0.0, 0.0, 0.0};
+        for (int k = 0; k < ss2; ++k) {
+            const int64_t i = px * ss2 + k;
+            double col[3] = {0.0, 0.0, 0.0};
+            const int32_t st = c->status[i];
+            if (st == BHO_ESCAPED) {
+                const double shift = c->energy ? p->observer_lapse / c->energy[i] : 0.0;
+                starfield_one(c->escape_dir + 3 * i, shift, c->energy != NULL, col);
+            } else if (st == BHO_DISK) {
+                disk_one(p, c->hit_pos + 3 * i, c->hit_mom + 3 * i, c->temperature,
+                         c->lut_radii, c->bb, col);
+            } else if (st == BHO_TERMINATED) {
+                col[0] = p->sheet_rgb[0]; col[1] = p->sheet_rgb[1]; col[2] = p->sheet_rgb[2];
+            }
+            for (int j = 0; j < 3; ++j) sum[j] = k == 0 ? col[j] : sum[j] + col[j];
+        }
+        for (int j = 0; j < 3; ++j) c->hdr[3 * px + j] = (float)(sum[j] / (double)ss2);
+    }
+}
+
+void bho_offline_radiance(const bho_emission_params_t *p, const int32_t *status,
+                          const double *escape_dir, const double *hit_pos,
+                          const double *hit_mom, const double *energy,
+                          int64_t pixels, const float *temperature,
+                          const double *lut_radii, const float *bb_table,
+                          float *hdr, int nthreads) {
+    radiance_ctx_t c = {p, status, escape_dir, hit_pos, hit_mom, energy, lut_radii,
+                        temperature, bb_table, hdr};
+    bho_parallel_for(pixels, nthreads, 256, radiance_range, &c);
+}
+
+/* ------------------------------------------------------ offline/post.py */
+
+static void blur_pass(const float *src, float *dst, int64_t w, int64_t h,
+                      const double *wt, int radius, int axis) {
+    for (int64_t y = 0; y < h; ++y)
+        for (int64_t x = 0; x < w; ++x) {
+            float acc[3] = {0.0f, 0.0f, 0.0f};
+            for (int t = 0; t <= 2 * radius; ++t) {
+                int64_t yy = y, xx = x;
+                if (axis == 0) {
+                    yy = y + t - radius;
+                    yy = yy < 0 ? 0 : (yy >= h ? h - 1 : yy);
+                } else {
+                    xx = x + t - radius;
+                    xx = xx < 0 ? 0 : (xx >= w ? w - 1 : xx);
+                }
+                const float *s = src + 3 * (yy * w + xx);
+                for (int k = 0; k < 3; ++k) acc[k] = (float)((double)acc[k] + wt[t] * (double)s[k]);
+            }
+            for (int k = 0; k < 3; ++k) dst[3 * (y * w + x) + k] = acc[k];
+        }
+}
+
+static uint8_t develop_px(float x) {
+    const float a = 2.51f, b = 0.03f, c = 2.43f, d = 0.59f, e = 0.14f;
+    float m = (x * (a * x + b)) / (x * (c * x + d) + e);
+    m = m < 0.0f ? 0.0f : (m > 1.0f ? 1.0f : m);
+    const float enc = m <= 0.0031308f ? 12.92f * m
+                                      : 1.055f * powf(m, (float)(1.0 / 2.4)) - 0.055f;
+    return (uint8_t)(enc * 255.0f + 0.5f);
+}
+
+void bho_develop(const float *hdr, int64_t width, int64_t height, double exposure,
+                 double bloom_threshold, double bloom_strength,
+                 const double *weights, int radius, uint8_t *out) {
+    const int64_t n = width * height;
+    const float ex = (float)exposure;
+    float *img = (float *)malloc((size_t)n * 3 * sizeof(float));
+    for (int64_t i = 0; i < 3 * n; ++i) img[i] = hdr[i] * ex;
+    if (bloom_strength > 0.0) {
+        float *bright = (float *)malloc((size_t)n * 3 * sizeof(float));
+        float *tmp = (float *)malloc((size_t)n * 3 * sizeof(float));
+        const float thr = (float)bloom_threshold, st = (float)bloom_strength;
+        for (int64_t i = 0; i < n; ++i) {
+            const float *v = img + 3 * i;
+            const float lum = 0.2126f * v[0] + 0.7152f * v[1] + 0.0722f * v[2];
+            float excess = lum - thr;
+            excess = excess > 0.0f ? excess : 0.0f;
+            const float scale = lum > 1e-9f ? excess / (lum + 1e-9f) : 0.0f;
+            for (int k = 0; k < 3; ++k) bright[3 * i + k] = v[k] * scale;
+        }
+        blur_pass(bright, tmp, width, height, weights, radius, 0);
+        blur_pass(tmp, bright, width, height, weights, radius, 1);
+        for (int64_t i = 0; i < 3 * n; ++i) img[i] = img[i] + st * bright[i];
+        free(bright);
+        free(tmp);
+    }
+    for (int64_t i = 0; i < 3 * n; ++i) out[i] = develop_px(img[i]);
+    free(img);
 }

@@ -233,6 +233,41 @@ void bho_null_momentum_batch(double m, double a, const double *pos,
 
 int bho_num_threads(void);
 
+/* Shading constants of offline/render.py:487-560 for bho_offline_radiance. */
+typedef struct {
+    double mass, spin, disk_inner, disk_temperature, disk_detail, observer_lapse;
+    double bb_log_min, bb_log_max;
+    double sheet_rgb[3];
+    int32_t temperature_size, blackbody_size, supersample;
+} bho_emission_params_t;
+
+/* render.py:352-419 (_starfield_hdr) per direction (n,3) -> rgb (n,3);
+ * shift (n,) or NULL. */
+void bho_starfield(const double *dirs, const double *shift, int64_t n, double *rgb);
+
+/* render.py:422-484 (_disk_radiance) per hit (positions, momenta (n,3)). */
+void bho_disk_radiance(const bho_emission_params_t *p, const double *pos,
+                       const double *mom, int64_t n, const float *temperature,
+                       const double *lut_radii, const float *bb_table, double *rgb);
+
+/* The shading of render_hdr (render.py:630-680): per-ray radiance by status
+ * (starfield with shift observer_lapse / energy[i] when energy != NULL,
+ * disk, sheet_rgb for TERMINATED, else black), averaged over the
+ * supersample^2 consecutive rays of each pixel into hdr (pixels, 3) float32. */
+void bho_offline_radiance(const bho_emission_params_t *p, const int32_t *status,
+                          const double *escape_dir, const double *hit_pos,
+                          const double *hit_mom, const double *energy,
+                          int64_t pixels, const float *temperature,
+                          const double *lut_radii, const float *bb_table,
+                          float *hdr, int nthreads);
+
+/* offline/post.py:88-106 (develop) on an (height, width, 3) float32 image;
+ * weights (2 radius + 1) are gaussian_kernel(sigma); bloom_strength <= 0
+ * skips the bloom. */
+void bho_develop(const float *hdr, int64_t width, int64_t height, double exposure,
+                 double bloom_threshold, double bloom_strength,
+                 const double *weights, int radius, uint8_t *out);
+
 #ifdef __cplusplus
 }
 #endif

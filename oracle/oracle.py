@@ -379,3 +379,72 @@ class Vaidya:
                                _D(stop_radius), _I64(max_steps), _ptr(status), _ptr(edir),
                                _ptr(mass), _ptr(v_end), ctypes.c_int(nthreads))
         return status, edir, mass, v_end
+
+
+class EmissionParams(ctypes.Structure):
+    _fields_ = [("mass", _D), ("spin", _D), ("disk_inner", _D), ("disk_temperature", _D),
+                ("disk_detail", _D), ("observer_lapse", _D), ("bb_log_min", _D),
+                ("bb_log_max", _D), ("sheet_rgb", _D * 3), ("temperature_size", ctypes.c_int32),
+                ("blackbody_size", ctypes.c_int32), ("supersample", ctypes.c_int32)]
+
+
+def emission_params(mass, spin, tables, disk_temperature=6500.0, disk_detail=1.0,
+                    observer_lapse=1.0, sheet_rgb=(0.0, 0.0, 0.0), supersample=1):
+    """``tables``: dict with temperature (float32), radii, blackbody (float32
+    (B, 3)), bb_log_min, bb_log_max, disk_inner (numpy arrays)."""
+    return EmissionParams(float(mass), float(spin), float(tables["disk_inner"]),
+                          float(disk_temperature), float(disk_detail), float(observer_lapse),
+                          float(tables["bb_log_min"]), float(tables["bb_log_max"]),
+                          (_D * 3)(*(float(v) for v in sheet_rgb)),
+                          int(tables["temperature"].size), int(tables["blackbody"].shape[0]),
+                          int(supersample))
+
+
+def starfield(directions, shift=None):
+    """offline/render.py:352-419 (_starfield_hdr): (n, 3) float64."""
+    d = _f64(directions)
+    s = None if shift is None else _f64(shift)
+    out = np.empty((d.shape[0], 3))
+    lib().bho_starfield(_ptr(d), _ptr(s) if s is not None else None, _I64(d.shape[0]),
+                        _ptr(out))
+    return out
+
+
+def disk_radiance(params: EmissionParams, positions, momenta, tables):
+    """offline/render.py:422-484 (_disk_radiance): (n, 3) float64."""
+    pos, mom = _f64(positions), _f64(momenta)
+    t = np.ascontiguousarray(tables["temperature"], dtype=np.float32)
+    r = _f64(tables["radii"])
+    bb = np.ascontiguousarray(tables["blackbody"], dtype=np.float32)
+    out = np.empty((pos.shape[0], 3))
+    lib().bho_disk_radiance(ctypes.byref(params), _ptr(pos), _ptr(mom), _I64(pos.shape[0]),
+                            _ptr(t), _ptr(r), _ptr(bb), _ptr(out))
+    return out
+
+
+def offline_radiance(params: EmissionParams, status, escape_dir, hit_pos, hit_mom, tables,
+                     width: int, height: int, energy=None, nthreads: int = 0):
+    """The shading of render_hdr (render.py:630-680): (height, width, 3)
+    float32, supersample^2 consecutive rays per pixel."""
+    st = np.ascontiguousarray(status, dtype=np.int32)
+    ed, hp, hm = _f64(escape_dir), _f64(hit_pos), _f64(hit_mom)
+    e = None if energy is None else _f64(energy)
+    t = np.ascontiguousarray(tables["temperature"], dtype=np.float32)
+    r = _f64(tables["radii"])
+    bb = np.ascontiguousarray(tables["blackbody"], dtype=np.float32)
+    out = np.empty((height, width, 3), dtype=np.float32)
+    lib().bho_offline_radiance(ctypes.byref(params), _ptr(st), _ptr(ed), _ptr(hp), _ptr(hm),
+                               _ptr(e) if e is not None else None, _I64(width * height),
+                               _ptr(t), _ptr(r), _ptr(bb), _ptr(out), ctypes.c_int(nthreads))
+    return out
+
+
+def develop(hdr, weights, exposure=1.0, bloom_threshold=1.0, bloom_strength=0.35):
+    """offline/post.py:88-106 (develop); weights = gaussian_kernel(sigma)."""
+    img = np.ascontiguousarray(hdr, dtype=np.float32)
+    w = _f64(weights)
+    out = np.empty(img.shape, dtype=np.uint8)
+    lib().bho_develop(_ptr(img), _I64(img.shape[1]), _I64(img.shape[0]), _D(exposure),
+                      _D(bloom_threshold), _D(bloom_strength), _ptr(w),
+                      ctypes.c_int(w.size // 2), _ptr(out))
+    return out

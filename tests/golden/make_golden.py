@@ -52,6 +52,10 @@ REF_FILES = [
     "blackhorizon/vaidya.py",
     "blackhorizon/offline/inflation.py",
     "blackhorizon/emission/novikov_thorne.py",
+    "blackhorizon/emission/blackbody.py",
+    "blackhorizon/emission/redshift.py",
+    "blackhorizon/emission/bluesheet.py",
+    "blackhorizon/offline/post.py",
     "tests/test_kerr.py",
     "tests/test_shadow.py",
     "tests/test_bluesheet.py",
@@ -442,6 +446,138 @@ def gen_offline_interior(ref, out):
     np.savez_compressed(os.path.join(out, "offline_interior.npz"), **arrs)
 
 
+def _reference_frame_rays(render, st, state0, escape_radius, settings, disk_radii,
+                          interior_stop):
+    """The tracing half of render_hdr (render.py:599-630) for one tile: the
+    first pass and the photon-shell retrace merged."""
+    res = render._trace_tile(st, state0, escape_radius, settings, disk_radii, settings.rtol,
+                             settings.max_steps, interior_stop=interior_stop)
+    retrace = res.saturated & (res.status != 5) & (res.status != 6)
+    if retrace.any():
+        idx = np.nonzero(retrace)[0]
+        ref2 = render._trace_tile(st, state0[idx], escape_radius, settings, disk_radii,
+                                  settings.refine_rtol, settings.max_steps * 4,
+                                  interior_stop=interior_stop)
+        for name in ("status", "escape_directions", "hit_positions", "hit_momenta"):
+            getattr(res, name)[retrace] = getattr(ref2, name)
+    return res
+
+
+def gen_emission(ref, out):
+    """The emission half of render_hdr (render.py:352-484, 630-680) and
+    develop (post.py:88-106): the temperature and blackbody tables, the
+    starfield and disk radiance per ray, three small frames traced and shaded
+    by render_hdr (exterior default view 48x30 supersample 2; interior tetrad
+    cameras near the blue sheet (tests/test_bluesheet.py's close observer,
+    looking down the spin axis) and inside a=0.6 with the disk), their
+    per-ray trace outputs, and developed 8-bit images."""
+    render, FlyCamera, disk_inner_radius = _offline_modules(_REFERENCE_PATH)
+    from blackhorizon.emission.blackbody import blackbody_lut
+    from blackhorizon.emission.bluesheet import (SHEET_COLOR, blueshift_amplification,
+                                                 sheet_radiance)
+    from blackhorizon.emission.novikov_thorne import temperature_lut
+    from blackhorizon.emission.redshift import static_observer_lapse
+    from blackhorizon.frames import build_tetrad, rain_four_velocity, tetrad_ray_momenta
+    from blackhorizon.offline.post import develop, gaussian_kernel
+
+    G = ref["geodesics"]
+    arrs = {}
+    for tag, spin in (("a09", 0.9), ("am07", -0.7), ("a0", 0.0)):
+        st = ref["KerrSpacetime"](1.0, spin)
+        r_in = float(disk_inner_radius(st))
+        table, lo, hi = temperature_lut(spin, max(18.0, r_in + 1.0), size=2048)
+        arrs[f"temperature_{tag}"] = table
+        arrs[f"temperature_{tag}_range"] = np.array([lo, hi])
+    bb, bb_lo, bb_hi = blackbody_lut(size=1024)
+    arrs["blackbody"] = bb
+    arrs["blackbody_log_range"] = np.array([bb_lo, bb_hi])
+    for sigma in (6.0, 3.0, 0.2):
+        arrs[f"gauss_{sigma}"] = gaussian_kernel(sigma)
+    rng = np.random.default_rng(5)
+    d = rng.normal(size=(4096, 3))
+    d /= np.linalg.norm(d, axis=-1, keepdims=True)
+    shift = rng.uniform(0.3, 3.0, 4096)
+    arrs["star_dirs"] = d
+    arrs["star_shift"] = shift
+    arrs["star_rgb"] = render._starfield_hdr(d)
+    arrs["star_rgb_shift"] = render._starfield_hdr(d, shift=shift)
+    frames = [
+        ("ext", 0.9, 48, 30, 2, None, None, True),
+        ("sheet", 0.9, 48, 32, 1, ((0.03, 0.03, 0.68), (0.0, 0.0, -1.0), (0.0, 1.0, 0.0)),
+         "real", False),
+        ("indisk", 0.6, 48, 32, 1, ((0.6, 0.3, 1.0), (0.0, 1.0, 0.0), (0.0, 0.0, 1.0)),
+         "real", True),
+    ]
+    for tag, spin, w, h, ss, tetrad_seed, stop, disk in frames:
+        st = ref["KerrSpacetime"](1.0, spin)
+        fov = 70.0 if tetrad_seed is None else 80.0
+        settings = render.OfflineSettings(spin=spin, supersample=ss, fov_degrees=fov,
+                                          disk_enabled=disk)
+        r_in = float(disk_inner_radius(st))
+        r_out = max(settings.disk_outer_radius, r_in + 1.0)
+        radii = (r_in, r_out) if disk else None
+        table, _, _ = temperature_lut(spin, r_out, size=2048)
+        kw = {}
+        if tetrad_seed is None:
+            cam = FlyCamera.from_orbit(26.0, 82.0, 0.0)
+            dirs = render.subpixel_directions(cam, w, h, fov, ss)
+            pos = np.tile(cam.position[None, :], (dirs.shape[0], 1))
+            mom = G.null_momentum_from_velocity(st, pos, dirs, time_orientation="past")
+            esc = 1.3 * max(cam.distance_from_origin, r_out)
+            lapse = static_observer_lapse(st, cam.position)
+            energy = None
+            interior = None
+            sheet = np.zeros(3)
+        else:
+            position, fwd, up = (np.array(v) for v in tetrad_seed)
+            interior = st.inner_horizon_radius * 1.02
+            vel = rain_four_velocity(st, position[None, :])[0]
+            tet = build_tetrad(st, position, vel, fwd, up)
+            cam = FlyCamera(position=position.copy(), yaw=0.0, pitch=0.0)
+            dirs = render.pinhole_grid(w, h, fov, ss)
+            pos = np.tile(position[None, :], (dirs.shape[0], 1))
+            mom = tetrad_ray_momenta(st, position, tet, dirs)
+            esc = max(100.0, 1.3 * r_out)
+            cam_r = float(st.kerr_schild_radius(position[None, 0], position[None, 1],
+                                                position[None, 2])[0])
+            lapse = float(blueshift_amplification(st, np.array([cam_r]))[0])
+            energy = mom[:, 0]
+            sheet = (float(sheet_radiance(np.array([lapse]))[0])
+                     * np.array(SHEET_COLOR, dtype=np.float32)) if lapse > 1.0 else np.zeros(3)
+            kw = dict(camera_tetrad=tet, interior_stop=interior)
+            arrs[f"{tag}_tetrad"] = tet
+        s0 = G.build_state(pos, mom)
+        res = _reference_frame_rays(render, st, s0, esc, settings, radii, interior)
+        rad = np.zeros((s0.shape[0], 3))
+        esc_m = res.status == 2
+        if esc_m.any():
+            shift = None if energy is None else lapse / energy[esc_m]
+            rad[esc_m] = render._starfield_hdr(res.escape_directions[esc_m], shift=shift)
+        hit = res.status == 5
+        if hit.any():
+            rad[hit] = render._disk_radiance(st, res.hit_positions[hit], res.hit_momenta[hit],
+                                             settings, r_in, r_out, table, lapse, bb, bb_lo,
+                                             bb_hi)
+        rad[res.status == 6] = sheet
+        hdr = render.render_hdr(cam, w, h, settings, progress=False, **kw)
+        mean = rad.reshape(h, w, ss * ss, 3).mean(axis=2).astype(np.float32)
+        assert np.array_equal(mean, hdr), tag
+        for k, v in (("state0", s0), ("status", res.status.astype(np.int8)),
+                     ("escape_directions", res.escape_directions),
+                     ("hit_positions", res.hit_positions), ("hit_momenta", res.hit_momenta),
+                     ("radiance", rad), ("hdr", hdr),
+                     ("params", np.array([spin, w, h, ss, fov, esc, lapse, r_in, r_out,
+                                          -1.0 if interior is None else interior,
+                                          1.0 if disk else 0.0])),
+                     ("sheet_rgb", np.asarray(sheet, dtype=np.float64)),
+                     ("position", cam.position)):
+            arrs[f"{tag}_{k}"] = v
+        arrs[f"{tag}_developed"] = develop(hdr)
+        arrs[f"{tag}_developed_e2s3"] = develop(hdr, exposure=2.5, bloom_sigma=3.0)
+        arrs[f"{tag}_developed_nobloom"] = develop(hdr, exposure=0.7, bloom_strength=0.0)
+    np.savez_compressed(os.path.join(out, "emission.npz"), **arrs)
+
+
 def gen_images(ref, out):
     """imaging.py:27-91 on the reference's own traces.
 
@@ -705,6 +841,7 @@ def main():
         ("raw_throughput", lambda: gen_raw_throughput(ref, args.out)),
         ("offline_tile", lambda: gen_offline_tile(ref, args.out)),
         ("offline_interior", lambda: gen_offline_interior(ref, args.out)),
+        ("emission", lambda: gen_emission(ref, args.out)),
         ("images", lambda: gen_images(ref, args.out)),
         ("realtime", lambda: gen_realtime(ref, args.out)),
         ("vaidya", lambda: gen_vaidya(ref, args.out)),

@@ -298,3 +298,80 @@ def test_vaidya_surrogate(oracle):
         assert _rel(edir, g[f"{t}_escape_dir"]) < 1e-9
         assert _rel(mass, g[f"{t}_end_mass"]) < 1e-9
         assert _rel(v_end, g[f"{t}_v_end"]) < 1e-9
+
+
+FRAMES = ("ext", "sheet", "indisk")
+
+
+def _frame_tables(spin, r_in, r_out):
+    """Lookup tables of render_hdr (render.py:527-532), made by the b200 host
+    code (pinned to the reference's by test_emission_tables_match_reference)."""
+    from blackhorizon_b200.emission import blackbody_lut, temperature_lut
+
+    t, _, _ = temperature_lut(spin, r_out, size=2048)
+    bb, lo, hi = blackbody_lut(size=1024)
+    return {"temperature": t, "radii": np.linspace(r_in, r_out, t.size), "blackbody": bb,
+            "bb_log_min": lo, "bb_log_max": hi, "disk_inner": r_in}
+
+
+def test_emission_tables_match_reference():
+    """novikov_thorne.py:103-126 and blackbody.py:88-106 tables, and
+    post.py:15-20 blur weights, made on the host: bit-exact."""
+    from blackhorizon_b200.emission import blackbody_lut, temperature_lut
+    from blackhorizon_b200.kerr import KerrSpacetime
+    from blackhorizon_b200.offline import disk_inner_radius
+    from blackhorizon_b200.post import gaussian_kernel
+
+    g = golden("emission.npz")
+    for tag, spin in (("a09", 0.9), ("am07", -0.7), ("a0", 0.0)):
+        r_in = disk_inner_radius(KerrSpacetime(1.0, spin))
+        t, lo, hi = temperature_lut(spin, max(18.0, r_in + 1.0), size=2048)
+        np.testing.assert_array_equal(t, g[f"temperature_{tag}"])
+        np.testing.assert_array_equal([lo, hi], g[f"temperature_{tag}_range"])
+    bb, lo, hi = blackbody_lut(size=1024)
+    np.testing.assert_array_equal(bb, g["blackbody"])
+    np.testing.assert_array_equal([lo, hi], g["blackbody_log_range"])
+    for sigma in (6.0, 3.0, 0.2):
+        np.testing.assert_array_equal(gaussian_kernel(sigma), g[f"gauss_{sigma}"])
+
+
+def test_oracle_emission_and_develop(oracle):
+    """render.py:352-484 and 630-680, post.py:88-106 in the oracle against
+    the reference's outputs: starfield and disk radiance per ray, the
+    supersample-averaged HDR frames, and the developed 8-bit images."""
+    g = golden("emission.npz")
+    # The star hash multiplies sin() by 43758.5453: an ulp of libm's against
+    # NumPy's sin moves a star's centre by ~1e-12 cells, its point spread by
+    # up to ~1e-9 relative.
+    np.testing.assert_allclose(oracle.starfield(g["star_dirs"]), g["star_rgb"], rtol=1e-8,
+                               atol=1e-15)
+    np.testing.assert_allclose(oracle.starfield(g["star_dirs"], g["star_shift"]),
+                               g["star_rgb_shift"], rtol=1e-8, atol=1e-15)
+    for tag in FRAMES:
+        spin, w, h, ss, fov, esc, lapse, r_in, r_out, stop, disk = g[f"{tag}_params"]
+        w, h, ss = int(w), int(h), int(ss)
+        tables = _frame_tables(spin, r_in, r_out)
+        energy = g[f"{tag}_state0"][:, 4] if stop > 0 else None
+        p = oracle.emission_params(1.0, spin, tables, observer_lapse=lapse,
+                                   sheet_rgb=g[f"{tag}_sheet_rgb"], supersample=ss)
+        hit = g[f"{tag}_status"] == 5
+        if hit.any():
+            rad = oracle.disk_radiance(p, g[f"{tag}_hit_positions"][hit],
+                                       g[f"{tag}_hit_momenta"][hit], tables)
+            # NumPy's vectorised sin/pow may differ from libm's by an ulp.
+            np.testing.assert_allclose(rad, g[f"{tag}_radiance"][hit], rtol=1e-10)
+        hdr = oracle.offline_radiance(p, g[f"{tag}_status"], g[f"{tag}_escape_directions"],
+                                      g[f"{tag}_hit_positions"], g[f"{tag}_hit_momenta"],
+                                      tables, w, h, energy=energy)
+        np.testing.assert_allclose(hdr, g[f"{tag}_hdr"], rtol=2e-7, atol=0)
+        ref = g[f"{tag}_hdr"]
+        for key, kw in (("developed", {}), ("developed_e2s3", dict(exposure=2.5, sigma=3.0)),
+                        ("developed_nobloom", dict(exposure=0.7, strength=0.0))):
+            from blackhorizon_b200.post import gaussian_kernel
+
+            out = oracle.develop(ref, gaussian_kernel(kw.get("sigma", 6.0)),
+                                 exposure=kw.get("exposure", 1.0),
+                                 bloom_strength=kw.get("strength", 0.35))
+            diff = np.abs(out.astype(int) - g[f"{tag}_{key}"].astype(int))
+            print(tag, key, "levels off:", int(diff.max()), "pixels:", int((diff > 0).sum()))
+            assert diff.max() <= 1 and (diff > 0).mean() < 1e-3
