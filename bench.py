@@ -72,14 +72,17 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-workloads", action="store_true",
                     help="skip the full-HD frame, the 64-camera batch and the adjoint")
-    ap.add_argument("--profile-case", choices=("trace", "adjoint", "tile", "realtime"),
+    ap.add_argument("--profile-case",
+                    choices=("trace", "adjoint", "tile", "realtime", "emission"),
                     default=None,
                     help="run one small untimed case of that kernel (for ncu captures): "
                          "trace = the 1920x1080 frame (2 warm-up launches, then 1); "
                          "adjoint = the 256x256 differentiable frame with a 2000-step "
                          "tape (1 warm-up sweep, then 1); tile = the offline frame at "
                          "640x400 supersample 2 (1,024,000 rays), first pass only, twice; "
-                         "realtime = the 1280x720 real-time frame, three launches")
+                         "realtime = the 1280x720 real-time frame, three launches; "
+                         "emission = the offline frame traced once, then its radiance "
+                         "and development twice")
     return ap.parse_args()
 
 
@@ -546,6 +549,63 @@ def offline_workload(device, with_cpu=True, warmup=1, reps=3, cpu_stride=16):
                                                   second.get("iterations", 0))}
     out["mixed_status_agreement_with_fp64"] = float(
         (frames["mixed"].status == frames["fp64"].status).double().mean())
+    # The emission half of render_hdr and develop (render.py:352-484,
+    # 630-680; post.py:88-106) on the device, from the fp64 frame's rays.
+    from blackhorizon_b200.emission import frame_tables, radiance_image, render_hdr
+    from blackhorizon_b200.emission import static_observer_lapse
+    from blackhorizon_b200.post import develop
+
+    fr = frames["fp64"]
+    tables = frame_tables(st, settings, s0.device)
+    lapse = float(static_observer_lapse(st, cam.position))
+
+    def shade():
+        return radiance_image(st, fr.status, fr.escape_directions, fr.hit_positions,
+                              fr.hit_momenta, F.width, F.height, settings, lapse, tables=tables)
+
+    hdr = shade()
+    out["radiance_ms"] = min(_event_ms(shade, reps))
+    develop(hdr)
+    out["develop_ms"] = min(_event_ms(lambda: develop(hdr), reps))
+
+    def frame_to_host():
+        # Camera to display image on the host: trace, retrace, shade, develop.
+        return develop(render_hdr(cam, F.width, F.height, settings, precision="mixed")).cpu()
+
+    frame_to_host()
+    t = time.perf_counter()
+    for _ in range(reps):
+        image = frame_to_host()
+    out["mixed_frame_to_host_image_ms"] = (time.perf_counter() - t) * 1e3 / reps
+    out["image_d2h_bytes"] = int(image.numel())
+    if with_cpu:
+        from oracle import oracle
+
+        threads = host_threads()
+        host_tables = {k: (v.cpu().numpy() if torch.is_tensor(v) else v)
+                       for k, v in tables.items()}
+        p = oracle.emission_params(1.0, F.spin, host_tables, observer_lapse=lapse,
+                                   supersample=F.supersample)
+        args = [a.cpu().numpy() for a in (fr.status, fr.escape_directions, fr.hit_positions,
+                                          fr.hit_momenta)]
+        t = time.perf_counter()
+        hdr_cpu = oracle.offline_radiance(p, *args, host_tables, F.width, F.height,
+                                          nthreads=threads)
+        t_rad = time.perf_counter() - t
+        from blackhorizon_b200.post import gaussian_kernel
+
+        t = time.perf_counter()
+        img_cpu = oracle.develop(hdr_cpu, gaussian_kernel(6.0))
+        t_dev = time.perf_counter() - t
+        out["emission_cpu_baseline"] = {
+            "radiance_ms": t_rad * 1e3, "develop_ms": t_dev * 1e3, "cores": threads,
+            "kind": "port",
+            "sample": "the whole frame: oracle/bh_oracle.c radiance on "
+                      f"{threads} threads, develop on 1 thread"}
+        rel = np.abs(hdr.cpu().numpy() - hdr_cpu) / np.maximum(np.abs(hdr_cpu), 1e-6)
+        out["hdr_pixels_off_by_1e-5_vs_oracle"] = int((rel.max(axis=2) > 1e-5).sum())
+        out["developed_channels_off_vs_oracle"] = int(
+            (develop(hdr).cpu().numpy() != img_cpu).sum())
     if with_cpu:
         from oracle import oracle
 
@@ -934,6 +994,25 @@ def profile_case(args):
         for _ in range(2):
             trace_tile(st, s0, esc, settings, radii, settings.rtol, settings.max_steps,
                        precision=prec, variant=args.variant)
+    elif args.profile_case == "emission":
+        from blackhorizon_b200.emission import (frame_tables, radiance_image,
+                                                static_observer_lapse)
+        from blackhorizon_b200.offline import FlyCamera, OfflineSettings, trace_frame
+        from blackhorizon_b200.post import develop
+        from blackhorizon_b200.workloads import OFFLINE_FRAME as F
+
+        settings = OfflineSettings(spin=F.spin, supersample=F.supersample,
+                                   max_steps=F.max_steps)
+        cam = FlyCamera.from_orbit(F.distance, F.inclination, F.azimuth)
+        st = KerrSpacetime(1.0, F.spin)
+        fr = trace_frame(cam, F.width, F.height, settings, precision=prec)
+        tables = frame_tables(st, settings, device)
+        lapse = float(static_observer_lapse(st, cam.position))
+        for _ in range(2):
+            hdr = radiance_image(st, fr.status, fr.escape_directions, fr.hit_positions,
+                                 fr.hit_momenta, F.width, F.height, settings, lapse,
+                                 tables=tables)
+            develop(hdr)
     else:
         C = DIFFERENTIABLE
         t = lambda x: torch.tensor(x, dtype=torch.float64, device=device)  # noqa: E731

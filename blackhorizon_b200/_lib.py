@@ -70,6 +70,12 @@ class RealtimeConfig(ctypes.Structure):
                 ("precision", _I32), ("reserved", _I32)]
 
 
+class OfflineCamera(ctypes.Structure):
+    _fields_ = [("position", _D * 3), ("basis", (_D * 3) * 3), ("tetrad", (_D * 4) * 4),
+                ("tan_half", _D), ("tan_half_aspect", _D), ("width", _I64), ("height", _I64),
+                ("supersample", _I32), ("use_tetrad", _I32)]
+
+
 class EmissionConfig(ctypes.Structure):
     _fields_ = [("mass", _D), ("spin", _D), ("disk_inner", _D), ("disk_temperature", _D),
                 ("disk_detail", _D), ("observer_lapse", _D), ("bb_log_min", _D),
@@ -141,6 +147,7 @@ _SIGNATURES = {
     "bh_trace_tile": (ctypes.c_int, [ctypes.POINTER(TraceConfig), ctypes.POINTER(Scene), _D, _D,
                                      _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _SZ,
                                      ctypes.POINTER(TileStats), _P]),
+    "bh_offline_camera_rays": (ctypes.c_int, [_D, _D, ctypes.POINTER(OfflineCamera), _P, _P]),
     "bh_offline_radiance": (ctypes.c_int, [ctypes.POINTER(EmissionConfig), _P, _P, _P, _P, _P,
                                            _I64, _I64, _P, _P, _P, _P, _P]),
     "bh_develop_workspace_bytes": (_SZ, [_I64, _I64]),

@@ -222,9 +222,14 @@ __global__ void bright_kernel(const float *hdr, long long pixels, float exposure
 }
 
 // post.py:23-32: one separable pass with edge padding; each tap adds
-// w * x in float64 to the float32 pixel.  axis 0 blurs along rows (y).
+// w * x in float64 to the float32 pixel.  axis 0 blurs along rows (y).  The
+// 2 radius + 1 weights are staged in shared memory: every thread reads every
+// weight.
 __global__ void blur_kernel(const float *src, long long width, long long height,
-                            const double *w, int radius, int axis, float *dst) {
+                            const double *weights, int radius, int axis, float *dst) {
+    extern __shared__ double w[];
+    for (int t = threadIdx.x; t <= 2 * radius; t += blockDim.x) w[t] = weights[t];
+    __syncthreads();
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= width * height) return;
     const long long y = p / width, x = p - y * width;
@@ -273,6 +278,9 @@ __global__ void develop_kernel(const float *hdr, const float *blurred, long long
         out[3 * p + k] = develop_channel(v);
     }
 }
+
+// Largest blur radius whose weights fit the default 48 KiB of shared memory.
+constexpr int kMaxBlurRadius = 6000;
 
 static unsigned grid_of(long long n, int block) {
     const long long g = (n + block - 1) / block;
@@ -359,8 +367,8 @@ extern "C" int bh_develop(const float *hdr, int64_t width, int64_t height, doubl
     if (pixels == 0) return BH_OK;
     if (!hdr || !out) return em_invalid("NULL pointer argument");
     const bool bloom = bloom_strength > 0.0;
-    if (bloom && (!blur_weights || blur_radius < 1))
-        return em_invalid("bloom needs blur weights and a radius >= 1");
+    if (bloom && (!blur_weights || blur_radius < 1 || blur_radius > kMaxBlurRadius))
+        return em_invalid("bloom needs blur weights and a radius in [1, 6000]");
     cudaStream_t s = (cudaStream_t)stream;
     const float ex = (float)exposure;
     if (!bloom) {
@@ -379,10 +387,11 @@ extern "C" int bh_develop(const float *hdr, int64_t width, int64_t height, doubl
                                                        bright);
     // post.py:23-32: rows (axis 0) first, then columns; the second pass
     // writes over the bright pass, which is no longer needed.
-    blur_kernel<<<grid_of(pixels, 256), 256, 0, s>>>(bright, width, height, blur_weights,
-                                                     blur_radius, 0, tmp);
-    blur_kernel<<<grid_of(pixels, 256), 256, 0, s>>>(tmp, width, height, blur_weights,
-                                                     blur_radius, 1, bright);
+    const size_t wbytes = (size_t)(2 * blur_radius + 1) * sizeof(double);
+    blur_kernel<<<grid_of(pixels, 256), 256, wbytes, s>>>(bright, width, height, blur_weights,
+                                                          blur_radius, 0, tmp);
+    blur_kernel<<<grid_of(pixels, 256), 256, wbytes, s>>>(tmp, width, height, blur_weights,
+                                                          blur_radius, 1, bright);
     develop_kernel<<<grid_of(pixels, 256), 256, 0, s>>>(hdr, bright, pixels, ex,
                                                         (float)bloom_strength, out);
     return em_launch("bh_develop launch");

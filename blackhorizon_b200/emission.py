@@ -20,6 +20,7 @@ NumPy, as the reference builds them; everything per ray runs on the device.
 
 from __future__ import annotations
 
+import functools
 import math
 
 import numpy
@@ -227,16 +228,31 @@ def radiance_image(spacetime: KerrSpacetime, status, escape_directions, hit_posi
     return hdr
 
 
+@functools.lru_cache(maxsize=32)
+def _host_tables(spin: float, disk_outer_radius: float):
+    disk_inner = disk_inner_radius(KerrSpacetime(1.0, spin))
+    disk_outer = max(disk_outer_radius, disk_inner + 1.0)
+    temperature, _, _ = temperature_lut(spin, disk_outer, size=2048)
+    radii = numpy.linspace(disk_inner, disk_outer, temperature.shape[0])
+    return float(disk_inner), float(disk_outer), temperature, radii
+
+
+@functools.lru_cache(maxsize=1)
+def _host_blackbody():
+    return blackbody_lut(size=1024)
+
+
 def frame_tables(spacetime: KerrSpacetime, settings: OfflineSettings, device) -> dict:
     """The lookup tables of render_hdr (render.py:527-532) on the device:
     the 2048-entry temperature table on its radii, the 1024-row blackbody
-    table and its log-temperature range."""
-    disk_inner = disk_inner_radius(spacetime)
-    disk_outer = max(settings.disk_outer_radius, disk_inner + 1.0)
-    temperature, _, _ = temperature_lut(spacetime.spin, disk_outer, size=2048)
-    blackbody, log_min, log_max = blackbody_lut(size=1024)
-    radii = numpy.linspace(disk_inner, disk_outer, temperature.shape[0])
-    return {"disk_inner": float(disk_inner), "disk_outer": float(disk_outer),
+    table and its log-temperature range.  The host tables are built once per
+    (spin, outer radius) and kept."""
+    if spacetime.mass != 1.0:
+        raise ValueError("the offline renderer's tables assume M = 1")
+    disk_inner, disk_outer, temperature, radii = _host_tables(float(spacetime.spin),
+                                                              float(settings.disk_outer_radius))
+    blackbody, log_min, log_max = _host_blackbody()
+    return {"disk_inner": disk_inner, "disk_outer": disk_outer,
             "temperature": torch.as_tensor(temperature, device=device),
             "radii": torch.as_tensor(radii, device=device),
             "blackbody": torch.as_tensor(blackbody, device=device).contiguous(),
@@ -285,7 +301,7 @@ def render_hdr(camera: FlyCamera, width: int, height: int, settings: OfflineSett
         sheet = glow * numpy.array(SHEET_COLOR, dtype=numpy.float32)  # float32, as render.py:646
     hdr = radiance_image(spacetime, rays.status, rays.escape_directions, rays.hit_positions,
                          rays.hit_momenta, width, height, settings, lapse, energy=energy,
-                         sheet_rgb=sheet)
+                         sheet_rgb=sheet, tables=frame_tables(spacetime, settings, dev))
     return (hdr, rays) if return_rays else hdr
 
 

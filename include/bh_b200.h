@@ -470,6 +470,31 @@ int bh_trace_tile(const bh_trace_config *config, const bh_scene *scene,
                   void *workspace, size_t workspace_bytes,
                   bh_tile_stats *stats, void *stream);
 
+/* ---------------------------------------------------- offline camera rays */
+
+/* A camera of the offline renderer and its supersampled pixel grid
+ * (render.py:103-161, 520-599). */
+typedef struct {
+    double position[3];     /* Kerr-Schild camera position */
+    double basis[3][3];     /* forward, right, up of a FlyCamera (pinhole mode) */
+    double tetrad[4][4];    /* e0..e3 of the observer, one per row (tetrad mode) */
+    double tan_half;        /* tan(fov / 2) */
+    double tan_half_aspect; /* tan(fov / 2) / (width / height) */
+    int64_t width, height;
+    int32_t supersample;    /* supersample^2 rays per pixel */
+    int32_t use_tetrad;     /* 0: pinhole basis, past-directed null momenta;
+                               1: tetrad rays with unit camera frequency */
+} bh_offline_camera;
+
+/* The (width height supersample^2, 8) initial states of a frame in pixel-major
+ * order (row, column, subpixel row, subpixel column), as render_hdr builds them
+ * (render.py:555-599): pinhole grid directions (render.py:103-145), rotated by
+ * the basis and given the past-directed null momentum at the camera
+ * (geodesics.py:109-170), or taken as local tetrad directions with the traced
+ * momentum -g(e0 - n.e) (frames.py:182-218); t = 0. */
+int bh_offline_camera_rays(double mass, double spin, const bh_offline_camera *camera,
+                           double *states, void *stream);
+
 /* ------------------------------------------------------- offline emission */
 
 /* Shading constants of one offline frame (offline/render.py:487-560). */
@@ -509,7 +534,7 @@ size_t bh_develop_workspace_bytes(int64_t width, int64_t height);
 
 /* offline/post.py:88-106 (develop): hdr * exposure, bloom (bright pass above
  * bloom_threshold, separable Gaussian blur with edge padding by
- * blur_weights[2 radius + 1], added with bloom_strength; skipped when
+ * blur_weights[2 radius + 1], radius <= 6000, added with bloom_strength; skipped when
  * bloom_strength <= 0), ACES filmic curve, sRGB encoding to out (height,
  * width, 3) uint8.  float32 arithmetic in NumPy's order. */
 int bh_develop(const float *hdr, int64_t width, int64_t height, double exposure,

@@ -249,3 +249,28 @@ def test_tetrad_frame_matches_reference(cuda):
         agree = float(np.mean(fr.status.cpu().numpy() == g[f"{tag}_status"]))
         print(f"{tag} tetrad frame status agreement {agree:.4f}")
         assert agree >= 0.99
+
+
+def test_device_camera_rays_match_reference(cuda):
+    """bh_offline_camera_rays builds render_hdr's initial states on the device
+    (render.py:103-161, 555-599): the reference's states for its 32x20 tiles
+    and the 48x30 supersample-2 frame; tetrad states are covered by
+    test_tetrad_frame_matches_reference."""
+    from blackhorizon_b200.kerr import KerrSpacetime
+    from blackhorizon_b200.offline import FlyCamera, OfflineSettings, camera_states
+
+    g = golden("offline_tile.npz")
+    cases = [(g[f"{t}_state0"], float(g[f"{t}_spin"]), inc, az, 32, 20, 1)
+             for t, inc, az in (("a09", 82.0, 0.0), ("am07", 75.0, 40.0))]
+    e = golden("emission.npz")
+    cases.append((e["ext_state0"], 0.9, 82.0, 0.0, 48, 30, 2))
+    for ref, spin, inc, az, w, h, ss in cases:
+        cam = FlyCamera.from_orbit(26.0, inc, az)
+        s0 = camera_states(cam, KerrSpacetime(1.0, spin), w, h,
+                           OfflineSettings(spin=spin, supersample=ss))
+        assert s0.shape == ref.shape
+        got = s0.cpu().numpy()
+        np.testing.assert_array_equal(got[:, :4], ref[:, :4])
+        rel = np.abs(got - ref) / np.maximum(np.abs(ref), 1e-300)
+        print("camera rays: max relative difference", float(rel.max()))
+        assert float(rel.max()) < 1e-14

@@ -127,3 +127,27 @@ def test_save_png_roundtrip(tmp_path):
     path = tmp_path / "frame.png"
     save_png(img, str(path))
     np.testing.assert_array_equal(np.asarray(Image.open(path).convert("RGB")), img)
+
+
+def test_offline_pixel_grid_matches_reference(oracle):
+    """pinhole_grid / subpixel_directions (render.py:103-161) equal the
+    reference's directions on its tiles, and with supersample 2 give the
+    reference's initial states through the oracle's null momenta."""
+    import numpy as np
+
+    from blackhorizon_b200.offline import FlyCamera, subpixel_directions
+    from conftest import golden
+
+    g = golden("offline_tile.npz")
+    for tag, inc, az in (("a09", 82.0, 0.0), ("am07", 75.0, 40.0)):
+        cam = FlyCamera.from_orbit(26.0, inc, az)
+        np.testing.assert_array_equal(cam.position, g[f"{tag}_position"])
+        np.testing.assert_array_equal(subpixel_directions(cam, 32, 20, 70.0, 1),
+                                      g[f"{tag}_directions"])
+    e = golden("emission.npz")
+    spin, w, h, ss = (e["ext_params"][k] for k in range(4))
+    cam = FlyCamera.from_orbit(26.0, 82.0, 0.0)
+    d = subpixel_directions(cam, int(w), int(h), 70.0, int(ss))
+    pos = np.tile(cam.position[None, :], (d.shape[0], 1))
+    p = oracle.null_momentum(1.0, float(spin), pos, d, True, True)
+    np.testing.assert_array_equal(p, e["ext_state0"][:, 4:8])
