@@ -580,8 +580,11 @@ __device__ __forceinline__ StageV<V> first_stage(const KerrV<V> &K, const WState
 // derivatives, so the scales and quotients are float32 too and the scale
 // reciprocal is one MUFU instruction (a float64 norm of float32 data would
 // add cost, not accuracy); each scale is at least the rounding floor
-// kMixedNoise |increment|; the sum of squares, its square root and the
-// accept test are float64.
+// kMixedNoise |increment|.  The value written per lane is what the
+// controller compares with 1: the ratio r for the float64 policy, its square
+// r^2 (the mean of squares, summed in float32) for the mixed one, whose
+// accept test r^2 <= 1 and step factor (step_factor<false>) need no square
+// root.  Non-finite values become +inf.
 template <class V>
 __device__ __forceinline__ void error_ratio_v(const WStateV<V> &y, const AttemptV<V> &a,
                                               V hw, V rt, V at, double ratio[VT<V>::N]) {
@@ -608,16 +611,27 @@ __device__ __forceinline__ void error_ratio_v(const WStateV<V> &y, const Attempt
         }
         q[i] = e * e;
     }
+    if constexpr (sizeof(typename T::S) == 4) {
+        // Components t x y z | p_t(=0) px py pz: r^2 = sum / 8.
+        const V sum = ((q[0] + q[1]) + (q[2] + q[3])) + (q[4] + (q[5] + q[6]));
 #pragma unroll
-    for (int l = 0; l < T::N; ++l) {
-        const double g[7] = {double(T::get(q[0], l)), double(T::get(q[1], l)),
-                             double(T::get(q[2], l)), double(T::get(q[3], l)),
-                             double(T::get(q[4], l)), double(T::get(q[5], l)),
-                             double(T::get(q[6], l))};
-        // Components t x y z | p_t(=0) px py pz.
-        const double sum = ((g[0] + g[1]) + (g[2] + g[3])) + ((0.0 + g[4]) + (g[5] + g[6]));
-        const double r = ::sqrt(sum * 0.125);
-        ratio[l] = isfinite(r) ? r : __longlong_as_double(0x7ff0000000000000LL);
+        for (int l = 0; l < T::N; ++l) {
+            const double ms = double(T::get(sum, l)) * 0.125;
+            ratio[l] = isfinite(ms) ? ms : __longlong_as_double(0x7ff0000000000000LL);
+        }
+    } else {
+#pragma unroll
+        for (int l = 0; l < T::N; ++l) {
+            const double g[7] = {double(T::get(q[0], l)), double(T::get(q[1], l)),
+                                 double(T::get(q[2], l)), double(T::get(q[3], l)),
+                                 double(T::get(q[4], l)), double(T::get(q[5], l)),
+                                 double(T::get(q[6], l))};
+            // Components t x y z | p_t(=0) px py pz, NumPy's pairwise order.
+            const double sum =
+                ((g[0] + g[1]) + (g[2] + g[3])) + ((0.0 + g[4]) + (g[5] + g[6]));
+            const double r = ::sqrt(sum * 0.125);
+            ratio[l] = isfinite(r) ? r : __longlong_as_double(0x7ff0000000000000LL);
+        }
     }
 }
 
@@ -707,17 +721,18 @@ __device__ __forceinline__ void project_null(double m, double a, RayState &y) {
     y.pz -= s * vz;
 }
 
-// step_factor (integrators.py:120-124): clip(0.9 max(ratio,1e-16)^-0.2, 0.2, 5).
+// step_factor (integrators.py:120-124): clip(0.9 max(r,1e-16)^-0.2, 0.2, 5).
+// The float64 policy passes r; the mixed policy passes r^2 (error_ratio_v)
+// and takes (r^2)^-0.1 through float32 exp2/log2 (only the step heuristic
+// uses it).
 template <bool F64>
 __device__ __forceinline__ double step_factor(double ratio) {
-    const double safe = np_max(ratio, 1e-16);
     double f;
     if constexpr (F64) {
-        f = 0.9 * ::pow(safe, -0.2);
+        f = 0.9 * ::pow(np_max(ratio, 1e-16), -0.2);
     } else {
-        // float32 power through exp2/log2; only the step heuristic uses it.
-        const float sf = float(fmin(safe, 3.0e38));
-        f = double(0.9f * ex2_approx(-0.2f * lg2_approx(sf)));
+        const float sf = float(fmin(np_max(ratio, 1e-32), 3.0e38));
+        f = double(0.9f * ex2_approx(-0.1f * lg2_approx(sf)));
     }
     return np_min(np_max(f, 0.2), 5.0);
 }
