@@ -670,6 +670,23 @@ def realtime_workload(device, with_cpu=True, warmup=2, reps=5, cpu_stride=8):
                      "captured": int((r.status == 1).sum())}
     out["mixed_status_agreement_with_fp64"] = float(
         (res["mixed"].status == res["fp64"].status).double().mean())
+    # The viewer's whole frame on the device (headless.py:32-48): camera rays,
+    # the shader algorithm and the shader's colours into an 8-bit buffer.
+    from blackhorizon_b200.offline import FlyCamera
+    from blackhorizon_b200.realtime import BackgroundMode, render_frame_device
+
+    fly = FlyCamera.from_orbit(F.distance, F.inclination, 0.0)
+    frame_settings = RenderSettings(spin=F.spin, fov_degrees=F.fov,
+                                    background=BackgroundMode.STARFIELD).apply_preset(
+                                        QualityPreset(F.preset))
+    for prec in ("mixed", "fp64"):
+        def frame():
+            return render_frame_device(frame_settings, fly, F.width, F.height, precision=prec)
+
+        for _ in range(warmup):
+            frame()
+        ms = min(_event_ms(frame, reps))
+        out[f"{prec}_headless_frame_ms"] = ms
     if with_cpu:
         from oracle import oracle
 

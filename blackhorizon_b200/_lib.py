@@ -70,6 +70,15 @@ class RealtimeConfig(ctypes.Structure):
                 ("precision", _I32), ("reserved", _I32)]
 
 
+class RealtimeShading(ctypes.Structure):
+    _fields_ = [("mass", _D), ("spin", _D), ("disk_inner", _D), ("disk_outer", _D),
+                ("disk_temperature", _D), ("disk_detail", _D), ("exposure", _D),
+                ("observer_lapse", _D), ("bb_log_min", _D), ("bb_log_max", _D),
+                ("sky_amplification", _D), ("sheet_radiance", _D), ("whiteout", _D),
+                ("background", _I32), ("temperature_size", _I32), ("blackbody_size", _I32),
+                ("reserved", _I32)]
+
+
 class OfflineCamera(ctypes.Structure):
     _fields_ = [("position", _D * 3), ("basis", (_D * 3) * 3), ("tetrad", (_D * 4) * 4),
                 ("tan_half", _D), ("tan_half_aspect", _D), ("width", _I64), ("height", _I64),
@@ -147,6 +156,8 @@ _SIGNATURES = {
     "bh_trace_tile": (ctypes.c_int, [ctypes.POINTER(TraceConfig), ctypes.POINTER(Scene), _D, _D,
                                      _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _SZ,
                                      ctypes.POINTER(TileStats), _P]),
+    "bh_realtime_shade": (ctypes.c_int, [ctypes.POINTER(RealtimeShading), _P, _P, _P, _P, _I64,
+                                         _I64, _P, _P, _P, _P]),
     "bh_offline_camera_rays": (ctypes.c_int, [_D, _D, ctypes.POINTER(OfflineCamera), _P, _P]),
     "bh_offline_radiance": (ctypes.c_int, [ctypes.POINTER(EmissionConfig), _P, _P, _P, _P, _P,
                                            _I64, _I64, _P, _P, _P, _P, _P]),

@@ -166,6 +166,19 @@ struct EmissionArgs {
     float *hdr;
 };
 
+// Arguments of the real-time shading kernel (bh_realtime_shade.cu), float32.
+struct RealtimeShadeArgs {
+    float mass, spin, disk_inner, disk_outer, disk_temperature, disk_detail;
+    float exposure, observer_lapse, bb_log_min, bb_log_max;
+    float sky_amplification, sheet_radiance, whiteout;
+    int background, temperature_size, blackbody_size;
+    long long pixels;
+    const int32_t *status;
+    const double *states, *hit_pos, *hit_mom;
+    const float *temperature, *blackbody;
+    uint8_t *rgb;
+};
+
 int tile_default_variant(int precision);
 cudaError_t launch_tile(const TileArgs &args, int precision, int variant,
                         int blocks_per_sm, cudaStream_t stream);

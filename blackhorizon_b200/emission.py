@@ -185,6 +185,23 @@ def blueshift_amplification(spacetime: KerrSpacetime, radius,
     return numpy.clip(matching_proximity / x, 1.0, cap)
 
 
+DISPLAY_CAP = 8.0
+WHITEOUT_START = 8.0
+WHITEOUT_END = 30.0
+
+
+def display_amplification(amplification):
+    """The amplification a display adapts to: clip(B, 1, 8) (bluesheet.py:126-136)."""
+    return numpy.clip(numpy.asarray(amplification, dtype=float), 1.0, DISPLAY_CAP)
+
+
+def whiteout_fraction(amplification):
+    """0.92 smoothstep((B - 8) / 22) (bluesheet.py:139-155)."""
+    t = numpy.clip((numpy.asarray(amplification, dtype=float) - WHITEOUT_START)
+                   / (WHITEOUT_END - WHITEOUT_START), 0.0, 1.0)
+    return 0.92 * t * t * (3.0 - 2.0 * t)
+
+
 def sheet_radiance(amplification, base_intensity: float = 0.02):
     """Radiance of rays ending on the blue sheet: base (B - 1)^4
     (bluesheet.py:98-108)."""

@@ -175,3 +175,142 @@ def trace_like_shader(spacetime: KerrSpacetime, state0: Array, settings: RenderS
                            hit_positions=conv(hit_p) if disk else None,
                            hit_momenta=conv(hit_m) if disk else None,
                            steps=int(stats.attempts))
+
+
+# ------------------------------------------------------------ headless frame
+
+
+def _viewer_tables(spin: float, outer: float):
+    """The viewer's lookup textures (engine.py:55-58, 102-123): the 512-entry
+    temperature table and the 256-row blackbody table, kept per (spin, outer)."""
+    from .emission import blackbody_lut, temperature_lut
+
+    key = (round(float(spin), 12), round(float(outer), 12))
+    hit = _TABLE_CACHE.get(key)
+    if hit is None:
+        temperature, r_inner, _ = temperature_lut(spin, outer)
+        blackbody, log_min, log_max = blackbody_lut()
+        hit = (temperature, float(r_inner), blackbody, float(log_min), float(log_max))
+        _TABLE_CACHE[key] = hit
+    return hit
+
+
+_TABLE_CACHE: dict = {}
+
+
+def _interior_view(spacetime: KerrSpacetime, camera, settings: RenderSettings):
+    """Tetrad, stop radius and blue-sheet uniforms of an interior camera
+    (engine.py:125-215): the camera's 4-velocity when it carries a finite
+    one, else the rain observer; the terminal surface at max(stop, 1.02
+    r_minus) on the realistic journey; the amplification B of the camera
+    radius, its display value clip(B, 1, 8), the glow and the whiteout."""
+    from .emission import (blueshift_amplification, display_amplification, sheet_radiance,
+                           whiteout_fraction)
+    from .frames import build_tetrad, rain_four_velocity
+
+    position = numpy.asarray(camera.position, dtype=float)
+    stop = float(settings.interior_stop)
+    radius = float(numpy.linalg.norm(position))
+    if not numpy.isfinite(position).all() or radius < stop:
+        direction = position / radius if radius > 1e-9 else numpy.array([1.0, 0.0, 0.0])
+        position = direction * max(stop, 1e-3)
+    forward, _, up = camera.basis()
+    velocity = getattr(camera, "four_velocity", None)
+    try:
+        if velocity is None or not numpy.isfinite(velocity).all():
+            raise ValueError("missing or non-finite 4-velocity")
+        tetrad = build_tetrad(spacetime, position, velocity, forward, up)
+    except ValueError:
+        tetrad = build_tetrad(spacetime, position,
+                              rain_four_velocity(spacetime, position[None, :])[0], forward, up)
+    inner = float(spacetime.inner_horizon_radius)
+    effective_stop = stop if settings.interior_journey == "idealized" else max(stop, inner * 1.02)
+    amplification = 1.0
+    if settings.interior_journey == "realistic" and inner > 1e-9:
+        r_cam = float(numpy.asarray(spacetime.kerr_schild_radius(
+            position[None, 0], position[None, 1], position[None, 2]))[0])
+        amplification = float(blueshift_amplification(spacetime, numpy.array([r_cam]))[0])
+    display = float(display_amplification(numpy.array([amplification]))[0])
+    return {"tetrad": tetrad, "stop": effective_stop, "display": display,
+            "glow": float(sheet_radiance(numpy.array([display]))[0]),
+            "white": float(whiteout_fraction(numpy.array([amplification]))[0])}
+
+
+def _static_lapse(spacetime: KerrSpacetime, position) -> float:
+    """engine.py:217-233: 1 / sqrt(-g_tt), 1 where g_tt >= -1e-3."""
+    p = numpy.asarray(position, dtype=float)
+    geo = spacetime.geometry(p[None, 0], p[None, 1], p[None, 2])
+    g_tt = 2.0 * float(numpy.asarray(geo.h)[0]) - 1.0
+    return 1.0 if g_tt >= -1e-3 else 1.0 / float(numpy.sqrt(-g_tt))
+
+
+def render_frame_device(settings: RenderSettings, camera, width: int, height: int, *,
+                        precision: str = "fp64", return_rays: bool = False):
+    """One frame of the real-time viewer as an (height, width, 3) uint8 device
+    tensor, row 0 at the top (headless.py:32-48, engine.py:235-330): the
+    camera's rays (pinhole, or the observer's tetrad in interior mode) built
+    on the device, traced by the shader algorithm (``trace_like_shader``) and
+    shaded as kerr_tracer.frag shades them (``bh_realtime_shade``).
+    ``return_rays`` also returns the trace (a ReferenceResult of device
+    tensors) and the shading uniforms with their tables."""
+    from .offline import device_camera_rays, disk_inner_radius
+
+    settings.validate()
+    if width < 1 or height < 1:
+        raise ValueError("width and height must be >= 1")
+    spacetime = KerrSpacetime(mass=1.0, spin=settings.spin)
+    inner = disk_inner_radius(spacetime)
+    outer = max(settings.disk_outer_radius, inner + 1.0)
+    temperature, t_inner, blackbody, log_min, log_max = _viewer_tables(settings.spin, outer)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    interior = _interior_view(spacetime, camera, settings) if settings.interior_mode else None
+    s0 = device_camera_rays(spacetime, camera, width, height, settings.fov_degrees, 1,
+                            interior["tetrad"] if interior else None, dev)
+    escape = settings.effective_escape_radius(camera.distance_from_origin)
+    res = trace_like_shader(spacetime, s0, settings, escape,
+                            disk_radii=(inner, outer) if settings.disk_enabled else None,
+                            interior_stop=interior["stop"] if interior else None,
+                            precision=precision)
+    n = s0.shape[0]
+    states = torch.cat([torch.zeros((n, 1), dtype=torch.float64, device=dev), res.positions,
+                        res.momenta], dim=1).contiguous()
+    hit_p = res.hit_positions if res.hit_positions is not None else torch.zeros(
+        (n, 3), dtype=torch.float64, device=dev)
+    hit_m = res.hit_momenta if res.hit_momenta is not None else torch.zeros(
+        (n, 4), dtype=torch.float64, device=dev)
+    cfg = _lib.RealtimeShading(
+        mass=1.0, spin=float(settings.spin), disk_inner=t_inner, disk_outer=float(outer),
+        disk_temperature=float(settings.disk_temperature),
+        disk_detail=float(settings.disk_detail), exposure=float(settings.exposure),
+        observer_lapse=interior["display"] if interior else _static_lapse(spacetime,
+                                                                          camera.position),
+        bb_log_min=log_min, bb_log_max=log_max,
+        sky_amplification=interior["display"] if interior else 0.0,
+        sheet_radiance=interior["glow"] if interior else 0.0,
+        whiteout=interior["white"] if interior else 0.0,
+        background=int(settings.background), temperature_size=int(temperature.size),
+        blackbody_size=int(blackbody.shape[0]), reserved=0)
+    t_dev = torch.as_tensor(temperature, device=dev)
+    bb_dev = torch.as_tensor(blackbody, device=dev).contiguous()
+    rgb = torch.empty((height, width, 3), dtype=torch.uint8, device=dev)
+    _lib.check(_lib.load().bh_realtime_shade(
+        cfg, ptr(res.status.to(torch.int32).contiguous()), ptr(states),
+        ptr(hit_p.contiguous()), ptr(hit_m.contiguous()), width, height, ptr(t_dev),
+        ptr(bb_dev), ptr(rgb), stream_handle()), "realtime shade")
+    if return_rays:
+        shading = {k: getattr(cfg, k) for k, _ in _lib.RealtimeShading._fields_}
+        shading.update(temperature=temperature, blackbody=blackbody, states=states,
+                       hit_positions=hit_p, hit_momenta=hit_m)
+        return rgb, res, shading
+    return rgb
+
+
+def render_frame(settings: RenderSettings, camera, width: int, height: int, ctx=None, *,
+                 precision: str = "fp64") -> numpy.ndarray:
+    """headless.render_frame (headless.py:32-48): one frame of the real-time
+    viewer as a (height, width, 3) uint8 array, row 0 at the top, rendered by
+    the device kernels instead of an OpenGL context (``ctx`` is accepted for
+    signature parity and must be None)."""
+    if ctx is not None:
+        raise ValueError("the b200 backend renders without an OpenGL context")
+    return render_frame_device(settings, camera, width, height, precision=precision).cpu().numpy()

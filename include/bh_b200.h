@@ -470,6 +470,37 @@ int bh_trace_tile(const bh_trace_config *config, const bh_scene *scene,
                   void *workspace, size_t workspace_bytes,
                   bh_tile_stats *stats, void *stream);
 
+/* The real-time viewer's shading uniforms (realtime/engine.py:116-285). */
+typedef struct {
+    double mass, spin;
+    double disk_inner, disk_outer; /* the temperature texture's radius range */
+    double disk_temperature;       /* RenderSettings.disk_temperature, K */
+    double disk_detail, exposure;
+    double observer_lapse;         /* static lapse (exterior) or display amplification (interior) */
+    double bb_log_min, bb_log_max; /* log-temperature range of the blackbody texture */
+    double sky_amplification;      /* interior cameras: B of the sky shift g = B / E; 0: none */
+    double sheet_radiance;         /* glow of captured / terminated rays; 0: black */
+    double whiteout;               /* fraction mixed toward (0.90, 0.95, 1.0) */
+    int32_t background;            /* 0 checkerboard, 1 starfield */
+    int32_t temperature_size;      /* texels of the temperature texture */
+    int32_t blackbody_size;        /* texels of the blackbody texture (RGB) */
+    int32_t reserved;              /* 0 */
+} bh_realtime_shading;
+
+/* The pixel colours of the real-time viewer (realtime/shaders/
+ * kerr_tracer.frag:205-420) from bh_trace_realtime's outputs for a
+ * (height, width) frame, row 0 at the top: disk emission with the lookup
+ * textures sampled linearly with repeat wrapping and the Reinhard curve, the
+ * checkerboard or starfield sky by the asymptotic direction (shifted for
+ * interior cameras), the blue-sheet glow, the whiteout; 8-bit unsigned
+ * normalised RGB.  float32, like the shader.  states (n, 8) final states,
+ * hit_positions (n, 3), hit_momenta (n, 4). */
+int bh_realtime_shade(const bh_realtime_shading *shading, const int32_t *status,
+                      const double *states, const double *hit_positions,
+                      const double *hit_momenta, int64_t width, int64_t height,
+                      const float *temperature_table, const float *blackbody_table,
+                      uint8_t *rgb, void *stream);
+
 /* ---------------------------------------------------- offline camera rays */
 
 /* A camera of the offline renderer and its supersampled pixel grid

@@ -1247,3 +1247,154 @@ void bho_develop(const float *hdr, int64_t width, int64_t height, double exposur
     for (int64_t i = 0; i < 3 * n; ++i) out[i] = develop_px(img[i]);
     free(img);
 }
+
+/* ------------------------------------------ realtime/shaders/kerr_tracer.frag */
+
+typedef struct { float r, h, l[3]; } geo_f_t;
+
+static geo_f_t geo_f(float m, float a, float x, float y, float z) {
+    /* kerr_tracer.frag:96-114 */
+    geo_f_t g;
+    const float a2 = a * a;
+    const float q = (x * x + y * y + z * z) - a2;
+    float s = sqrtf(q * q + 4.0f * a2 * z * z);
+    s = s > 1e-12f ? s : 1e-12f;
+    float r2 = 0.5f * (q + s);
+    r2 = r2 > 1e-12f ? r2 : 1e-12f;
+    const float r = sqrtf(r2);
+    float qd = r2 * r2 + a2 * z * z;
+    qd = qd > 1e-12f ? qd : 1e-12f;
+    g.r = r;
+    g.h = m * r * r2 / qd;
+    const float inv_r2a2 = 1.0f / (r2 + a2), inv_r = 1.0f / r;
+    g.l[0] = (r * x + a * y) * inv_r2a2;
+    g.l[1] = (r * y - a * x) * inv_r2a2;
+    g.l[2] = z * inv_r;
+    return g;
+}
+
+static float clampf(float x, float lo, float hi) { return x < lo ? lo : (x > hi ? hi : x); }
+static float fractf(float x) { return x - floorf(x); }
+
+static float tex1d(const float *t, int n, int stride, int col, float s) {
+    /* linear filtering between texel centres, repeat wrapping */
+    const float u = s * (float)n - 0.5f;
+    const float f = floorf(u);
+    const float alpha = u - f;
+    int i0 = (int)f % n;
+    if (i0 < 0) i0 += n;
+    const int i1 = (i0 + 1) % n;
+    return (1.0f - alpha) * t[i0 * stride + col] + alpha * t[i1 * stride + col];
+}
+
+static float hash13f(float x, float y, float z) {
+    /* kerr_tracer.frag:243-247 */
+    x = fractf(x * 0.1031f);
+    y = fractf(y * 0.1031f);
+    z = fractf(z * 0.1031f);
+    const float d = x * (z + 31.32f) + y * (y + 31.32f) + z * (x + 31.32f);
+    x += d; y += d; z += d;
+    return fractf((x + y) * z);
+}
+
+static float smoothstepf(float e0, float e1, float x) {
+    const float t = clampf((x - e0) / (e1 - e0), 0.0f, 1.0f);
+    return t * t * (3.0f - 2.0f * t);
+}
+
+static void sky_f(int mode, const float *d, float *c) {
+    /* kerr_tracer.frag:249-268 */
+    const float theta = acosf(clampf(d[2], -1.0f, 1.0f));
+    const float phi = atan2f(d[1], d[0]);
+    if (mode == 0) {
+        const float it = floorf(theta / 3.14159265f * 12.0f);
+        const float ip = floorf((phi + 3.14159265f) / 6.2831853f * 2.0f * 12.0f);
+        const float sum = it + ip;
+        const int light = sum - 2.0f * floorf(sum * 0.5f) >= 1.0f;
+        c[0] = light ? 0.408f : 0.094f;
+        c[1] = light ? 0.502f : 0.118f;
+        c[2] = light ? 0.698f : 0.204f;
+        return;
+    }
+    const float star = powf(hash13f(floorf(d[0] * 220.0f), floorf(d[1] * 220.0f),
+                                    floorf(d[2] * 220.0f)), 60.0f);
+    const float gt = smoothstepf(0.006f, 0.0f, fabsf(fractf(theta / 0.19635f) - 0.5f) * 0.19635f);
+    const float gp = smoothstepf(0.006f, 0.0f, fabsf(fractf(phi / 0.19635f) - 0.5f) * 0.19635f);
+    const float g = gt > gp ? gt : gp;
+    c[0] = 0.012f + star + 0.02f * g;
+    c[1] = 0.014f + star + 0.03f * g;
+    c[2] = 0.028f + star + 0.05f * g;
+}
+
+static void disk_f(const bho_realtime_shading_t *p, float pt, const float *pos, const float *mom,
+                   const float *temperature, const float *bb, float *c) {
+    /* kerr_tracer.frag:205-241 */
+    const geo_f_t g = geo_f(p->mass, p->spin, pos[0], pos[1], pos[2]);
+    const float omega = 1.0f / (powf(g.r, 1.5f) + p->spin);
+    const float v[3] = {-omega * pos[1], omega * pos[0], 0.0f};
+    const float ldv = 1.0f + (g.l[0] * v[0] + g.l[1] * v[1] + g.l[2] * v[2]);
+    const float norm2 = -1.0f + (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) + 2.0f * g.h * ldv * ldv;
+    const float u_t = 1.0f / sqrtf(-norm2 > 1e-9f ? -norm2 : 1e-9f);
+    const float nu = u_t * (pt + (mom[0] * v[0] + mom[1] * v[1] + mom[2] * v[2]));
+    const float shift = p->observer_lapse / (nu > 1e-6f ? nu : 1e-6f);
+    const float lut_u = clampf((g.r - p->disk_inner) / (p->disk_outer - p->disk_inner), 0.0f, 1.0f);
+    const float t_obs = shift * tex1d(temperature, p->temperature_size, 1, 0, lut_u) *
+                        p->disk_temperature;
+    const float bb_u = clampf((logf(t_obs > 1.0f ? t_obs : 1.0f) - p->bb_log_min) /
+                              (p->bb_log_max - p->bb_log_min), 0.0f, 1.0f);
+    const float phi = atan2f(pos[1], pos[0]);
+    const float detail = 1.0f + p->disk_detail * (0.18f * sinf(9.0f * phi + 2.2f * g.r) +
+                                                  0.12f * sinf(23.0f * phi - 5.0f * g.r) +
+                                                  0.15f * sinf(3.5f * (g.r - p->disk_inner)));
+    const float brightness = p->exposure * powf(t_obs / 6500.0f, 4.0f) * (detail > 0.2f ? detail : 0.2f);
+    for (int k = 0; k < 3; ++k) {
+        const float col = tex1d(bb, p->blackbody_size, 3, k, bb_u) * brightness;
+        c[k] = col / (1.0f + col);
+    }
+}
+
+void bho_realtime_shade(const bho_realtime_shading_t *p, const int32_t *status,
+                        const double *states, const double *hit_pos,
+                        const double *hit_mom, int64_t n, const float *temperature,
+                        const float *blackbody, uint8_t *rgb) {
+    for (int64_t i = 0; i < n; ++i) {
+        float c[3] = {0.0f, 0.0f, 0.0f};
+        const int32_t st = status[i];
+        if (st == BHO_DISK) {
+            const float pos[3] = {(float)hit_pos[3 * i], (float)hit_pos[3 * i + 1],
+                                  (float)hit_pos[3 * i + 2]};
+            const float mom[3] = {(float)hit_mom[4 * i + 1], (float)hit_mom[4 * i + 2],
+                                  (float)hit_mom[4 * i + 3]};
+            disk_f(p, (float)hit_mom[4 * i], pos, mom, temperature, blackbody, c);
+        } else if (st == BHO_ESCAPED) {
+            const double *y = states + 8 * i;
+            const float pos[3] = {(float)y[1], (float)y[2], (float)y[3]};
+            const float pt = (float)y[4];
+            const float mom[3] = {(float)y[5], (float)y[6], (float)y[7]};
+            const geo_f_t g = geo_f(p->mass, p->spin, pos[0], pos[1], pos[2]);
+            const float lp = -pt + (g.l[0] * mom[0] + g.l[1] * mom[1] + g.l[2] * mom[2]);
+            float d[3];
+            for (int k = 0; k < 3; ++k) d[k] = mom[k] - 2.0f * g.h * lp * g.l[k];
+            const float inv = 1.0f / sqrtf(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+            for (int k = 0; k < 3; ++k) d[k] *= inv;
+            sky_f(p->background, d, c);
+            if (p->sky_amplification > 0.0f) {
+                const float gs = p->sky_amplification / (pt > 1e-6f ? pt : 1e-6f);
+                const float gain = clampf(gs * gs * gs * gs, 0.0f, 4.0e4f);
+                const float slide = clampf(0.35f * logf(gs > 1e-6f ? gs : 1e-6f), -0.6f, 0.6f);
+                const float t[3] = {1.0f - slide, 1.0f, 1.0f + slide};
+                const float tn = 1.732f / sqrtf(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+                for (int k = 0; k < 3; ++k) c[k] = c[k] * gain * (t[k] * tn);
+            }
+        } else if ((st == BHO_CAPTURED || st == BHO_TERMINATED) && p->sheet_radiance > 0.0f) {
+            c[0] = p->sheet_radiance * 0.62f;
+            c[1] = p->sheet_radiance * 0.78f;
+            c[2] = p->sheet_radiance * 1.0f;
+        }
+        if (p->whiteout > 0.0f) {
+            const float w[3] = {0.90f, 0.95f, 1.0f};
+            for (int k = 0; k < 3; ++k) c[k] = c[k] * (1.0f - p->whiteout) + w[k] * p->whiteout;
+        }
+        for (int k = 0; k < 3; ++k) rgb[3 * i + k] = (uint8_t)lrintf(clampf(c[k], 0.0f, 1.0f) * 255.0f);
+    }
+}

@@ -261,6 +261,22 @@ void bho_offline_radiance(const bho_emission_params_t *p, const int32_t *status,
                           const double *lut_radii, const float *bb_table,
                           float *hdr, int nthreads);
 
+/* The real-time viewer's shading uniforms (realtime/engine.py:235-285). */
+typedef struct {
+    float mass, spin, disk_inner, disk_outer, disk_temperature, disk_detail;
+    float exposure, observer_lapse, bb_log_min, bb_log_max;
+    float sky_amplification, sheet_radiance, whiteout;
+    int32_t background, temperature_size, blackbody_size;
+} bho_realtime_shading_t;
+
+/* realtime/shaders/kerr_tracer.frag:205-420: the 8-bit pixel colour of each
+ * traced ray (status, final state (n,8), hit position (n,3), hit momentum
+ * (n,4)) in float32 as the shader computes it. */
+void bho_realtime_shade(const bho_realtime_shading_t *p, const int32_t *status,
+                        const double *states, const double *hit_pos,
+                        const double *hit_mom, int64_t n, const float *temperature,
+                        const float *blackbody, uint8_t *rgb);
+
 /* offline/post.py:88-106 (develop) on an (height, width, 3) float32 image;
  * weights (2 radius + 1) are gaussian_kernel(sigma); bloom_strength <= 0
  * skips the bloom. */

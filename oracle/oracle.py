@@ -448,3 +448,24 @@ def develop(hdr, weights, exposure=1.0, bloom_threshold=1.0, bloom_strength=0.35
                       _D(bloom_threshold), _D(bloom_strength), _ptr(w),
                       ctypes.c_int(w.size // 2), _ptr(out))
     return out
+
+
+class RealtimeShading(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_float) for k in (
+        "mass", "spin", "disk_inner", "disk_outer", "disk_temperature", "disk_detail",
+        "exposure", "observer_lapse", "bb_log_min", "bb_log_max", "sky_amplification",
+        "sheet_radiance", "whiteout")] + [(k, ctypes.c_int32) for k in (
+            "background", "temperature_size", "blackbody_size")]
+
+
+def realtime_shade(params: RealtimeShading, status, states, hit_pos, hit_mom, temperature,
+                   blackbody):
+    """realtime/shaders/kerr_tracer.frag:205-420: (n, 3) uint8."""
+    st = np.ascontiguousarray(status, dtype=np.int32)
+    s, hp, hm = _f64(states), _f64(hit_pos), _f64(hit_mom)
+    t = np.ascontiguousarray(temperature, dtype=np.float32)
+    bb = np.ascontiguousarray(blackbody, dtype=np.float32)
+    out = np.empty((st.size, 3), dtype=np.uint8)
+    lib().bho_realtime_shade(ctypes.byref(params), _ptr(st), _ptr(s), _ptr(hp), _ptr(hm),
+                             _I64(st.size), _ptr(t), _ptr(bb), _ptr(out))
+    return out
