@@ -745,6 +745,20 @@ def inflation_workload(device, with_cpu=True, warmup=1, reps=3, side=256, cpu_st
     out = {"rays": side * side, "ms_per_tile": ms, "rays_per_s": side * side / (ms * 1e-3),
            "escaped": int((status == 0).sum()), "terminal": int((status == 1).sum()),
            "budget": int((status == 2).sum())}
+    # The flythrough frame end to end (offline/inflation.py:243-346): the same
+    # camera, 128x128 pixels with supersample 2 (the same ray count), host
+    # wall time of ray set-up, trace and shading to a float32 image.
+    from blackhorizon_b200.offline import OfflineSettings
+    from blackhorizon_b200.vaidya import render_layer_frame_device
+
+    fs = OfflineSettings(supersample=2, fov_degrees=70.0)
+    render_layer_frame_device(st, state[0], side // 2, side // 2, fs, "inward")
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for _ in range(reps):
+        render_layer_frame_device(st, state[0], side // 2, side // 2, fs, "inward")
+    torch.cuda.synchronize()
+    out["frame_ms"] = (time.perf_counter() - t) * 1e3 / reps
     if with_cpu:
         from oracle import oracle
 

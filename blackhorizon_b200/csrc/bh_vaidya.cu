@@ -338,9 +338,106 @@ static double h_f(const bh_vaidya *p, double m, double r) {
     return 1.0 - 2.0 * m / r + std::pow(p->charge, 2.0) / std::pow(r, 2.0);
 }
 
+// ----------------------------------------------- the mass-inflation frame
+
+// numpy.remainder(x, 1.0): fmod, moved into [0, 1).
+__device__ __forceinline__ double mod1(double x) {
+    double m = ::fmod(x, 1.0);
+    if (m != 0.0) {
+        if (m < 0.0) m = __dadd_rn(m, 1.0);
+    } else {
+        m = 0.0;
+    }
+    return m;
+}
+
+// offline/inflation.py:140-142: (sin(a 12.9898 + b 78.233 + salt 37.719)
+// 43758.5453) mod 1.
+__device__ __forceinline__ double sky_hash(double a, double b, double salt37) {
+    const double h = ::sin(__dadd_rn(__dadd_rn(__dmul_rn(a, 12.9898), __dmul_rn(b, 78.233)),
+                                     salt37));
+    return mod1(__dmul_rn(h, 43758.5453));
+}
+
+// offline/inflation.py:138-162 (_surrogate_sky) for one unit direction,
+// float64 in NumPy's operation order.
+__device__ void surrogate_sky(const double *d, double c[3]) {
+    const double theta = ::acos(np_min(np_max(d[2], -1.0), 1.0));
+    const double phi = ::atan2(d[1], d[0]);
+    c[0] = c[1] = c[2] = 0.0;
+#pragma unroll
+    for (int layer = 0; layer < 2; ++layer) {
+        const double cells = layer == 0 ? 38.0 : 85.0;
+        const double brightness = layer == 0 ? 1.6 : 0.8;
+        const double pu = __dmul_rn(__ddiv_rn(phi, 2.0 * M_PI), cells);
+        const double pv = __dmul_rn(__ddiv_rn(theta, M_PI), cells);
+        const double iu = ::floor(pu), iv = ::floor(pv);
+        const double fu = mod1(pu), fv = mod1(pv);
+        const double cx = sky_hash(iu, iv, 37.719), cy = sky_hash(iu, iv, 2.0 * 37.719);
+        const double du = __dsub_rn(fu, cx), dv = __dsub_rn(fv, cy);
+        const double dist2 = __dadd_rn(__dmul_rn(du, du), __dmul_rn(dv, dv));
+        const double mag = sky_hash(iu, iv, 4.0 * 37.719);
+        const double amp = __dmul_rn(__dmul_rn(brightness, __dadd_rn(0.2, ::pow(mag, 4.0))),
+                                     ::exp(__ddiv_rn(-dist2, 0.004)));
+        const double warmth = sky_hash(iu, iv, 5.0 * 37.719);
+        const double tint[3] = {__dadd_rn(0.6, __dmul_rn(0.4, warmth)),
+                                __dadd_rn(0.6, __dmul_rn(0.2, warmth)),
+                                __dsub_rn(1.0, __dmul_rn(0.3, warmth))};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) c[k] = __dadd_rn(c[k], __dmul_rn(amp, tint[k]));
+    }
+}
+
+// offline/inflation.py:322-346: escaped rays (status 0) take the surrogate
+// sky, rays ended in the layer (status 1) glow by the Misner-Sharp mass
+// excess, rays out of budget are black; each ray's radiance is stored as
+// float32, and the supersamples of a pixel are averaged in float32.
+__global__ void inflation_radiance_kernel(double mass, const int32_t *status,
+                                          const double *escape_dir, const double *end_mass,
+                                          long long pixels, int ss2, float *hdr) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= pixels) return;
+    const float sheet[3] = {0.62f, 0.78f, 1.0f};
+    float acc[3] = {0.0f, 0.0f, 0.0f};
+    for (int k = 0; k < ss2; ++k) {
+        const long long i = p * ss2 + k;
+        float c[3] = {0.0f, 0.0f, 0.0f};
+        if (status[i] == 0) {
+            double sky[3];
+            surrogate_sky(escape_dir + 3 * i, sky);
+            c[0] = (float)sky[0]; c[1] = (float)sky[1]; c[2] = (float)sky[2];
+        } else if (status[i] == 1) {
+            const double excess = __ddiv_rn(np_max(__dsub_rn(end_mass[i], mass), 0.0), mass);
+            const double lg = ::log1p(excess);
+            const double glow = __dadd_rn(0.35, __dmul_rn(1.2, __dmul_rn(lg, lg)));
+#pragma unroll
+            for (int j = 0; j < 3; ++j) c[j] = (float)__dmul_rn(glow, (double)sheet[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < 3; ++j) acc[j] = k == 0 ? c[j] : __fadd_rn(acc[j], c[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < 3; ++j) hdr[3 * p + j] = __fdiv_rn(acc[j], (float)ss2);
+}
+
 }  // namespace bh
 
 using namespace bh;
+
+extern "C" int bh_inflation_radiance(double mass, const int32_t *status,
+                                     const double *escape_directions, const double *end_mass,
+                                     int64_t width, int64_t height, int32_t supersample,
+                                     float *hdr, void *stream) {
+    if (!(mass > 0.0) || width < 0 || height < 0 || supersample < 1)
+        return vd_invalid("mass must be > 0, width and height >= 0, supersample >= 1");
+    const long long pixels = (long long)width * height;
+    if (pixels == 0) return BH_OK;
+    if (!status || !escape_directions || !end_mass || !hdr)
+        return vd_invalid("NULL pointer argument");
+    inflation_radiance_kernel<<<vd_grid(pixels), 128, 0, (cudaStream_t)stream>>>(
+        mass, status, escape_directions, end_mass, pixels, supersample * supersample, hdr);
+    return vd_launch("bh_inflation_radiance launch");
+}
 
 extern "C" int64_t bh_vaidya_shell_table(const bh_vaidya *p, double *vs, double *rs,
                                          double *m2s, int64_t capacity) {

@@ -275,3 +275,111 @@ def camera_four_velocity(spacetime: ChargedVaidyaSpacetime, state) -> numpy.ndar
 
     s = numpy.asarray(state, dtype=float)
     return raise_index(spacetime.frozen(float(s[0, 0])), s[:, 1:4], s[:, 4:8])[0]
+
+
+# ------------------------------------------------------ mass-inflation frame
+
+
+def _layer_tetrad(spacetime: ChargedVaidyaSpacetime, state: numpy.ndarray, look: str):
+    """The camera tetrad of a flythrough frame on the frozen slice
+    (offline/inflation.py:252-289): the worldline's 4-velocity, or the rain
+    observer where the worldline sample has diverged; forward along the
+    outward radial direction, its opposite, or sideways."""
+    from .frames import build_tetrad, raise_index
+
+    position = state[1:4]
+    slice_geo = spacetime.frozen(float(state[0]))
+    outward = position / max(numpy.linalg.norm(position), 1e-12)
+    up_seed = numpy.array([0.0, 0.0, 1.0])
+    if abs(float(numpy.dot(outward, up_seed))) > 0.98:
+        up_seed = numpy.array([0.0, 1.0, 0.0])
+    if look == "inward":
+        forward = -outward
+    elif look == "side":
+        forward = numpy.cross(up_seed, outward)
+        forward = forward / max(numpy.linalg.norm(forward), 1e-12)
+    else:
+        forward = outward
+    try:
+        velocity = camera_four_velocity(spacetime, state[None, :])
+        if not numpy.isfinite(velocity).all() or float(numpy.linalg.norm(velocity)) > 1e4:
+            raise ValueError("diverged worldline sample")
+        return slice_geo, build_tetrad(slice_geo, position, velocity, forward, up_seed)
+    except ValueError:
+        geo = slice_geo.geometry(position[None, 0], position[None, 1], position[None, 2])
+        h = float(numpy.asarray(geo.h)[0])
+        l = numpy.asarray(geo.l)[0]
+        root = math.sqrt(max(2.0 * h, 0.0))
+        w = -root / (1.0 + root)
+        rain = raise_index(slice_geo, position[None, :],
+                           numpy.array([[-1.0, w * l[0], w * l[1], w * l[2]]]))[0]
+        return slice_geo, build_tetrad(slice_geo, position, rain, forward, up_seed)
+
+
+def layer_frame_states(spacetime: ChargedVaidyaSpacetime, state, width: int, height: int,
+                       fov_degrees: float, supersample: int, look: str = "outward"):
+    """(width height supersample^2, 8) tetrad rays of a flythrough frame
+    (offline/inflation.py:291-318): the supersampled pinhole grid in the
+    camera's frame, momenta -g(e0 - n.e) lowered on the frozen slice, t the
+    worldline's time.  Host NumPy for the grid, slice geometry from the
+    device."""
+    from .frames import lower_index
+
+    state = numpy.asarray(state, dtype=float)
+    slice_geo, tetrad = _layer_tetrad(spacetime, state, look)
+    tan_half = math.tan(math.radians(fov_degrees) / 2.0)
+    ss = supersample
+    ray = numpy.arange(width * height * ss * ss)
+    pixel, sub = numpy.divmod(ray, ss * ss)
+    row, col = numpy.divmod(pixel, width)
+    sub_row, sub_col = numpy.divmod(sub, ss)
+    u = (col + (sub_col + 0.5) / ss) / width * 2.0 - 1.0
+    v = 1.0 - (row + (sub_row + 0.5) / ss) / height * 2.0
+    right = u * tan_half
+    up = v * tan_half / (width / height)
+    norm = numpy.sqrt(1.0 + right * right + up * up)
+    local = numpy.stack([1.0 / norm, right / norm, up / norm], axis=-1)
+    spatial = sum(local[:, k:k + 1] * tetrad[k + 1] for k in range(3))
+    physical = tetrad[0][None, :] - spatial
+    positions = numpy.tile(state[1:4][None, :], (local.shape[0], 1))
+    momenta = numpy.asarray(lower_index(slice_geo, positions, -physical))
+    out = numpy.empty((local.shape[0], 8))
+    out[:, 0] = state[0]
+    out[:, 1:4] = positions
+    out[:, 4:8] = momenta
+    return out
+
+
+def render_layer_frame_device(spacetime: ChargedVaidyaSpacetime, state, width: int,
+                              height: int, settings, look: str = "outward", *,
+                              return_rays: bool = False):
+    """One frame of the mass-inflation flythrough as a float32 (height,
+    width, 3) device tensor (offline/inflation.py:243-346): tetrad rays from
+    the worldline state, traced through the surrogate to max(12, 2.5 r) or
+    the terminal surface at 1.001 r_minus (``trace_vaidya_tile``), then
+    shaded and averaged on the device (``bh_inflation_radiance``).
+    ``settings`` supplies fov_degrees and supersample (OfflineSettings)."""
+    state = numpy.asarray(state, dtype=float)
+    ss = int(settings.supersample)
+    s0 = layer_frame_states(spacetime, state, width, height, settings.fov_degrees, ss, look)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    escape_radius = max(12.0, 2.5 * float(numpy.linalg.norm(state[1:4])))
+    status, edir, mass, v_end = trace_vaidya_tile(
+        spacetime, torch.as_tensor(s0, device=dev), escape_radius,
+        spacetime.inner_horizon_radius * 1.001)
+    hdr = torch.empty((height, width, 3), dtype=torch.float32, device=dev)
+    _lib.check(_lib.load().bh_inflation_radiance(
+        float(spacetime.mass), ptr(status), ptr(edir.contiguous()), ptr(mass.contiguous()),
+        width, height, ss, ptr(hdr), stream_handle()), "inflation radiance")
+    if return_rays:
+        return hdr, {"state0": s0, "status": status, "escape_directions": edir,
+                     "end_mass": mass, "v_end": v_end}
+    return hdr
+
+
+def render_layer_frame(spacetime: ChargedVaidyaSpacetime, state, width: int, height: int,
+                       settings, look: str = "outward") -> numpy.ndarray:
+    """render_layer_frame (offline/inflation.py:243-346): the frame as a
+    (height, width, 3) float32 NumPy array."""
+    return render_layer_frame_device(spacetime, state, width, height, settings,
+                                     look).cpu().numpy()

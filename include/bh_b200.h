@@ -425,6 +425,17 @@ int bh_vaidya_trace(const bh_vaidya *spacetime, const double *state0, int64_t n,
                     double *states, int32_t *status, double *escape_dir,
                     double *end_mass, double *v_end, void *workspace, void *stream);
 
+/* offline/inflation.py:138-162 and 322-346 (the shading of
+ * render_layer_frame): per ray of bh_vaidya_trace, status 0 takes the
+ * surrogate starfield of its escape direction, status 1 the glow 0.35 +
+ * 1.2 log1p(max(end_mass - mass, 0) / mass)^2 times the sheet colour (0.62,
+ * 0.78, 1.0), status 2 black; each ray's radiance rounded to float32 and the
+ * supersample^2 consecutive rays of a pixel averaged in float32 into hdr
+ * (height, width, 3). */
+int bh_inflation_radiance(double mass, const int32_t *status, const double *escape_directions,
+                          const double *end_mass, int64_t width, int64_t height,
+                          int32_t supersample, float *hdr, void *stream);
+
 /* ------------------------------------------------------------ offline tile */
 
 /* Counters of one bh_trace_tile call. */

@@ -1398,3 +1398,68 @@ void bho_realtime_shade(const bho_realtime_shading_t *p, const int32_t *status,
         for (int k = 0; k < 3; ++k) rgb[3 * i + k] = (uint8_t)lrintf(clampf(c[k], 0.0f, 1.0f) * 255.0f);
     }
 }
+
+/* ------------------------------------------ offline/inflation.py frame shading */
+
+static double np_mod1(double x) {
+    double m = fmod(x, 1.0);
+    if (m != 0.0) {
+        if (m < 0.0) m += 1.0;
+    } else {
+        m = 0.0;
+    }
+    return m;
+}
+
+static double sky_hash(double a, double b, double salt) {
+    /* inflation.py:140-142 */
+    const double h = sin(a * 12.9898 + b * 78.233 + salt * 37.719);
+    return np_mod1(h * 43758.5453);
+}
+
+static void surrogate_sky(const double *d, double *c) {
+    /* inflation.py:138-162 */
+    const double theta = acos(np_clip(d[2], -1.0, 1.0));
+    const double phi = atan2(d[1], d[0]);
+    static const double cells_of[2] = {38.0, 85.0}, bright_of[2] = {1.6, 0.8};
+    c[0] = c[1] = c[2] = 0.0;
+    for (int layer = 0; layer < 2; ++layer) {
+        const double cells = cells_of[layer];
+        const double pu = phi / (2.0 * M_PI) * cells, pv = theta / M_PI * cells;
+        const double iu = floor(pu), iv = floor(pv);
+        const double fu = np_mod1(pu), fv = np_mod1(pv);
+        const double cx = sky_hash(iu, iv, 1.0), cy = sky_hash(iu, iv, 2.0);
+        const double dist2 = (fu - cx) * (fu - cx) + (fv - cy) * (fv - cy);
+        const double mag = sky_hash(iu, iv, 4.0);
+        const double amp = bright_of[layer] * (0.2 + pow(mag, 4.0)) * exp(-dist2 / 0.004);
+        const double w = sky_hash(iu, iv, 5.0);
+        const double tint[3] = {0.6 + 0.4 * w, 0.6 + 0.2 * w, 1.0 - 0.3 * w};
+        for (int k = 0; k < 3; ++k) c[k] = c[k] + amp * tint[k];
+    }
+}
+
+void bho_inflation_radiance(double mass, const int32_t *status, const double *escape_dir,
+                            const double *end_mass, int64_t pixels, int supersample,
+                            float *hdr) {
+    const int ss2 = supersample * supersample;
+    const float sheet[3] = {0.62f, 0.78f, 1.0f};
+    for (int64_t p = 0; p < pixels; ++p) {
+        float acc[3] = {0.0f, 0.0f, 0.0f};
+        for (int k = 0; k < ss2; ++k) {
+            const int64_t i = p * ss2 + k;
+            float c[3] = {0.0f, 0.0f, 0.0f};
+            if (status[i] == 0) {
+                double sky[3];
+                surrogate_sky(escape_dir + 3 * i, sky);
+                for (int j = 0; j < 3; ++j) c[j] = (float)sky[j];
+            } else if (status[i] == 1) {
+                const double excess = np_max(end_mass[i] - mass, 0.0) / mass;
+                const double lg = log1p(excess);
+                const double glow = 0.35 + 1.2 * (lg * lg);
+                for (int j = 0; j < 3; ++j) c[j] = (float)(glow * (double)sheet[j]);
+            }
+            for (int j = 0; j < 3; ++j) acc[j] = k == 0 ? c[j] : acc[j] + c[j];
+        }
+        for (int j = 0; j < 3; ++j) hdr[3 * p + j] = acc[j] / (float)ss2;
+    }
+}

@@ -277,6 +277,13 @@ void bho_realtime_shade(const bho_realtime_shading_t *p, const int32_t *status,
                         const double *hit_mom, int64_t n, const float *temperature,
                         const float *blackbody, uint8_t *rgb);
 
+/* offline/inflation.py:138-162, 322-346: the shading of render_layer_frame
+ * (surrogate sky, layer glow, black) averaged over supersample^2 consecutive
+ * rays per pixel in float32, into hdr (pixels, 3). */
+void bho_inflation_radiance(double mass, const int32_t *status, const double *escape_dir,
+                            const double *end_mass, int64_t pixels, int supersample,
+                            float *hdr);
+
 /* offline/post.py:88-106 (develop) on an (height, width, 3) float32 image;
  * weights (2 radius + 1) are gaussian_kernel(sigma); bloom_strength <= 0
  * skips the bloom. */

@@ -469,3 +469,14 @@ def realtime_shade(params: RealtimeShading, status, states, hit_pos, hit_mom, te
     lib().bho_realtime_shade(ctypes.byref(params), _ptr(st), _ptr(s), _ptr(hp), _ptr(hm),
                              _I64(st.size), _ptr(t), _ptr(bb), _ptr(out))
     return out
+
+
+def inflation_radiance(mass: float, status, escape_dir, end_mass, width: int, height: int,
+                       supersample: int = 1):
+    """offline/inflation.py:138-162, 322-346: (height, width, 3) float32."""
+    st = np.ascontiguousarray(status, dtype=np.int32)
+    ed, em = _f64(escape_dir), _f64(end_mass)
+    out = np.empty((height, width, 3), dtype=np.float32)
+    lib().bho_inflation_radiance(_D(mass), _ptr(st), _ptr(ed), _ptr(em),
+                                 _I64(width * height), ctypes.c_int(supersample), _ptr(out))
+    return out

@@ -578,6 +578,70 @@ def gen_emission(ref, out):
     np.savez_compressed(os.path.join(out, "emission.npz"), **arrs)
 
 
+def gen_inflation_frame(ref, out):
+    """render_layer_frame (offline/inflation.py:243-346) on small flythrough
+    frames of the q = 0.9 surrogate with the shell at v = 6, R = 1.2: rain
+    observers at r = 1.3 (looking outward and inward) and at r = 0.8, 24x16
+    pixels with supersample 2, fov 90.  The per-ray trace outputs are made
+    by the same steps as render_layer_frame and checked against its image."""
+    _offline_modules(_REFERENCE_PATH)
+    from blackhorizon.frames import build_tetrad, lower_index
+    from blackhorizon.offline import inflation as infl
+    from blackhorizon.offline.render import OfflineSettings
+    from blackhorizon.vaidya import ChargedVaidyaSpacetime
+
+    st = ChargedVaidyaSpacetime(charge=0.9, shell_start_v=6.0, shell_start_radius=1.2)
+    settings = OfflineSettings(supersample=2, fov_degrees=90.0)
+    w, h, ss = 24, 16, 2
+    arrs = {"params": np.array([st.mass, st.charge, st.tail_mass, st.tail_start, st.tail_power,
+                                st.shell_energy, st.shell_start_v, st.shell_start_radius,
+                                st.shell_width, st.mass_cap]),
+            "frame": np.array([w, h, ss, settings.fov_degrees])}
+    for tag, radius, look in (("out13", 1.3, "outward"), ("in13", 1.3, "inward"),
+                              ("out08", 0.8, "outward")):
+        state = infl.rain_state(st, np.array([radius, 0.0, 0.0]), 6.0)[0]
+        hdr = infl.render_layer_frame(st, state, w, h, settings, look)
+        # The rays of render_layer_frame (inflation.py:252-320), step by step.
+        position = state[1:4]
+        velocity = infl.camera_four_velocity(st, state[None, :])
+        slice_geo = st.frozen(float(state[0]))
+        outward = position / max(np.linalg.norm(position), 1e-12)
+        up_seed = np.array([0.0, 0.0, 1.0])
+        forward = -outward if look == "inward" else outward
+        tetrad = build_tetrad(slice_geo, position, velocity, forward, up_seed)
+        tan_half = np.tan(np.radians(settings.fov_degrees) / 2.0)
+        offsets = (np.arange(ss) + 0.5) / ss
+        u = (np.arange(w)[:, None] + offsets[None, :]).reshape(-1) / w * 2.0 - 1.0
+        v = 1.0 - (np.arange(h)[:, None] + offsets[None, :]).reshape(-1) / h * 2.0
+        ug = np.tile(u.reshape(w, ss)[None, :, None, :], (h, 1, ss, 1)).reshape(-1)
+        vg = np.tile(v.reshape(h, ss)[:, None, :, None], (1, w, 1, ss)).reshape(-1)
+        local = np.stack([np.ones_like(ug), ug * tan_half, vg * tan_half / (w / h)], axis=-1)
+        local /= np.linalg.norm(local, axis=-1, keepdims=True)
+        spatial = local[:, 0:1] * tetrad[1] + local[:, 1:2] * tetrad[2] + local[:, 2:3] * tetrad[3]
+        positions = np.tile(position[None, :], (local.shape[0], 1))
+        momenta = lower_index(slice_geo, positions, -(tetrad[0][None, :] - spatial))
+        s0 = np.concatenate([np.full((local.shape[0], 1), float(state[0])), positions, momenta],
+                            axis=1)
+        esc = max(12.0, 2.5 * float(np.linalg.norm(position)))
+        status, edir, mass, _ = infl._trace_vaidya_tile(st, s0, esc,
+                                                        st.inner_horizon_radius * 1.001)
+        rad = np.zeros((s0.shape[0], 3), dtype=np.float32)
+        if (status == 0).any():
+            rad[status == 0] = infl._surrogate_sky(edir[status == 0])
+        lay = status == 1
+        if lay.any():
+            excess = np.maximum(mass[lay] - st.mass, 0.0) / st.mass
+            glow = 0.35 + 1.2 * np.log1p(excess) ** 2
+            rad[lay] = glow[:, None] * np.array(infl.SHEET_COLOR, dtype=np.float32)
+        assert np.array_equal(rad.reshape(h, w, ss * ss, 3).mean(axis=2), hdr), tag
+        for k, val in (("state", state), ("tetrad", tetrad), ("state0", s0),
+                       ("status", status.astype(np.int8)), ("escape_dir", edir),
+                       ("end_mass", mass), ("radiance", rad), ("hdr", hdr)):
+            arrs[f"{tag}_{k}"] = val
+        arrs[f"{tag}_look"] = np.array(look)
+    np.savez_compressed(os.path.join(out, "inflation_frame.npz"), **arrs)
+
+
 def gen_images(ref, out):
     """imaging.py:27-91 on the reference's own traces.
 
@@ -842,6 +906,7 @@ def main():
         ("offline_tile", lambda: gen_offline_tile(ref, args.out)),
         ("offline_interior", lambda: gen_offline_interior(ref, args.out)),
         ("emission", lambda: gen_emission(ref, args.out)),
+        ("inflation_frame", lambda: gen_inflation_frame(ref, args.out)),
         ("images", lambda: gen_images(ref, args.out)),
         ("realtime", lambda: gen_realtime(ref, args.out)),
         ("vaidya", lambda: gen_vaidya(ref, args.out)),

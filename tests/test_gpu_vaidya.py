@@ -156,3 +156,47 @@ def test_flythrough_camera_tile(cuda):
     status, _, _, _ = trace_vaidya_tile(st, torch.as_tensor(s0, device="cuda"), esc, stop)
     assert status.is_cuda
     np.testing.assert_array_equal(status.cpu().numpy(), g["tile_out_status"])
+
+
+def test_inflation_frame_matches_reference(cuda):
+    """render_layer_frame (offline/inflation.py:243-346): the flythrough
+    camera's tetrad rays on the frozen slice, the device shading of the
+    reference's traced rays, and whole frames traced and shaded on the
+    device, against the reference's frames (tests/golden/inflation_frame.npz)."""
+    from blackhorizon_b200 import _lib
+    from blackhorizon_b200.backend import ptr
+    from blackhorizon_b200.offline import OfflineSettings
+    from blackhorizon_b200.vaidya import (ChargedVaidyaSpacetime, layer_frame_states,
+                                          render_layer_frame, render_layer_frame_device)
+
+    g = golden("inflation_frame.npz")
+    st = ChargedVaidyaSpacetime(**dict(zip(FIELDS, (float(x) for x in g["params"]))))
+    w, h, ss, fov = g["frame"]
+    w, h, ss = int(w), int(h), int(ss)
+    settings = OfflineSettings(supersample=ss, fov_degrees=float(fov))
+    for tag in ("out13", "in13", "out08"):
+        look = str(g[f"{tag}_look"])
+        s0 = layer_frame_states(st, g[f"{tag}_state"], w, h, float(fov), ss, look)
+        assert _rel(s0, g[f"{tag}_state0"]) < 1e-12
+        # The device shading of the reference's own trace outputs.
+        hdr = torch.empty((h, w, 3), dtype=torch.float32, device="cuda")
+        dev = lambda k: torch.as_tensor(g[f"{tag}_{k}"], device="cuda")  # noqa: E731
+        status = dev("status").to(torch.int32)
+        edir, mass = dev("escape_dir"), dev("end_mass")
+        _lib.check(_lib.load().bh_inflation_radiance(
+            float(st.mass), ptr(status), ptr(edir), ptr(mass), w, h, ss, ptr(hdr), None))
+        torch.cuda.synchronize()
+        ref = g[f"{tag}_hdr"]
+        np.testing.assert_allclose(hdr.cpu().numpy(), ref, rtol=1e-6, atol=1e-12)
+        # The whole frame on the device.
+        out, rays = render_layer_frame_device(st, g[f"{tag}_state"], w, h, settings, look,
+                                              return_rays=True)
+        got_status = rays["status"].cpu().numpy()
+        agree = float(np.mean(got_status == g[f"{tag}_status"]))
+        same_px = (got_status == g[f"{tag}_status"]).reshape(h, w, ss * ss).all(axis=2)
+        rel = (np.abs(out.cpu().numpy() - ref) / np.maximum(np.abs(ref), 1e-6)).max(axis=2)
+        print(tag, "status agreement", agree, "max rel on equal pixels", float(rel[same_px].max()))
+        assert agree >= 0.99
+        assert float(np.mean(rel[same_px] < 1e-5)) >= 0.99
+    host = render_layer_frame(st, g["out13_state"], w, h, settings)
+    assert isinstance(host, np.ndarray) and host.dtype == np.float32 and host.shape == (h, w, 3)

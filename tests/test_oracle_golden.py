@@ -375,3 +375,14 @@ def test_oracle_emission_and_develop(oracle):
             diff = np.abs(out.astype(int) - g[f"{tag}_{key}"].astype(int))
             print(tag, key, "levels off:", int(diff.max()), "pixels:", int((diff > 0).sum()))
             assert diff.max() <= 1 and (diff > 0).mean() < 1e-3
+
+
+def test_oracle_inflation_frame(oracle):
+    """offline/inflation.py:138-162, 322-346: the oracle shades the
+    reference's traced flythrough rays into the reference's frames."""
+    g = golden("inflation_frame.npz")
+    w, h, ss, _ = (int(x) for x in g["frame"])
+    for tag in ("out13", "in13", "out08"):
+        hdr = oracle.inflation_radiance(float(g["params"][0]), g[f"{tag}_status"],
+                                        g[f"{tag}_escape_dir"], g[f"{tag}_end_mass"], w, h, ss)
+        np.testing.assert_allclose(hdr, g[f"{tag}_hdr"], rtol=1e-6, atol=1e-12)
