@@ -156,6 +156,8 @@ _SIGNATURES = {
     "bh_trace_tile": (ctypes.c_int, [ctypes.POINTER(TraceConfig), ctypes.POINTER(Scene), _D, _D,
                                      _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _SZ,
                                      ctypes.POINTER(TileStats), _P]),
+    "bh_radial_momentum": (ctypes.c_int, [_D, _D, _P, _D, _P]),
+    "bh_plunge_worldline": (_I64, [_D, _D, _D, _D, _D, _D, _I64, _P, _P]),
     "bh_inflation_radiance": (ctypes.c_int, [_D, _P, _P, _P, _I64, _I64, _I32, _P, _P]),
     "bh_realtime_shade": (ctypes.c_int, [ctypes.POINTER(RealtimeShading), _P, _P, _P, _P, _I64,
                                          _I64, _P, _P, _P, _P]),

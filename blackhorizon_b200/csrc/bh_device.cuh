@@ -101,13 +101,13 @@ template <> struct Math<float> {
     static __device__ __forceinline__ float tiny2() { return 1e-37f; }
 };
 
-// numpy.maximum propagates NaN (fmax would drop it).
+// numpy.maximum propagates NaN (fmax would drop it).  Host code uses them too.
 template <typename T>
-__device__ __forceinline__ T np_max(T a, T b) {
+__host__ __device__ __forceinline__ T np_max(T a, T b) {
     return (a != a || b != b) ? (a + b) : (a >= b ? a : b);
 }
 template <typename T>
-__device__ __forceinline__ T np_min(T a, T b) {
+__host__ __device__ __forceinline__ T np_min(T a, T b) {
     return (a != a || b != b) ? (a + b) : (a <= b ? a : b);
 }
 
@@ -117,7 +117,7 @@ struct Geometry {
     double r, h, l[3], grad_h[3], grad_l[3][3];
 };
 
-__device__ __forceinline__ void geometry_full(double m, double a, double x,
+__host__ __device__ __forceinline__ void geometry_full(double m, double a, double x,
                                               double y, double z, bool grads,
                                               Geometry &o) {
     const double a2 = a * a;

@@ -512,6 +512,26 @@ int bh_realtime_shade(const bh_realtime_shading *shading, const int32_t *status,
                       const float *temperature_table, const float *blackbody_table,
                       uint8_t *rgb, void *stream);
 
+/* ------------------------------------------------------ plunge worldline */
+
+/* offline/infall.py:38-91 (radial_momentum): the covariant momentum
+ * (p_t, p_x, p_y, p_z) = (-E, w l) of a radial infaller with conserved
+ * energy E >= 0 at position[3], the future-directed inward root of the
+ * timelike mass shell.  Host computation. */
+int bh_radial_momentum(double mass, double spin, const double *position, double energy,
+                       double *momentum);
+
+/* offline/infall.py:94-153 (build_plunge): the plunging camera's worldline
+ * from (start_radius, 0, 0) with energy E, integrated on the host by RK4 in
+ * proper time with step min(step, max(0.04 r^1.5, 1e-6)), the mass shell held
+ * at H = -1/2, to r <= stop_radius, the chart's edge or 2,000,000 steps.
+ * Writes up to `capacity` samples (proper times taus, states (k, 8)) and
+ * returns the number of samples of the whole worldline (call with capacity 0
+ * to size it), or -1. */
+int64_t bh_plunge_worldline(double mass, double spin, double start_radius, double energy,
+                            double stop_radius, double step, int64_t capacity, double *taus,
+                            double *states);
+
 /* ---------------------------------------------------- offline camera rays */
 
 /* A camera of the offline renderer and its supersampled pixel grid

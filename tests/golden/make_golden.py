@@ -56,6 +56,7 @@ REF_FILES = [
     "blackhorizon/emission/redshift.py",
     "blackhorizon/emission/bluesheet.py",
     "blackhorizon/offline/post.py",
+    "blackhorizon/offline/infall.py",
     "tests/test_kerr.py",
     "tests/test_shadow.py",
     "tests/test_bluesheet.py",
@@ -642,6 +643,49 @@ def gen_inflation_frame(ref, out):
     np.savez_compressed(os.path.join(out, "inflation_frame.npz"), **arrs)
 
 
+def gen_plunge(ref, out):
+    """offline/infall.py:38-262: radial momenta, the plunge worldlines of
+    three presets (rain at a = 0.6 from r = 3 to the Cauchy horizon, fast
+    E = 1.5 in Schwarzschild from r = 6 to 0.02, maximal E = 0 at a = 0.9
+    from just inside r_plus), the camera tetrads at samples of the first, and
+    one 32x20 frame of it rendered by render_hdr with the tetrad and stop."""
+    render, FlyCamera, _ = _offline_modules(_REFERENCE_PATH)
+    from blackhorizon.offline import infall
+
+    arrs = {}
+    cases = (("rain06", 0.6, 3.0, 1.0, "real"), ("fast0", 0.0, 6.0, 1.5, 0.02),
+             ("max09", 0.9, None, 0.0, "real"))
+    for tag, spin, start, energy, stop in cases:
+        st = ref["KerrSpacetime"](1.0, spin)
+        if start is None:
+            start = st.outer_horizon_radius * 0.995
+        if stop == "real":
+            stop = st.inner_horizon_radius * 1.02
+        mom = infall.radial_momentum(st, np.array([start, 0.0, 0.0]), energy)
+        taus, states = infall.build_plunge(st, start, energy, stop)
+        idx = np.unique(np.concatenate([np.arange(0, taus.size, 25), [taus.size - 1]]))
+        arrs[f"{tag}_args"] = np.array([spin, start, energy, stop])
+        arrs[f"{tag}_momentum"] = mom
+        arrs[f"{tag}_count"] = np.int64(taus.size)
+        arrs[f"{tag}_index"] = idx
+        arrs[f"{tag}_taus"] = taus[idx]
+        arrs[f"{tag}_states"] = states[idx]
+        if tag == "rain06":
+            samples = [0, taus.size // 2, taus.size - 1]
+            for k, look in zip(samples, ("inward", "outward", "side")):
+                pos, tet = infall.plunge_tetrad(st, states[k], look)
+                arrs[f"tetrad_{look}_sample"] = states[k]
+                arrs[f"tetrad_{look}"] = tet
+            settings = render.OfflineSettings(spin=spin, supersample=1, fov_degrees=80.0)
+            k = taus.size // 2
+            pos, tet = infall.plunge_tetrad(st, states[k], "inward")
+            cam = FlyCamera(position=pos.copy(), yaw=0.0, pitch=0.0)
+            arrs["frame_sample"] = states[k]
+            arrs["frame_hdr"] = render.render_hdr(cam, 32, 20, settings, progress=False,
+                                                  camera_tetrad=tet, interior_stop=stop)
+    np.savez_compressed(os.path.join(out, "plunge.npz"), **arrs)
+
+
 def gen_images(ref, out):
     """imaging.py:27-91 on the reference's own traces.
 
@@ -907,6 +951,7 @@ def main():
         ("offline_interior", lambda: gen_offline_interior(ref, args.out)),
         ("emission", lambda: gen_emission(ref, args.out)),
         ("inflation_frame", lambda: gen_inflation_frame(ref, args.out)),
+        ("plunge", lambda: gen_plunge(ref, args.out)),
         ("images", lambda: gen_images(ref, args.out)),
         ("realtime", lambda: gen_realtime(ref, args.out)),
         ("vaidya", lambda: gen_vaidya(ref, args.out)),

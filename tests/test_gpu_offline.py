@@ -274,3 +274,26 @@ def test_device_camera_rays_match_reference(cuda):
         rel = np.abs(got - ref) / np.maximum(np.abs(ref), 1e-300)
         print("camera rays: max relative difference", float(rel.max()))
         assert float(rel.max()) < 1e-14
+
+
+def test_plunge_tetrads_and_frame(cuda):
+    """offline/infall.py:156-262: the camera tetrads at worldline samples
+    equal the reference's, and a plunge frame rendered on the device (tetrad
+    rays, interior stop at the Cauchy horizon, disk) matches the reference's
+    render_hdr frame."""
+    from blackhorizon_b200.infall import plunge_frame, plunge_tetrad
+    from blackhorizon_b200.kerr import KerrSpacetime
+    from blackhorizon_b200.offline import OfflineSettings
+
+    g = golden("plunge.npz")
+    spin, start, energy, stop = (float(x) for x in g["rain06_args"])
+    st = KerrSpacetime(1.0, spin)
+    for look in ("inward", "outward", "side"):
+        _, tet = plunge_tetrad(st, g[f"tetrad_{look}_sample"], look)
+        np.testing.assert_allclose(tet, g[f"tetrad_{look}"], rtol=1e-12, atol=1e-12)
+    settings = OfflineSettings(spin=spin, supersample=1, fov_degrees=80.0)
+    hdr = plunge_frame(st, g["frame_sample"], 32, 20, settings, "inward", stop)
+    ref = g["frame_hdr"]
+    rel = (np.abs(hdr.cpu().numpy() - ref) / np.maximum(np.abs(ref), 1e-6)).max(axis=2)
+    print("plunge frame: pixels within 1e-5:", float(np.mean(rel < 1e-5)), "max", float(rel.max()))
+    assert float(np.mean(rel < 1e-5)) >= 0.99

@@ -151,3 +151,33 @@ def test_offline_pixel_grid_matches_reference(oracle):
     pos = np.tile(cam.position[None, :], (d.shape[0], 1))
     p = oracle.null_momentum(1.0, float(spin), pos, d, True, True)
     np.testing.assert_array_equal(p, e["ext_state0"][:, 4:8])
+
+
+def test_plunge_worldline_matches_reference():
+    """offline/infall.py:38-153 (radial_momentum, build_plunge), integrated
+    by the library on the host: the reference's momenta, step counts, proper
+    times and sampled states for the rain, fast and maximal presets."""
+    import numpy as np
+
+    from blackhorizon_b200.infall import build_plunge, radial_momentum
+    from blackhorizon_b200.kerr import KerrSpacetime
+    from conftest import golden
+
+    g = golden("plunge.npz")
+    for tag in ("rain06", "fast0", "max09"):
+        spin, start, energy, stop = (float(x) for x in g[f"{tag}_args"])
+        st = KerrSpacetime(1.0, spin)
+        np.testing.assert_allclose(radial_momentum(st, [start, 0.0, 0.0], energy),
+                                   g[f"{tag}_momentum"], rtol=1e-14, atol=1e-15)
+        taus, states = build_plunge(st, start, energy, stop)
+        assert taus.size == int(g[f"{tag}_count"]), tag
+        idx = g[f"{tag}_index"]
+        np.testing.assert_allclose(taus[idx], g[f"{tag}_taus"], rtol=1e-12)
+        ref = g[f"{tag}_states"]
+        rel = np.abs(states[idx] - ref) / np.maximum(np.abs(ref), 1.0)
+        print(tag, "max state difference", float(rel.max()))
+        assert float(rel.max()) < 1e-8
+    import pytest
+
+    with pytest.raises(ValueError):
+        radial_momentum(KerrSpacetime(1.0, 0.5), [4.0, 0.0, 0.0], 0.0)  # E = 0 outside
