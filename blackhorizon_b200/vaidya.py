@@ -383,3 +383,40 @@ def render_layer_frame(spacetime: ChargedVaidyaSpacetime, state, width: int, hei
     (height, width, 3) float32 NumPy array."""
     return render_layer_frame_device(spacetime, state, width, height, settings,
                                      look).cpu().numpy()
+
+
+def build_worldline(spacetime: ChargedVaidyaSpacetime, start_radius: float, start_time: float,
+                    stop_radius: float, step: float = 2e-3, mass_threshold: float = 1e4):
+    """(taus (k,), states (k, 8)): the flythrough camera's worldline
+    (offline/inflation.py:77-135), a rain observer from (start_radius, 0, 0)
+    at start_time, RK4 in proper time with the step min(step, max(0.05 (r -
+    r_minus floored at 5e-3), 2e-3)), sampled every 8 steps and at the end,
+    stopped at r <= stop_radius, where the Misner-Sharp mass reaches
+    mass_threshold, on a non-finite state or after 120000 steps.  The steps
+    run on the device (``vaidya_rk4``, ``misner_sharp_mass``), the loop on
+    the host: the worldline is one sequential trajectory."""
+    state = rain_state(spacetime, numpy.array([float(start_radius), 0.0, 0.0]),
+                       float(start_time))
+    r_minus = spacetime.inner_horizon_radius
+    tau = 0.0
+    taus = [0.0]
+    states = [state[0].copy()]
+    for iteration in range(120000):
+        radius = float(numpy.sqrt(numpy.sum(state[0, 1:4] ** 2)))
+        proximity = max(radius - r_minus, 5e-3)
+        step_now = float(min(step, max(0.05 * proximity, 2e-3)))
+        state = vaidya_rk4(spacetime, state, numpy.array([step_now]), 1)
+        if not numpy.isfinite(state).all():
+            break
+        tau += step_now
+        radius = float(numpy.sqrt(numpy.sum(state[0, 1:4] ** 2)))
+        v_here = float(state[0, 0]) + radius
+        mass_here = float(numpy.asarray(spacetime.misner_sharp_mass(
+            numpy.array([v_here]), numpy.array([radius])))[0])
+        reached = radius <= stop_radius or mass_here >= mass_threshold
+        if iteration % 8 == 0 or reached:
+            taus.append(tau)
+            states.append(state[0].copy())
+        if reached:
+            break
+    return numpy.asarray(taus), numpy.stack(states)

@@ -640,6 +640,11 @@ def gen_inflation_frame(ref, out):
                        ("end_mass", mass), ("radiance", rad), ("hdr", hdr)):
             arrs[f"{tag}_{k}"] = val
         arrs[f"{tag}_look"] = np.array(look)
+    # The flythrough's camera worldline (inflation.py:77-135) with the CLI's
+    # defaults: start at r = 1.3, v = 6, stop at 1.001 r_minus.
+    taus, states = infl.build_worldline(st, 1.3, 6.0, st.inner_horizon_radius * 1.001)
+    arrs["worldline_taus"] = taus
+    arrs["worldline_states"] = states
     np.savez_compressed(os.path.join(out, "inflation_frame.npz"), **arrs)
 
 

@@ -200,3 +200,17 @@ def test_inflation_frame_matches_reference(cuda):
         assert float(np.mean(rel[same_px] < 1e-5)) >= 0.99
     host = render_layer_frame(st, g["out13_state"], w, h, settings)
     assert isinstance(host, np.ndarray) and host.dtype == np.float32 and host.shape == (h, w, 3)
+
+
+def test_flythrough_worldline_matches_reference(cuda):
+    """build_worldline (offline/inflation.py:77-135): the camera's worldline
+    with the flythrough's defaults, against the reference's samples."""
+    from blackhorizon_b200.vaidya import ChargedVaidyaSpacetime, build_worldline
+
+    g = golden("inflation_frame.npz")
+    st = ChargedVaidyaSpacetime(**dict(zip(FIELDS, (float(x) for x in g["params"]))))
+    taus, states = build_worldline(st, 1.3, 6.0, st.inner_horizon_radius * 1.001)
+    assert taus.size == g["worldline_taus"].size
+    np.testing.assert_allclose(taus, g["worldline_taus"], rtol=1e-13)
+    print("worldline: max state difference", _rel(states, g["worldline_states"]))
+    assert _rel(states, g["worldline_states"]) < 1e-9
