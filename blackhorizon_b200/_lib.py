@@ -165,6 +165,9 @@ _SIGNATURES = {
     "bh_offline_radiance": (ctypes.c_int, [ctypes.POINTER(EmissionConfig), _P, _P, _P, _P, _P,
                                            _I64, _I64, _P, _P, _P, _P, _P]),
     "bh_develop_workspace_bytes": (_SZ, [_I64, _I64]),
+    "bh_downsample": (ctypes.c_int, [_P, _I64, _I64, _I32, _P, _P]),
+    "bh_frame_bloom_workspace_bytes": (_SZ, [_I64, _I64]),
+    "bh_frame_bloom": (ctypes.c_int, [_P, _I64, _I64, _D, _P, _I32, _P, _P, _SZ, _P]),
     "bh_develop": (ctypes.c_int, [_P, _I64, _I64, _D, _D, _D, _P, _I32, _P, _P, _SZ, _P]),
     "bh_fma_peak_launch": (ctypes.c_int, [_I32, _I64, _P, ctypes.POINTER(_I64), _P]),
 }

@@ -254,16 +254,58 @@ __global__ void blur_kernel(const float *src, long long width, long long height,
 }
 
 // post.py:59-85: ACES (Narkowicz 2015 fit) and the sRGB curve, float32.
-__device__ __forceinline__ uint8_t develop_channel(float x) {
-    const float a = 2.51f, b = 0.03f, c = 2.43f, d = 0.59f, e = 0.14f;
-    const float num = __fmul_rn(x, __fadd_rn(__fmul_rn(a, x), b));
-    const float den = __fadd_rn(__fmul_rn(x, __fadd_rn(__fmul_rn(c, x), d)), e);
-    float m = __fdiv_rn(num, den);
+// post.py:70-85 (encode_srgb): linear [0, 1] to 8 bits, float32.
+__device__ __forceinline__ uint8_t srgb8(float m) {
     m = fminf(fmaxf(m, 0.0f), 1.0f);
     const float enc = m <= 0.0031308f
                           ? __fmul_rn(12.92f, m)
                           : __fsub_rn(__fmul_rn(1.055f, powf(m, (float)(1.0 / 2.4))), 0.055f);
     return (uint8_t)__fadd_rn(__fmul_rn(enc, 255.0f), 0.5f);
+}
+
+__device__ __forceinline__ uint8_t develop_channel(float x) {
+    const float a = 2.51f, b = 0.03f, c = 2.43f, d = 0.59f, e = 0.14f;
+    const float num = __fmul_rn(x, __fadd_rn(__fmul_rn(a, x), b));
+    const float den = __fadd_rn(__fmul_rn(x, __fadd_rn(__fmul_rn(c, x), d)), e);
+    return srgb8(fminf(fmaxf(__fdiv_rn(num, den), 0.0f), 1.0f));
+}
+
+// ------------------------------------------------------------ video frames
+
+// offline/video.py:33-43 (downsample): the mean of each factor x factor block
+// of an 8-bit image, truncated to 8 bits.  The float32 block sum of integers
+// below 2^24 is exact in any order.
+__global__ void downsample_kernel(const uint8_t *in, long long in_w, int factor,
+                                  long long out_w, long long out_h, uint8_t *out) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= out_w * out_h) return;
+    const long long oy = p / out_w, ox = p - oy * out_w;
+    float sum[3] = {0.0f, 0.0f, 0.0f};
+    for (int dy = 0; dy < factor; ++dy)
+        for (int dx = 0; dx < factor; ++dx) {
+            const uint8_t *s = in + 3 * ((oy * factor + dy) * in_w + ox * factor + dx);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) sum[k] += (float)s[k];
+        }
+    const float n = (float)(factor * factor);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) out[3 * p + k] = (uint8_t)__fdiv_rn(sum[k], n);
+}
+
+// offline/video.py:46-59 (frame_bloom): the frame lifted to a pseudo-linear
+// domain, (x / 255)^2.2 in float32.
+__global__ void lift_kernel(const uint8_t *in, long long n, float *out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = powf(__fdiv_rn((float)in[i], 255.0f), 2.2f);
+}
+
+// linear + strength * blurred bright pass, clipped to [0, 1], sRGB-encoded.
+__global__ void bloom_encode_kernel(const float *linear, const float *blurred, long long n,
+                                    float strength, uint8_t *out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = srgb8(__fadd_rn(linear[i], __fmul_rn(strength, blurred[i])));
 }
 
 // img = hdr * exposure (+ strength * blurred bright pass), tone-mapped.
@@ -395,4 +437,65 @@ extern "C" int bh_develop(const float *hdr, int64_t width, int64_t height, doubl
     develop_kernel<<<grid_of(pixels, 256), 256, 0, s>>>(hdr, bright, pixels, ex,
                                                         (float)bloom_strength, out);
     return em_launch("bh_develop launch");
+}
+
+extern "C" int bh_downsample(const uint8_t *image, int64_t width, int64_t height,
+                             int32_t factor, uint8_t *out, void *stream) {
+    if (width < 0 || height < 0 || factor < 1 || factor > 256)
+        return em_invalid("width and height must be >= 0 and factor in [1, 256]");
+    const long long ow = width / factor, oh = height / factor;
+    if (ow * oh == 0) return BH_OK;
+    if (!image || !out) return em_invalid("NULL pointer argument");
+    downsample_kernel<<<grid_of(ow * oh, 256), 256, 0, (cudaStream_t)stream>>>(
+        image, width, factor, ow, oh, out);
+    return em_launch("bh_downsample launch");
+}
+
+extern "C" size_t bh_frame_bloom_workspace_bytes(int64_t width, int64_t height) {
+    if (width <= 0 || height <= 0) return 256;
+    const size_t img = (size_t)width * (size_t)height * 3 * sizeof(float);
+    return 3 * ((img + 255) & ~(size_t)255);
+}
+
+extern "C" int bh_frame_bloom(const uint8_t *image, int64_t width, int64_t height,
+                              double strength, const double *blur_weights, int32_t blur_radius,
+                              uint8_t *out, void *workspace, size_t workspace_bytes,
+                              void *stream) {
+    if (width < 0 || height < 0) return em_invalid("width and height must be >= 0");
+    const long long pixels = (long long)width * height;
+    if (pixels == 0) return BH_OK;
+    if (!image || !out) return em_invalid("NULL pointer argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!(strength > 0.0)) {  // video.py:53-54: the frame unchanged
+        const cudaError_t e =
+            cudaMemcpyAsync(out, image, (size_t)pixels * 3, cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) {
+            set_error("bh_frame_bloom copy: %s", cudaGetErrorString(e));
+            return BH_ERR_CUDA;
+        }
+        return BH_OK;
+    }
+    if (!blur_weights || blur_radius < 1 || blur_radius > kMaxBlurRadius)
+        return em_invalid("bloom needs blur weights and a radius in [1, 6000]");
+    if (!workspace || (reinterpret_cast<uintptr_t>(workspace) & 255u) ||
+        workspace_bytes < bh_frame_bloom_workspace_bytes(width, height)) {
+        set_error("workspace must be 256-byte aligned and hold bh_frame_bloom_workspace_bytes()");
+        return BH_ERR_WORKSPACE;
+    }
+    const size_t img = ((size_t)pixels * 3 * sizeof(float) + 255) & ~(size_t)255;
+    float *linear = static_cast<float *>(workspace);
+    float *bright = reinterpret_cast<float *>(static_cast<char *>(workspace) + img);
+    float *tmp = reinterpret_cast<float *>(static_cast<char *>(workspace) + 2 * img);
+    lift_kernel<<<grid_of(3 * pixels, 256), 256, 0, s>>>(image, 3 * pixels, linear);
+    // post.py:40-56 with threshold 0.55, no exposure: the bright pass,
+    // two blur passes (rows, then columns), added back with the strength.
+    bright_kernel<<<grid_of(pixels, 256), 256, 0, s>>>(linear, pixels, 1.0f, 0.55f, bright);
+    const size_t wbytes = (size_t)(2 * blur_radius + 1) * sizeof(double);
+    blur_kernel<<<grid_of(pixels, 256), 256, wbytes, s>>>(bright, width, height, blur_weights,
+                                                          blur_radius, 0, tmp);
+    blur_kernel<<<grid_of(pixels, 256), 256, wbytes, s>>>(tmp, width, height, blur_weights,
+                                                          blur_radius, 1, bright);
+    bloom_encode_kernel<<<grid_of(3 * pixels, 256), 256, 0, s>>>(linear, bright, 3 * pixels,
+                                                                 (float)strength, out);
+    return em_launch("bh_frame_bloom launch");
 }

@@ -604,6 +604,23 @@ int bh_develop(const float *hdr, int64_t width, int64_t height, double exposure,
                int32_t blur_radius, uint8_t *out, void *workspace, size_t workspace_bytes,
                void *stream);
 
+/* offline/video.py:33-43 (downsample): each factor x factor block of an 8-bit
+ * (height, width, 3) image averaged and truncated to 8 bits into out
+ * (height / factor, width / factor, 3); factor in [1, 256]. */
+int bh_downsample(const uint8_t *image, int64_t width, int64_t height, int32_t factor,
+                  uint8_t *out, void *stream);
+
+/* Device workspace of bh_frame_bloom: three float32 images. */
+size_t bh_frame_bloom_workspace_bytes(int64_t width, int64_t height);
+
+/* offline/video.py:46-59 (frame_bloom): the 8-bit frame lifted to
+ * (x / 255)^2.2, the bloom of post.py (bright pass above 0.55, separable
+ * Gaussian by blur_weights[2 radius + 1]) added with `strength`, clipped and
+ * sRGB-encoded into out; strength <= 0 copies the frame.  float32. */
+int bh_frame_bloom(const uint8_t *image, int64_t width, int64_t height, double strength,
+                   const double *blur_weights, int32_t blur_radius, uint8_t *out,
+                   void *workspace, size_t workspace_bytes, void *stream);
+
 /* ------------------------------------------------------------ diagnostics */
 
 /* Launches a vector-FMA throughput kernel of sms*8 blocks x 256 threads, each

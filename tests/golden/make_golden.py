@@ -57,6 +57,8 @@ REF_FILES = [
     "blackhorizon/emission/bluesheet.py",
     "blackhorizon/offline/post.py",
     "blackhorizon/offline/infall.py",
+    "blackhorizon/offline/camera_path.py",
+    "blackhorizon/offline/video.py",
     "tests/test_kerr.py",
     "tests/test_shadow.py",
     "tests/test_bluesheet.py",
@@ -691,6 +693,44 @@ def gen_plunge(ref, out):
     np.savez_compressed(os.path.join(out, "plunge.npz"), **arrs)
 
 
+def gen_video(ref, out):
+    """offline/camera_path.py and offline/video.py:33-59: poses and cameras
+    along a three-keyframe path and an orbit path, and downsample /
+    frame_bloom of a seeded random frame and of a developed offline frame."""
+    _offline_modules(_REFERENCE_PATH)
+    from blackhorizon.offline import camera_path as cp
+    from blackhorizon.offline import video
+
+    keys = [cp.CameraKeyframe(0.0, 30.0, 80.0, 0.0, 60.0),
+            cp.CameraKeyframe(2.0, 15.0, 60.0, 90.0, 70.0),
+            cp.CameraKeyframe(5.0, 20.0, 85.0, 400.0, 50.0)]
+    times = np.array([-1.0, 0.0, 0.7, 2.0, 3.3, 4.99, 5.0, 6.0])
+    arrs = {"keys": np.array([[k.time, k.distance, k.inclination_degrees, k.azimuth_degrees,
+                               k.fov_degrees] for k in keys]), "times": times}
+    for tag, path in (("path", cp.CameraPath(keys)), ("orbit", cp.orbit_path(4.0, 25.0, 70.0, 1.5))):
+        poses, positions, bases = [], [], []
+        for t in times:
+            p = path.pose_at(float(t))
+            poses.append([p.time, p.distance, p.inclination_degrees, p.azimuth_degrees,
+                          p.fov_degrees])
+            cam = path.camera_at(float(t))
+            positions.append(cam.position)
+            bases.append(np.stack(cam.basis()))
+        arrs[f"{tag}_poses"] = np.array(poses)
+        arrs[f"{tag}_positions"] = np.array(positions)
+        arrs[f"{tag}_bases"] = np.array(bases)
+    rng = np.random.default_rng(11)
+    frames = {"random": rng.integers(0, 256, size=(67, 97, 3), dtype=np.uint8),
+              "developed": np.load(os.path.join(out, "emission.npz"))["ext_developed"]}
+    for tag, img in frames.items():
+        arrs[f"{tag}_frame"] = img
+        for f in (2, 3):
+            arrs[f"{tag}_down{f}"] = video.downsample(img, f)
+        for st in (0.25, 0.6):
+            arrs[f"{tag}_bloom{st}"] = video.frame_bloom(img, st)
+    np.savez_compressed(os.path.join(out, "video.npz"), **arrs)
+
+
 def gen_images(ref, out):
     """imaging.py:27-91 on the reference's own traces.
 
@@ -957,6 +997,7 @@ def main():
         ("emission", lambda: gen_emission(ref, args.out)),
         ("inflation_frame", lambda: gen_inflation_frame(ref, args.out)),
         ("plunge", lambda: gen_plunge(ref, args.out)),
+        ("video", lambda: gen_video(ref, args.out)),
         ("images", lambda: gen_images(ref, args.out)),
         ("realtime", lambda: gen_realtime(ref, args.out)),
         ("vaidya", lambda: gen_vaidya(ref, args.out)),

@@ -181,3 +181,29 @@ def test_plunge_worldline_matches_reference():
 
     with pytest.raises(ValueError):
         radial_momentum(KerrSpacetime(1.0, 0.5), [4.0, 0.0, 0.0], 0.0)  # E = 0 outside
+
+
+def test_camera_paths_match_reference():
+    """offline/camera_path.py: eased keyframe poses, clamping at the ends,
+    orbit sweeps and the cameras they give, against the reference's."""
+    import numpy as np
+    import pytest
+
+    from blackhorizon_b200.video import CameraKeyframe, CameraPath, orbit_path
+    from conftest import golden
+
+    g = golden("video.npz")
+    keys = [CameraKeyframe(*row) for row in g["keys"]]
+    for tag, path in (("path", CameraPath(keys)), ("orbit", orbit_path(4.0, 25.0, 70.0, 1.5))):
+        for i, t in enumerate(g["times"]):
+            p = path.pose_at(float(t))
+            np.testing.assert_array_equal([p.time, p.distance, p.inclination_degrees,
+                                           p.azimuth_degrees, p.fov_degrees], g[f"{tag}_poses"][i])
+            cam = path.camera_at(float(t))
+            np.testing.assert_allclose(cam.position, g[f"{tag}_positions"][i], rtol=1e-14,
+                                       atol=1e-14)
+            np.testing.assert_allclose(np.stack(cam.basis()), g[f"{tag}_bases"][i], atol=1e-14)
+    with pytest.raises(ValueError):
+        CameraPath([])
+    with pytest.raises(ValueError):
+        CameraPath([keys[1], keys[0]])
