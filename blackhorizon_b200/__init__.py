@@ -13,8 +13,8 @@ from .camera import PinholeCamera
 from .geodesics import (GeodesicRhs, build_state, conserved_quantities,
                         coordinate_velocity, geodesic_rhs, hamiltonian,
                         null_momentum_from_velocity, timelike_momentum)
-from .integrators import (dormand_prince_step, error_ratio, integrate_dense,
-                          propagate, rk4_step, step_factor)
+from .integrators import (dormand_prince_step, error_ratio, implicit_midpoint_step,
+                          integrate_dense, propagate, rk4_step, step_factor)
 from .kerr import KerrSchildGeometry, KerrSpacetime
 from .tracer import CameraBatch, CameraScene, RayStatus, TraceResult, trace_cameras, trace_rays
 
@@ -23,7 +23,8 @@ __all__ = [
     "PinholeCamera", "GeodesicRhs", "build_state", "conserved_quantities",
     "coordinate_velocity", "geodesic_rhs", "hamiltonian",
     "null_momentum_from_velocity", "timelike_momentum", "dormand_prince_step",
-    "error_ratio", "integrate_dense", "propagate", "rk4_step", "step_factor",
+    "error_ratio", "implicit_midpoint_step", "integrate_dense", "propagate", "rk4_step",
+    "step_factor",
     "KerrSchildGeometry", "KerrSpacetime", "CameraBatch", "CameraScene", "RayStatus",
     "TraceResult", "trace_cameras", "trace_rays",
 ]

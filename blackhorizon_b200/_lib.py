@@ -113,6 +113,7 @@ _SIGNATURES = {
     "bh_error_ratio": (ctypes.c_int, [_P, _P, _P, _D, _D, _P, _I64, _P]),
     "bh_step_factor": (ctypes.c_int, [_P, _P, _I64, _P]),
     "bh_rk4": (ctypes.c_int, [_D, _D, _P, _P, _P, _I64, _I64, _I32, _P]),
+    "bh_implicit_midpoint": (ctypes.c_int, [_D, _D, _P, _P, _P, _I64, _I32, _I64, _P]),
     "bh_trace_variant_count": (ctypes.c_int, [_I32]),
     "bh_trace_variant": (ctypes.c_int, [_I32, _I32, ctypes.POINTER(_I32),
                                          ctypes.POINTER(_I32), ctypes.POINTER(_I32),

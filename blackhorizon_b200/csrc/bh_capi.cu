@@ -235,6 +235,50 @@ __global__ void rk4_kernel(double m, double a, const double *state,
     write_state(out, i, y);
 }
 
+// geodesics.py:42-74 for one state, float64: d(t, x, y, z, p_t, p_x, p_y, p_z).
+__device__ __forceinline__ void full_rhs(const KerrV<double> &K, const RayState &y, double d[8]) {
+    WStateV<double> yw;
+    put_work<double>(yw, 0, y);
+    const StageV<double> s = first_stage<double>(K, yw);
+    d[0] = -y.pt + s.thl;
+    d[1] = y.px + s.kx;
+    d[2] = y.py + s.ky;
+    d[3] = y.pz + s.kz;
+    d[4] = 0.0;
+    d[5] = s.px;
+    d[6] = s.py;
+    d[7] = s.pz;
+}
+
+__device__ __forceinline__ RayState add_scaled(const RayState &y, double c, const double d[8]) {
+    return RayState{y.t + c * d[0], y.x + c * d[1], y.y + c * d[2], y.z + c * d[3],
+                    y.pt + c * d[4], y.px + c * d[5], y.py + c * d[6], y.pz + c * d[7]};
+}
+
+// integrators.py:177-207 (implicit_midpoint_step), n_steps times: the
+// midpoint y + h/2 f(y) refined `iterations` times by y + h/2 f(midpoint),
+// then y + h f(midpoint).
+__global__ void midpoint_kernel(double m, double a, const double *state, const double *hs,
+                                double *out, long long n, int iterations, long long n_steps) {
+    const long long i = tid();
+    if (i >= n) return;
+    RayState y = read_state(state, i);
+    const double h = hs[i];
+    const KerrV<double> K = make_kerr<double>(m, a);
+    double d[8];
+    for (long long s = 0; s < n_steps; ++s) {
+        full_rhs(K, y, d);
+        RayState mid = add_scaled(y, 0.5 * h, d);
+        for (int k = 0; k < iterations; ++k) {
+            full_rhs(K, mid, d);
+            mid = add_scaled(y, 0.5 * h, d);
+        }
+        full_rhs(K, mid, d);
+        y = add_scaled(y, h, d);
+    }
+    write_state(out, i, y);
+}
+
 static CameraDev camera_dev(const bh_camera &c, long long first_ray) {
     CameraDev d;
     for (int i = 0; i < 3; ++i) {
@@ -494,6 +538,19 @@ int bh_rk4(double mass, double spin, const double *state, const double *h,
     else
         return invalid("unknown precision");
     return cuda_status(cudaGetLastError(), "bh_rk4 launch");
+}
+
+int bh_implicit_midpoint(double mass, double spin, const double *state, const double *h,
+                         double *new_state, int64_t n, int32_t iterations, int64_t n_steps,
+                         void *stream) {
+    if (!kerr_ok(mass, spin)) return invalid("Kerr bound violated or mass not positive");
+    if (n < 0 || n_steps < 0 || iterations < 0)
+        return invalid("n, n_steps and iterations must be >= 0");
+    if (n == 0) return BH_OK;
+    if (!state || !h || !new_state) return invalid("NULL pointer argument");
+    midpoint_kernel<<<grid_for(n), kBlock, 0, (cudaStream_t)stream>>>(
+        mass, spin, state, h, new_state, n, iterations, n_steps);
+    return cuda_status(cudaGetLastError(), "bh_implicit_midpoint launch");
 }
 
 int bh_trace_variant_count(int32_t precision) { return trace_variant_count(precision); }

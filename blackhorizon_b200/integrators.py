@@ -59,6 +59,24 @@ def rk4_step(rhs, state: Array, h: Array, precision: str = "fp64",
     return out_like(out, host, state)
 
 
+def implicit_midpoint_step(rhs, state: Array, h: Array, iterations: int = 4,
+                           n_steps: int = 1) -> Array:
+    """One implicit midpoint step (integrators.py:177-207), symplectic for
+    the Hamiltonian flow: y1 = y0 + h f((y0 + y1) / 2), solved by
+    ``iterations`` fixed-point refinements seeded with an explicit Euler
+    half step; float64.  ``n_steps`` > 1 repeats it in registers."""
+    st = spacetime_of_rhs(rhs)
+    s, host = to_device_f64(state, "state")
+    if s.dim() != 2 or s.shape[1] != 8:
+        raise ValueError("state must have shape (n, 8)")
+    hh = _h_vector(h, s.shape[0], s.device)
+    out = torch.empty_like(s)
+    _lib.check(_lib.load().bh_implicit_midpoint(st.mass, st.spin, ptr(s), ptr(hh), ptr(out),
+                                                s.shape[0], int(iterations), int(n_steps),
+                                                stream_handle()), "implicit_midpoint_step")
+    return out_like(out, host, state)
+
+
 def dormand_prince_step(rhs, state: Array, h: Array, precision: str = "fp64"):
     """Embedded Dormand-Prince 5(4) step (integrators.py:76-107): returns
     (new_state, error)."""

@@ -183,6 +183,14 @@ int bh_rk4(double mass, double spin, const double *state, const double *h,
            double *new_state, int64_t n, int64_t n_steps, int32_t precision,
            void *stream);
 
+/* implicit_midpoint_step (integrators.py:177-207), n_steps times: the
+ * symplectic midpoint rule y1 = y0 + h f((y0 + y1) / 2) solved by
+ * `iterations` fixed-point refinements of the explicit Euler half step;
+ * float64.  (n, 8) in, (n, 8) out, h (n,). */
+int bh_implicit_midpoint(double mass, double spin, const double *state, const double *h,
+                         double *new_state, int64_t n, int32_t iterations, int64_t n_steps,
+                         void *stream);
+
 /* ------------------------------------------------------------- tracer */
 
 /* Launch-shape variants of the trace and propagate kernels for a precision:

@@ -731,6 +731,28 @@ def gen_video(ref, out):
     np.savez_compressed(os.path.join(out, "video.npz"), **arrs)
 
 
+def gen_midpoint(ref, out):
+    """implicit_midpoint_step (integrators.py:177-207) from the states and
+    steps of steps.npz, with 4 and 6 fixed-point iterations, and 200 steps
+    of the bound timelike orbit of tests/test_offline.py:38-44 (h = 0.2)."""
+    G, I = ref["geodesics"], ref["integrators"]
+    g = np.load(os.path.join(out, "steps.npz"))
+    st = ref["KerrSpacetime"](1.0, float(g["spin"]))
+    rhs = lambda b: G.geodesic_rhs(st, b)  # noqa: E731
+    arrs = {"spin": g["spin"], "state": g["state"], "h": g["h"]}
+    for it in (4, 6):
+        arrs[f"step_it{it}"] = I.implicit_midpoint_step(rhs, g["state"], g["h"], iterations=it)
+    orbit_st = ref["KerrSpacetime"](1.0, 0.9)
+    pos = np.array([[14.0, 0.0, 0.0]])
+    y = G.build_state(pos, G.timelike_momentum(orbit_st, pos, np.array([[0.0, 0.21, 0.02]])))
+    arrs["orbit_state0"] = y.copy()
+    orhs = lambda b: G.geodesic_rhs(orbit_st, b)  # noqa: E731
+    for _ in range(200):
+        y = I.implicit_midpoint_step(orhs, y, np.array([0.2]))
+    arrs["orbit_200"] = y
+    np.savez_compressed(os.path.join(out, "midpoint.npz"), **arrs)
+
+
 def gen_images(ref, out):
     """imaging.py:27-91 on the reference's own traces.
 
@@ -998,6 +1020,7 @@ def main():
         ("inflation_frame", lambda: gen_inflation_frame(ref, args.out)),
         ("plunge", lambda: gen_plunge(ref, args.out)),
         ("video", lambda: gen_video(ref, args.out)),
+        ("midpoint", lambda: gen_midpoint(ref, args.out)),
         ("images", lambda: gen_images(ref, args.out)),
         ("realtime", lambda: gen_realtime(ref, args.out)),
         ("vaidya", lambda: gen_vaidya(ref, args.out)),

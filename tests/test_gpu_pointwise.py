@@ -172,3 +172,58 @@ def test_nan_error_is_infinite_ratio(cuda):
     bad[0, 1] = float("nan")
     r = integrators.error_ratio(s, s, bad, 1e-9, 1e-12)
     assert torch.isinf(r[0])
+
+
+def test_implicit_midpoint_matches_reference(cuda):
+    """implicit_midpoint_step (integrators.py:177-207): one step from the
+    golden states with 4 and 6 iterations, and 200 steps of the bound orbit
+    of tests/test_offline.py, against the reference's outputs."""
+    import numpy as np
+
+    from blackhorizon_b200 import GeodesicRhs, implicit_midpoint_step
+    from blackhorizon_b200.kerr import KerrSpacetime
+    from conftest import golden
+
+    g = golden("midpoint.npz")
+    rhs = GeodesicRhs(KerrSpacetime(1.0, float(g["spin"])))
+    for it in (4, 6):
+        got = implicit_midpoint_step(rhs, g["state"], g["h"], iterations=it)
+        ref = g[f"step_it{it}"]
+        np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-13)
+    orbit = GeodesicRhs(KerrSpacetime(1.0, 0.9))
+    got = implicit_midpoint_step(orbit, g["orbit_state0"], np.array([0.2]), n_steps=200)
+    np.testing.assert_allclose(got, g["orbit_200"], rtol=1e-10, atol=1e-11)
+
+
+def test_implicit_midpoint_properties(cuda):
+    """tests/test_offline.py:46-103 through the b200 steppers: second-order
+    convergence on one orbit, and a bounded Hamiltonian error where RK4's
+    grows secularly over 30000 steps of h = 0.6."""
+    import numpy as np
+
+    from blackhorizon_b200 import (GeodesicRhs, build_state, hamiltonian,
+                                   implicit_midpoint_step, rk4_step, timelike_momentum)
+    from blackhorizon_b200.kerr import KerrSpacetime
+
+    st = KerrSpacetime(1.0, 0.9)
+    pos = np.array([[14.0, 0.0, 0.0]])
+    s0 = build_state(pos, timelike_momentum(st, pos, np.array([[0.0, 0.21, 0.02]])))
+    rhs = GeodesicRhs(st)
+
+    def endpoint(h, steps):
+        return implicit_midpoint_step(rhs, s0, np.array([h]), iterations=6, n_steps=steps)
+
+    ref = endpoint(0.025, 4000)
+    e_coarse = np.abs(endpoint(0.2, 500)[0, 1:4] - ref[0, 1:4]).max()
+    e_fine = np.abs(endpoint(0.1, 1000)[0, 1:4] - ref[0, 1:4]).max()
+    assert 1.6 < np.log2(e_coarse / e_fine) < 2.6
+    samples = {}
+    for name, stepper in (("rk4", rk4_step), ("midpoint", implicit_midpoint_step)):
+        y, errors = s0.copy(), []
+        for _ in range(12):
+            y = stepper(rhs, y, np.array([0.6]), n_steps=2500)
+            errors.append(abs(float(hamiltonian(st, y)[0]) + 0.5))
+        samples[name] = np.asarray(errors)
+    assert bool(np.all(np.diff(samples["rk4"]) > 0.0)) and samples["rk4"][-1] > 5 * samples["rk4"][0]
+    mid = samples["midpoint"]
+    assert float(mid[-1]) < 0.05 * float(mid.max()) and float(mid.max()) < 1e-2
