@@ -73,7 +73,7 @@ def parse():
     ap.add_argument("--no-workloads", action="store_true",
                     help="skip the full-HD frame, the 64-camera batch and the adjoint")
     ap.add_argument("--profile-case",
-                    choices=("trace", "adjoint", "tile", "realtime", "emission"),
+                    choices=("trace", "adjoint", "tile", "realtime", "emission", "viewer"),
                     default=None,
                     help="run one small untimed case of that kernel (for ncu captures): "
                          "trace = the 1920x1080 frame (2 warm-up launches, then 1); "
@@ -82,7 +82,8 @@ def parse():
                          "640x400 supersample 2 (1,024,000 rays), first pass only, twice; "
                          "realtime = the 1280x720 real-time frame, three launches; "
                          "emission = the offline frame traced once, then its radiance "
-                         "and development twice")
+                         "and development twice; viewer = the real-time viewer's whole "
+                         "1280x720 frame (rays, trace, shading), three times")
     return ap.parse_args()
 
 
@@ -1028,6 +1029,18 @@ def profile_case(args):
         for _ in range(2):
             trace_tile(st, s0, esc, settings, radii, settings.rtol, settings.max_steps,
                        precision=prec, variant=args.variant)
+    elif args.profile_case == "viewer":
+        from blackhorizon_b200.offline import FlyCamera
+        from blackhorizon_b200.realtime import (BackgroundMode, QualityPreset, RenderSettings,
+                                                render_frame_device)
+        from blackhorizon_b200.workloads import REALTIME_FRAME as F
+
+        settings = RenderSettings(spin=F.spin, fov_degrees=F.fov,
+                                  background=BackgroundMode.STARFIELD).apply_preset(
+                                      QualityPreset(F.preset))
+        fly = FlyCamera.from_orbit(F.distance, F.inclination, 0.0)
+        for _ in range(3):
+            render_frame_device(settings, fly, F.width, F.height, precision=prec)
     elif args.profile_case == "emission":
         from blackhorizon_b200.emission import (frame_tables, radiance_image,
                                                 static_observer_lapse)
