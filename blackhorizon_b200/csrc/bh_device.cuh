@@ -251,19 +251,19 @@ template <> struct VT<F2> {
 // Per-ray Kerr constants in the lane type, formed once per ray.
 template <class V>
 struct KerrV {
-    V m, a, na, a2, a2x4, a2x3, n2ma2;
+    V m2, a, na, a2, na2, a2x4, a2x3h;
 };
 template <class V>
 __device__ __forceinline__ KerrV<V> make_kerr(V m, V a) {
     using T = VT<V>;
     KerrV<V> k;
-    k.m = m;
+    k.m2 = m * T::set(2.0);
     k.a = a;
     k.na = -a;
     k.a2 = a * a;
+    k.na2 = -k.a2;
     k.a2x4 = k.a2 * T::set(4.0);
-    k.a2x3 = k.a2 * T::set(3.0);
-    k.n2ma2 = (m * k.a2) * T::set(-2.0);
+    k.a2x3h = k.a2 * T::set(1.5);
     return k;
 }
 
@@ -286,6 +286,9 @@ struct StageV {
 // and with grad H = dH/dr grad r + (0, 0, dH/dz|_r) the momentum derivative is
 //   pdot_i = r_i (dH/dr lp^2 + thl G) + [thl * the explicit terms above]
 // which is the reference's grad_h * lp^2 + thl * (grad_l . p) regrouped.
+// The mass enters through one factor 2m/qd: thl = (2m/qd) r^3 lp, and with
+// mlp = 2m lp^2/qd^2, dH/dr lp^2 = r^2 (3a^2z^2 - r^4)/2 mlp and
+// dH/dz|_r lp^2 = -a^2 z r^3 mlp.
 // The radius uses the reference's r^2 = (q + s)/2 (kerr.py:141) for every
 // lane type.
 template <class V>
@@ -293,10 +296,17 @@ __device__ __forceinline__ StageV<V> rhs_v(const KerrV<V> &K, V x, V y, V z,
                                            V npt, V px, V py, V pz, V dpx,
                                            V dpy, V dpz) {
     using T = VT<V>;
+    // Float lanes add the clamp constants of s^2 and qd instead of taking a
+    // maximum: both sums are non-negative, and the constant changes neither
+    // unless it is within 2^24 of the sum, i.e. at the ring itself; that
+    // saves the unpacked max instructions on the critical path.  Double
+    // lanes keep the reference's clamps.
+    constexpr bool kAddTiny = sizeof(typename T::S) == 4;
     const V z2 = z * z;
-    const V a2z2 = K.a2 * z2;
+    const V a2z2 = kAddTiny ? T::fma(K.a2, z2, T::set(T::tiny())) : K.a2 * z2;
     const V q = T::fma(x, x, T::fma(y, y, z2 - K.a2));
-    const V s2 = T::max(T::fma(q, q, K.a2x4 * z2), T::set(T::tiny2()));
+    const V s2 = kAddTiny ? T::fma(q, q, T::fma(K.a2x4, z2, T::set(T::tiny2())))
+                          : T::max(T::fma(q, q, K.a2x4 * z2), T::set(T::tiny2()));
     const V inv_s = T::rsqrt(s2);
     const V s = s2 * inv_s;
     const V r2 = T::max((q + s) * T::set(0.5), T::set(T::tiny()));
@@ -304,18 +314,18 @@ __device__ __forceinline__ StageV<V> rhs_v(const KerrV<V> &K, V x, V y, V z,
     const V r = r2 * inv_r;
     const V w = r2 + K.a2;
     const V r2sq = r2 * r2;
-    const V qd = T::max(r2sq + a2z2, T::set(T::tiny()));
+    const V qd = kAddTiny ? r2sq + a2z2 : T::max(r2sq + a2z2, T::set(T::tiny()));
     const V inv_qd = T::rcp(qd);
     const V inv_w = T::rcp(w);
     const V r3 = r * r2;
-    const V h = (K.m * r3) * inv_qd;
+    const V m2i = K.m2 * inv_qd;  // 2m / qd
     const V lx = T::fma(r, x, K.a * y) * inv_w;
     const V ly = T::fma(r, y, K.na * x) * inv_w;
     const V lz = z * inv_r;
     const V lxy = T::fma(lx, px, ly * py);
     const V lzpz = lz * pz;
     const V lp = (lxy + lzpz) + npt;
-    const V thl = (h + h) * lp;
+    const V thl = (m2i * r3) * lp;  // 2 H lp
     const V nthl = -thl;
     StageV<V> o;
     o.thl = thl;
@@ -325,19 +335,16 @@ __device__ __forceinline__ StageV<V> rhs_v(const KerrV<V> &K, V x, V y, V z,
     const V rs = r * inv_s;
     const V r_x = x * rs, r_y = y * rs;
     const V r_z = z * (w * (inv_r * inv_s));
-    const V inv_qd2 = inv_qd * inv_qd;
-    const V lp2 = lp * lp;
-    const V t3 = K.a2x3 * z2 - r2sq;
-    const V dh_dr = ((K.m * r2) * t3) * inv_qd2;
-    const V dh_dz = ((K.n2ma2 * z) * r3) * inv_qd2;
+    const V mlp = (m2i * inv_qd) * (lp * lp);  // 2m lp^2 / qd^2
+    const V t3h = T::fma(K.a2x3h, z2, r2sq * T::set(-0.5));
+    // thl G = thl (x p_x + y p_y - 2 r lxy) / w - thl lzpz / r.
     const V u = T::fma(x, px, y * py);
     const V g1 = T::fma(r * T::set(-2.0), lxy, u);
-    const V g = g1 * inv_w - lzpz * inv_r;
-    const V k = T::fma(dh_dr, lp2, thl * g);
     const V tw = thl * inv_w;
+    const V k = T::fma(nthl * inv_r, lzpz, T::fma(tw, g1, (r2 * t3h) * mlp));
     o.px = T::fma(r_x, k, tw * T::fma(r, px, K.na * py));
     o.py = T::fma(r_y, k, tw * T::fma(r, py, K.a * px));
-    o.pz = T::fma(r_z, k, T::fma(dh_dz, lp2, (thl * pz) * inv_r));
+    o.pz = T::fma(r_z, k, T::fma((K.na2 * z) * r3, mlp, thl * (pz * inv_r)));
     return o;
 }
 
@@ -607,13 +614,15 @@ __device__ __forceinline__ void error_ratio_v(const WStateV<V> &y, const Attempt
         if constexpr (sizeof(V) == 8 && T::N == 1) {
             e = (hw * err[i]) / sc;
         } else {
-            e = (hw * err[i]) * T::rcp(sc);
+            // float lanes: the factor h goes on the sum (h^2 / 8 below).
+            e = err[i] * T::rcp(sc);
         }
         q[i] = e * e;
     }
     if constexpr (sizeof(typename T::S) == 4) {
-        // Components t x y z | p_t(=0) px py pz: r^2 = sum / 8.
-        const V sum = ((q[0] + q[1]) + (q[2] + q[3])) + (q[4] + (q[5] + q[6]));
+        // Components t x y z | p_t(=0) px py pz: r^2 = h^2 sum / 8.
+        const V sum = (((q[0] + q[1]) + (q[2] + q[3])) + (q[4] + (q[5] + q[6]))) *
+                      (hw * hw);
 #pragma unroll
         for (int l = 0; l < T::N; ++l) {
             const double ms = double(T::get(sum, l)) * 0.125;
