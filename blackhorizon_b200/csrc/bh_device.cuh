@@ -251,7 +251,7 @@ template <> struct VT<F2> {
 // Per-ray Kerr constants in the lane type, formed once per ray.
 template <class V>
 struct KerrV {
-    V m2, a, na, a2, na2, a2x4, a2x3h;
+    V m2, a, na, a2, na2, a2x4;
 };
 template <class V>
 __device__ __forceinline__ KerrV<V> make_kerr(V m, V a) {
@@ -263,7 +263,6 @@ __device__ __forceinline__ KerrV<V> make_kerr(V m, V a) {
     k.a2 = a * a;
     k.na2 = -k.a2;
     k.a2x4 = k.a2 * T::set(4.0);
-    k.a2x3h = k.a2 * T::set(1.5);
     return k;
 }
 
@@ -313,8 +312,7 @@ __device__ __forceinline__ StageV<V> rhs_v(const KerrV<V> &K, V x, V y, V z,
     const V inv_r = T::rsqrt(r2);
     const V r = r2 * inv_r;
     const V w = r2 + K.a2;
-    const V r2sq = r2 * r2;
-    const V qd = kAddTiny ? r2sq + a2z2 : T::max(r2sq + a2z2, T::set(T::tiny()));
+    const V qd = kAddTiny ? T::fma(r2, r2, a2z2) : T::max(T::fma(r2, r2, a2z2), T::set(T::tiny()));
     const V inv_qd = T::rcp(qd);
     const V inv_w = T::rcp(w);
     const V r3 = r * r2;
@@ -323,28 +321,30 @@ __device__ __forceinline__ StageV<V> rhs_v(const KerrV<V> &K, V x, V y, V z,
     const V ly = T::fma(r, y, K.na * x) * inv_w;
     const V lz = z * inv_r;
     const V lxy = T::fma(lx, px, ly * py);
-    const V lzpz = lz * pz;
-    const V lp = (lxy + lzpz) + npt;
+    const V lp = T::fma(lz, pz, lxy) + npt;
     const V thl = (m2i * r3) * lp;  // 2 H lp
     const V nthl = -thl;
+    const V tz = nthl * lz;
     StageV<V> o;
     o.thl = thl;
     o.kx = T::fma(nthl, lx, dpx);
     o.ky = T::fma(nthl, ly, dpy);
-    o.kz = T::fma(nthl, lz, dpz);
+    o.kz = tz + dpz;
     const V rs = r * inv_s;
     const V r_x = x * rs, r_y = y * rs;
-    const V r_z = z * (w * (inv_r * inv_s));
+    const V r_z = (lz * w) * inv_s;
     const V mlp = (m2i * inv_qd) * (lp * lp);  // 2m lp^2 / qd^2
-    const V t3h = T::fma(K.a2x3h, z2, r2sq * T::set(-0.5));
-    // thl G = thl (x p_x + y p_y - 2 r lxy) / w - thl lzpz / r.
+    // (3 a^2 z^2 - r^4) / 2 = 2 a^2 z^2 - qd / 2.
+    const V t3h = T::fma(qd, T::set(-0.5), a2z2 + a2z2);
+    // thl G = thl (x p_x + y p_y - 2 r (l_x p_x + l_y p_y)) / w - thl l_z p_z / r.
     const V u = T::fma(x, px, y * py);
     const V g1 = T::fma(r * T::set(-2.0), lxy, u);
     const V tw = thl * inv_w;
-    const V k = T::fma(nthl * inv_r, lzpz, T::fma(tw, g1, (r2 * t3h) * mlp));
+    const V pzr = pz * inv_r;
+    const V k = T::fma(tz, pzr, T::fma(tw, g1, (r2 * t3h) * mlp));
     o.px = T::fma(r_x, k, tw * T::fma(r, px, K.na * py));
     o.py = T::fma(r_y, k, tw * T::fma(r, py, K.a * px));
-    o.pz = T::fma(r_z, k, T::fma((K.na2 * z) * r3, mlp, thl * (pz * inv_r)));
+    o.pz = T::fma(r_z, k, T::fma((K.na2 * z) * r3, mlp, thl * pzr));
     return o;
 }
 
