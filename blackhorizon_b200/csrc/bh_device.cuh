@@ -251,7 +251,7 @@ template <> struct VT<F2> {
 // Per-ray Kerr constants in the lane type, formed once per ray.
 template <class V>
 struct KerrV {
-    V m2, a, na, a2, na2, a2x4;
+    V m2, a, na, a2, na2;
 };
 template <class V>
 __device__ __forceinline__ KerrV<V> make_kerr(V m, V a) {
@@ -262,7 +262,6 @@ __device__ __forceinline__ KerrV<V> make_kerr(V m, V a) {
     k.na = -a;
     k.a2 = a * a;
     k.na2 = -k.a2;
-    k.a2x4 = k.a2 * T::set(4.0);
     return k;
 }
 
@@ -295,20 +294,20 @@ __device__ __forceinline__ StageV<V> rhs_v(const KerrV<V> &K, V x, V y, V z,
                                            V npt, V px, V py, V pz, V dpx,
                                            V dpy, V dpz) {
     using T = VT<V>;
-    // Float lanes add the clamp constants of s^2 and qd instead of taking a
-    // maximum: both sums are non-negative, and the constant changes neither
-    // unless it is within 2^24 of the sum, i.e. at the ring itself; that
-    // saves the unpacked max instructions on the critical path.  Double
-    // lanes keep the reference's clamps.
+    // Float lanes add the clamp constant to a^2 z^2, which enters s^2 and qd,
+    // instead of taking a maximum: both sums are non-negative, and the
+    // constant changes neither unless it is within 2^24 of the sum, i.e. at
+    // the ring itself; that saves the unpacked max instructions on the
+    // critical path.  Double lanes keep the reference's clamps.
     constexpr bool kAddTiny = sizeof(typename T::S) == 4;
     const V z2 = z * z;
     const V a2z2 = kAddTiny ? T::fma(K.a2, z2, T::set(T::tiny())) : K.a2 * z2;
     const V q = T::fma(x, x, T::fma(y, y, z2 - K.a2));
-    const V s2 = kAddTiny ? T::fma(q, q, T::fma(K.a2x4, z2, T::set(T::tiny2())))
-                          : T::max(T::fma(q, q, K.a2x4 * z2), T::set(T::tiny2()));
+    const V s2 = kAddTiny ? T::fma(a2z2, T::set(4.0), q * q)
+                          : T::max(T::fma(q, q, a2z2 * T::set(4.0)), T::set(T::tiny2()));
     const V inv_s = T::rsqrt(s2);
     const V s = s2 * inv_s;
-    const V r2 = T::max((q + s) * T::set(0.5), T::set(T::tiny()));
+    const V r2 = T::max(T::fma(s, T::set(0.5), q * T::set(0.5)), T::set(T::tiny()));
     const V inv_r = T::rsqrt(r2);
     const V r = r2 * inv_r;
     const V w = r2 + K.a2;
@@ -610,19 +609,20 @@ __device__ __forceinline__ void error_ratio_v(const WStateV<V> &y, const Attempt
         V sc = T::fma(rt, T::max(T::abs(yv[i]), T::abs(nv[i])), at);
         if constexpr (sizeof(typename T::S) == 4)
             sc = T::max(sc, (i < 4 ? hn : T::set(kMixedNoise)) * T::abs(inc[i]));
-        V e;
         if constexpr (sizeof(V) == 8 && T::N == 1) {
-            e = (hw * err[i]) / sc;
+            const V e = (hw * err[i]) / sc;
+            q[i] = e * e;
         } else {
-            // float lanes: the factor h goes on the sum (h^2 / 8 below).
-            e = err[i] * T::rcp(sc);
+            // float lanes: q holds err / scale; the factor h goes on the sum.
+            q[i] = err[i] * T::rcp(sc);
         }
-        q[i] = e * e;
     }
     if constexpr (sizeof(typename T::S) == 4) {
-        // Components t x y z | p_t(=0) px py pz: r^2 = h^2 sum / 8.
-        const V sum = (((q[0] + q[1]) + (q[2] + q[3])) + (q[4] + (q[5] + q[6]))) *
-                      (hw * hw);
+        // Components t x y z | p_t(=0) px py pz: r^2 = h^2 sum q^2 / 8, the
+        // squares summed by two chains of fused multiply-adds.
+        const V s0 = T::fma(q[3], q[3], T::fma(q[2], q[2], T::fma(q[1], q[1], q[0] * q[0])));
+        const V s1 = T::fma(q[6], q[6], T::fma(q[5], q[5], q[4] * q[4]));
+        const V sum = (s0 + s1) * (hw * hw);
 #pragma unroll
         for (int l = 0; l < T::N; ++l) {
             const double ms = double(T::get(sum, l)) * 0.125;

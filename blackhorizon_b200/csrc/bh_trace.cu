@@ -257,8 +257,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args
 }
 
 // n_steps attempted DP5(4) steps per ray with the tracer's accept/reject and
-// step update (tracer.py:111-120) and no termination; grid-stride over groups
-// of N rays.
+// step update (tracer.py:111-120) and no termination.  Each warp claims 32
+// groups of N rays at a time from the workspace's queue head, so warps that
+// the scheduler runs ahead take more groups and all of them stay resident
+// until the queue drains (a fixed grid-stride split left a quarter of the
+// warp slots idle while the slowest warps finished).
 template <class V, int BLOCK, int MINB, bool PROJECT>
 __global__ void __launch_bounds__(BLOCK, MINB) propagate_kernel(const TraceArgs args) {
     using T = VT<V>;
@@ -276,93 +279,99 @@ __global__ void __launch_bounds__(BLOCK, MINB) propagate_kernel(const TraceArgs 
     long long my_max = 0;
     bool late = false;
     const long long groups = (n + N - 1) / N;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    const long long first = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     extern __shared__ double bh_state_smem[];
     StateStore<V, BLOCK> ys(bh_state_smem);
-    for (long long g = first; g < groups && !late; g += stride) {
-        double h[N], lam[N], spin[N], mass[N];
-        long long acc[N];
-        bool valid[N];
-#pragma unroll
-        for (int l = 0; l < N; ++l) {
-            const long long i = g * N + l;
-            valid[l] = i < n;
-            // A missing last ray repeats the group's first ray; its results
-            // are not stored.
-            const long long src = valid[l] ? i : g * N;
-            RayState y0;
-            load_state(args.state0, n, args.layout, src, y0);
-            ys.set(l, y0);
-            spin[l] = args.spin_of_ray ? args.spin_of_ray[src] : args.spin;
-            mass[l] = args.mass;
-            h[l] = args.h_io[src];
-            lam[l] = args.lam_io ? args.lam_io[src] : 0.0;
-            acc[l] = 0;
-        }
-        const KerrV<V> K = make_kerr<V>(lanes_of<V>(mass), lanes_of<V>(spin));
-        WStateV<V> yw;
-#pragma unroll
-        for (int l = 0; l < N; ++l) put_work<V>(yw, l, ys.get(l));
-        StageV<V> k1 = first_stage<V>(K, yw);
-        long long k = 0;
-        for (; k < args.max_attempts; ++k) {
-            V hw = T::set(0.0);
-#pragma unroll
-            for (int l = 0; l < N; ++l) T::put(hw, l, typename T::S(h[l]));
-            AttemptV<V> a;
-            dp5_attempt<V>(K, yw, hw, k1, a);
-            double ratio[N];
-            error_ratio_v<V>(yw, a, hw, rt, at, ratio);
-            bool ok[N];
+    for (;;) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(&ws->queue_head, 32ull);
+        base = __shfl_sync(full, base, 0);
+        if ((long long)base >= groups) break;
+        const long long g = (long long)base + lane;
+        if (g < groups) {
+            double h[N], lam[N], spin[N], mass[N];
+            long long acc[N];
+            bool valid[N];
 #pragma unroll
             for (int l = 0; l < N; ++l) {
-                ok[l] = ratio[l] <= 1.0;
-                if (ok[l]) {
-                    RayState yl = ys.get(l);
-                    commit<V>(yl, yw, a, l, h[l]);
-                    ys.set(l, yl);
-                    lam[l] += h[l];
-                    ++acc[l];
-                }
-                h[l] = np_min(np_max(h[l] * step_factor<F64>(ratio[l]), 0.0), args.max_step);
+                const long long i = g * N + l;
+                valid[l] = i < n;
+                // A missing last ray repeats the group's first ray; its results
+                // are not stored.
+                const long long src = valid[l] ? i : g * N;
+                RayState y0;
+                load_state(args.state0, n, args.layout, src, y0);
+                ys.set(l, y0);
+                spin[l] = args.spin_of_ray ? args.spin_of_ray[src] : args.spin;
+                mass[l] = args.mass;
+                h[l] = args.h_io[src];
+                lam[l] = args.lam_io ? args.lam_io[src] : 0.0;
+                acc[l] = 0;
             }
-            take_stage(k1, a.k7, ok);
-            if constexpr (PROJECT) {
-                if ((k + 1) % args.project_every == 0) {
-                    bool proj[N];
+            const KerrV<V> K = make_kerr<V>(lanes_of<V>(mass), lanes_of<V>(spin));
+            WStateV<V> yw;
 #pragma unroll
-                    for (int l = 0; l < N; ++l) {
-                        proj[l] = true;
+            for (int l = 0; l < N; ++l) put_work<V>(yw, l, ys.get(l));
+            StageV<V> k1 = first_stage<V>(K, yw);
+            long long k = 0;
+            for (; k < args.max_attempts; ++k) {
+                V hw = T::set(0.0);
+#pragma unroll
+                for (int l = 0; l < N; ++l) T::put(hw, l, typename T::S(h[l]));
+                AttemptV<V> a;
+                dp5_attempt<V>(K, yw, hw, k1, a);
+                double ratio[N];
+                error_ratio_v<V>(yw, a, hw, rt, at, ratio);
+                bool ok[N];
+#pragma unroll
+                for (int l = 0; l < N; ++l) {
+                    ok[l] = ratio[l] <= 1.0;
+                    if (ok[l]) {
                         RayState yl = ys.get(l);
-                        project_null(mass[l], spin[l], yl);
+                        commit<V>(yl, yw, a, l, h[l]);
                         ys.set(l, yl);
-                        put_work<V>(yw, l, yl);
+                        lam[l] += h[l];
+                        ++acc[l];
                     }
-                    const StageV<V> f = first_stage<V>(K, yw);
-                    take_stage(k1, f, proj);
+                    h[l] = np_min(np_max(h[l] * step_factor<F64>(ratio[l]), 0.0), args.max_step);
+                }
+                take_stage(k1, a.k7, ok);
+                if constexpr (PROJECT) {
+                    if ((k + 1) % args.project_every == 0) {
+                        bool proj[N];
+#pragma unroll
+                        for (int l = 0; l < N; ++l) {
+                            proj[l] = true;
+                            RayState yl = ys.get(l);
+                            project_null(mass[l], spin[l], yl);
+                            ys.set(l, yl);
+                            put_work<V>(yw, l, yl);
+                        }
+                        const StageV<V> f = first_stage<V>(K, yw);
+                        take_stage(k1, f, proj);
+                    }
+                }
+                if (has_deadline && (k & 63) == 63 && global_timer_ns() > deadline) {
+                    late = true;
+                    ++k;
+                    break;
                 }
             }
-            if (has_deadline && (k & 63) == 63 && global_timer_ns() > deadline) {
-                late = true;
-                ++k;
-                break;
-            }
-        }
 #pragma unroll
-        for (int l = 0; l < N; ++l) {
-            if (!valid[l]) continue;
-            const long long i = g * N + l;
-            RayState yl = ys.get(l);
-            if constexpr (PROJECT) project_null(mass[l], spin[l], yl);
-            store_state(args.states, n, args.layout, i, yl);
-            args.h_io[i] = h[l];
-            if (args.lam_io) args.lam_io[i] = lam[l];
-            args.steps[i] = acc[l];
-            my_attempts += (unsigned long long)k;
-            my_accepted += (unsigned long long)acc[l];
+            for (int l = 0; l < N; ++l) {
+                if (!valid[l]) continue;
+                const long long i = g * N + l;
+                RayState yl = ys.get(l);
+                if constexpr (PROJECT) project_null(mass[l], spin[l], yl);
+                store_state(args.states, n, args.layout, i, yl);
+                args.h_io[i] = h[l];
+                if (args.lam_io) args.lam_io[i] = lam[l];
+                args.steps[i] = acc[l];
+                my_attempts += (unsigned long long)k;
+                my_accepted += (unsigned long long)acc[l];
+            }
+            if (k > my_max) my_max = k;
         }
-        if (k > my_max) my_max = k;
+        if (__any_sync(full, late)) break;
     }
     if (late) atomicExch(&ws->timed_out, 1);
     for (int off = 16; off > 0; off >>= 1) {
