@@ -329,9 +329,6 @@ __device__ __forceinline__ StageV<V> rhs_v(const KerrV<V> &K, V x, V y, V z,
     o.kx = T::fma(nthl, lx, dpx);
     o.ky = T::fma(nthl, ly, dpy);
     o.kz = tz + dpz;
-    const V rs = r * inv_s;
-    const V r_x = x * rs, r_y = y * rs;
-    const V r_z = (lz * w) * inv_s;
     const V mlp = (m2i * inv_qd) * (lp * lp);  // 2m lp^2 / qd^2
     // (3 a^2 z^2 - r^4) / 2 = 2 a^2 z^2 - qd / 2.
     const V t3h = T::fma(qd, T::set(-0.5), a2z2 + a2z2);
@@ -341,9 +338,12 @@ __device__ __forceinline__ StageV<V> rhs_v(const KerrV<V> &K, V x, V y, V z,
     const V tw = thl * inv_w;
     const V pzr = pz * inv_r;
     const V k = T::fma(tz, pzr, T::fma(tw, g1, (r2 * t3h) * mlp));
-    o.px = T::fma(r_x, k, tw * T::fma(r, px, K.na * py));
-    o.py = T::fma(r_y, k, tw * T::fma(r, py, K.a * px));
-    o.pz = T::fma(r_z, k, T::fma((K.na2 * z) * r3, mlp, thl * pzr));
+    // grad r = (x r, y r, z w / r) / s, applied to k / s.
+    const V sk = k * inv_s;
+    const V rsk = r * sk;
+    o.px = T::fma(x, rsk, tw * T::fma(r, px, K.na * py));
+    o.py = T::fma(y, rsk, tw * T::fma(r, py, K.a * px));
+    o.pz = T::fma(lz * w, sk, T::fma((K.na2 * z) * r3, mlp, thl * pzr));
     return o;
 }
 
@@ -619,10 +619,11 @@ __device__ __forceinline__ void error_ratio_v(const WStateV<V> &y, const Attempt
     }
     if constexpr (sizeof(typename T::S) == 4) {
         // Components t x y z | p_t(=0) px py pz: r^2 = h^2 sum q^2 / 8, the
-        // squares summed by two chains of fused multiply-adds.
-        const V s0 = T::fma(q[3], q[3], T::fma(q[2], q[2], T::fma(q[1], q[1], q[0] * q[0])));
-        const V s1 = T::fma(q[6], q[6], T::fma(q[5], q[5], q[4] * q[4]));
-        const V sum = (s0 + s1) * (hw * hw);
+        // squares summed pairwise by fused multiply-adds.
+        const V s01 = T::fma(q[1], q[1], q[0] * q[0]);
+        const V s23 = T::fma(q[3], q[3], q[2] * q[2]);
+        const V s456 = T::fma(q[6], q[6], T::fma(q[5], q[5], q[4] * q[4]));
+        const V sum = ((s01 + s23) + s456) * (hw * hw);
 #pragma unroll
         for (int l = 0; l < T::N; ++l) {
             const double ms = double(T::get(sum, l)) * 0.125;
