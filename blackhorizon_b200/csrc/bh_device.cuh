@@ -289,10 +289,12 @@ struct StageV {
 // dH/dz|_r lp^2 = -a^2 z r^3 mlp.
 // The radius uses the reference's r^2 = (q + s)/2 (kerr.py:141) for every
 // lane type.
+//
+// r2_out, when given, receives the radius r^2 the evaluation used.
 template <class V>
 __device__ __forceinline__ StageV<V> rhs_v(const KerrV<V> &K, V x, V y, V z,
                                            V npt, V px, V py, V pz, V dpx,
-                                           V dpy, V dpz) {
+                                           V dpy, V dpz, V *r2_out = nullptr) {
     using T = VT<V>;
     // Float lanes add the clamp constant to a^2 z^2, which enters s^2 and qd,
     // instead of taking a maximum: both sums are non-negative, and the
@@ -308,6 +310,7 @@ __device__ __forceinline__ StageV<V> rhs_v(const KerrV<V> &K, V x, V y, V z,
     const V inv_s = T::rsqrt(s2);
     const V s = s2 * inv_s;
     const V r2 = T::max(T::fma(s, T::set(0.5), q * T::set(0.5)), T::set(T::tiny()));
+    if (r2_out) *r2_out = r2;
     const V inv_r = T::rsqrt(r2);
     const V r = r2 * inv_r;
     const V w = r2 + K.a2;
@@ -418,6 +421,7 @@ struct AttemptV {
     V dpx, dpy, dpz;         // momentum increments h sum_i b_i pdot_i
     V err[7];        // sum_i e_i k_i for t x y z px py pz (the p_t error is 0)
     StageV<V> k7;    // derivative at y_new relative to y_new's momentum
+    V r2n;           // Kerr-Schild r^2 at ynw, from the k7 evaluation
 };
 
 // Rounding floor of the mixed policy's error scale.  The embedded error
@@ -525,7 +529,7 @@ __device__ __forceinline__ void dp5_attempt(const KerrV<V> &K, const WStateV<V> 
     // k7 = f(y_new), FSAL for the next step.  Relative to this step's base
     // momentum its position part carries dP_7 = p_new - p.
     const StageV<V> s7 = rhs_v<V>(K, nw.x, nw.y, nw.z, nw.npt, nw.px, nw.py, nw.pz,
-                                  out.dpx, out.dpy, out.dpz);
+                                  out.dpx, out.dpy, out.dpz, &out.r2n);
     out.k7 = s7;
     out.k7.kx = s7.kx - out.dpx;
     out.k7.ky = s7.ky - out.dpy;

@@ -42,12 +42,17 @@
 namespace bh {
 
 // Termination test before an attempt (render.py:231-260, exterior camera):
-// -1 while the ray stays in flight.
+// -1 while the ray stays in flight.  r2_est: r^2 of y from the stage
+// arithmetic, or NaN; see settled_radius (the interior camera's lowest radius
+// threshold is 1.002 capture radii).
 __device__ __forceinline__ int tile_check(const TileArgs &a, const RayState &y,
-                                          long long steps, long long attempts) {
+                                          long long steps, long long attempts,
+                                          double r2_est) {
     // render.py:223: the loop ends after 4 max_steps iterations.
     if (attempts >= a.max_attempts) return BH_RAY_IN_FLIGHT;
-    const double r = ks_radius(a.spin, y);
+    const double r = settled_radius(
+        r2_est, a.interior ? a.capture_radius * 1.002 : a.capture_radius, a.escape_radius,
+        a.spin, y);
     if (a.interior) {
         // render.py:234-248: diverging spatial momentum ends the ray on the
         // terminal surface.
@@ -299,7 +304,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) tile_kernel(const TileArgs args) 
                             h[l] = r.h;
                         }
                         const int st = flush ? BH_RAY_IN_FLIGHT
-                                             : tile_check(args, y0, steps[l], attempts[l]);
+                                             : tile_check(args, y0, steps[l], attempts[l],
+                                                          __longlong_as_double(0x7ff8000000000000LL));
                         if (st >= 0) {
                             finish(l, y0, st, nullptr);
                         } else {
@@ -380,7 +386,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) tile_kernel(const TileArgs args) 
                 h[l] = h_next;
                 int st = -1;
                 if (attempts[l] >= args.max_attempts) st = BH_RAY_IN_FLIGHT;
-                else if (acc[l]) st = tile_check(args, ys.get(l), steps[l], attempts[l]);
+                else if (acc[l])
+                    st = tile_check(args, ys.get(l), steps[l], attempts[l],
+                                    double(T::get(a.r2n, l)));
                 if (st >= 0) finish(l, ys.get(l), st, nullptr);
             }
             take_stage(k1, a.k7, acc);

@@ -44,6 +44,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args
     extern __shared__ double bh_state_smem[];
     StateStore<V, BLOCK> ys(bh_state_smem);
     long long ray[N], steps[N], attempts[N];
+    // r: Kerr-Schild radius of the slot's state, NaN while it lies clear of
+    // both termination radii (settled_radius).
     double h[N], mass[N], spin[N], rcap[N], resc[N], r[N], lam[N];
     WStateV<V> yw;
 #pragma unroll
@@ -175,7 +177,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args
                     ys.set(l, yl);
                     lam[l] += h[l];
                     ++steps[l];
-                    r[l] = ks_radius(spin[l], yl);
+                    r[l] = settled_radius(double(T::get(a.r2n, l)), rcap[l], resc[l], spin[l], yl);
                 }
                 h[l] = np_min(np_max(h[l] * step_factor<F64>(ratio[l]), 0.0), args.max_step);
 

@@ -74,6 +74,25 @@ __device__ __forceinline__ double ks_radius(double a, const RayState &y) {
     return ::sqrt(ks_radius2(a, y.x, y.y, y.z));
 }
 
+// The radius the termination cascade compares with the capture and escape
+// radii, after an accepted step.  r2_est is r^2 at the new state from the
+// stage arithmetic (the FSAL evaluation, at the float32 rounding of the new
+// state for float lanes).  Its error is below 1e-6 (r^2 + 2 a^2) absolute:
+// rounding of the position and of q = |x|^2 - a^2 and s (which cancel in
+// (q + s)/2 inside |x| < |a|), all bounded by a few units in the last place
+// of |x|^2 + a^2 <= r^2 + 2 a^2.  Where the estimate lies inside both
+// thresholds by 1e-3 r^2 + 1e-4 a^2 or more, the float64 tests would both
+// fail, and NaN, which fails them too, stands in for the radius.  Only near
+// a threshold, or for a non-finite estimate, is the float64 radius computed.
+__device__ __forceinline__ double settled_radius(double r2_est, double rcap, double resc,
+                                                 double a, const RayState &y) {
+    const double slack = 1e-4 * (a * a);
+    if (r2_est - slack > rcap * rcap * (1.0 + 1e-3) &&
+        r2_est + slack < resc * resc * (1.0 - 1e-3))
+        return __longlong_as_double(0x7ff8000000000000LL);
+    return ks_radius(a, y);
+}
+
 // Lane-wise select of a lane-type value: dst[l] = src[l] where take[l].
 template <class V>
 __device__ __forceinline__ void take_lanes(V &dst, const V &src, const bool *take) {
