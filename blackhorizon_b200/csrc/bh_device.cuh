@@ -607,12 +607,24 @@ __device__ __forceinline__ void error_ratio_v(const WStateV<V> &y, const Attempt
     // first four carry the factor h in hn), dP for the momenta.
     const V inc[7] = {a.it, a.ix, a.iy, a.iz, a.dpx, a.dpy, a.dpz};
     const V hn = hw * T::set(kMixedNoise);
+    // The floor of a position or momentum component follows the largest
+    // increment of its 3-vector: a small component (p_y near zero on a
+    // near-meridional orbit) is the difference of terms as large as the
+    // others, and carries their rounding noise.
+    V fl[7];
+    if constexpr (sizeof(typename T::S) == 4) {
+        const V fx = hn * T::max(T::abs(inc[1]), T::max(T::abs(inc[2]), T::abs(inc[3])));
+        const V fp = T::set(kMixedNoise) *
+                     T::max(T::abs(inc[4]), T::max(T::abs(inc[5]), T::abs(inc[6])));
+        fl[0] = hn * T::abs(inc[0]);
+        fl[1] = fl[2] = fl[3] = fx;
+        fl[4] = fl[5] = fl[6] = fp;
+    }
     V q[7];
 #pragma unroll
     for (int i = 0; i < 7; ++i) {
         V sc = T::fma(rt, T::max(T::abs(yv[i]), T::abs(nv[i])), at);
-        if constexpr (sizeof(typename T::S) == 4)
-            sc = T::max(sc, (i < 4 ? hn : T::set(kMixedNoise)) * T::abs(inc[i]));
+        if constexpr (sizeof(typename T::S) == 4) sc = T::max(sc, fl[i]);
         if constexpr (sizeof(V) == 8 && T::N == 1) {
             const V e = (hw * err[i]) / sc;
             q[i] = e * e;
