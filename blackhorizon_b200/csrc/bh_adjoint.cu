@@ -29,8 +29,9 @@ __device__ __forceinline__ void write8(double *p, const RayState &y) {
 }
 
 // Accepted DP5(4) steps of a frozen sequence h[0..n_steps) from y, in the
-// tracer's own arithmetic (dp5_attempt + commit with lane type V); writes
-// the state before each step into `before` when non-null.
+// tracer's own arithmetic (dp5_attempt + commit with lane type V).  With
+// `before` non-null it writes the state before each step there and stops
+// before the last step, whose result the caller does not use.
 template <class V>
 __device__ __forceinline__ RayState replay_steps(double m, double a, RayState y,
                                                  const double *h, long long n_steps,
@@ -41,7 +42,10 @@ __device__ __forceinline__ RayState replay_steps(double m, double a, RayState y,
     put_work<V>(yw, 0, y);
     StageV<V> k1 = first_stage<V>(K, yw);
     for (long long k = 0; k < n_steps; ++k) {
-        if (before) before[k] = y;
+        if (before) {
+            before[k] = y;
+            if (k == n_steps - 1) break;
+        }
         const double hk = h[k];
         AttemptV<V> at;
         dp5_attempt<V>(K, yw, T::set(hk), k1, at);

@@ -8,7 +8,9 @@
 // differentiation of the RHS evaluated as the straight-line program below
 // (geodesics.py:42-74 with kerr.py:118-193 folded in, the regrouped gradient
 // contraction of rhs_v).  The clamps of kerr.py (_TINY) are inactive away
-// from the ring singularity and are treated as the identity.
+// from the ring singularity and are treated as the identity.  Reciprocals
+// and square roots go through Math<W> (one MUFU instruction for float, the
+// MUFU seed and two Newton steps for double), as in the forward stages.
 //
 // Work type W: double, or float for the mixed-precision adjoint; cotangents
 // of the state are accumulated in double across steps either way.
@@ -37,12 +39,15 @@ __device__ __forceinline__ Vec8<W> rhs_full(W m, W a, const Vec8<W> &Y) {
     const W z2 = z * z;
     const W a2z2 = a2 * z2;
     const W q = x * x + y * y + z2 - a2;
-    const W s = ::sqrt(q * q + W(4) * a2z2);
+    const W s2 = q * q + W(4) * a2z2;
+    const W is = Math<W>::rsqrt(s2);
+    const W s = s2 * is;
     const W r2 = (q + s) * W(0.5);
-    const W r = ::sqrt(r2);
+    const W ir = Math<W>::rsqrt(r2);
+    const W r = r2 * ir;
     const W w = r2 + a2;
     const W qd = r2 * r2 + a2z2;
-    const W iq = W(1) / qd, iw = W(1) / w, ir = W(1) / r, is = W(1) / s;
+    const W iq = Math<W>::rcp(qd), iw = Math<W>::rcp(w);
     const W r3 = r * r2;
     const W h = m * r3 * iq;
     const W lx = (r * x + a * y) * iw;
@@ -87,12 +92,15 @@ __device__ __forceinline__ void rhs_vjp(W m, W a, const Vec8<W> &Y, const Vec8<W
     const W z2 = z * z;
     const W a2z2 = a2 * z2;
     const W q = x * x + y * y + z2 - a2;
-    const W s = ::sqrt(q * q + W(4) * a2z2);
+    const W s2 = q * q + W(4) * a2z2;
+    const W is = Math<W>::rsqrt(s2);
+    const W s = s2 * is;
     const W r2 = (q + s) * W(0.5);
-    const W r = ::sqrt(r2);
+    const W ir = Math<W>::rsqrt(r2);
+    const W r = r2 * ir;
     const W w = r2 + a2;
     const W qd = r2 * r2 + a2z2;
-    const W iq = W(1) / qd, iw = W(1) / w, ir = W(1) / r, is = W(1) / s;
+    const W iq = Math<W>::rcp(qd), iw = Math<W>::rcp(w);
     const W r3 = r * r2;
     const W h = m * r3 * iq;
     const W Lx = r * x + a * y, Ly = r * y - a * x;
