@@ -10,8 +10,9 @@
 // camera pose and pixel coordinates) and the spin at once.  States are not
 // stored per step: the tape holds one float64 checkpoint every K accepted
 // steps; each segment is replayed forward from its checkpoint into a
-// per-thread buffer of K states and then swept backward, the stages of each
-// step recomputed inside the vector-Jacobian product.  One ray per thread.
+// per-thread buffer of K states (rounded to the sweep's work type: 32 bytes
+// each for the float sweep) and then swept backward, the stages of each step
+// recomputed inside the vector-Jacobian product.  One ray per thread.
 #include "bh_adjoint.cuh"
 #include "bh_internal.h"
 
@@ -30,12 +31,13 @@ __device__ __forceinline__ void write8(double *p, const RayState &y) {
 
 // Accepted DP5(4) steps of a frozen sequence h[0..n_steps) from y, in the
 // tracer's own arithmetic (dp5_attempt + commit with lane type V).  With
-// `before` non-null it writes the state before each step there and stops
+// `before` non-null it writes the state before each step there, rounded to
+// the sweep's work type W (all the vector-Jacobian product reads), and stops
 // before the last step, whose result the caller does not use.
-template <class V>
+template <class V, typename W>
 __device__ __forceinline__ RayState replay_steps(double m, double a, RayState y,
                                                  const double *h, long long n_steps,
-                                                 RayState *before) {
+                                                 Vec8<W> *before) {
     using T = VT<V>;
     const KerrV<V> K = make_kerr<V>(T::set(m), T::set(a));
     WStateV<V> yw;
@@ -43,7 +45,7 @@ __device__ __forceinline__ RayState replay_steps(double m, double a, RayState y,
     StageV<V> k1 = first_stage<V>(K, yw);
     for (long long k = 0; k < n_steps; ++k) {
         if (before) {
-            before[k] = y;
+            before[k] = to_work<W>(y);
             if (k == n_steps - 1) break;
         }
         const double hk = h[k];
@@ -78,18 +80,18 @@ __global__ void __launch_bounds__(kAdjointBlock, 3) adjoint_kernel(
     if (!zero && N > 0) {
         const long long nck = (cap + every - 1) / every;
         const double *h = h_tape + i * cap;
-        RayState seg_states[kMaxCheckpointEvery];
+        Vec8<W> seg_states[kMaxCheckpointEvery];
         for (long long seg = (N - 1) / every; seg >= 0; --seg) {
             const long long k0 = seg * every;
             const long long len = (N - k0 < every) ? (N - k0) : every;
             const RayState y0 = read8(ckpt + (i * nck + seg) * 8);
-            replay_steps<V>(m, a, y0, h + k0, len, seg_states);
+            replay_steps<V, W>(m, a, y0, h + k0, len, seg_states);
             // The next step's state and size are loaded before this step's
             // vector-Jacobian product, which hides their latency.
-            RayState cur = seg_states[len - 1];
+            Vec8<W> cur = seg_states[len - 1];
             double hc = h[k0 + len - 1];
             for (long long k = len - 1; k >= 0; --k) {
-                RayState nxt = cur;
+                Vec8<W> nxt = cur;
                 double hn = hc;
                 if (k > 0) {
                     nxt = seg_states[k - 1];
@@ -115,8 +117,8 @@ __global__ void __launch_bounds__(128) replay_kernel(
     if (i >= n) return;
     long long N = steps[i];
     if (N > cap) N = cap;
-    const RayState y = replay_steps<V>(m, a, read8(state0 + 8 * i), h_tape + i * cap, N,
-                                       nullptr);
+    const RayState y = replay_steps<V, double>(m, a, read8(state0 + 8 * i), h_tape + i * cap,
+                                               N, nullptr);
     write8(states + 8 * i, y);
 }
 

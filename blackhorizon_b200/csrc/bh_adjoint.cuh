@@ -278,11 +278,17 @@ __device__ __forceinline__ Vec8<W> axpy(W s, const Vec8<W> &x, const Vec8<W> &y)
 // (integrators.py:92-103 without the error estimate), and ga += (d y_new /
 // d a)^T lam.  The stages are recomputed from y in W.
 template <typename W>
-__device__ __forceinline__ void dp5_step_vjp(W m, W a, const RayState &y0, double h,
+__device__ __forceinline__ Vec8<W> to_work(const RayState &y) {
+    return Vec8<W>{W(y.t), W(y.x), W(y.y), W(y.z), W(y.pt), W(y.px), W(y.py), W(y.pz)};
+}
+
+// y0: the state before the step, rounded to W.
+template <typename W>
+__device__ __forceinline__ void dp5_step_vjp(W m, W a, const Vec8<W> &y0, double h,
                                              Vec8<double> &lam, double &ga) {
     const W hw = W(h);
     Vec8<W> Y[6], K[6];
-    Y[0] = Vec8<W>{W(y0.t), W(y0.x), W(y0.y), W(y0.z), W(y0.pt), W(y0.px), W(y0.py), W(y0.pz)};
+    Y[0] = y0;
     K[0] = rhs_full<W>(m, a, Y[0]);
     // The stage loops are kept rolled: one copy of the RHS and of its
     // reverse sweep keeps the kernel inside the instruction cache (the
