@@ -216,7 +216,7 @@ __global__ void error_ratio_kernel(const double *s, const double *sn,
 __global__ void step_factor_kernel(const double *ratio, double *out, long long n) {
     const long long i = tid();
     if (i >= n) return;
-    out[i] = step_factor<true>(ratio[i]);
+    out[i] = step_factor(ratio[i]);
 }
 
 // rk4_step (integrators.py:57-73) n_steps times with the state in registers;

@@ -593,7 +593,7 @@ __device__ __forceinline__ StageV<V> first_stage(const KerrV<V> &K, const WState
 // kMixedNoise |increment|.  The value written per lane is what the
 // controller compares with 1: the ratio r for the float64 policy, its square
 // r^2 (the mean of squares, summed in float32) for the mixed one, whose
-// accept test r^2 <= 1 and step factor (step_factor<false>) need no square
+// accept test r^2 <= 1 and step factor (next_step<false>) need no square
 // root.  Non-finite values become +inf.
 template <class V>
 __device__ __forceinline__ void error_ratio_v(const WStateV<V> &y, const AttemptV<V> &a,
@@ -748,19 +748,27 @@ __device__ __forceinline__ void project_null(double m, double a, RayState &y) {
 }
 
 // step_factor (integrators.py:120-124): clip(0.9 max(r,1e-16)^-0.2, 0.2, 5).
-// The float64 policy passes r; the mixed policy passes r^2 (error_ratio_v)
-// and takes (r^2)^-0.1 through float32 exp2/log2 (only the step heuristic
-// uses it).
-template <bool F64>
 __device__ __forceinline__ double step_factor(double ratio) {
-    double f;
-    if constexpr (F64) {
-        f = 0.9 * ::pow(np_max(ratio, 1e-16), -0.2);
-    } else {
-        const float sf = float(fmin(np_max(ratio, 1e-32), 3.0e38));
-        f = double(0.9f * ex2_approx(-0.1f * lg2_approx(sf)));
-    }
+    const double f = 0.9 * ::pow(np_max(ratio, 1e-16), -0.2);
     return np_min(np_max(f, 0.2), 5.0);
+}
+
+// The controller's next step size (tracer.py:113-120): clip(h factor, 0,
+// max_step) after accept and reject alike.  The float64 policy passes r and
+// keeps the reference's forms.  The mixed policy passes r^2 (error_ratio_v)
+// and takes the factor 0.9 (r^2)^-0.1 through float32 exp2/log2 (only the
+// step heuristic uses it); its r^2 is >= 0 or +inf, never NaN, so the factor
+// is finite and plain maxima and minima give the values NumPy's
+// NaN-propagating ones would, with fewer instructions.
+template <bool F64>
+__device__ __forceinline__ double next_step(double h, double ratio, double max_step) {
+    if constexpr (F64) {
+        return np_min(np_max(h * step_factor(ratio), 0.0), max_step);
+    } else {
+        const float sf = fminf(fmaxf(float(ratio), 1e-32f), 3.0e38f);
+        const double f = double(0.9f * ex2_approx(-0.1f * lg2_approx(sf)));
+        return fmin(fmax(h * fmin(fmax(f, 0.2), 5.0), 0.0), max_step);
+    }
 }
 
 __device__ __forceinline__ bool all_finite(const RayState &y) {

@@ -348,7 +348,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) tile_kernel(const TileArgs args) 
                 acc[l] = ratio[l] <= 1.0;
                 ++attempts[l];
                 const double h_next =
-                    np_min(np_max(h[l] * step_factor<F64>(ratio[l]), 0.0), args.max_step);
+                    next_step<F64>(h[l], ratio[l], args.max_step);
                 if (acc[l]) {
                     const RayState y0 = ys.get(l);
                     RayState y1 = y0;

@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args
                     ++steps[l];
                     r[l] = settled_radius(double(T::get(a.r2n, l)), rcap[l], resc[l], spin[l], yl);
                 }
-                h[l] = np_min(np_max(h[l] * step_factor<F64>(ratio[l]), 0.0), args.max_step);
+                h[l] = next_step<F64>(h[l], ratio[l], args.max_step);
 
                 const bool finite = all_finite(yl);
                 int st = BH_RAY_IN_FLIGHT;
@@ -334,7 +334,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) propagate_kernel(const TraceArgs 
                         lam[l] += h[l];
                         ++acc[l];
                     }
-                    h[l] = np_min(np_max(h[l] * step_factor<F64>(ratio[l]), 0.0), args.max_step);
+                    h[l] = next_step<F64>(h[l], ratio[l], args.max_step);
                 }
                 take_stage(k1, a.k7, ok);
                 if constexpr (PROJECT) {
