@@ -591,13 +591,13 @@ __device__ __forceinline__ StageV<V> first_stage(const KerrV<V> &K, const WState
 // reciprocal is one MUFU instruction (a float64 norm of float32 data would
 // add cost, not accuracy); each scale is at least the rounding floor
 // kMixedNoise |increment|.  The value written per lane is what the
-// controller compares with 1: the ratio r for the float64 policy, its square
-// r^2 (the mean of squares, summed in float32) for the mixed one, whose
-// accept test r^2 <= 1 and step factor (next_step<false>) need no square
-// root.  Non-finite values become +inf.
+// controller compares with 1: the ratio r (double) for the float64 policy,
+// its square r^2 (float: the mean of squares, summed in float32) for the
+// mixed one, whose accept test r^2 <= 1 and step factor (next_step<false>)
+// need no square root and no conversion.  Non-finite values become +inf.
 template <class V>
 __device__ __forceinline__ void error_ratio_v(const WStateV<V> &y, const AttemptV<V> &a,
-                                              V hw, V rt, V at, double ratio[VT<V>::N]) {
+                                              V hw, V rt, V at, typename VT<V>::S ratio[VT<V>::N]) {
     using T = VT<V>;
     const WStateV<V> &yn = a.ynw;
     const V *err = a.err;
@@ -642,8 +642,8 @@ __device__ __forceinline__ void error_ratio_v(const WStateV<V> &y, const Attempt
         const V sum = ((s01 + s23) + s456) * (hw * hw);
 #pragma unroll
         for (int l = 0; l < T::N; ++l) {
-            const double ms = double(T::get(sum, l)) * 0.125;
-            ratio[l] = isfinite(ms) ? ms : __longlong_as_double(0x7ff0000000000000LL);
+            const float ms = T::get(sum, l) * 0.125f;
+            ratio[l] = isfinite(ms) ? ms : __int_as_float(0x7f800000);
         }
     } else {
 #pragma unroll
@@ -760,12 +760,12 @@ __device__ __forceinline__ double step_factor(double ratio) {
 // step heuristic uses it); its r^2 is >= 0 or +inf, never NaN, so the factor
 // is finite and plain maxima and minima give the values NumPy's
 // NaN-propagating ones would, with fewer instructions.
-template <bool F64>
-__device__ __forceinline__ double next_step(double h, double ratio, double max_step) {
+template <bool F64, typename R>
+__device__ __forceinline__ double next_step(double h, R ratio, double max_step) {
     if constexpr (F64) {
         return np_min(np_max(h * step_factor(ratio), 0.0), max_step);
     } else {
-        const float sf = fminf(fmaxf(float(ratio), 1e-32f), 3.0e38f);
+        const float sf = fminf(fmaxf(ratio, 1e-32f), 3.0e38f);
         const double f = double(0.9f * ex2_approx(-0.1f * lg2_approx(sf)));
         return fmin(fmax(h * fmin(fmax(f, 0.2), 5.0), 0.0), max_step);
     }

@@ -338,14 +338,14 @@ __global__ void __launch_bounds__(BLOCK, MINB) tile_kernel(const TileArgs args) 
             for (int l = 0; l < N; ++l) T::put(hw, l, typename T::S(h[l]));
             AttemptV<V> a;
             dp5_attempt<V>(K, yw, hw, k1, a);
-            double ratio[N];
+            typename T::S ratio[N];
             error_ratio_v<V>(yw, a, hw, rt, at, ratio);
             bool acc[N];
 #pragma unroll
             for (int l = 0; l < N; ++l) {
                 acc[l] = false;
                 if (ray[l] < 0) continue;
-                acc[l] = ratio[l] <= 1.0;
+                acc[l] = ratio[l] <= typename T::S(1);
                 ++attempts[l];
                 const double h_next =
                     next_step<F64>(h[l], ratio[l], args.max_step);

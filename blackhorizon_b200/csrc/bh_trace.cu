@@ -147,14 +147,14 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args
             for (int l = 0; l < N; ++l) T::put(hw, l, typename T::S(h[l]));
             AttemptV<V> a;
             dp5_attempt<V>(K, yw, hw, k1, a);
-            double ratio[N];
+            typename T::S ratio[N];
             error_ratio_v<V>(yw, a, hw, rt, at, ratio);
             bool acc[N];
 #pragma unroll
             for (int l = 0; l < N; ++l) {
                 acc[l] = false;
                 if (ray[l] < 0) continue;
-                acc[l] = ratio[l] <= 1.0;
+                acc[l] = ratio[l] <= typename T::S(1);
                 ++attempts[l];
                 RayState yl = ys.get(l);
                 if (acc[l] && args.h_tape) {
@@ -321,12 +321,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) propagate_kernel(const TraceArgs 
                 for (int l = 0; l < N; ++l) T::put(hw, l, typename T::S(h[l]));
                 AttemptV<V> a;
                 dp5_attempt<V>(K, yw, hw, k1, a);
-                double ratio[N];
+                typename T::S ratio[N];
                 error_ratio_v<V>(yw, a, hw, rt, at, ratio);
                 bool ok[N];
 #pragma unroll
                 for (int l = 0; l < N; ++l) {
-                    ok[l] = ratio[l] <= 1.0;
+                    ok[l] = ratio[l] <= typename T::S(1);
                     if (ok[l]) {
                         RayState yl = ys.get(l);
                         commit<V>(yl, yw, a, l, h[l]);
