@@ -65,6 +65,15 @@ __global__ void __launch_bounds__(BLOCK, MINB) realtime_kernel(const RealtimeArg
     const long long n = args.n;
     const KerrV<V> K = make_kerr<V>(T::set(args.mass), T::set(args.spin));
     const bool disk = args.disk_outer > 0.0;
+    // Float lanes: squared termination thresholds moved inward by 1e-3 for
+    // the float32 fast path below.  An interior camera's lowest radius
+    // threshold is 1.002 stop radii; above it its |p|^2 > 2500 test cannot
+    // end the ray, so only the bail-out bound remains for |p|^2.
+    constexpr bool kFloatLanes = sizeof(typename T::S) == 4 && N == 1;
+    const double rt_lo = args.interior ? args.capture_radius * 1.002 : args.capture_radius;
+    const float rt_lo2 = float(rt_lo * rt_lo * (1.0 + 1e-3));
+    const float rt_hi2 = float(args.escape_radius * args.escape_radius * (1.0 - 1e-3));
+    const float rt_bail2 = float(args.bail2 * (1.0 - 1e-3));
     extern __shared__ double bh_state_smem[];
     StateStore<V, BLOCK> ys(bh_state_smem);
     WStateV<V> yw;
@@ -150,6 +159,38 @@ __global__ void __launch_bounds__(BLOCK, MINB) realtime_kernel(const RealtimeArg
             h[l] = 0.0;
             step[l] = false;
             if (ray[l] < 0) continue;
+            if constexpr (kFloatLanes) {
+                // The radius and |p|^2 of the float32 copy of the state lie
+                // within 1e-6 (r^2 + 2 a^2) and 1e-6 |p|^2 of the float64
+                // values (the bounds of settled_radius); clear of every
+                // threshold by 1e-3 r^2 + 1e-4 a^2 (1e-3 |p|^2), the float64
+                // tests would all fail, and the step size follows from the
+                // float32 values (the policy's stages are float32 anyway).
+                const float a2f = T::get(K.a2, l);
+                const float xf = T::get(yw.x, l), yf = T::get(yw.y, l), zf = T::get(yw.z, l);
+                const float pxf = T::get(yw.px, l), pyf = T::get(yw.py, l),
+                            pzf = T::get(yw.pz, l);
+                const float q = fmaf(xf, xf, fmaf(yf, yf, fmaf(zf, zf, -a2f)));
+                const float s2 = fmaf(q, q, 4.0f * a2f * zf * zf);
+                const float r2 = 0.5f * (q + s2 * rsqrt_approx(s2));
+                const float mom2 = fmaf(pxf, pxf, fmaf(pyf, pyf, pzf * pzf));
+                const float slack = 1e-4f * a2f;
+                if (it[l] < args.max_steps && r2 - slack > rt_lo2 && r2 + slack < rt_hi2 &&
+                    mom2 < rt_bail2) {
+                    const float r = r2 * rsqrt_approx(r2);
+                    const float rp = float(args.r_plus);
+                    const float scale = args.interior
+                                            ? fminf(fmaxf(fabsf(r - rp), 0.15f * r), 0.5f * r)
+                                            : r - rp;
+                    const float hl = fminf(fmaxf(float(args.step_scale) * scale,
+                                                 float(args.min_step)),
+                                           float(args.max_step));
+                    h[l] = double(fminf(hl, rcp_approx(fmaxf(1.0f, mom2 * rsqrt_approx(mom2)))));
+                    step[l] = true;
+                    any_step = true;
+                    continue;
+                }
+            }
             const RayState y = ys.get(l);
             if (it[l] >= args.max_steps) {
                 finish(l, y, BH_RAY_MAX_STEPS, nullptr, 0.0);
