@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) realtime_kernel(const RealtimeArg
     // the float32 fast path below.  An interior camera's lowest radius
     // threshold is 1.002 stop radii; above it its |p|^2 > 2500 test cannot
     // end the ray, so only the bail-out bound remains for |p|^2.
-    constexpr bool kFloatLanes = sizeof(typename T::S) == 4 && N == 1;
+    constexpr bool kFloatLanes = sizeof(typename T::S) == 4;
     const double rt_lo = args.interior ? args.capture_radius * 1.002 : args.capture_radius;
     const float rt_lo2 = float(rt_lo * rt_lo * (1.0 + 1e-3));
     const float rt_hi2 = float(args.escape_radius * args.escape_radius * (1.0 - 1e-3));
@@ -350,10 +350,10 @@ extern "C" int bh_trace_realtime(const bh_realtime_config *config, double mass, 
     a.hit_mom = hit_momenta;
     a.ws = reinterpret_cast<TraceWorkspace *>(workspace);
     // One ray per thread in both policies.  Two rays per thread in packed
-    // float32x2 arithmetic were measured slower here (1.76 against 1.64 ms
-    // per 1280x720 frame): the per-step float64 work (termination radius,
-    // step bound, state update) does not pack and weighs as much as the
-    // float32 stages.
+    // float32x2 arithmetic were measured slower here (1.34-1.37 against 1.30
+    // ms per 1280x720 frame, 128 x 2 and 128 x 3 blocks): the per-step
+    // float64 state update does not pack, and the packed kernel's 138-150
+    // registers leave fewer warps.
     e = c.precision == BH_PRECISION_FP64 ? launch_realtime<double, 128, 3>(a, s)
                                          : launch_realtime<float, 128, 4>(a, s);
     if (e != cudaSuccess) {
