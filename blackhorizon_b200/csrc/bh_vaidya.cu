@@ -28,20 +28,39 @@ struct VaidyaDev {
 };
 
 // numpy.interp for an increasing table: end values outside, exact table
-// values at nodes, slope (x - x_j) + y_j between.
-__device__ __forceinline__ double vd_interp(double x, const double *xp, const double *fp,
-                                            long long n) {
-    if (x != x) return x;
-    if (x < xp[0]) return fp[0];
-    if (x >= xp[n - 1]) return fp[n - 1];
+// values at nodes, slope (x - x_j) + y_j between.  vd_locate finds the
+// bracket xp[lo] <= x < xp[lo + 1] of an interior x (xp[0] <= x <
+// xp[n - 1]); vd_locate_near finds it from the bracket of a nearby point,
+// the same index the bisection gives.
+__device__ __forceinline__ long long vd_locate(double x, const double *xp, long long n) {
     long long lo = 0, hi = n - 1;
     while (hi - lo > 1) {  // xp[lo] <= x < xp[hi]
         const long long mid = (lo + hi) >> 1;
         if (xp[mid] <= x) lo = mid; else hi = mid;
     }
+    return lo;
+}
+__device__ __forceinline__ long long vd_locate_near(double x, long long lo, const double *xp,
+                                                    long long n) {
+    for (int k = 0; k < 4; ++k) {
+        if (xp[lo] > x) --lo;
+        else if (xp[lo + 1] <= x) ++lo;
+        else return lo;
+    }
+    return vd_locate(x, xp, n);
+}
+__device__ __forceinline__ double vd_interp_in(double x, long long lo, const double *xp,
+                                               const double *fp) {
     if (xp[lo] == x) return fp[lo];
     const double slope = __ddiv_rn(__dsub_rn(fp[lo + 1], fp[lo]), __dsub_rn(xp[lo + 1], xp[lo]));
     return __dadd_rn(__dmul_rn(slope, __dsub_rn(x, xp[lo])), fp[lo]);
+}
+__device__ __forceinline__ double vd_interp(double x, const double *xp, const double *fp,
+                                            long long n) {
+    if (x != x) return x;
+    if (x < xp[0]) return fp[0];
+    if (x >= xp[n - 1]) return fp[n - 1];
+    return vd_interp_in(x, vd_locate(x, xp, n), xp, fp);
 }
 
 // vaidya.py:153-159: m1(v) = M - dm (v_tail / max(v, v_tail))^(p - 1).
@@ -50,18 +69,49 @@ __device__ __forceinline__ double vd_m1(const VaidyaDev &d, double v) {
     return d.mass - d.tail_mass * ::pow(d.tail_start / vs, d.tail_power - 1.0);
 }
 
+// The v-dependent parts of m(v, r) (vaidya.py:244-269): the Price-tail mass
+// m1(v), the shell radius R(v) and the inflated excess, clipped.  The two
+// table columns share one bracket; *lo carries it to a nearby v (hint >= 0)
+// and returns this v's bracket (unchanged for v outside the table).
+struct VdMassAt {
+    double m1, shell_r, inc;
+};
+__device__ __forceinline__ VdMassAt vd_mass_at(const VaidyaDev &d, double v, long long *lo,
+                                               bool hint) {
+    VdMassAt o;
+    double m2;
+    if (v != v) {
+        o.shell_r = v;
+        m2 = v;
+    } else if (v < d.sv[0]) {
+        o.shell_r = d.sr[0];
+        m2 = d.sm2[0];
+    } else if (v >= d.sv[d.n - 1]) {
+        o.shell_r = d.sr[d.n - 1];
+        m2 = d.sm2[d.n - 1];
+    } else {
+        const long long j = hint ? vd_locate_near(v, *lo, d.sv, d.n) : vd_locate(v, d.sv, d.n);
+        *lo = j;
+        o.shell_r = vd_interp_in(v, j, d.sv, d.sr);
+        m2 = vd_interp_in(v, j, d.sv, d.sm2);
+    }
+    o.m1 = vd_m1(d, v);
+    o.inc = 0.0;
+    if (!(v < d.shell_start_v)) o.inc = np_min(np_max(m2 - o.m1, 0.0), d.mass_cap);
+    return o;
+}
+
+// m(v, r) from the v-dependent parts: the blend across the shell width.
+__device__ __forceinline__ double vd_mass_r(const VaidyaDev &d, const VdMassAt &a, double r) {
+    const double t = np_min(np_max((a.shell_r - r) / d.shell_width + 0.5, 0.0), 1.0);
+    const double blend = t * t * (3.0 - 2.0 * t);
+    return a.m1 + blend * a.inc;
+}
+
 // vaidya.py:244-269: m(v, r).
 __device__ __forceinline__ double vd_mass(const VaidyaDev &d, double v, double r) {
-    const double shell_r = vd_interp(v, d.sv, d.sr, d.n);
-    const double t = np_min(np_max((shell_r - r) / d.shell_width + 0.5, 0.0), 1.0);
-    const double blend = t * t * (3.0 - 2.0 * t);
-    const double m1 = vd_m1(d, v);
-    double inc = 0.0;
-    if (!(v < d.shell_start_v)) {
-        const double m2 = vd_interp(v, d.sv, d.sm2, d.n);
-        inc = np_min(np_max(m2 - m1, 0.0), d.mass_cap);
-    }
-    return m1 + blend * inc;
+    long long lo = 0;
+    return vd_mass_r(d, vd_mass_at(d, v, &lo, false), r);
 }
 
 struct VaidyaGeo {
@@ -75,9 +125,16 @@ __device__ __forceinline__ void vd_geometry(const VaidyaDev &d, double t, double
     g.r = r;
     g.l[0] = x / r; g.l[1] = y / r; g.l[2] = z / r;
     const double v = t + r, eps = 1e-4;
-    const double m0 = vd_mass(d, v, r);
-    const double m_v = (vd_mass(d, v + eps, r) - vd_mass(d, v - eps, r)) / (2.0 * eps);
-    const double m_r = (vd_mass(d, v, r + eps) - vd_mass(d, v, r - eps)) / (2.0 * eps);
+    // The five mass samples of the central differences need the v-dependent
+    // parts at three times only, and v +- eps lie in or next to v's bracket.
+    long long lo = 0;
+    const VdMassAt a0 = vd_mass_at(d, v, &lo, false);
+    long long lo_p = lo, lo_m = lo;
+    const VdMassAt ap = vd_mass_at(d, v + eps, &lo_p, true);
+    const VdMassAt am = vd_mass_at(d, v - eps, &lo_m, true);
+    const double m0 = vd_mass_r(d, a0, r);
+    const double m_v = (vd_mass_r(d, ap, r) - vd_mass_r(d, am, r)) / (2.0 * eps);
+    const double m_r = (vd_mass_r(d, a0, r + eps) - vd_mass_r(d, a0, r - eps)) / (2.0 * eps);
     const double r2 = r * r;
     g.h = m0 / r - d.q2 / (2.0 * r2);
     const double h_v = m_v / r;
