@@ -262,3 +262,50 @@ def test_camera_batch_matches_single_traces(cuda):
             assert torch.equal(one.status, res.status)
             assert torch.equal(one.steps, res.steps)
             assert torch.equal(one.states, res.states)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_termination_near_the_thresholds(cuda, precision):
+    """Rays that start from 1e-6 to 5e-2 outside the capture radius heading in,
+    and as far inside the escape radius heading out, cross a threshold within
+    a few steps: the kernels' radius test (the stage arithmetic's r^2 away
+    from a threshold, float64 near one) must classify them as the oracle's
+    float64 test does, in the tracer and in the tile tracer."""
+    from blackhorizon_b200 import build_state, null_momentum_from_velocity, trace_rays
+    from blackhorizon_b200.kerr import KerrSpacetime
+    from blackhorizon_b200.offline import OfflineSettings, trace_tile
+    from oracle import oracle
+
+    a, margin, esc = 0.9, 0.01, 30.0
+    st = KerrSpacetime(1.0, a)
+    rcap = st.capture_radius(margin)
+    f = np.geomspace(1e-6, 5e-2, 48)
+    r0 = np.concatenate([rcap * (1.0 + f), esc * (1.0 - f)])
+    out = np.concatenate([-np.ones(48), np.ones(48)])
+    pos, d = [], []
+    for k, (r, s) in enumerate(zip(r0, out)):
+        # Polar angle of the start point: near the pole for the capture group,
+        # which starts outside the ergosphere there (null_momentum_from_velocity
+        # needs it, geodesics.py:130-131).
+        th = 0.02 + 0.002 * k if s < 0 else 0.3 + 0.05 * (k - 48)
+        w = np.sqrt(r * r + a * a)
+        p = np.array([w * np.sin(th), 0.0, r * np.cos(th)])
+        u = s * p / np.linalg.norm(p) + np.array([0.0, 0.15 * np.sin(k), 0.0])
+        pos.append(p)
+        d.append(u / np.linalg.norm(u))
+    pos, d = np.array(pos), np.array(d)
+    s0 = build_state(pos, null_momentum_from_velocity(st, pos, d, time_orientation="future"))
+    # A small first step walks each ray across its threshold in 1 to 9 steps,
+    # so accepted states land on both sides of the 1e-3 band around it.
+    kw = dict(rtol=1e-9, atol=1e-12, capture_margin=margin, initial_step=1e-5)
+    res = trace_rays(st, dev(s0), esc, precision=precision, **kw)
+    _, ostatus, osteps, _ = oracle.trace(1.0, a, s0, esc, **kw)
+    np.testing.assert_array_equal(res.status.cpu().numpy(), ostatus)
+    assert set(ostatus[:48]) == {1} and set(ostatus[48:]) == {2}
+    if precision == "fp64":
+        np.testing.assert_array_equal(res.steps.cpu().numpy(), osteps)
+    settings = OfflineSettings(spin=a, capture_margin=margin)
+    tile = trace_tile(st, dev(s0), esc, settings, None, 1e-9, 12000, precision=precision)
+    otile = oracle.trace_tile(1.0, a, s0, esc, None, rtol=1e-9, capture_margin=margin,
+                              max_step=settings.max_step)
+    np.testing.assert_array_equal(tile.status.cpu().numpy(), otile["status"])
