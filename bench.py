@@ -52,7 +52,7 @@ BYTES_PER_RAY = 176
 # launch of the default variants).  The state stays on chip between steps,
 # so the traffic grows with the ray count only; the benchmark scales it to
 # its own ray count.
-NCU_DRAM_BYTES_PER_RAY = {"mixed": 151.3, "fp64": 153.1}
+NCU_DRAM_BYTES_PER_RAY = {"mixed": 150.6, "fp64": 153.7}
 
 METRIC = "ray-steps/s"
 
