@@ -136,6 +136,7 @@ struct TileArgs {
     int round;  // 0: rays from state0; r > 0: resume records of parity r & 1
     int flush;  // finalise every ray in flight as IN_FLIGHT without stepping
     int interior;  // interior camera: capture_radius is the stop radius
+    int inline_refine;  // refine crossings in place instead of parking them
     double mass, spin, capture_radius, escape_radius;
     double disk_inner, disk_outer;  // disk_outer <= 0: no crossing tests
     double rtol, atol, initial_step, max_step;

@@ -211,9 +211,10 @@ __device__ __forceinline__ bool refine_hit(double m, double a, double r_in, doub
     return r >= r_in && r <= r_out;
 }
 
-// INLINE = false (the first round): every crossing is parked for the
-// refinement kernel.  INLINE = true (resumed rays): crossings are refined in
-// place, so no ray needs a third round.
+// INLINE = false: every crossing is parked for the refinement kernel, and
+// the misses come back as the next round's resumed rays.  INLINE = true
+// (the rounds that start with few resumed rays): crossings are refined in
+// place, so no ray needs another round.
 template <class V, int BLOCK, int MINB, bool INLINE>
 __global__ void __launch_bounds__(BLOCK, MINB) tile_kernel(const TileArgs args) {
     using T = VT<V>;
@@ -539,7 +540,7 @@ cudaError_t launch_tile(const TileArgs &args, int precision, int variant,
         variant = tile_default_variant(precision);
     const Variant v = trace_variant(precision, variant);
     size_t smem = 0;
-    const void *fn = tile_kernel_for(precision, variant, args.round > 0, &smem);
+    const void *fn = tile_kernel_for(precision, variant, args.inline_refine != 0, &smem);
     int dev = 0, sms = 0, occ = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
@@ -553,6 +554,77 @@ cudaError_t launch_tile(const TileArgs &args, int precision, int variant,
     void *params[] = {(void *)&a};
     return cudaLaunchKernel(fn, dim3((unsigned)((long long)sms * per_sm)), dim3(v.block),
                             params, smem, stream);
+}
+
+// Resumed rays are reordered before the next round, most attempts so far
+// first: rays that reach their first equatorial crossing only after many
+// small steps are those winding near the photon sphere, which keep going
+// longest after a miss.  Started first, they run beside the bulk of the
+// round instead of after it, when the other slots would idle.  A counting
+// sort by attempts (8 per bucket); the order inside a bucket does not matter,
+// because every ray's result is independent of its slot.
+constexpr int kResumeBuckets = 128;
+// Rounds with fewer resumed rays than this refine their crossings in place.
+constexpr unsigned long long kInlineRefineBelow = 65536;
+struct TileResumeSort {
+    unsigned count[kResumeBuckets];
+    unsigned cursor[kResumeBuckets];
+};
+static_assert(sizeof(TileResumeSort) == 1024, "resume sort counters are 1 KiB");
+
+__device__ __forceinline__ int resume_bucket(const TileResume &r) {
+    const long long b = r.attempts >> 3;
+    return (int)(b < kResumeBuckets - 1 ? b : kResumeBuckets - 1);
+}
+
+__global__ void __launch_bounds__(256) resume_count_kernel(const TileResume *in, long long n,
+                                                           TileResumeSort *srt) {
+    __shared__ unsigned hist[kResumeBuckets];
+    for (int b = threadIdx.x; b < kResumeBuckets; b += blockDim.x) hist[b] = 0;
+    __syncthreads();
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        atomicAdd(&hist[resume_bucket(in[i])], 1u);
+    __syncthreads();
+    for (int b = threadIdx.x; b < kResumeBuckets; b += blockDim.x)
+        if (hist[b]) atomicAdd(&srt->count[b], hist[b]);
+}
+
+__global__ void resume_offsets_kernel(TileResumeSort *srt) {
+    if (threadIdx.x != 0) return;
+    unsigned acc = 0;
+    for (int b = kResumeBuckets - 1; b >= 0; --b) {
+        srt->cursor[b] = acc;
+        acc += srt->count[b];
+    }
+}
+
+__global__ void __launch_bounds__(256) resume_scatter_kernel(const TileResume *in, long long n,
+                                                             TileResumeSort *srt,
+                                                             TileResume *out) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const TileResume r = in[i];
+        out[atomicAdd(&srt->cursor[resume_bucket(r)], 1u)] = r;
+    }
+}
+
+// Reorders in[0, n) into out (counters in srt, zeroed here).
+static cudaError_t sort_resumed(const TileResume *in, long long n, TileResumeSort *srt,
+                                TileResume *out, cudaStream_t stream) {
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(srt, 0, sizeof(TileResumeSort), stream);
+    if (e != cudaSuccess) return e;
+    const long long need = (n + 255) / 256;
+    const unsigned grid = (unsigned)(need < 4LL * sms ? need : 4LL * sms);
+    resume_count_kernel<<<grid, 256, 0, stream>>>(in, n, srt);
+    resume_offsets_kernel<<<1, 32, 0, stream>>>(srt);
+    resume_scatter_kernel<<<grid, 256, 0, stream>>>(in, n, srt, out);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_refine(const TileArgs &args, cudaStream_t stream) {
@@ -580,9 +652,12 @@ static int tile_cuda(cudaError_t e, const char *what) {
 
 using namespace bh;
 
+// Workspace: header, resume-sort counters, crossing records, and two
+// resume arrays (the second receives the reordered records).
 extern "C" size_t bh_trace_tile_workspace_bytes(int64_t n) {
     if (n < 0) n = 0;
-    return sizeof(TileWorkspace) + (size_t)n * (sizeof(TileCrossing) + sizeof(TileResume));
+    return sizeof(TileWorkspace) + sizeof(TileResumeSort) +
+           (size_t)n * (sizeof(TileCrossing) + 2 * sizeof(TileResume));
 }
 
 extern "C" int bh_trace_tile(const bh_trace_config *config, const bh_scene *scene,
@@ -648,9 +723,13 @@ extern "C" int bh_trace_tile(const bh_trace_config *config, const bh_scene *scen
     a.max_attempts = 4 * c.max_steps;
     a.saturate_steps = (long long)(0.85 * (double)c.max_steps);
     a.ws = reinterpret_cast<TileWorkspace *>(base);
-    a.cross = reinterpret_cast<TileCrossing *>(base + sizeof(TileWorkspace));
+    TileResumeSort *resume_sort = reinterpret_cast<TileResumeSort *>(base + sizeof(TileWorkspace));
+    a.cross = reinterpret_cast<TileCrossing *>(base + sizeof(TileWorkspace) +
+                                               sizeof(TileResumeSort));
     a.resume = reinterpret_cast<TileResume *>(base + sizeof(TileWorkspace) +
+                                              sizeof(TileResumeSort) +
                                               (size_t)n * sizeof(TileCrossing));
+    TileResume *resume_sorted = a.resume + n;
     a.states = states;
     a.status = status;
     a.steps = steps;
@@ -667,9 +746,15 @@ extern "C" int bh_trace_tile(const bh_trace_config *config, const bh_scene *scen
     const long long max_rounds = c.max_steps + 2;
     int rounds = 0;
     bool flush = false, host_late = false;
+    unsigned long long entering = (unsigned long long)n;  // rays of this round
     for (long long r = 0;; ++r) {
         if (r >= max_rounds) flush = true;
         a.round = r == 0 ? 0 : (r & 1 ? 1 : 2);
+        // A crossing refined in place runs about ten float64 RK4 substeps
+        // for one lane while the warp's other lanes wait; parked crossings
+        // are refined one per thread.  Rounds park them while many rays
+        // remain and refine in place once few do, which ends the rounds.
+        a.inline_refine = r > 0 && entering < kInlineRefineBelow ? 1 : 0;
         a.flush = flush ? 1 : 0;
         if (c.timeout_ns > 0) {
             const long long used = std::chrono::duration_cast<std::chrono::nanoseconds>(
@@ -693,6 +778,13 @@ extern "C" int bh_trace_tile(const bh_trace_config *config, const bh_scene *scen
         rc = tile_cuda(cudaStreamSynchronize(s), "bh_trace_tile round");
         if (rc != BH_OK) return rc;
         if (next == 0 || a.flush) break;
+        entering = next;
+        if (r == 0 && next >= 1024 && next < (1ull << 31)) {
+            rc = tile_cuda(sort_resumed(a.resume, (long long)next, resume_sort, resume_sorted, s),
+                           "bh_trace_tile resume ordering");
+            if (rc != BH_OK) return rc;
+            a.resume = resume_sorted;
+        }
     }
     TileWorkspace hw;
     rc = tile_cuda(cudaMemcpyAsync(&hw, a.ws, sizeof(hw), cudaMemcpyDeviceToHost, s),

@@ -457,8 +457,9 @@ typedef struct {
     int32_t timed_out;  /* 1: rays were left BH_RAY_IN_FLIGHT at the deadline */
 } bh_tile_stats;
 
-/* Device workspace of bh_trace_tile for n rays: a 256-byte header, n
- * crossing records (168 B) and n resume records (96 B). */
+/* Device workspace of bh_trace_tile for n rays: a 256-byte header, 1 KiB of
+ * counters for ordering resumed rays, n crossing records (168 B) and two
+ * arrays of n resume records (96 B each). */
 size_t bh_trace_tile_workspace_bytes(int64_t n);
 
 /* blackhorizon/offline/render.py:184-309 (_trace_tile) with the crossing

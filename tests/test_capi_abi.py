@@ -135,7 +135,7 @@ def test_trace_tile_argument_validation(bhlib):
     assert call(cfg, 2.3, 18.0, 0) == 0  # empty tile: nothing to do
     assert call(cfg, 2.3, 18.0, 4) == -5  # no workspace
     assert call(cfg, 2.3, 18.0, 4, C.c_void_p(0x10000), 100) == -5  # too small
-    assert bhlib.bh_trace_tile_workspace_bytes(10) == 256 + 10 * (168 + 96)
+    assert bhlib.bh_trace_tile_workspace_bytes(10) == 256 + 1024 + 10 * (168 + 2 * 96)
     # Config flags: BH_TRACE_INTERIOR only, and only with a stop radius > 0.
     cfg.flags = 2
     assert call(cfg, 2.3, 18.0, 4) == -1
