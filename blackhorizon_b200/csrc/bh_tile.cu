@@ -599,13 +599,32 @@ __global__ void resume_offsets_kernel(TileResumeSort *srt) {
     }
 }
 
+// Each block places a tile of 256 records: ranks within the tile from
+// shared-memory counters, one global reservation per non-empty bucket.
 __global__ void __launch_bounds__(256) resume_scatter_kernel(const TileResume *in, long long n,
                                                              TileResumeSort *srt,
                                                              TileResume *out) {
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
-        const TileResume r = in[i];
-        out[atomicAdd(&srt->cursor[resume_bucket(r)], 1u)] = r;
+    __shared__ unsigned cnt[kResumeBuckets], base[kResumeBuckets];
+    for (long long t0 = (long long)blockIdx.x * blockDim.x; t0 < n;
+         t0 += (long long)gridDim.x * blockDim.x) {
+        for (int b = threadIdx.x; b < kResumeBuckets; b += blockDim.x) cnt[b] = 0;
+        __syncthreads();
+        const long long i = t0 + threadIdx.x;
+        const bool valid = i < n;
+        TileResume r;
+        int b = 0;
+        unsigned rank = 0;
+        if (valid) {
+            r = in[i];
+            b = resume_bucket(r);
+            rank = atomicAdd(&cnt[b], 1u);
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < kResumeBuckets; k += blockDim.x)
+            if (cnt[k]) base[k] = atomicAdd(&srt->cursor[k], cnt[k]);
+        __syncthreads();
+        if (valid) out[base[b] + rank] = r;
+        __syncthreads();
     }
 }
 
