@@ -290,13 +290,16 @@ __device__ __forceinline__ void dp5_step_vjp(W m, W a, const Vec8<W> &y0, double
     Vec8<W> Y[6], K[6];
     Y[0] = y0;
     K[0] = rhs_full<W>(m, a, Y[0]);
-    // The stage loops are kept rolled: one copy of the RHS and of its
-    // reverse sweep keeps the kernel inside the instruction cache (the
-    // stage arrays live in local memory either way).
-#pragma unroll 1
+    // Float sweeps unroll the stage loops, which keeps the stage arrays in
+    // registers (the long rays' sweeps are latency-bound, and local-memory
+    // round trips sat on their critical path: 2.55 against 1.85 ms on the
+    // 256x256 frame).  Double sweeps keep them rolled: unrolled, they spill
+    // 3 KB per thread and ran 1.5x slower.
+    constexpr int U = sizeof(W) == 4 ? 8 : 1;
+#pragma unroll U
     for (int i = 1; i < 6; ++i) {
         Vec8<W> acc = vzero<W>();
-#pragma unroll 1
+#pragma unroll U
         for (int j = 0; j < i; ++j) acc = axpy<W>(W(dpa::A[i][j]), K[j], acc);
         Y[i] = axpy<W>(hw, acc, Y[0]);
         K[i] = rhs_full<W>(m, a, Y[i]);
@@ -304,13 +307,13 @@ __device__ __forceinline__ void dp5_step_vjp(W m, W a, const Vec8<W> &y0, double
     const Vec8<W> lw{W(lam.t), W(lam.x), W(lam.y), W(lam.z), W(lam.pt), W(lam.px),
                      W(lam.py), W(lam.pz)};
     Vec8<W> Kb[6];
-#pragma unroll 1
+#pragma unroll U
     for (int j = 0; j < 6; ++j) {
         const W c = hw * W(dpa::B[j]);
         Kb[j] = Vec8<W>{c * lw.t, c * lw.x, c * lw.y, c * lw.z, c * lw.pt, c * lw.px,
                         c * lw.py, c * lw.pz};
     }
-#pragma unroll 1
+#pragma unroll U
     for (int i = 5; i >= 0; --i) {
         Vec8<W> Yb = vzero<W>();
         W ab = W(0);
@@ -319,7 +322,7 @@ __device__ __forceinline__ void dp5_step_vjp(W m, W a, const Vec8<W> &y0, double
         lam.t += double(Yb.t); lam.x += double(Yb.x); lam.y += double(Yb.y);
         lam.z += double(Yb.z); lam.pt += double(Yb.pt); lam.px += double(Yb.px);
         lam.py += double(Yb.py); lam.pz += double(Yb.pz);
-#pragma unroll 1
+#pragma unroll U
         for (int j = 0; j < i; ++j) Kb[j] = axpy<W>(hw * W(dpa::A[i][j]), Yb, Kb[j]);
     }
 }
