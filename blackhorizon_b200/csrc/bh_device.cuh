@@ -250,20 +250,28 @@ template <> struct VT<F2> {
 
 // Per-ray Kerr constants in the lane type, formed once per ray.
 template <class V>
+// m2, na2: the float lanes' form of the RHS; m, a2x4, a2x3, n2ma2: the
+// double lanes' (each form reads only its own).
 struct KerrV {
-    V m2, a, na, a2, na2;
+    V m, m2, a, na, a2, na2, a2x4, a2x3, n2ma2;
 };
 template <class V>
 __device__ __forceinline__ KerrV<V> make_kerr(V m, V a) {
     using T = VT<V>;
     KerrV<V> k;
+    k.m = m;
     k.m2 = m * T::set(2.0);
     k.a = a;
     k.na = -a;
     k.a2 = a * a;
     k.na2 = -k.a2;
+    k.a2x4 = k.a2 * T::set(4.0);
+    k.a2x3 = k.a2 * T::set(3.0);
+    k.n2ma2 = (m * k.a2) * T::set(-2.0);
     return k;
 }
+
+
 
 // Stage derivative in split form (see the top of this file):
 //   kx..kz = dP - 2 H lp l   (position part)   thl = 2 H lp   (time part)
@@ -272,6 +280,63 @@ template <class V>
 struct StageV {
     V kx, ky, kz, thl, px, py, pz;
 };
+
+// The RHS of the double lanes (the float64 policy), in the operation order
+// it has always had: its trajectories are pinned to the reference's end
+// points within 1e-7 where the step counts agree, and near the photon sphere
+// any rounding change grows past that.  See rhs_v for the regrouping.
+__device__ __forceinline__ StageV<double> rhs_f64(const KerrV<double> &K, double x,
+                                                  double y, double z, double npt, double px,
+                                                  double py, double pz, double dpx,
+                                                  double dpy, double dpz, double *r2_out) {
+    const double z2 = z * z;
+    const double a2z2 = K.a2 * z2;
+    const double q = fma(x, x, fma(y, y, z2 - K.a2));
+    const double s2 = fmax(fma(q, q, K.a2x4 * z2), kTiny * kTiny);
+    const double inv_s = rsqrt_f64(s2);
+    const double s = s2 * inv_s;
+    const double r2 = fmax((q + s) * 0.5, kTiny);
+    if (r2_out) *r2_out = r2;
+    const double inv_r = rsqrt_f64(r2);
+    const double r = r2 * inv_r;
+    const double w = r2 + K.a2;
+    const double r2sq = r2 * r2;
+    const double qd = fmax(r2sq + a2z2, kTiny);
+    const double inv_qd = rcp_f64(qd);
+    const double inv_w = rcp_f64(w);
+    const double r3 = r * r2;
+    const double h = (K.m * r3) * inv_qd;
+    const double lx = fma(r, x, K.a * y) * inv_w;
+    const double ly = fma(r, y, K.na * x) * inv_w;
+    const double lz = z * inv_r;
+    const double lxy = fma(lx, px, ly * py);
+    const double lzpz = lz * pz;
+    const double lp = (lxy + lzpz) + npt;
+    const double thl = (h + h) * lp;
+    const double nthl = -thl;
+    StageV<double> o;
+    o.thl = thl;
+    o.kx = fma(nthl, lx, dpx);
+    o.ky = fma(nthl, ly, dpy);
+    o.kz = fma(nthl, lz, dpz);
+    const double rs = r * inv_s;
+    const double r_x = x * rs, r_y = y * rs;
+    const double r_z = z * (w * (inv_r * inv_s));
+    const double inv_qd2 = inv_qd * inv_qd;
+    const double lp2 = lp * lp;
+    const double t3 = K.a2x3 * z2 - r2sq;
+    const double dh_dr = ((K.m * r2) * t3) * inv_qd2;
+    const double dh_dz = ((K.n2ma2 * z) * r3) * inv_qd2;
+    const double u = fma(x, px, y * py);
+    const double g1 = fma(r * -2.0, lxy, u);
+    const double g = g1 * inv_w - lzpz * inv_r;
+    const double k = fma(dh_dr, lp2, thl * g);
+    const double tw = thl * inv_w;
+    o.px = fma(r_x, k, tw * fma(r, px, K.na * py));
+    o.py = fma(r_y, k, tw * fma(r, py, K.a * px));
+    o.pz = fma(r_z, k, fma(dh_dz, lp2, (thl * pz) * inv_r));
+    return o;
+}
 
 // ------------------------------------------------------------ compact RHS
 // geodesics.py:42-74 with kerr.py:118-193 folded in, evaluated at position
@@ -296,6 +361,9 @@ __device__ __forceinline__ StageV<V> rhs_v(const KerrV<V> &K, V x, V y, V z,
                                            V npt, V px, V py, V pz, V dpx,
                                            V dpy, V dpz, V *r2_out = nullptr) {
     using T = VT<V>;
+    if constexpr (sizeof(typename T::S) == 8) {
+        return rhs_f64(K, x, y, z, npt, px, py, pz, dpx, dpy, dpz, r2_out);
+    } else {
     // Float lanes add the clamp constant to a^2 z^2, which enters s^2 and qd,
     // instead of taking a maximum: both sums are non-negative, and the
     // constant changes neither unless it is within 2^24 of the sum, i.e. at
@@ -348,6 +416,7 @@ __device__ __forceinline__ StageV<V> rhs_v(const KerrV<V> &K, V x, V y, V z,
     o.py = T::fma(y, rsk, tw * T::fma(r, py, K.a * px));
     o.pz = T::fma(lz * w, sk, T::fma((K.na2 * z) * r3, mlp, thl * pzr));
     return o;
+    }
 }
 
 // ---------------------------------------------------------------- tableau
