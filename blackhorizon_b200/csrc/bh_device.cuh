@@ -349,11 +349,15 @@ __device__ __forceinline__ StageV<double> rhs_f64(const KerrV<double> &K, double
 // and with grad H = dH/dr grad r + (0, 0, dH/dz|_r) the momentum derivative is
 //   pdot_i = r_i (dH/dr lp^2 + thl G) + [thl * the explicit terms above]
 // which is the reference's grad_h * lp^2 + thl * (grad_l . p) regrouped.
-// The mass enters through one factor 2m/qd: thl = (2m/qd) r^3 lp, and with
-// mlp = 2m lp^2/qd^2, dH/dr lp^2 = r^2 (3a^2z^2 - r^4)/2 mlp and
-// dH/dz|_r lp^2 = -a^2 z r^3 mlp.
 // The radius uses the reference's r^2 = (q + s)/2 (kerr.py:141) for every
-// lane type.
+// lane type.  Double lanes take rhs_f64.  Float lanes regroup further:
+// - the mass enters through one factor 2m/qd: thl = (2m/qd) r^3 lp, and with
+//   mlp = 2m lp^2/qd^2, dH/dr lp^2 = r^2 (3a^2z^2 - r^4)/2 mlp and
+//   dH/dz|_r lp^2 = -a^2 z r^3 mlp, (3a^2z^2 - r^4)/2 = 2 a^2 z^2 - qd/2;
+// - the clamp constant is added to a^2 z^2, which enters s^2 and qd, instead
+//   of taking maxima: both sums are non-negative, and the constant changes
+//   neither unless it is within 2^24 of the sum, i.e. at the ring itself;
+// - grad r is applied to k/s in one product, dr/dz = l_z (r^2+a^2)/s.
 //
 // r2_out, when given, receives the radius r^2 the evaluation used.
 template <class V>
@@ -364,58 +368,50 @@ __device__ __forceinline__ StageV<V> rhs_v(const KerrV<V> &K, V x, V y, V z,
     if constexpr (sizeof(typename T::S) == 8) {
         return rhs_f64(K, x, y, z, npt, px, py, pz, dpx, dpy, dpz, r2_out);
     } else {
-    // Float lanes add the clamp constant to a^2 z^2, which enters s^2 and qd,
-    // instead of taking a maximum: both sums are non-negative, and the
-    // constant changes neither unless it is within 2^24 of the sum, i.e. at
-    // the ring itself; that saves the unpacked max instructions on the
-    // critical path.  Double lanes keep the reference's clamps.
-    constexpr bool kAddTiny = sizeof(typename T::S) == 4;
-    const V z2 = z * z;
-    const V a2z2 = kAddTiny ? T::fma(K.a2, z2, T::set(T::tiny())) : K.a2 * z2;
-    const V q = T::fma(x, x, T::fma(y, y, z2 - K.a2));
-    const V s2 = kAddTiny ? T::fma(a2z2, T::set(4.0), q * q)
-                          : T::max(T::fma(q, q, a2z2 * T::set(4.0)), T::set(T::tiny2()));
-    const V inv_s = T::rsqrt(s2);
-    const V s = s2 * inv_s;
-    const V r2 = T::max(T::fma(s, T::set(0.5), q * T::set(0.5)), T::set(T::tiny()));
-    if (r2_out) *r2_out = r2;
-    const V inv_r = T::rsqrt(r2);
-    const V r = r2 * inv_r;
-    const V w = r2 + K.a2;
-    const V qd = kAddTiny ? T::fma(r2, r2, a2z2) : T::max(T::fma(r2, r2, a2z2), T::set(T::tiny()));
-    const V inv_qd = T::rcp(qd);
-    const V inv_w = T::rcp(w);
-    const V r3 = r * r2;
-    const V m2i = K.m2 * inv_qd;  // 2m / qd
-    const V lx = T::fma(r, x, K.a * y) * inv_w;
-    const V ly = T::fma(r, y, K.na * x) * inv_w;
-    const V lz = z * inv_r;
-    const V lxy = T::fma(lx, px, ly * py);
-    const V lp = T::fma(lz, pz, lxy) + npt;
-    const V thl = (m2i * r3) * lp;  // 2 H lp
-    const V nthl = -thl;
-    const V tz = nthl * lz;
-    StageV<V> o;
-    o.thl = thl;
-    o.kx = T::fma(nthl, lx, dpx);
-    o.ky = T::fma(nthl, ly, dpy);
-    o.kz = tz + dpz;
-    const V mlp = (m2i * inv_qd) * (lp * lp);  // 2m lp^2 / qd^2
-    // (3 a^2 z^2 - r^4) / 2 = 2 a^2 z^2 - qd / 2.
-    const V t3h = T::fma(qd, T::set(-0.5), a2z2 + a2z2);
-    // thl G = thl (x p_x + y p_y - 2 r (l_x p_x + l_y p_y)) / w - thl l_z p_z / r.
-    const V u = T::fma(x, px, y * py);
-    const V g1 = T::fma(r * T::set(-2.0), lxy, u);
-    const V tw = thl * inv_w;
-    const V pzr = pz * inv_r;
-    const V k = T::fma(tz, pzr, T::fma(tw, g1, (r2 * t3h) * mlp));
-    // grad r = (x r, y r, z w / r) / s, applied to k / s.
-    const V sk = k * inv_s;
-    const V rsk = r * sk;
-    o.px = T::fma(x, rsk, tw * T::fma(r, px, K.na * py));
-    o.py = T::fma(y, rsk, tw * T::fma(r, py, K.a * px));
-    o.pz = T::fma(lz * w, sk, T::fma((K.na2 * z) * r3, mlp, thl * pzr));
-    return o;
+        const V z2 = z * z;
+        const V a2z2 = T::fma(K.a2, z2, T::set(T::tiny()));
+        const V q = T::fma(x, x, T::fma(y, y, z2 - K.a2));
+        const V s2 = T::fma(a2z2, T::set(4.0), q * q);
+        const V inv_s = T::rsqrt(s2);
+        const V s = s2 * inv_s;
+        const V r2 = T::max(T::fma(s, T::set(0.5), q * T::set(0.5)), T::set(T::tiny()));
+        if (r2_out) *r2_out = r2;
+        const V inv_r = T::rsqrt(r2);
+        const V r = r2 * inv_r;
+        const V w = r2 + K.a2;
+        const V qd = T::fma(r2, r2, a2z2);
+        const V inv_qd = T::rcp(qd);
+        const V inv_w = T::rcp(w);
+        const V r3 = r * r2;
+        const V m2i = K.m2 * inv_qd;  // 2m / qd
+        const V lx = T::fma(r, x, K.a * y) * inv_w;
+        const V ly = T::fma(r, y, K.na * x) * inv_w;
+        const V lz = z * inv_r;
+        const V lxy = T::fma(lx, px, ly * py);
+        const V lp = T::fma(lz, pz, lxy) + npt;
+        const V thl = (m2i * r3) * lp;  // 2 H lp
+        const V nthl = -thl;
+        const V tz = nthl * lz;
+        StageV<V> o;
+        o.thl = thl;
+        o.kx = T::fma(nthl, lx, dpx);
+        o.ky = T::fma(nthl, ly, dpy);
+        o.kz = tz + dpz;
+        const V mlp = (m2i * inv_qd) * (lp * lp);  // 2m lp^2 / qd^2
+        const V t3h = T::fma(qd, T::set(-0.5), a2z2 + a2z2);
+        // thl G = thl (x p_x + y p_y - 2 r (l_x p_x + l_y p_y)) / w - thl l_z p_z / r.
+        const V u = T::fma(x, px, y * py);
+        const V g1 = T::fma(r * T::set(-2.0), lxy, u);
+        const V tw = thl * inv_w;
+        const V pzr = pz * inv_r;
+        const V k = T::fma(tz, pzr, T::fma(tw, g1, (r2 * t3h) * mlp));
+        // grad r = (x r, y r, z w / r) / s, applied to k / s.
+        const V sk = k * inv_s;
+        const V rsk = r * sk;
+        o.px = T::fma(x, rsk, tw * T::fma(r, px, K.na * py));
+        o.py = T::fma(y, rsk, tw * T::fma(r, py, K.a * px));
+        o.pz = T::fma(lz * w, sk, T::fma((K.na2 * z) * r3, mlp, thl * pzr));
+        return o;
     }
 }
 
