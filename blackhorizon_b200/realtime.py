@@ -144,6 +144,23 @@ def trace_like_shader(spacetime: KerrSpacetime, state0: Array, settings: RenderS
     s, host = to_device_f64(state0, "state0")
     if s.dim() != 2 or s.shape[1] != 8:
         raise ValueError("state0 must have shape (n, 8)")
+    status, states, hit_r, hit_p, hit_m, steps = _trace_shader_device(
+        spacetime, s, settings, escape_radius, disk_radii, interior_stop, precision)
+    conv = (lambda t: t.cpu().numpy()) if host is not None else (lambda t: t)  # noqa: E731
+    disk = disk_radii is not None
+    return ReferenceResult(status=conv(status), positions=conv(states[:, 1:4].contiguous()),
+                           momenta=conv(states[:, 4:8].contiguous()),
+                           hit_radii=conv(hit_r) if disk else None,
+                           hit_positions=conv(hit_p) if disk else None,
+                           hit_momenta=conv(hit_m) if disk else None,
+                           steps=steps)
+
+
+def _trace_shader_device(spacetime, s, settings, escape_radius, disk_radii, interior_stop,
+                         precision):
+    """bh_trace_realtime on a device state tensor: (status, final states (n, 8),
+    hit radii, hit positions, hit momenta, RK4 steps), all device tensors but
+    the step count."""
     n = s.shape[0]
     dev = s.device
     lib = _lib.load()
@@ -167,14 +184,7 @@ def trace_like_shader(spacetime: KerrSpacetime, state0: Array, settings: RenderS
                                      n, ptr(ws), stream), "trace_like_shader")
     stats = _lib.TraceStats()
     _lib.check(lib.bh_trace_stats_read(ptr(ws), stats, stream), "trace_like_shader")
-    conv = (lambda t: t.cpu().numpy()) if host is not None else (lambda t: t)  # noqa: E731
-    disk = disk_radii is not None
-    return ReferenceResult(status=conv(status), positions=conv(states[:, 1:4].contiguous()),
-                           momenta=conv(states[:, 4:8].contiguous()),
-                           hit_radii=conv(hit_r) if disk else None,
-                           hit_positions=conv(hit_p) if disk else None,
-                           hit_momenta=conv(hit_m) if disk else None,
-                           steps=int(stats.attempts))
+    return status, states, hit_r, hit_p, hit_m, int(stats.attempts)
 
 
 # ------------------------------------------------------------ headless frame
@@ -267,17 +277,12 @@ def render_frame_device(settings: RenderSettings, camera, width: int, height: in
     s0 = device_camera_rays(spacetime, camera, width, height, settings.fov_degrees, 1,
                             interior["tetrad"] if interior else None, dev)
     escape = settings.effective_escape_radius(camera.distance_from_origin)
-    res = trace_like_shader(spacetime, s0, settings, escape,
-                            disk_radii=(inner, outer) if settings.disk_enabled else None,
-                            interior_stop=interior["stop"] if interior else None,
-                            precision=precision)
-    n = s0.shape[0]
-    states = torch.cat([torch.zeros((n, 1), dtype=torch.float64, device=dev), res.positions,
-                        res.momenta], dim=1).contiguous()
-    hit_p = res.hit_positions if res.hit_positions is not None else torch.zeros(
-        (n, 3), dtype=torch.float64, device=dev)
-    hit_m = res.hit_momenta if res.hit_momenta is not None else torch.zeros(
-        (n, 4), dtype=torch.float64, device=dev)
+    disk_radii = (inner, outer) if settings.disk_enabled else None
+    # The shader reads the traced states and hits where the kernel wrote them
+    # (it reads columns 1-7 of a state, and the hits only of disk rays).
+    status, states, hit_r, hit_p, hit_m, steps = _trace_shader_device(
+        spacetime, s0, settings, escape, disk_radii,
+        interior["stop"] if interior else None, precision)
     cfg = _lib.RealtimeShading(
         mass=1.0, spin=float(settings.spin), disk_inner=t_inner, disk_outer=float(outer),
         disk_temperature=float(settings.disk_temperature),
@@ -294,10 +299,15 @@ def render_frame_device(settings: RenderSettings, camera, width: int, height: in
     bb_dev = torch.as_tensor(blackbody, device=dev).contiguous()
     rgb = torch.empty((height, width, 3), dtype=torch.uint8, device=dev)
     _lib.check(_lib.load().bh_realtime_shade(
-        cfg, ptr(res.status.to(torch.int32).contiguous()), ptr(states),
-        ptr(hit_p.contiguous()), ptr(hit_m.contiguous()), width, height, ptr(t_dev),
+        cfg, ptr(status), ptr(states), ptr(hit_p), ptr(hit_m), width, height, ptr(t_dev),
         ptr(bb_dev), ptr(rgb), stream_handle()), "realtime shade")
     if return_rays:
+        disk = disk_radii is not None
+        res = ReferenceResult(status=status, positions=states[:, 1:4].contiguous(),
+                              momenta=states[:, 4:8].contiguous(),
+                              hit_radii=hit_r if disk else None,
+                              hit_positions=hit_p if disk else None,
+                              hit_momenta=hit_m if disk else None, steps=steps)
         shading = {k: getattr(cfg, k) for k, _ in _lib.RealtimeShading._fields_}
         shading.update(temperature=temperature, blackbody=blackbody, states=states,
                        hit_positions=hit_p, hit_momenta=hit_m)
