@@ -169,7 +169,8 @@ def propagate(spacetime, state0: Array, n_steps: int, rtol: float = 1e-8,
               max_step: float = 2.0, precision: str = "fp64", spins=None,
               h0: Array | None = None, layout: str = "aos",
               timeout_s: float = 0.0, variant: int = -1, workspace=None,
-              in_place: bool = False, project_every: int = 0):
+              in_place: bool = False, project_every: int = 0, out=None,
+              chunks: int = 4):
     """n_steps attempted DP5(4) steps per ray with per-ray accept/reject and
     step update (tracer.py:111-120), no termination.
 
@@ -178,7 +179,22 @@ def propagate(spacetime, state0: Array, n_steps: int, rtol: float = 1e-8,
     ``spins`` (n,) gives each ray its own spin.  With ``in_place`` and a
     device float64 ``state0`` the states are advanced in place.
     ``project_every`` K > 0 projects every ray onto the null constraint in
-    float64 after every K-th attempt (not in the reference; off by default)."""
+    float64 after every K-th attempt (not in the reference; off by default).
+
+    Streaming from host memory: with ``state0`` (and ``spins``, if given) a
+    float64 CPU tensor in pinned memory and ``out`` a pinned (n, 8) float64
+    CPU tensor, the rays go through in ``chunks`` contiguous pieces on two
+    CUDA streams, each piece's host-to-device copy, kernel and device-to-host
+    copy of its final states overlapping the other pieces' work.  The final
+    states land in ``out`` (returned); h, lam and accepted stay on the device.
+    Results equal the single-launch path's."""
+    if out is not None:
+        if h0 is not None or layout != "aos" or in_place:
+            raise ValueError("streaming from host memory takes neither h0, layout 'soa' "
+                             "nor in_place")
+        return _propagate_streamed(spacetime, state0, n_steps, rtol, atol, initial_step,
+                                   max_step, precision, spins, timeout_s, variant,
+                                   project_every, out, chunks)
     s, host = to_device_f64(state0, "state0")
     n = s.shape[0] if layout == "aos" else s.shape[-1]
     if layout == "aos" and (s.dim() != 2 or s.shape[1] != 8):
@@ -221,3 +237,62 @@ def propagate(spacetime, state0: Array, n_steps: int, rtol: float = 1e-8,
     return (out_like(states, host, state0), out_like(h, host, state0),
             out_like(lam, host, state0),
             acc.cpu().numpy() if host is not None else acc, stats)
+
+
+def _propagate_streamed(spacetime, state0, n_steps, rtol, atol, initial_step, max_step,
+                        precision, spins, timeout_s, variant, project_every, out, chunks):
+    def pinned_f64(t, name, shape):
+        if not (torch.is_tensor(t) and not t.is_cuda and t.is_pinned()
+                and t.dtype == torch.float64 and t.is_contiguous() and tuple(t.shape) == shape):
+            raise ValueError(f"{name} must be a contiguous pinned float64 CPU tensor of "
+                             f"shape {shape}")
+
+    n = int(state0.shape[0]) if torch.is_tensor(state0) else -1
+    pinned_f64(state0, "state0", (n, 8))
+    pinned_f64(out, "out", (n, 8))
+    if spins is not None:
+        pinned_f64(spins, "spins", (n,))
+        if bool((spins.abs() > spacetime.mass).any()):
+            raise ValueError("Kerr bound violated: |spin| must be <= mass")
+    if int(chunks) < 1:
+        raise ValueError("chunks must be >= 1")
+    dev = torch.device("cuda", torch.cuda.current_device())
+    lib = _lib.load()
+    states = torch.empty((n, 8), dtype=torch.float64, device=dev)
+    h = torch.full((n,), float(initial_step), dtype=torch.float64, device=dev)
+    lam = torch.zeros(n, dtype=torch.float64, device=dev)
+    acc = torch.empty(n, dtype=torch.int64, device=dev)
+    spin_d = None if spins is None else torch.empty(n, dtype=torch.float64, device=dev)
+    k = max(1, min(int(chunks), n))
+    bounds = [(n * c // k, n * (c + 1) // k) for c in range(k)]
+    ws = [torch.empty(lib.bh_trace_workspace_bytes(), dtype=torch.uint8, device=dev)
+          for _ in range(k)]
+    cfg = make_config(1, rtol, atol, initial_step, max_step, 0.0, precision, "aos", timeout_s,
+                      variant, 0, project_every)
+    main = torch.cuda.current_stream(dev)
+    streams = [torch.cuda.Stream(dev), torch.cuda.Stream(dev)]
+    for st in streams:
+        st.wait_stream(main)  # h and lam are initialised on the main stream
+    for c, (a, b) in enumerate(bounds):
+        st = streams[c % 2]
+        with torch.cuda.stream(st):
+            states[a:b].copy_(state0[a:b], non_blocking=True)
+            if spin_d is not None:
+                spin_d[a:b].copy_(spins[a:b], non_blocking=True)
+            _lib.check(lib.bh_propagate(cfg, float(spacetime.mass), float(spacetime.spin),
+                                        ptr(None if spin_d is None else spin_d[a:b]),
+                                        ptr(states[a:b]), ptr(h[a:b]), ptr(lam[a:b]),
+                                        ptr(acc[a:b]), b - a, int(n_steps), ptr(ws[c]),
+                                        st.cuda_stream), "propagate")
+            out[a:b].copy_(states[a:b], non_blocking=True)
+    for st in streams:
+        main.wait_stream(st)
+    stats = _lib.TraceStats()
+    for c in range(k):
+        part = _lib.TraceStats()
+        _lib.check(lib.bh_trace_stats_read(ptr(ws[c]), part, stream_handle()), "propagate")
+        stats.attempts += part.attempts
+        stats.accepted += part.accepted
+        stats.iterations = max(stats.iterations, part.iterations)
+        stats.timed_out = stats.timed_out or part.timed_out
+    return out, h, lam, acc, stats

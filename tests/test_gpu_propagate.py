@@ -106,3 +106,27 @@ def test_mixed_variants_agree(cuda, variant):
     assert np.median(err) <= 1e-6
     assert np.quantile(err, 0.9) <= 1e-5
     assert np.quantile(err, 0.99) <= 1e-4
+
+
+def test_streamed_from_host_memory_equals_device_path(cuda):
+    """propagate with pinned host input and output buffers streams the rays
+    through in pieces on two streams; the results equal the single launch."""
+    import bench
+    from blackhorizon_b200.integrators import propagate
+    from blackhorizon_b200.kerr import KerrSpacetime
+
+    state0, spins, _, _, _ = bench.make_inputs(50_000, 0, torch.device("cuda", 0))
+    st = KerrSpacetime(1.0, 0.0)
+    for precision in ("mixed", "fp64"):
+        ref = propagate(st, state0, 150, precision=precision, spins=spins)
+        host_s = state0.cpu().pin_memory()
+        host_sp = spins.cpu().pin_memory()
+        out = torch.empty_like(host_s).pin_memory()
+        got = propagate(st, host_s, 150, precision=precision, spins=host_sp, out=out, chunks=3)
+        assert got[0] is out
+        assert torch.equal(out, ref[0].cpu())
+        for k in (1, 2, 3):
+            assert torch.equal(got[k], ref[k])
+        assert got[4].attempts == ref[4].attempts and got[4].iterations == ref[4].iterations
+    with pytest.raises(ValueError):
+        propagate(st, state0.cpu(), 10, out=torch.empty(state0.shape, dtype=torch.float64))
