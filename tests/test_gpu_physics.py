@@ -200,3 +200,36 @@ def test_tracer_conservation_small_frame(cuda, precision, h_tol, lz_tol):
     _, lz = conserved_quantities(res.states)
     assert float(ham.abs().max()) <= h_tol
     assert float((lz - lz0)[esc].abs().max()) <= lz_tol
+
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_full_hd_frame_edges_on_the_critical_curve(cuda, precision):
+    """The 1920x1080 frame (a = 0.9, inclination 80 deg, fov 25, rtol 1e-9):
+    along seven rows across the shadow (heights -0.85 .. 0.85 of its half
+    height) and down the column through its middle, the traced capture
+    boundary lies where the photons' constants cross the general critical
+    curve of spherical photon orbits (Bardeen 1973): the impact parameter
+    sqrt(eta + xi^2) at the traced edge (midway between the last captured and
+    the first escaped pixel) is within 0.5 % of the analytic edge's, and the
+    two edges are within two pixels.  The prograde and retrograde edges are
+    the two ends of the middle row."""
+    from blackhorizon_b200 import trace_rays
+    from blackhorizon_b200.camera import PinholeCamera
+    from blackhorizon_b200.kerr import KerrSpacetime
+    from blackhorizon_b200.workloads import SHADOW_FULL_HD as C
+
+    st = KerrSpacetime(1.0, C.spin)
+    cam = PinholeCamera.from_orbit(C.distance, C.inclination, fov_degrees=C.fov,
+                                   width=C.width, height=C.height)
+    res = trace_rays(st, cam.initial_states(st), C.escape_radius, max_steps=C.max_steps,
+                     rtol=C.rtol, atol=C.atol, capture_margin=C.capture_margin,
+                     precision=precision)
+    from oracle import bardeen
+
+    checks = bardeen.frame_edges_against_curve(cam, C.spin, res.status.cpu().numpy())
+    worst = max(c["relative"] for c in checks)
+    print(f"{precision}: {len(checks)} edges, worst impact-parameter difference {worst:.2e}")
+    for c in checks:
+        assert abs(c["traced"] - c["analytic"]) <= 2.0, c
+        assert c["relative"] <= 5e-3, c
