@@ -49,7 +49,7 @@ class TraceConfig(ctypes.Structure):
                 ("initial_step", _D), ("max_step", _D), ("min_step", _D),
                 ("precision", _I32), ("layout", _I32), ("timeout_ns", _I64),
                 ("variant", _I32), ("blocks_per_sm", _I32), ("project_every", _I32),
-                ("flags", _I32)]
+                ("flags", _I32), ("reserved", _I32), ("f64_radius", _D)]
 
 
 class TraceStats(ctypes.Structure):
@@ -112,6 +112,7 @@ _SIGNATURES = {
     "bh_dp5_step": (ctypes.c_int, [_D, _D, _P, _P, _P, _P, _I64, _I32, _P]),
     "bh_error_ratio": (ctypes.c_int, [_P, _P, _P, _D, _D, _P, _I64, _P]),
     "bh_step_factor": (ctypes.c_int, [_P, _P, _I64, _P]),
+    "bh_device_math": (ctypes.c_int, [_I32, _P, _P, _I64, _P]),
     "bh_rk4": (ctypes.c_int, [_D, _D, _P, _P, _P, _I64, _I64, _I32, _P]),
     "bh_implicit_midpoint": (ctypes.c_int, [_D, _D, _P, _P, _P, _I64, _I32, _I64, _P]),
     "bh_trace_variant_count": (ctypes.c_int, [_I32]),

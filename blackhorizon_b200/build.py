@@ -16,6 +16,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -53,35 +54,45 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(d) <= t for d in _deps())
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and up_to_date():
+def build(force: bool = False, verbose: bool = False, defines=(), out: str = LIB) -> str:
+    """Compile and link the library to `out`; `defines` are extra
+    preprocessor definitions (NAME or NAME=VALUE)."""
+    if not force and not defines and out == LIB and up_to_date():
         return LIB
     os.makedirs(BUILD, exist_ok=True)
     cc = nvcc()
+    extra = [f"-D{d}" for d in defines]
+
+    def compile_one(src):
+        obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
+        cmd = [cc, *ARCH, *FLAGS, *extra, "-I", os.path.join(ROOT, "include"), "-c", src,
+               "-o", obj]
+        return obj, cmd, subprocess.run(cmd, capture_output=True, text=True)
+
+    # The translation units are independent: compile them in parallel.
+    with ThreadPoolExecutor(max_workers=max(1, min(len(sources()), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(compile_one, sources()))
     objs = []
     log = []
-    for src in sources():
-        obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
-        cmd = [cc, *ARCH, *FLAGS, "-I", os.path.join(ROOT, "include"), "-c", src, "-o", obj]
-        res = subprocess.run(cmd, capture_output=True, text=True)
+    for obj, cmd, res in results:
         log.append(" ".join(cmd) + "\n" + res.stdout + res.stderr)
         if res.returncode != 0:
             sys.stderr.write(res.stdout + res.stderr)
-            raise RuntimeError(f"nvcc failed on {src}")
+            raise RuntimeError(f"nvcc failed on {cmd[-3]}")
         objs.append(obj)
-    tmp = LIB + ".tmp"
+    tmp = out + ".tmp"
     cmd = [cc, *ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs]
     res = subprocess.run(cmd, capture_output=True, text=True)
     log.append(" ".join(cmd) + "\n" + res.stdout + res.stderr)
     if res.returncode != 0:
         sys.stderr.write(res.stdout + res.stderr)
         raise RuntimeError("nvcc link failed")
-    os.replace(tmp, LIB)
+    os.replace(tmp, out)
     with open(os.path.join(BUILD, "ptxas.log"), "w") as f:
         f.write("\n".join(log))
     if verbose:
         print("\n".join(log))
-    return LIB
+    return out
 
 
 if __name__ == "__main__":

@@ -219,6 +219,14 @@ __global__ void step_factor_kernel(const double *ratio, double *out, long long n
     out[i] = step_factor(ratio[i]);
 }
 
+// The device arithmetic that bh_device_math exposes point-wise.
+__global__ void device_math_kernel(int op, const double *x, double *out, long long n) {
+    const long long i = tid();
+    if (i >= n) return;
+    const double v = x[i];
+    out[i] = op == 0 ? rcp_f64(v) : op == 1 ? rsqrt_f64(v) : step_factor_r2(v);
+}
+
 // rk4_step (integrators.py:57-73) n_steps times with the state in registers;
 // stage arithmetic in the lane type V, the state update in double.
 template <typename V>
@@ -324,6 +332,16 @@ static int config_ok(const bh_trace_config *c) {
     if (c->timeout_ns < 0) return invalid("timeout_ns must be >= 0");
     if (c->project_every < 0) return invalid("project_every must be >= 0");
     if (c->flags != 0) return invalid("config flags are accepted by bh_trace_tile only");
+    if (c->reserved != 0) return invalid("config reserved field must be 0");
+    if (!(c->f64_radius == c->f64_radius)) return invalid("f64_radius must not be NaN");
+    return BH_OK;
+}
+
+// Trace-family calls (everything but bh_propagate) take no float64 band.
+static int trace_config_ok(const bh_trace_config *c) {
+    int rc = config_ok(c);
+    if (rc != BH_OK) return rc;
+    if (c->f64_radius != 0.0) return invalid("f64_radius is accepted by bh_propagate only");
     return BH_OK;
 }
 
@@ -354,7 +372,7 @@ int bh_trace_with_tape(const bh_trace_config *config, const bh_scene *scene,
                        const double *state0, double *states, int32_t *status,
                        int64_t *steps, int64_t n, void *workspace, void *stream,
                        double *h_tape, double *ckpt, int64_t tape_cap, int ckpt_every) {
-    int rc = config_ok(config);
+    int rc = trace_config_ok(config);
     if (rc != BH_OK) return rc;
     if (h_tape && config->project_every > 0)
         return invalid("a taped trace cannot project: the adjoint replays unprojected steps");
@@ -522,6 +540,15 @@ int bh_step_factor(const double *ratio, double *factor, int64_t n, void *stream)
     return cuda_status(cudaGetLastError(), "bh_step_factor launch");
 }
 
+int bh_device_math(int32_t op, const double *x, double *y, int64_t n, void *stream) {
+    if (op < 0 || op > 2) return invalid("op must be 0 (rcp), 1 (rsqrt) or 2 (step factor of r^2)");
+    if (n < 0) return invalid("n must be >= 0");
+    if (n == 0) return BH_OK;
+    if (!x || !y) return invalid("NULL pointer argument");
+    device_math_kernel<<<grid_for(n), kBlock, 0, (cudaStream_t)stream>>>(op, x, y, n);
+    return cuda_status(cudaGetLastError(), "bh_device_math launch");
+}
+
 int bh_rk4(double mass, double spin, const double *state, const double *h,
            double *new_state, int64_t n, int64_t n_steps, int32_t precision,
            void *stream) {
@@ -625,7 +652,7 @@ int bh_trace_cameras(const bh_trace_config *config, int32_t ncameras,
                      int64_t n_rays, double *states, int32_t *status,
                      int64_t *steps, void *workspace, size_t workspace_bytes,
                      void *stream) {
-    int rc = config_ok(config);
+    int rc = trace_config_ok(config);
     if (rc != BH_OK) return rc;
     if (ncameras < 1) return invalid("need at least one camera");
     if (n_rays < 0) return invalid("n_rays must be >= 0");
@@ -691,6 +718,8 @@ int bh_propagate(const bh_trace_config *config, double mass, double spin,
                  void *workspace, void *stream) {
     int rc = config_ok(config);
     if (rc != BH_OK) return rc;
+    if (config->f64_radius != 0.0 && config->project_every > 0)
+        return invalid("f64_radius and project_every cannot be combined");
     if (!(mass > 0.0)) return invalid("mass must be positive");
     if (!spin_of_ray && !kerr_ok(mass, spin)) return invalid("Kerr bound violated");
     if (n < 0 || n_steps < 0) return invalid("n and n_steps must be >= 0");
@@ -705,6 +734,15 @@ int bh_propagate(const bh_trace_config *config, double mass, double spin,
     if (config->layout == BH_LAYOUT_AOS && !aligned(states, 16))
         return invalid("state buffers must be 16-byte aligned");
     TraceArgs a = base_args(config);
+    if (config->precision == BH_PRECISION_MIXED && config->f64_radius != 0.0) {
+        // 8 u M / rtol: the radius where float32 rounding of the curvature
+        // terms (about 4 u of their relative size 2 M / r) reaches rtol.
+        const double radius = config->f64_radius > 0.0
+                                  ? config->f64_radius
+                                  : (config->rtol > 0.0 ? 8.0 * 0x1p-24 * mass / config->rtol
+                                                        : 1e150);
+        a.f64_r2 = fmin(radius, 1e150) * fmin(radius, 1e150);
+    }
     a.state0 = states;
     a.states = states;
     a.mass = mass;
@@ -838,7 +876,7 @@ extern "C" int bh_trace_cameras_noalloc(const bh_trace_config *config,
                                         int32_t ncameras, double *states,
                                         int32_t *status, int64_t *steps,
                                         bh_trace_stats *stats, void *stream) {
-    int rc = config_ok(config);
+    int rc = trace_config_ok(config);
     if (rc != BH_OK) return rc;
     if (ncameras < 1 || !cameras) return invalid("need at least one camera");
     if (ncameras > kNoAllocMaxCameras) {

@@ -30,6 +30,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 namespace bh {
@@ -66,8 +67,13 @@ __device__ __forceinline__ float lg2_approx(float x) {
 }
 
 // Reciprocal and reciprocal square root of the stage arithmetic.  float32:
-// one MUFU instruction (<= 2 ulp).  float64: the MUFU seed refined by two
-// Newton steps on the FP64 pipe (<= 2 ulp, no IEEE slow path).
+// one MUFU instruction (<= 2 ulp).  float64: the MUFU seed (about 23 correct
+// bits) refined by two Newton-Raphson steps on the FP64 pipe, each of which
+// roughly doubles the correct bits: r <- r + r (1 - x r) for 1/x and
+// r <- r (3 - x r^2) / 2 for 1/sqrt(x), the residual formed with a fused
+// multiply-add.  Within 2 ulp of the correctly rounded result for normal
+// inputs (bh_device_math exposes both for that check), with no IEEE slow
+// path.
 __device__ __forceinline__ double rcp_f64(double x) {
     double r;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
@@ -647,22 +653,47 @@ __device__ __forceinline__ StageV<V> first_stage(const KerrV<V> &K, const WState
     return rhs_v<V>(K, yw.x, yw.y, yw.z, yw.npt, yw.px, yw.py, yw.pz, zero, zero, zero);
 }
 
+// first_stage that also returns the evaluation's r^2 when r2 is not null.
+template <class V>
+__device__ __forceinline__ StageV<V> first_stage_r2(const KerrV<V> &K, const WStateV<V> &yw,
+                                                    V *r2) {
+    using T = VT<V>;
+    const V zero = T::set(0.0);
+    return rhs_v<V>(K, yw.x, yw.y, yw.z, yw.npt, yw.px, yw.py, yw.pz, zero, zero, zero, r2);
+}
+
+// Type of the controller's error ratio.  float64 lanes: the ratio r.  Mixed
+// lanes: r^2, in float64 (BH_MIXED_NORM_F64 = 1, the default: the sum of
+// squares, the accept test and the step factor in float64) or, built with
+// BH_MIXED_NORM_F64 = 0, in float32 (the sum of squares in float32 and the
+// factor through float32 exp2/log2; kept to measure the float64 controller
+// against).
+#ifndef BH_MIXED_NORM_F64
+#define BH_MIXED_NORM_F64 1
+#endif
+template <class V>
+using RatioT = typename std::conditional<sizeof(typename VT<V>::S) == 8 || BH_MIXED_NORM_F64 != 0,
+                                         double, float>::type;
+
 // error_ratio (integrators.py:110-117) per lane: RMS over all 8 components of
 // h err / (atol + rtol max(|y|, |y_new|)), non-finite -> +inf, NumPy's
 // pairwise summation order.  The p_t term is exactly zero (p_t is conserved)
 // and is counted in the mean.  float64 policy: every operation in double.
 // Mixed policy: the error is a float32 combination of float32 stage
-// derivatives, so the scales and quotients are float32 too and the scale
-// reciprocal is one MUFU instruction (a float64 norm of float32 data would
-// add cost, not accuracy); each scale is at least the rounding floor
-// kMixedNoise |increment|.  The value written per lane is what the
-// controller compares with 1: the ratio r (double) for the float64 policy,
-// its square r^2 (float: the mean of squares, summed in float32) for the
-// mixed one, whose accept test r^2 <= 1 and step factor (next_step<false>)
-// need no square root and no conversion.  Non-finite values become +inf.
+// derivatives; its scales and quotients err_i / scale_i are float32 (the
+// scale reciprocal is one MUFU instruction), each scale at least the
+// rounding floor kMixedNoise |increment|.  The quotients are then converted
+// once and the mean of squares h^2 sum q_i^2 / 8 is summed in float64 with
+// the lane's float64 step size h (the squares of float32 values are exact in
+// float64).  The value written per lane is what the controller compares with
+// 1: the ratio r for the float64 policy, its square r^2 for the mixed one,
+// whose accept test r^2 <= 1 decides as r <= 1 does (the square root is
+// monotone) and whose step factor (next_step<false>) takes r^2 directly.
+// Non-finite values become +inf.
 template <class V>
 __device__ __forceinline__ void error_ratio_v(const WStateV<V> &y, const AttemptV<V> &a,
-                                              V hw, V rt, V at, typename VT<V>::S ratio[VT<V>::N]) {
+                                              V hw, V rt, V at, RatioT<V> ratio[VT<V>::N],
+                                              const double *hd) {
     using T = VT<V>;
     const WStateV<V> &yn = a.ynw;
     const V *err = a.err;
@@ -698,7 +729,21 @@ __device__ __forceinline__ void error_ratio_v(const WStateV<V> &y, const Attempt
             q[i] = err[i] * T::rcp(sc);
         }
     }
-    if constexpr (sizeof(typename T::S) == 4) {
+    if constexpr (sizeof(typename T::S) == 4 && sizeof(RatioT<V>) == 8) {
+        // Components t x y z | p_t(=0) px py pz: r^2 = h^2 sum q^2 / 8 in
+        // float64, the squares summed pairwise by fused multiply-adds.
+#pragma unroll
+        for (int l = 0; l < T::N; ++l) {
+            double g[7];
+#pragma unroll
+            for (int i = 0; i < 7; ++i) g[i] = double(T::get(q[i], l));
+            const double s01 = fma(g[1], g[1], g[0] * g[0]);
+            const double s23 = fma(g[3], g[3], g[2] * g[2]);
+            const double s456 = fma(g[6], g[6], fma(g[5], g[5], g[4] * g[4]));
+            const double r2 = ((s01 + s23) + s456) * ((hd[l] * hd[l]) * 0.125);
+            ratio[l] = isfinite(r2) ? r2 : __longlong_as_double(0x7ff0000000000000LL);
+        }
+    } else if constexpr (sizeof(typename T::S) == 4) {
         // Components t x y z | p_t(=0) px py pz: r^2 = h^2 sum q^2 / 8, the
         // squares summed pairwise by fused multiply-adds.
         const V s01 = T::fma(q[1], q[1], q[0] * q[0]);
@@ -818,17 +863,39 @@ __device__ __forceinline__ double step_factor(double ratio) {
     return np_min(np_max(f, 0.2), 5.0);
 }
 
+// Step factor of the mixed policy from r^2, in float64:
+// clip(0.9 (r^2)^-0.1, 0.2, 5), which equals step_factor(r).  y = x^-0.1 is
+// one Newton-Raphson step on phi(y) = y^-10 - x, y <- y (1 + (1 - x y^10)/10),
+// from the float32 seed exp2(-0.1 log2 x) (two MUFU instructions, relative
+// error below 1e-6); the iteration converges quadratically with constant
+// 11/2, so the result is within 1e-11 of x^-0.1 (relative).  x is clamped to
+// [1e-12, 1e12] before the seed: outside [0.18^10, 4.5^10] the clip decides
+// the factor, so the clamp changes no result.  r^2 is >= 0 or +inf, never NaN.
+__device__ __forceinline__ double step_factor_r2(double r2) {
+    const double x = fmin(fmax(r2, 1e-12), 1e12);
+    const float xs = float(x);
+    double y = double(ex2_approx(-0.1f * lg2_approx(xs)));
+    const double y2 = y * y;
+    const double y4 = y2 * y2;
+    const double y10 = (y4 * y4) * y2;
+    y = fma(y * 0.1, fma(-x, y10, 1.0), y);
+    return fmin(fmax(0.9 * y, 0.2), 5.0);
+}
+
 // The controller's next step size (tracer.py:113-120): clip(h factor, 0,
 // max_step) after accept and reject alike.  The float64 policy passes r and
-// keeps the reference's forms.  The mixed policy passes r^2 (error_ratio_v)
-// and takes the factor 0.9 (r^2)^-0.1 through float32 exp2/log2 (only the
-// step heuristic uses it); its r^2 is >= 0 or +inf, never NaN, so the factor
-// is finite and plain maxima and minima give the values NumPy's
-// NaN-propagating ones would, with fewer instructions.
+// keeps the reference's forms.  The mixed policy passes r^2 (error_ratio_v):
+// in float64 (RatioT = double) the factor is step_factor_r2; the float32
+// controller kept for measurement takes 0.9 (r^2)^-0.1 through float32
+// exp2/log2.  r^2 is >= 0 or +inf, never NaN, so the factor is finite and
+// plain maxima and minima give the values NumPy's NaN-propagating ones
+// would, with fewer instructions.
 template <bool F64, typename R>
 __device__ __forceinline__ double next_step(double h, R ratio, double max_step) {
     if constexpr (F64) {
         return np_min(np_max(h * step_factor(ratio), 0.0), max_step);
+    } else if constexpr (sizeof(R) == 8) {
+        return fmin(fmax(h * step_factor_r2(ratio), 0.0), max_step);
     } else {
         const float sf = fminf(fmaxf(ratio, 1e-32f), 3.0e38f);
         const double f = double(0.9f * ex2_approx(-0.1f * lg2_approx(sf)));

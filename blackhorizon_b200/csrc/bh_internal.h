@@ -31,6 +31,9 @@ struct CameraDev {
     long long first_ray;
     double mass, spin, capture_radius, escape_radius;
 };
+// The camera tables' sizes (bh_trace_cameras_workspace_bytes and the static
+// table of bh_trace_cameras_noalloc) are stated in bytes per camera.
+static_assert(sizeof(CameraDev) == 168, "camera record is 168 bytes");
 
 struct TraceArgs {
     // ray source: states (source == 0) or cameras (source == 1)
@@ -55,6 +58,10 @@ struct TraceArgs {
     long long max_attempts;  // trace: 4 * max_steps; propagate: n_steps
     long long timeout_ns;
     int project_every;       // null-constraint projection period (iterations); 0 = off
+    // Mixed propagate: squared radius of the float64 band; an attempt runs
+    // float64 stage arithmetic for the whole warp while one of its rays lies
+    // at r_+ < r < sqrt(f64_r2).  0 = no band.
+    double f64_r2;
     TraceWorkspace *ws;
     // optional tape of the accepted steps (trace only): step sizes
     // (n x tape_cap) and float64 states before every ckpt_every-th accepted

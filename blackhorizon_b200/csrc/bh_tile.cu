@@ -339,14 +339,14 @@ __global__ void __launch_bounds__(BLOCK, MINB) tile_kernel(const TileArgs args) 
             for (int l = 0; l < N; ++l) T::put(hw, l, typename T::S(h[l]));
             AttemptV<V> a;
             dp5_attempt<V>(K, yw, hw, k1, a);
-            typename T::S ratio[N];
-            error_ratio_v<V>(yw, a, hw, rt, at, ratio);
+            RatioT<V> ratio[N];
+            error_ratio_v<V>(yw, a, hw, rt, at, ratio, h);
             bool acc[N];
 #pragma unroll
             for (int l = 0; l < N; ++l) {
                 acc[l] = false;
                 if (ray[l] < 0) continue;
-                acc[l] = ratio[l] <= typename T::S(1);
+                acc[l] = ratio[l] <= RatioT<V>(1);
                 ++attempts[l];
                 const double h_next =
                     next_step<F64>(h[l], ratio[l], args.max_step);
@@ -701,6 +701,8 @@ extern "C" int bh_trace_tile(const bh_trace_config *config, const bh_scene *scen
         return tile_invalid("max_steps must be in [1, 2^60]");
     if (c.timeout_ns < 0) return tile_invalid("timeout_ns must be >= 0");
     if (c.flags & ~BH_TRACE_INTERIOR) return tile_invalid("unknown config flags");
+    if (c.reserved != 0) return tile_invalid("config reserved field must be 0");
+    if (c.f64_radius != 0.0) return tile_invalid("f64_radius is accepted by bh_propagate only");
     if ((c.flags & BH_TRACE_INTERIOR) && !(scene->capture_radius > 0.0))
         return tile_invalid("an interior camera needs a stop radius > 0");
     if (!(scene->mass > 0.0) || !(std::fabs(scene->spin) <= scene->mass))

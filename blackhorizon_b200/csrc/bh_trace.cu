@@ -147,14 +147,14 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args
             for (int l = 0; l < N; ++l) T::put(hw, l, typename T::S(h[l]));
             AttemptV<V> a;
             dp5_attempt<V>(K, yw, hw, k1, a);
-            typename T::S ratio[N];
-            error_ratio_v<V>(yw, a, hw, rt, at, ratio);
+            RatioT<V> ratio[N];
+            error_ratio_v<V>(yw, a, hw, rt, at, ratio, h);
             bool acc[N];
 #pragma unroll
             for (int l = 0; l < N; ++l) {
                 acc[l] = false;
                 if (ray[l] < 0) continue;
-                acc[l] = ratio[l] <= typename T::S(1);
+                acc[l] = ratio[l] <= RatioT<V>(1);
                 ++attempts[l];
                 RayState yl = ys.get(l);
                 if (acc[l] && args.h_tape) {
@@ -258,17 +258,59 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args
     }
 }
 
+// One float64 DP5(4) attempt with the float64 policy's controller, for one
+// ray of a mixed thread: the float64 band of propagate_kernel.  p points at
+// the ray's float64 state in the block's state store (P doubles between
+// components); the state is updated there when the attempt is accepted.
+// The first-same-as-last derivative is evaluated afresh in float64 (the
+// float path keeps its own).  Not inlined: the band is the rare path, and
+// one out-of-line copy keeps the float loop's code compact.
+struct BandStep {
+    double h;       // the controller's next step size
+    bool accepted;
+};
+template <int P>
+__device__ __noinline__ BandStep band_attempt(double *p, double mass, double spin, double h,
+                                              double rtol, double atol, double max_step) {
+    RayState y{p[0], p[P], p[2 * P], p[3 * P], p[4 * P], p[5 * P], p[6 * P], p[7 * P]};
+    const KerrV<double> K = make_kerr<double>(mass, spin);
+    WStateV<double> w;
+    put_work<double>(w, 0, y);
+    const StageV<double> k1 = first_stage<double>(K, w);
+    AttemptV<double> a;
+    dp5_attempt<double>(K, w, h, k1, a);
+    double ratio[1];
+    const double hl[1] = {h};
+    error_ratio_v<double>(w, a, h, rtol, atol, ratio, hl);
+    const bool ok = ratio[0] <= 1.0;
+    if (ok) {
+        commit<double>(y, w, a, 0, h);
+        p[0] = y.t; p[P] = y.x; p[2 * P] = y.y; p[3 * P] = y.z;
+        p[5 * P] = y.px; p[6 * P] = y.py; p[7 * P] = y.pz;
+    }
+    return BandStep{next_step<true>(h, ratio[0], max_step), ok};
+}
+
 // n_steps attempted DP5(4) steps per ray with the tracer's accept/reject and
 // step update (tracer.py:111-120) and no termination.  Each warp claims 32
 // groups of N rays at a time from the workspace's queue head, so warps that
 // the scheduler runs ahead take more groups and all of them stay resident
 // until the queue drains (a fixed grid-stride split left a quarter of the
 // warp slots idle while the slowest warps finished).
-template <class V, int BLOCK, int MINB, bool PROJECT>
+//
+// BAND (mixed lanes only): while one of the warp's rays lies between the
+// outer horizon and the band radius (args.f64_r2), the whole warp's attempt
+// runs in float64 (band_attempt, the float64 policy's step); outside it the
+// float stages run.  The test reads r^2 at each ray's current state from its
+// last derivative evaluation, and is warp-uniform, so the two paths never
+// diverge within a warp.  Inside the horizon the float stages run: the
+// reference's tracer captures such rays.
+template <class V, int BLOCK, int MINB, bool PROJECT, bool BAND = false>
 __global__ void __launch_bounds__(BLOCK, MINB) propagate_kernel(const TraceArgs args) {
     using T = VT<V>;
     constexpr int N = T::N;
     constexpr bool F64 = sizeof(typename T::S) == 8;
+    static_assert(!(BAND && F64), "the float64 band is a mixed-policy option");
     TraceWorkspace *ws = args.ws;
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -289,6 +331,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) propagate_kernel(const TraceArgs 
         base = __shfl_sync(full, base, 0);
         if ((long long)base >= groups) break;
         const long long g = (long long)base + lane;
+        // The lanes that hold a group run the same attempts in lock step;
+        // the band test and the deadline are agreed among them.
+        const unsigned act = __ballot_sync(full, g < groups);
         if (g < groups) {
             double h[N], lam[N], spin[N], mass[N];
             long long acc[N];
@@ -313,30 +358,68 @@ __global__ void __launch_bounds__(BLOCK, MINB) propagate_kernel(const TraceArgs 
             WStateV<V> yw;
 #pragma unroll
             for (int l = 0; l < N; ++l) put_work<V>(yw, l, ys.get(l));
-            StageV<V> k1 = first_stage<V>(K, yw);
+            // r2c: r^2 of each lane's current state from its last derivative
+            // evaluation (BAND only).
+            V r2c = T::set(0.0);
+            StageV<V> k1 = first_stage_r2<V>(K, yw, BAND ? &r2c : nullptr);
+            float rp2[N];  // squared outer-horizon radius per lane (BAND)
+#pragma unroll
+            for (int l = 0; l < N; ++l) {
+                const double rp = mass[l] + ::sqrt(fmax(mass[l] * mass[l] - spin[l] * spin[l], 0.0));
+                rp2[l] = float(rp * rp);
+            }
+            const float band2 = float(args.f64_r2);
             long long k = 0;
             for (; k < args.max_attempts; ++k) {
-                V hw = T::set(0.0);
+                bool in_band = false;
+                if constexpr (BAND) {
+                    bool mine = false;
 #pragma unroll
-                for (int l = 0; l < N; ++l) T::put(hw, l, typename T::S(h[l]));
-                AttemptV<V> a;
-                dp5_attempt<V>(K, yw, hw, k1, a);
-                typename T::S ratio[N];
-                error_ratio_v<V>(yw, a, hw, rt, at, ratio);
-                bool ok[N];
-#pragma unroll
-                for (int l = 0; l < N; ++l) {
-                    ok[l] = ratio[l] <= typename T::S(1);
-                    if (ok[l]) {
-                        RayState yl = ys.get(l);
-                        commit<V>(yl, yw, a, l, h[l]);
-                        ys.set(l, yl);
-                        lam[l] += h[l];
-                        ++acc[l];
+                    for (int l = 0; l < N; ++l) {
+                        const float r2l = T::get(r2c, l);
+                        mine |= r2l > rp2[l] && r2l < band2;
                     }
-                    h[l] = next_step<F64>(h[l], ratio[l], args.max_step);
+                    in_band = __any_sync(act, mine);
                 }
-                take_stage(k1, a.k7, ok);
+                if (in_band) {
+#pragma unroll
+                    for (int l = 0; l < N; ++l) {
+                        const BandStep b = band_attempt<N * BLOCK>(
+                            ys.sh + l * BLOCK + threadIdx.x, mass[l], spin[l], h[l], args.rtol,
+                            args.atol, args.max_step);
+                        if (b.accepted) {
+                            lam[l] += h[l];
+                            ++acc[l];
+                        }
+                        h[l] = b.h;
+                    }
+#pragma unroll
+                    for (int l = 0; l < N; ++l) put_work<V>(yw, l, ys.get(l));
+                    k1 = first_stage_r2<V>(K, yw, &r2c);
+                } else {
+                    V hw = T::set(0.0);
+#pragma unroll
+                    for (int l = 0; l < N; ++l) T::put(hw, l, typename T::S(h[l]));
+                    AttemptV<V> a;
+                    dp5_attempt<V>(K, yw, hw, k1, a);
+                    RatioT<V> ratio[N];
+                    error_ratio_v<V>(yw, a, hw, rt, at, ratio, h);
+                    bool ok[N];
+#pragma unroll
+                    for (int l = 0; l < N; ++l) {
+                        ok[l] = ratio[l] <= RatioT<V>(1);
+                        if (ok[l]) {
+                            RayState yl = ys.get(l);
+                            commit<V>(yl, yw, a, l, h[l]);
+                            ys.set(l, yl);
+                            lam[l] += h[l];
+                            ++acc[l];
+                        }
+                        h[l] = next_step<F64>(h[l], ratio[l], args.max_step);
+                    }
+                    take_stage(k1, a.k7, ok);
+                    if constexpr (BAND) take_lanes(r2c, a.r2n, ok);
+                }
                 if constexpr (PROJECT) {
                     if ((k + 1) % args.project_every == 0) {
                         bool proj[N];
@@ -352,7 +435,16 @@ __global__ void __launch_bounds__(BLOCK, MINB) propagate_kernel(const TraceArgs 
                         take_stage(k1, f, proj);
                     }
                 }
-                if (has_deadline && (k & 63) == 63 && global_timer_ns() > deadline) {
+                if constexpr (BAND) {
+                    // Agreed among the lanes, which keep their attempts in
+                    // lock step for the band test.
+                    if (has_deadline && (k & 63) == 63 &&
+                        __any_sync(act, global_timer_ns() > deadline)) {
+                        late = true;
+                        ++k;
+                        break;
+                    }
+                } else if (has_deadline && (k & 63) == 63 && global_timer_ns() > deadline) {
                     late = true;
                     ++k;
                     break;
@@ -423,9 +515,14 @@ static const void *kfn(bool propagate, size_t *smem) {
 }
 
 // project: the null-constraint projection is compiled for the default launch
-// shapes only (the launcher switches to them).
+// shapes only (the launcher switches to them); so is the float64 band of the
+// mixed propagator (band).
 static const void *kernel_for(bool propagate, int precision, int idx, bool project,
-                              size_t *smem) {
+                              size_t *smem, bool band = false) {
+    if (band && propagate && precision == BH_PRECISION_MIXED) {
+        *smem = StateStore<F2, 128>::shared_bytes();
+        return (const void *)propagate_kernel<F2, 128, 3, false, true>;
+    }
     if (project) {
         if (precision != BH_PRECISION_MIXED) return kfn<double, 256, 2, true>(propagate, smem);
         return propagate ? kfn<F2, 128, 3, true>(propagate, smem)
@@ -472,12 +569,13 @@ int kernel_attributes(bool propagate, int precision, int idx, int *regs,
 static cudaError_t launch(bool propagate, const TraceArgs &args, int precision,
                           int variant, int blocks_per_sm, cudaStream_t stream) {
     const bool project = args.project_every > 0;
-    if (project || variant < 0 || variant >= trace_variant_count(precision))
+    const bool band = propagate && precision == BH_PRECISION_MIXED && args.f64_r2 > 0.0;
+    if (project || band || variant < 0 || variant >= trace_variant_count(precision))
         variant = propagate ? propagate_default_variant(precision)
                             : trace_default_variant(precision);
     const Variant v = trace_variant(precision, variant);
     size_t smem = 0;
-    const void *fn = kernel_for(propagate, precision, variant, project, &smem);
+    const void *fn = kernel_for(propagate, precision, variant, project, &smem, band);
     int dev = 0, sms = 0, occ = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;

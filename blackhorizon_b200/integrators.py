@@ -152,7 +152,10 @@ def make_config(max_steps: int = 1, rtol: float = 1e-9, atol: float = 1e-12,
                 min_step: float = 1e-10, precision: str = "fp64",
                 layout: str = "aos", timeout_s: float = 0.0, variant: int = -1,
                 blocks_per_sm: int = 0, project_every: int = 0,
-                flags: int = 0) -> "_lib.TraceConfig":
+                flags: int = 0, f64_radius: float | str = 0.0) -> "_lib.TraceConfig":
+    """The C ABI's bh_trace_config.  ``f64_radius`` (propagate, mixed
+    policy): radius in units of M of the float64 band, ``"auto"`` for
+    8 u M / rtol (u = 2^-24), 0 for none."""
     if layout not in _lib.LAYOUT:
         raise ValueError("layout must be 'aos' or 'soa'")
     if int(project_every) < 0:
@@ -161,7 +164,18 @@ def make_config(max_steps: int = 1, rtol: float = 1e-9, atol: float = 1e-12,
         int(max_steps), float(rtol), float(atol), float(initial_step),
         float(max_step), float(min_step), _precision_code(precision),
         _lib.LAYOUT[layout], int(max(0.0, timeout_s) * 1e9), int(variant),
-        int(blocks_per_sm), int(project_every), int(flags))
+        int(blocks_per_sm), int(project_every), int(flags), 0, _band_radius(f64_radius))
+
+
+def _band_radius(f64_radius) -> float:
+    if isinstance(f64_radius, str):
+        if f64_radius != "auto":
+            raise ValueError("f64_radius must be a radius >= 0 or 'auto'")
+        return -1.0
+    r = float(f64_radius)
+    if not r >= 0.0:
+        raise ValueError("f64_radius must be a radius >= 0 or 'auto'")
+    return r
 
 
 def propagate(spacetime, state0: Array, n_steps: int, rtol: float = 1e-8,
@@ -170,9 +184,17 @@ def propagate(spacetime, state0: Array, n_steps: int, rtol: float = 1e-8,
               h0: Array | None = None, layout: str = "aos",
               timeout_s: float = 0.0, variant: int = -1, workspace=None,
               in_place: bool = False, project_every: int = 0, out=None,
-              chunks: int = 4):
+              chunks: int = 4, f64_radius: float | str = "auto"):
     """n_steps attempted DP5(4) steps per ray with per-ray accept/reject and
     step update (tracer.py:111-120), no termination.
+
+    Mixed policy: the stage arithmetic runs in float32 except in the float64
+    band: while a ray of a warp lies between the outer horizon and
+    ``f64_radius`` (units of M), the warp's attempt runs in float64 (with the
+    default launch shape).  The default ``"auto"`` puts the band's edge at
+    8 u M / rtol (u = 2^-24), where float32 rounding of the curvature terms
+    reaches the tolerance; 0 runs float32 stages everywhere.  Ignored by the
+    float64 policy and, under ``"auto"``, by projecting calls.
 
     Returns (states, h, lam, accepted, stats): ``lam`` is the affine
     parameter each ray advanced (sum of its accepted step sizes, float64).
@@ -186,15 +208,17 @@ def propagate(spacetime, state0: Array, n_steps: int, rtol: float = 1e-8,
     CPU tensor, the rays go through in ``chunks`` contiguous pieces on two
     CUDA streams, each piece's host-to-device copy, kernel and device-to-host
     copy of its final states overlapping the other pieces' work.  The final
-    states land in ``out`` (returned); h, lam and accepted stay on the device.
-    Results equal the single-launch path's."""
+    states land in ``out`` (returned); h, lam and accepted stay on the device,
+    as every result of a call with torch input does (only NumPy input gets
+    NumPy results back).  The stats sum the pieces' counters.  Results equal
+    the single-launch path's."""
     if out is not None:
         if h0 is not None or layout != "aos" or in_place:
             raise ValueError("streaming from host memory takes neither h0, layout 'soa' "
                              "nor in_place")
         return _propagate_streamed(spacetime, state0, n_steps, rtol, atol, initial_step,
                                    max_step, precision, spins, timeout_s, variant,
-                                   project_every, out, chunks)
+                                   project_every, out, chunks, f64_radius)
     s, host = to_device_f64(state0, "state0")
     n = s.shape[0] if layout == "aos" else s.shape[-1]
     if layout == "aos" and (s.dim() != 2 or s.shape[1] != 8):
@@ -227,7 +251,8 @@ def propagate(spacetime, state0: Array, n_steps: int, rtol: float = 1e-8,
     ws = workspace if workspace is not None else torch.empty(
         lib.bh_trace_workspace_bytes(), dtype=torch.uint8, device=s.device)
     cfg = make_config(1, rtol, atol, initial_step, max_step, 0.0, precision,
-                      layout, timeout_s, variant, 0, project_every)
+                      layout, timeout_s, variant, 0, project_every,
+                      f64_radius=_propagate_band(f64_radius, precision, project_every))
     stream = stream_handle()
     _lib.check(lib.bh_propagate(cfg, float(spacetime.mass), float(spacetime.spin),
                                 ptr(spin_t), ptr(states), ptr(h), ptr(lam), ptr(acc), n,
@@ -239,8 +264,17 @@ def propagate(spacetime, state0: Array, n_steps: int, rtol: float = 1e-8,
             acc.cpu().numpy() if host is not None else acc, stats)
 
 
+def _propagate_band(f64_radius, precision: str, project_every: int):
+    """The band radius a propagate call passes: none for the float64 policy
+    and none by default under projection (the two do not combine)."""
+    if precision != "mixed" or (int(project_every) > 0 and f64_radius == "auto"):
+        return 0.0
+    return f64_radius
+
+
 def _propagate_streamed(spacetime, state0, n_steps, rtol, atol, initial_step, max_step,
-                        precision, spins, timeout_s, variant, project_every, out, chunks):
+                        precision, spins, timeout_s, variant, project_every, out, chunks,
+                        f64_radius="auto"):
     def pinned_f64(t, name, shape):
         if not (torch.is_tensor(t) and not t.is_cuda and t.is_pinned()
                 and t.dtype == torch.float64 and t.is_contiguous() and tuple(t.shape) == shape):
@@ -268,7 +302,8 @@ def _propagate_streamed(spacetime, state0, n_steps, rtol, atol, initial_step, ma
     ws = [torch.empty(lib.bh_trace_workspace_bytes(), dtype=torch.uint8, device=dev)
           for _ in range(k)]
     cfg = make_config(1, rtol, atol, initial_step, max_step, 0.0, precision, "aos", timeout_s,
-                      variant, 0, project_every)
+                      variant, 0, project_every,
+                      f64_radius=_propagate_band(f64_radius, precision, project_every))
     main = torch.cuda.current_stream(dev)
     streams = [torch.cuda.Stream(dev), torch.cuda.Stream(dev)]
     for st in streams:
@@ -295,4 +330,5 @@ def _propagate_streamed(spacetime, state0, n_steps, rtol, atol, initial_step, ma
         stats.accepted += part.accepted
         stats.iterations = max(stats.iterations, part.iterations)
         stats.timed_out = stats.timed_out or part.timed_out
+        stats.bad_rays += part.bad_rays
     return out, h, lam, acc, stats

@@ -24,7 +24,7 @@
 extern "C" {
 #endif
 
-#define BH_ABI_VERSION 3
+#define BH_ABI_VERSION 4
 
 typedef enum {
     BH_OK = 0,
@@ -49,8 +49,9 @@ enum {
 
 typedef enum {
     BH_PRECISION_FP64 = 0,  /* every operation in float64 */
-    BH_PRECISION_MIXED = 1  /* float32 stage arithmetic, float64 state, error norm,
-                               step control and termination radius */
+    BH_PRECISION_MIXED = 1  /* float32 stage arithmetic (float64 inside the
+                               f64_radius band of bh_propagate), float64 state,
+                               error norm, step control and termination radius */
 } bh_precision;
 
 typedef enum {
@@ -94,6 +95,15 @@ typedef struct {
     int32_t project_every; /* Hamiltonian-constraint projection every K controller
                               iterations, 0 = off (the reference never projects) */
     int32_t flags;         /* bh_trace_flag bits; 0 for every call but bh_trace_tile */
+    int32_t reserved;      /* 0 */
+    /* bh_propagate, BH_PRECISION_MIXED: radius (units of M) of the float64
+     * band.  An attempt runs float64 stage arithmetic for every ray of a
+     * warp while one of them lies between the outer horizon and f64_radius;
+     * elsewhere the stages run in float32.  0 = no band; < 0 = 8 u M / rtol
+     * (u = 2^-24), where the float32 rounding of the curvature terms, about
+     * 4 u of their relative size 2 M / r, reaches the tolerance.  Must be 0
+     * for every other call.  Not in the reference (float64 throughout). */
+    double f64_radius;
 } bh_trace_config;
 
 /* Bits of bh_trace_config.flags. */
@@ -174,6 +184,14 @@ int bh_error_ratio(const double *state, const double *new_state,
 /* step_factor (integrators.py:120-124). */
 int bh_step_factor(const double *ratio, double *factor, int64_t n,
                    void *stream);
+
+/* The device arithmetic of the stage and controller code, point-wise, so its
+ * accuracy can be checked against IEEE results: op 0 = the float64
+ * reciprocal (MUFU seed, two Newton-Raphson steps), op 1 = the float64
+ * reciprocal square root (likewise), op 2 = the mixed policy's step factor
+ * clip(0.9 x^-0.1, 0.2, 5) of x = r^2 (float32 seed, one Newton-Raphson
+ * step in float64).  No counterpart in the reference, which calls NumPy. */
+int bh_device_math(int32_t op, const double *x, double *y, int64_t n, void *stream);
 
 /* rk4_step (integrators.py:57-73) with the geodesic RHS, repeated n_steps
  * times in registers with the fixed per-ray step h (n,).  n_steps = 1 is one
@@ -263,7 +281,11 @@ int bh_graph_destroy(bh_graph *graph);
  * cameras is a HOST array.  The call uploads the table, launches, then copies
  * the counters into *stats (may be NULL) and synchronises `stream`; it
  * returns what bh_trace_stats_read would.  The first call on a device looks
- * up the array's device address, so make it before any stream capture.
+ * up the array's device address, so make it before any stream capture.  The
+ * address is kept for the life of the process: after cudaDeviceReset (or any
+ * other reset of the device's primary context) this entry point must not be
+ * called again in that process, since the kept address belongs to the
+ * destroyed context.
  * Every call shares the one array: calls that overlap on the GPU (on
  * different streams or host threads) race and must be serialised by the
  * caller.  Allocates nothing (no cudaMalloc / cudaFree, no heap). */

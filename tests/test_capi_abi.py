@@ -46,6 +46,7 @@ def test_struct_layouts_match_header(tmp_path):
         " offsetof(bh_trace_config, timeout_ns), offsetof(bh_camera, scene),"
         " offsetof(bh_trace_stats, bad_rays));\n"
         'printf("%zu %zu\\n", sizeof(bh_tile_stats), offsetof(bh_tile_stats, rounds));\n'
+        'printf("%zu\\n", offsetof(bh_trace_config, f64_radius));\n'
         "return 0;}\n"
     )
     exe = tmp_path / "probe"
@@ -60,10 +61,11 @@ def test_struct_layouts_match_header(tmp_path):
                     _lib.Camera.scene.offset, _lib.TraceStats.bad_rays.offset]
     tile = [int(v) for v in lines[2].split()]
     assert tile == [ctypes.sizeof(_lib.TileStats), _lib.TileStats.rounds.offset]
+    assert int(lines[3]) == _lib.TraceConfig.f64_radius.offset
 
 
 def test_status_strings(bhlib):
-    assert bhlib.bh_abi_version() == 3
+    assert bhlib.bh_abi_version() == 4
     assert bhlib.bh_status_string(0) == b"ok"
     assert b"escape_radius" in bhlib.bh_status_string(-4)
     assert bhlib.bh_trace_workspace_bytes() == 256
@@ -149,6 +151,42 @@ def test_trace_tile_argument_validation(bhlib):
     # The other tracers take no flags.
     assert bhlib.bh_trace(cfg, scene, None, None, None, None, 1, None, None) == -1
     assert b"flags" in bhlib.bh_last_error()
+
+
+def test_f64_band_config_validation(bhlib):
+    """The float64 band radius belongs to bh_propagate: the tracers reject a
+    nonzero one, and propagate rejects NaN and the band with projection,
+    all before any CUDA call."""
+    import ctypes as C
+
+    from blackhorizon_b200 import _lib
+    from blackhorizon_b200.integrators import make_config
+
+    scene = _lib.Scene(1.0, 0.9, 1.45, 100.0)
+    cfg = make_config(5000, 1e-8, 1e-10, 0.1, 2.0, 1e-10, "mixed", f64_radius=50.0)
+    assert cfg.f64_radius == 50.0
+    assert bhlib.bh_trace(cfg, scene, None, None, None, None, 1, None, None) == -1
+    assert b"f64_radius" in bhlib.bh_last_error()
+    fake = C.c_void_p(0x10000)  # never dereferenced: validation fails first
+    st = _lib.TileStats()
+    assert bhlib.bh_trace_tile(cfg, scene, 2.3, 18.0, fake, 4, *[fake] * 7, None, 0, st,
+                               None) == -1
+    assert b"f64_radius" in bhlib.bh_last_error()
+    assert make_config(f64_radius="auto").f64_radius == -1.0
+    with pytest.raises(ValueError):
+        make_config(f64_radius=-2.0)
+    with pytest.raises(ValueError):
+        make_config(f64_radius="inner")
+    nan = make_config(1, 1e-8, 1e-10, precision="mixed")
+    nan.f64_radius = float("nan")
+    assert bhlib.bh_propagate(nan, 1.0, 0.9, None, fake, fake, None, fake, 4, 10, fake,
+                              None) == -1
+    assert b"NaN" in bhlib.bh_last_error()
+    both = make_config(1, 1e-8, 1e-10, precision="mixed", project_every=2, f64_radius=40.0)
+    assert bhlib.bh_propagate(both, 1.0, 0.9, None, fake, fake, None, fake, 4, 10, fake,
+                              None) == -1
+    assert b"project_every" in bhlib.bh_last_error()
+    assert bhlib.bh_device_math(3, fake, fake, 4, None) == -1
 
 
 def test_check_maps_status_to_reference_exceptions(bhlib):
