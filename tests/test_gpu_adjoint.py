@@ -179,3 +179,121 @@ def test_ray_order_does_not_change_results(cuda):
         a0, as0 = adjoint(tape, g, precision=prec, sort=False)
         a1, as1 = adjoint(tape, g, precision=prec, sort=True)
         assert torch.equal(a0, a1) and torch.equal(as0, as1)
+
+
+def _c5_setup(precision, pixels_require_grad=False):
+    """The 256x256 differentiable-tracing workload (a = 0.7, inclination 60
+    deg, r_obs = 50 M, fov 30, rtol 1e-9, checkpoint every 64 accepted
+    steps): loss of the escaped rays' celestial angles against a target frame
+    at a = 0.9.  Returns the adjoint's gradients, a function evaluating the
+    loss through the frozen float64 step sequence at moved parameters or
+    pixel coordinates, and the pixel tensors."""
+    from blackhorizon_b200.adjoint import (angle_loss, celestial_angles, fly_camera_rays,
+                                           orbit_look_at, pixel_grid, replay,
+                                           trace_rays_differentiable, trace_with_tape)
+    from blackhorizon_b200.kerr import KerrSpacetime
+    from blackhorizon_b200.workloads import DIFFERENTIABLE as C
+
+    dev = torch.device("cuda", 0)
+    t = lambda x, g=False: torch.tensor(x, dtype=torch.float64, device=dev,  # noqa: E731
+                                        requires_grad=g)
+    yaw0, pitch0 = orbit_look_at(C.distance, C.inclination)
+    u, v = pixel_grid(C.width, C.height, C.fov, dev)
+    kw = dict(max_steps=C.max_steps, rtol=C.rtol, atol=C.atol, capture_margin=C.capture_margin)
+    y_tgt = fly_camera_rays(t(0.9), t(C.inclination), t(yaw0), t(pitch0), C.distance, u, v)
+    tgt, tgt_status, _, _ = trace_with_tape(KerrSpacetime(1.0, 0.9), y_tgt, C.escape_radius,
+                                            **kw)
+    th_t, ph_t = celestial_angles(t(0.9), tgt)
+    params = [t(x, True) for x in (C.spin, C.inclination, yaw0, pitch0)]
+    uu = u.clone().requires_grad_(pixels_require_grad)
+    vv = v.clone().requires_grad_(pixels_require_grad)
+    s0 = fly_camera_rays(*params, C.distance, uu, vv)
+    states, status, _ = trace_rays_differentiable(params[0], s0, C.escape_radius,
+                                                  precision=precision, checkpoint_every=64,
+                                                  **kw)
+    mask = ((status == 2) & (tgt_status == 2)).to(torch.float64)
+    th, ph = celestial_angles(params[0], states)
+    angle_loss(th, ph, th_t, ph_t, mask).backward()
+    _, _, _, tape = trace_with_tape(KerrSpacetime(1.0, C.spin), s0.detach(), C.escape_radius,
+                                    precision="fp64", checkpoint_every=64, **kw)
+
+    def frozen_loss(p, du=None, dv=None):
+        pt = [t(x) for x in p]
+        y0 = fly_camera_rays(*pt, C.distance, u if du is None else u + du,
+                             v if dv is None else v + dv)
+        yN = replay(tape, y0, spin=p[0], precision="fp64")
+        a_, b_ = celestial_angles(pt[0], yN)
+        return float(angle_loss(a_, b_, th_t, ph_t, mask))
+
+    grads = np.array([float(p.grad) for p in params])
+    base = [C.spin, C.inclination, yaw0, pitch0]
+    return grads, base, frozen_loss, (uu, vv, mask)
+
+
+def _central(f, base, k, h):
+    p, m = list(base), list(base)
+    p[k] += h
+    m[k] -= h
+    return (f(p) - f(m)) / (2.0 * h)
+
+
+def test_c5_gradients_against_finite_differences(cuda):
+    """fp64 adjoint gradients of the 256x256 workload with respect to spin,
+    inclination, yaw and pitch against central differences of the frozen
+    step sequence at h = 1e-6 and 1e-7 and their Richardson combination
+    (100 D(1e-7) - D(1e-6)) / 99, which removes the h^2 truncation term.
+    Per parameter: the Richardson estimate within 1e-5 relative, the plain
+    differences within 1e-4 at h = 1e-7 and 1e-2 at h = 1e-6 (the loss is
+    steep near the shadow edge, where the truncation term is large).  The
+    mixed policy's gradients (its own float32 trace and sweep) agree with
+    the fp64 Richardson estimate within 1e-2."""
+    grads, base, f, _ = _c5_setup("fp64")
+    names = ("spin", "inclination", "yaw", "pitch")
+    report = {}
+    for k, name in enumerate(names):
+        d6 = _central(f, base, k, 1e-6)
+        d7 = _central(f, base, k, 1e-7)
+        rich = (100.0 * d7 - d6) / 99.0
+        rel = [abs(grads[k] - d) / abs(d) for d in (d6, d7, rich)]
+        report[name] = (grads[k], d6, d7, rich, rel)
+        assert rel[2] <= 1e-5, (name, report[name])
+        assert rel[1] <= 1e-4, (name, report[name])
+        assert rel[0] <= 1e-2, (name, report[name])
+    print("fp64 adjoint vs FD (h=1e-6, 1e-7, Richardson):",
+          {k: ["%.2e" % r for r in v[4]] for k, v in report.items()})
+    mixed, _, _, _ = _c5_setup("mixed")
+    rich = np.array([report[n][3] for n in names])
+    rel_m = np.abs(mixed - rich) / np.abs(rich)
+    print("mixed adjoint vs fp64 Richardson:", dict(zip(names, ["%.2e" % r for r in rel_m])))
+    assert np.all(rel_m <= 1e-2)
+
+
+def test_c5_pixel_coordinate_gradients(cuda):
+    """Gradients with respect to the image-plane coordinates (u, v) of single
+    pixels (the pinhole grid of camera.py:96-113, through the yaw/pitch
+    camera of fly_camera.py:37-88): the adjoint's dL/du_i and dL/dv_i of 12
+    escaped pixels against Richardson-combined central differences of the
+    frozen sequence (h = 1e-6, 1e-7), within 1e-5 relative (1e-9 absolute
+    for pixels whose gradient is near zero)."""
+    grads, base, f, (uu, vv, mask) = _c5_setup("fp64", pixels_require_grad=True)
+    gu, gv = uu.grad.cpu().numpy(), vv.grad.cpu().numpy()
+    esc = np.nonzero(mask.cpu().numpy() > 0)[0]
+    rng = np.random.default_rng(9)
+    pick = rng.choice(esc, 12, replace=False)
+    n = uu.shape[0]
+    checked = 0
+    for i in pick:
+        for g, which in ((gu, "u"), (gv, "v")):
+            d = []
+            for h in (1e-6, 1e-7):
+                e = torch.zeros(n, dtype=torch.float64, device=uu.device)
+                e[i] = h
+                if which == "u":
+                    d.append((f(base, du=e) - f(base, du=-e)) / (2 * h))
+                else:
+                    d.append((f(base, dv=e) - f(base, dv=-e)) / (2 * h))
+            rich = (100.0 * d[1] - d[0]) / 99.0
+            err = abs(g[i] - rich)
+            assert err <= max(1e-5 * abs(rich), 1e-9), (i, which, g[i], d, rich)
+            checked += 1
+    assert checked == 24

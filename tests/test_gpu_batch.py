@@ -3,8 +3,9 @@
 The uneven 64-camera workload (resolutions log-uniform from 64x64 to
 1024x768, spin in [-0.998, 0.998], inclination in [0, 90] deg, distance in
 [20, 200] M, escape at twice the distance) runs as one persistent launch,
-captured into a CUDA graph; a strided subsample of every camera's pixels is
-checked against the oracle."""
+captured into a CUDA graph; 4096 strided pixels of every camera are checked
+against the oracle in both precision policies, disagreements allowed only at
+the shadow edge."""
 
 import numpy as np
 import pytest
@@ -58,37 +59,68 @@ def test_graph_replay_matches_direct_launch(cuda, precision):
     batch.close()
 
 
-def test_uneven_64_cameras_against_oracle(cuda):
-    """One graph-captured launch of all 64 cameras (float64 policy); 64
-    strided pixels of every camera traced by the oracle must agree on status
-    (at least 98 % overall: pixels at a shadow edge may flip)."""
-    from blackhorizon_b200 import CameraBatch
+def oracle_status(cs, idx):
+    """Statuses of pixels idx of a camera scene traced by the oracle from
+    initial states it builds itself (pinhole directions, null momenta)."""
     from oracle import oracle
+
+    cam, st = cs.camera, cs.spacetime
+    d = oracle.pinhole_directions(cam.forward, cam.right, cam.up, cam.fov_degrees,
+                                  cam.width, cam.height)[idx]
+    pos = cam.ray_origins()[idx]
+    p = oracle.null_momentum(1.0, st.spin, pos, d, True, True)
+    s0 = np.zeros((idx.size, 8))
+    s0[:, 1:4] = pos
+    s0[:, 4:8] = p
+    _, status, _, _ = oracle.trace(1.0, st.spin, s0, cs.escape_radius, max_steps=10000,
+                                   rtol=1e-8, atol=1e-10, capture_margin=0.01)
+    return status
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_uneven_64_cameras_against_oracle(cuda, precision):
+    """One graph-captured launch of all 64 cameras.  4096 strided pixels of
+    every camera (all pixels of the 64x48 ones) are traced by the oracle; the
+    statuses agree except at the shadow edge: every pixel that disagrees has
+    a 4-neighbour of another status in the oracle's own frame, and such
+    pixels are at most 0.5 % (float64) or 1 % (mixed) of the sample."""
+    from blackhorizon_b200 import CameraBatch
 
     sc = uneven_scenes()
     assert len(sc) == 64
-    batch = CameraBatch(sc, max_steps=10000, rtol=1e-8, atol=1e-10, precision="fp64")
+    batch = CameraBatch(sc, max_steps=10000, rtol=1e-8, atol=1e-10, precision=precision)
     batch.run()
     res = batch.results()
-    agree = total = 0
-    for cs, r in zip(sc, res):
-        cam, st = cs.camera, cs.spacetime
-        n = cam.width * cam.height
-        idx = np.linspace(0, n - 1, 64).astype(np.int64)
-        d = oracle.pinhole_directions(cam.forward, cam.right, cam.up, cam.fov_degrees,
-                                      cam.width, cam.height)[idx]
-        pos = cam.ray_origins()[idx]
-        p = oracle.null_momentum(1.0, st.spin, pos, d, True, True)
-        s0 = np.zeros((idx.size, 8))
-        s0[:, 1:4] = pos
-        s0[:, 4:8] = p
-        _, ostatus, _, _ = oracle.trace(1.0, st.spin, s0, cs.escape_radius, max_steps=10000,
-                                        rtol=1e-8, atol=1e-10, capture_margin=0.01)
-        got = r.status.cpu().numpy()[idx]
-        agree += int((got == ostatus).sum())
-        total += idx.size
-    assert agree / total >= 0.98
     batch.close()
+    total = differ = off_edge = 0
+    for cs, r in zip(sc, res):
+        w, h = cs.camera.width, cs.camera.height
+        n = w * h
+        idx = np.arange(n) if n <= 4096 else np.unique(
+            np.round(np.linspace(0, n - 1, 4096)).astype(np.int64))
+        assert idx.size >= min(n, 4096) - 1
+        own = oracle_status(cs, idx)
+        got = r.status.cpu().numpy()[idx]
+        bad = idx[got != own]
+        total += idx.size
+        differ += bad.size
+        if bad.size:
+            rows, cols = np.divmod(bad, w)
+            nbrs = np.stack([np.stack([rows - 1, cols], -1), np.stack([rows + 1, cols], -1),
+                             np.stack([rows, cols - 1], -1), np.stack([rows, cols + 1], -1)],
+                            axis=1)  # (bad, 4, 2)
+            inside = ((nbrs[..., 0] >= 0) & (nbrs[..., 0] < h) & (nbrs[..., 1] >= 0)
+                      & (nbrs[..., 1] < w))
+            flat = np.where(inside, nbrs[..., 0] * w + nbrs[..., 1], 0)
+            nb_status = oracle_status(cs, flat.reshape(-1)).reshape(flat.shape)
+            centre = own[got != own][:, None]
+            at_edge = np.any(inside & (nb_status != centre), axis=1)
+            off_edge += int((~at_edge).sum())
+    print("%s: %d of %d sampled pixels differ from the oracle, %d off the shadow edge"
+          % (precision, differ, total, off_edge))
+    assert total >= 64 * 3072
+    assert off_edge == 0
+    assert differ / total <= (0.005 if precision == "fp64" else 0.01)
 
 
 def test_autotuner_picks_and_caches(cuda, tmp_path, monkeypatch):

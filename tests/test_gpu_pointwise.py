@@ -227,3 +227,60 @@ def test_implicit_midpoint_properties(cuda):
     assert bool(np.all(np.diff(samples["rk4"]) > 0.0)) and samples["rk4"][-1] > 5 * samples["rk4"][0]
     mid = samples["midpoint"]
     assert float(mid[-1]) < 0.05 * float(mid.max()) and float(mid.max()) < 1e-2
+
+
+def _device_math(op, x):
+    from blackhorizon_b200 import _lib
+    from blackhorizon_b200.backend import stream_handle
+
+    xd = torch.as_tensor(x, device="cuda")
+    yd = torch.empty_like(xd)
+    _lib.check(_lib.load().bh_device_math(op, xd.data_ptr(), yd.data_ptr(), xd.numel(),
+                                          stream_handle()), "device_math")
+    return yd.cpu().numpy()
+
+
+def _ulps(got, ref):
+    return np.abs(got - ref) / np.spacing(np.abs(ref))
+
+
+def test_float64_reciprocals_within_two_ulp(cuda):
+    """The float64 reciprocal and reciprocal square root of the stage
+    arithmetic (MUFU seed and two Newton-Raphson steps) against the
+    correctly rounded results, from 80-bit extended NumPy arithmetic, on 10^6
+    inputs log-uniform over [1e-30, 1e30] (the range of r^2, w = r^2 + a^2
+    and r^4 + a^2 z^2 on the path), plus powers of two."""
+    rng = np.random.default_rng(11)
+    x = 10.0 ** rng.uniform(-30, 30, 1_000_000)
+    x = np.concatenate([x, 2.0 ** np.arange(-99, 100), [1.0, 3.0, 0.75]])
+    xl = x.astype(np.longdouble)
+    rcp_ref = (1 / xl).astype(np.float64)
+    rsq_ref = (1 / np.sqrt(xl)).astype(np.float64)
+    rcp = _device_math(0, x)
+    rsq = _device_math(1, x)
+    u_rcp, u_rsq = _ulps(rcp, rcp_ref), _ulps(rsq, rsq_ref)
+    print("rcp: max %.2f ulp, %.4f%% not correctly rounded; rsqrt: max %.2f ulp, %.4f%%"
+          % (u_rcp.max(), 100 * np.mean(u_rcp > 0), u_rsq.max(), 100 * np.mean(u_rsq > 0)))
+    assert u_rcp.max() <= 2.0 and u_rsq.max() <= 2.0
+    neg = -x[:1000]
+    assert np.all(_ulps(_device_math(0, neg), (1 / neg.astype(np.longdouble)).astype(np.float64))
+                  <= 2.0)
+
+
+def test_mixed_step_factor_from_r2(cuda):
+    """The mixed controller's float64 step factor clip(0.9 x^-0.1, 0.2, 5) of
+    x = r^2 (float32 seed, one Newton-Raphson step) equals the reference's
+    step_factor(sqrt(x)) (integrators.py:120-124) to 1e-11 relative, and
+    clips exactly at both ends."""
+    rng = np.random.default_rng(12)
+    x = np.concatenate([10.0 ** rng.uniform(-12, 12, 200_000),
+                        [0.0, 1e-40, 3.5e-8, 3.6e-8, 1.0, 3.4e6, 3.41e6, 1e300, np.inf]])
+    got = _device_math(2, x)
+    xl = x.astype(np.longdouble)
+    with np.errstate(divide="ignore"):
+        ref = np.clip(np.longdouble(0.9) * np.power(np.maximum(xl, np.longdouble(1e-32)),
+                                                    np.longdouble(-1) / 10), 0.2, 5.0)
+    rel = np.abs(got - ref.astype(np.float64)) / ref.astype(np.float64)
+    print("step factor: max relative error %.3g" % rel.max())
+    assert rel.max() <= 1e-11
+    assert got[-1] == 0.2 and got[-2] == 0.2 and got[-9] == 5.0

@@ -1,21 +1,25 @@
 """Raw-throughput workload (2000 attempted DP5(4) steps per ray, per-ray spin,
-no termination) against the reference's end points for its first 512 rays.
+no termination) against the reference's end points.
 
 Endpoint error of a ray = max over the 8 components of
 |y - y_ref| / max(|y_ref|, 1): relative for large components, absolute for
 components near zero (momenta of order 1, p_z of an equatorial ray ~ 0).
 
 Float64 policy: the same step sequence as the reference, so the end point
-after 2000 attempts matches it (median 1e-10, every ray 1e-6).
+after 2000 attempts matches the reference's own for its first 512 rays
+(median 1e-10, every ray 1e-6).
 
-Mixed policy: float32 rounding puts a noise floor of ~1e-3 under the error
-ratio near r = 30, so the controller's step sequence is not the float64 one
-and the end point after a fixed attempt count sits at a different affine
-parameter.  Its accuracy is therefore measured at equal affine parameter: the
-oracle integrates each ray to the lambda the kernel reached, at rtol 1e-12
-(the reference's DP5(4) and controller, last step cut to land on lambda).
-Bar: median <= 1e-6, 90th percentile <= 1e-5; the float64 kernel is held to
-the same comparison.
+Mixed policy: float32 stage arithmetic moves the controller's step sequence
+off the float64 one, so after a fixed attempt count the end point sits at a
+different affine parameter.  Accuracy is therefore measured at equal affine
+parameter: the oracle integrates each ray to the lambda the kernel reached,
+at rtol 1e-12 (the reference's DP5(4) and controller, last step cut to land
+on lambda).  The headline bar, on the first 16,384 rays, holds the default
+mixed path (float64 band inside 8 u M / rtol) to the float64 kernel: the
+fraction of rays within 1e-6 no more than 0.5 points below float64's, the
+99th percentile within 1e-6, and every ray within max(1e-6, 50 x its float64
+error).  Float32 stages everywhere (no band) are held to median 1e-6, 90th
+percentile 1e-5 and 99th percentile 1e-4 in every launch shape.
 """
 
 import numpy as np
@@ -31,7 +35,7 @@ def endpoint_error(got, ref):
     return np.max(np.abs(got - ref) / np.maximum(np.abs(ref), 1.0), axis=1)
 
 
-def run(precision, layout="aos", variant=-1):
+def run(precision, layout="aos", variant=-1, f64_radius="auto"):
     from blackhorizon_b200 import propagate
     from blackhorizon_b200.kerr import KerrSpacetime
 
@@ -42,7 +46,7 @@ def run(precision, layout="aos", variant=-1):
     states, h, lam, acc, stats = propagate(
         KerrSpacetime(1.0, 0.0), s0, int(g["n_steps"]), rtol=float(g["rtol"]),
         atol=float(g["atol"]), precision=precision, spins=g["spin"], layout=layout,
-        variant=variant)
+        variant=variant, f64_radius=f64_radius)
     if layout == "soa":
         states = states.t()
     run.lam = lam.cpu().numpy()
@@ -79,33 +83,96 @@ def equal_lambda_error(g, got, lam):
     return endpoint_error(got[ok], truth[ok]), int((~ok).sum())
 
 
-@pytest.mark.parametrize("precision", ["mixed", "fp64"])
-def test_endpoints_at_equal_affine_parameter(cuda, precision):
-    g, got, acc, stats = run(precision)
-    lam = run.lam
-    assert np.all(lam > 0) and np.all(np.isfinite(got))
-    err, dropped = equal_lambda_error(g, got, lam)
-    print("%s endpoint error at equal lambda: median %.3g p90 %.3g p99 %.3g max %.3g "
-          "(%d rays without a finite oracle state); accepted %.4f of ref"
-          % (precision, np.median(err), np.quantile(err, 0.9), np.quantile(err, 0.99),
-             np.max(err), dropped, acc.sum() / g["accepted"].sum()))
+def c2_rays(n):
+    import bench
+
+    state0, spins, _, _, spin_h = bench.make_inputs(n, 0, torch.device("cuda", 0))
+    return state0, spins, spin_h
+
+
+def equal_lambda_errors(spin, s0, got, lam):
+    """Per-ray endpoint error at equal affine parameter and the mask of rays
+    that stay outside the horizon (the others run toward the singularity and
+    are not comparable)."""
+    from oracle import oracle
+
+    from blackhorizon_b200.workloads import PLUNGE_RADIUS, ks_radius_np
+
+    truth, _ = oracle.propagate_to(1.0, spin, s0, lam, rtol=1e-12, atol=1e-14)
+    ok = np.all(np.isfinite(truth), axis=1) & np.all(np.isfinite(got), axis=1)
+    ok &= np.nan_to_num(ks_radius_np(truth, spin), nan=0.0) >= PLUNGE_RADIUS
+    err = np.full(got.shape[0], np.inf)
+    err[ok] = endpoint_error(got[ok], truth[ok])
+    return err, ok
+
+
+def test_mixed_meets_the_float64_accuracy_bar(cuda):
+    """The headline's accuracy condition on the first 16,384 raw-throughput
+    rays: the default mixed path (float32 stages, float64 band, float64
+    controller) against the float64 kernel, both at equal affine parameter."""
+    from blackhorizon_b200 import propagate
+    from blackhorizon_b200.kerr import KerrSpacetime
+
+    n = 16384
+    state0, spins, spin_h = c2_rays(n)
+    s0 = state0.cpu().numpy()
+    st = KerrSpacetime(1.0, 0.0)
+    errs, oks = {}, {}
+    for precision in ("mixed", "fp64"):
+        states, _, lam, _, stats = propagate(st, state0, 2000, rtol=1e-8, atol=1e-10,
+                                             precision=precision, spins=spins)
+        assert stats.attempts == n * 2000
+        errs[precision], oks[precision] = equal_lambda_errors(
+            spin_h, s0, states.cpu().numpy(), lam.cpu().numpy())
+    both = oks["mixed"] & oks["fp64"]
+    assert int((~both).sum()) <= 150  # rays that fall through the horizon (113 measured)
+    em, ef = errs["mixed"][both], errs["fp64"][both]
+    frac_m, frac_f = float(np.mean(em <= 1e-6)), float(np.mean(ef <= 1e-6))
+    print("within 1e-6: mixed %.5f fp64 %.5f; p99 mixed %.3g fp64 %.3g; worst ratio %.3g"
+          % (frac_m, frac_f, np.quantile(em, 0.99), np.quantile(ef, 0.99),
+             np.max(em / np.maximum(ef, 1e-300))))
+    assert frac_m >= frac_f - 0.005
+    assert np.quantile(em, 0.99) <= 1e-6
+    assert np.all(em <= np.maximum(1e-6, 50.0 * ef))
+
+
+def test_fp64_endpoints_at_equal_affine_parameter(cuda):
+    g, got, acc, stats = run("fp64")
+    err, dropped = equal_lambda_error(g, got, run.lam)
     assert dropped <= 8
-    assert np.median(err) <= 1e-6
-    assert np.quantile(err, 0.9) <= 1e-5
-    assert np.quantile(err, 0.99) <= 1e-4
+    assert np.median(err) <= 1e-9
+    assert np.quantile(err, 0.99) <= 1e-6
 
 
 @pytest.mark.parametrize("variant", range(8))
-def test_mixed_variants_agree(cuda, variant):
-    """Every mixed launch shape (one ray per thread, or two per thread in
-    packed float32x2) meets the equal-lambda bar on the same rays."""
-    g, got, acc, stats = run("mixed", variant=variant)
+def test_mixed_float_stages_every_variant(cuda, variant):
+    """Float32 stages everywhere (f64_radius = 0) in every mixed launch shape
+    (one ray per thread, or two per thread in packed float32x2)."""
+    g, got, acc, stats = run("mixed", variant=variant, f64_radius=0.0)
     assert stats.attempts == 512 * 2000
     err, dropped = equal_lambda_error(g, got, run.lam)
     assert dropped <= 8
     assert np.median(err) <= 1e-6
     assert np.quantile(err, 0.9) <= 1e-5
     assert np.quantile(err, 0.99) <= 1e-4
+
+
+def test_band_covering_the_path_takes_the_float64_steps(cuda):
+    """A band wider than every ray's path runs each attempt outside the
+    horizon as band_attempt, the float64 policy's step (its first stage
+    evaluated afresh instead of reused, a rounding-level difference): the
+    accepted-step counts equal the float64 kernel's on nearly every ray and
+    the end points agree there to rounding."""
+    from blackhorizon_b200.workloads import PLUNGE_RADIUS, ks_radius_np
+
+    g, fp64, acc64, _ = run("fp64")
+    _, wide, accw, stats = run("mixed", f64_radius=1e9)
+    assert stats.attempts == 512 * 2000
+    outside = np.nan_to_num(ks_radius_np(fp64, g["spin"]), nan=0.0) >= PLUNGE_RADIUS
+    same = outside & (accw == acc64)
+    assert same.sum() >= 0.95 * outside.sum()
+    assert np.quantile(endpoint_error(wide[same], fp64[same]), 0.9) <= 1e-10
+    assert np.median(endpoint_error(wide[same], fp64[same])) <= 1e-12
 
 
 def test_streamed_from_host_memory_equals_device_path(cuda):
