@@ -31,6 +31,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -67,13 +68,15 @@ def parse():
     ap.add_argument("--rays", type=int, default=1 << 20, help="rays per GPU")
     ap.add_argument("--dp5-steps", type=int, default=2000)
     ap.add_argument("--variant", type=int, default=-1)
+    ap.add_argument("--f64-radius", default="auto",
+                    help="float64 band radius of the mixed propagator (M), 'auto' = 8 u M / rtol")
     ap.add_argument("--no-fp64", action="store_true", help="skip the float64 comparison arm")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-workloads", action="store_true",
                     help="skip the full-HD frame, the 64-camera batch and the adjoint")
     ap.add_argument("--profile-case",
-                    choices=("trace", "adjoint", "tile", "realtime", "emission", "viewer"),
+                    choices=("trace", "propagate", "adjoint", "tile", "realtime"),
                     default=None,
                     help="run one small untimed case of that kernel (for ncu captures): "
                          "trace = the 1920x1080 frame (2 warm-up launches, then 1); "
@@ -81,9 +84,8 @@ def parse():
                          "tape (1 warm-up sweep, then 1); tile = the offline frame at "
                          "640x400 supersample 2 (1,024,000 rays), first pass only, twice; "
                          "realtime = the 1280x720 real-time frame, three launches; "
-                         "emission = the offline frame traced once, then its radiance "
-                         "and development twice; viewer = the real-time viewer's whole "
-                         "1280x720 frame (rays, trace, shading), three times")
+                         "propagate = the raw-throughput workload at --rays rays and "
+                         "--dp5-steps steps, three launches")
     return ap.parse_args()
 
 
@@ -105,7 +107,8 @@ class ClockSampler:
     def __init__(self, device_index: int):
         self.idx = device_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device_index}.csv")
+        self.path = os.path.join(tempfile.gettempdir(),
+                                 f"bh_bench_clocks_{os.getpid()}_{device_index}.csv")
 
     def start(self):
         try:
@@ -128,8 +131,11 @@ class ClockSampler:
             self.proc.kill()
         self.fh.close()
         sm, mx, reasons = [], 0.0, set()
+        with open(self.path) as fh:
+            lines = fh.readlines()
+        os.remove(self.path)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        for line in lines:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -248,12 +254,12 @@ def run_ours(args):
             dist.barrier(device_ids=[local])
         torch.cuda.synchronize()
 
-    def one_step(precision, kev=None, project_every=0):
+    def one_step(precision, kev=None, project_every=0, band=0.0):
         work.copy_(state0)
         h.fill_(0.1)
         lam.zero_()
         cfg = make_config(1, 1e-8, 1e-10, 0.1, 2.0, 0.0, precision, "aos", 600.0,
-                          args.variant, 0, project_every)
+                          args.variant, 0, project_every, f64_radius=band)
         if kev is not None:
             kev[0].record()
         rc = lib.bh_propagate(cfg, 1.0, 0.0, spins.data_ptr(), work.data_ptr(), h.data_ptr(),
@@ -262,9 +268,9 @@ def run_ours(args):
             kev[1].record()
         _lib.check(rc, "bench propagate")
 
-    def timed(precision, k, w, sample_clocks=False, project_every=0):
+    def timed(precision, k, w, sample_clocks=False, project_every=0, band=0.0):
         for _ in range(w):
-            one_step(precision, project_every=project_every)
+            one_step(precision, project_every=project_every, band=band)
         flush.fill_(1)
         barrier()
         sampler = ClockSampler(local) if sample_clocks else None
@@ -277,7 +283,7 @@ def run_ours(args):
         barrier()
         t0.record()
         for i in range(k):
-            one_step(precision, kevs[i], project_every)
+            one_step(precision, kevs[i], project_every, band)
             if i + 1 < k:
                 flush.fill_(i & 0xFF)
         t1.record()
@@ -292,10 +298,22 @@ def run_ours(args):
         return total_ms / k, kernel_ms, clocks
 
     prec = args.precision
-    ms_step, kernel_ms, clocks = timed(prec, args.steps, max(args.warmup, 3), True)
+    band = (args.f64_radius if args.f64_radius == "auto" else float(args.f64_radius)) \
+        if prec == "mixed" else 0.0
+    ms_step, kernel_ms, clocks = timed(prec, args.steps, max(args.warmup, 3), True, band=band)
     final = work.clone()
     final_lam = lam.clone()
     value = world * n * S / (ms_step * 1e-3)
+
+    # ---- the mixed policy with float32 stages everywhere (no float64 band)
+    float_stages = None
+    final_fs = lam_fs = None
+    if not args.no_fp64 and prec == "mixed":
+        msf, kf, _ = timed("mixed", max(1, min(args.steps, 5)), 1, band=0.0)
+        final_fs = work.clone()
+        lam_fs = lam.clone()
+        float_stages = {"value": world * n * S / (msf * 1e-3), "ms_per_step": msf,
+                        "kernel_ms": kf, "f64_radius": 0.0}
 
     fp64 = None
     final64 = lam64 = None
@@ -328,10 +346,13 @@ def run_ours(args):
         # Pinned host states and spins in, final states into a pinned host
         # buffer (the caller's result): the library streams the rays through
         # in pieces, copies overlapping the kernels.
-        out, _, _, _, _ = propagate(st_mass, host_state, S, rtol=1e-8, atol=1e-10,
-                                    precision=prec, spins=host_spin, timeout_s=600.0,
-                                    variant=args.variant, out=host_out)
+        out, _, _, _, stats = propagate(st_mass, host_state, S, rtol=1e-8, atol=1e-10,
+                                        precision=prec, spins=host_spin, timeout_s=600.0,
+                                        variant=args.variant, out=host_out, f64_radius=band)
         torch.cuda.current_stream().synchronize()
+        if stats.attempts != n * S:
+            raise RuntimeError(f"end-to-end propagate did {stats.attempts} attempts, "
+                               f"expected {n * S}")
         return out
 
     e2e_step()
@@ -367,6 +388,7 @@ def run_ours(args):
                 "rays_per_gpu": n, "dp5_steps_per_ray": S, "rtol": 1e-8, "atol": 1e-10,
                 "precision": prec, "l2": "flushed between timed steps (256 MiB write)",
                 "parallelism": f"weak: {n} rays per GPU, no collective",
+                "f64_band_radius": band_radius(band, 1.0, 1e-8),
             },
             "ns_per_ray_step": ms_step * 1e6 / (world * n * S),
             "roofline": {
@@ -399,6 +421,8 @@ def run_ours(args):
             out["speedup_vs_fp64"] = fp64["ms_per_step"] / ms_step
         if projected is not None:
             out["mixed_projected"] = projected
+        if float_stages is not None:
+            out["mixed_float_stages"] = float_stages
         if not args.no_workloads:
             out["workloads"] = tracer_workloads(device)
             out["workloads"]["differentiable_256x256"] = adjoint_workload(device)
@@ -406,9 +430,17 @@ def run_ours(args):
             out["workloads"]["realtime_frame"] = realtime_workload(device, not args.no_cpu)
             out["workloads"]["inflation_tile"] = inflation_workload(device, not args.no_cpu)
         if not args.no_cpu:
-            out["cpu_baseline"] = cpu_baseline(state0, spin_h, S, args.cpu_seconds)
+            port = cpu_baseline(state0, spin_h, S, args.cpu_seconds)
+            ref = reference_numpy_baseline(state0.cpu().numpy(), spin_h, args.cpu_seconds)
+            if "value" in ref:
+                out["cpu_baseline"] = ref
+                out["cpu_baseline_port"] = port
+            else:
+                port["reference_numpy"] = ref
+                out["cpu_baseline"] = port
             out["endpoint_err"] = endpoint_errors(
                 state0, spin_h, {prec: (final, final_lam), "fp64": (final64, lam64),
+                                 "mixed_float_stages": (final_fs, lam_fs),
                                  "mixed_projected": (final_proj, lam_proj)})
     if world > 1:
         dist.barrier(device_ids=[local])
@@ -549,63 +581,6 @@ def offline_workload(device, with_cpu=True, warmup=1, reps=3, cpu_stride=16):
                                                   second.get("iterations", 0))}
     out["mixed_status_agreement_with_fp64"] = float(
         (frames["mixed"].status == frames["fp64"].status).double().mean())
-    # The emission half of render_hdr and develop (render.py:352-484,
-    # 630-680; post.py:88-106) on the device, from the fp64 frame's rays.
-    from blackhorizon_b200.emission import frame_tables, radiance_image, render_hdr
-    from blackhorizon_b200.emission import static_observer_lapse
-    from blackhorizon_b200.post import develop
-
-    fr = frames["fp64"]
-    tables = frame_tables(st, settings, s0.device)
-    lapse = float(static_observer_lapse(st, cam.position))
-
-    def shade():
-        return radiance_image(st, fr.status, fr.escape_directions, fr.hit_positions,
-                              fr.hit_momenta, F.width, F.height, settings, lapse, tables=tables)
-
-    hdr = shade()
-    out["radiance_ms"] = min(_event_ms(shade, reps))
-    develop(hdr)
-    out["develop_ms"] = min(_event_ms(lambda: develop(hdr), reps))
-
-    def frame_to_host():
-        # Camera to display image on the host: trace, retrace, shade, develop.
-        return develop(render_hdr(cam, F.width, F.height, settings, precision="mixed")).cpu()
-
-    frame_to_host()
-    t = time.perf_counter()
-    for _ in range(reps):
-        image = frame_to_host()
-    out["mixed_frame_to_host_image_ms"] = (time.perf_counter() - t) * 1e3 / reps
-    out["image_d2h_bytes"] = int(image.numel())
-    if with_cpu:
-        from oracle import oracle
-
-        threads = host_threads()
-        host_tables = {k: (v.cpu().numpy() if torch.is_tensor(v) else v)
-                       for k, v in tables.items()}
-        p = oracle.emission_params(1.0, F.spin, host_tables, observer_lapse=lapse,
-                                   supersample=F.supersample)
-        args = [a.cpu().numpy() for a in (fr.status, fr.escape_directions, fr.hit_positions,
-                                          fr.hit_momenta)]
-        t = time.perf_counter()
-        hdr_cpu = oracle.offline_radiance(p, *args, host_tables, F.width, F.height,
-                                          nthreads=threads)
-        t_rad = time.perf_counter() - t
-        from blackhorizon_b200.post import gaussian_kernel
-
-        t = time.perf_counter()
-        img_cpu = oracle.develop(hdr_cpu, gaussian_kernel(6.0))
-        t_dev = time.perf_counter() - t
-        out["emission_cpu_baseline"] = {
-            "radiance_ms": t_rad * 1e3, "develop_ms": t_dev * 1e3, "cores": threads,
-            "kind": "port",
-            "sample": "the whole frame: oracle/bh_oracle.c radiance on "
-                      f"{threads} threads, develop on 1 thread"}
-        rel = np.abs(hdr.cpu().numpy() - hdr_cpu) / np.maximum(np.abs(hdr_cpu), 1e-6)
-        out["hdr_pixels_off_by_1e-5_vs_oracle"] = int((rel.max(axis=2) > 1e-5).sum())
-        out["developed_channels_off_vs_oracle"] = int(
-            (develop(hdr).cpu().numpy() != img_cpu).sum())
     if with_cpu:
         from oracle import oracle
 
@@ -670,23 +645,6 @@ def realtime_workload(device, with_cpu=True, warmup=2, reps=5, cpu_stride=8):
                      "captured": int((r.status == 1).sum())}
     out["mixed_status_agreement_with_fp64"] = float(
         (res["mixed"].status == res["fp64"].status).double().mean())
-    # The viewer's whole frame on the device (headless.py:32-48): camera rays,
-    # the shader algorithm and the shader's colours into an 8-bit buffer.
-    from blackhorizon_b200.offline import FlyCamera
-    from blackhorizon_b200.realtime import BackgroundMode, render_frame_device
-
-    fly = FlyCamera.from_orbit(F.distance, F.inclination, 0.0)
-    frame_settings = RenderSettings(spin=F.spin, fov_degrees=F.fov,
-                                    background=BackgroundMode.STARFIELD).apply_preset(
-                                        QualityPreset(F.preset))
-    for prec in ("mixed", "fp64"):
-        def frame():
-            return render_frame_device(frame_settings, fly, F.width, F.height, precision=prec)
-
-        for _ in range(warmup):
-            frame()
-        ms = min(_event_ms(frame, reps))
-        out[f"{prec}_headless_frame_ms"] = ms
     if with_cpu:
         from oracle import oracle
 
@@ -745,20 +703,6 @@ def inflation_workload(device, with_cpu=True, warmup=1, reps=3, side=256, cpu_st
     out = {"rays": side * side, "ms_per_tile": ms, "rays_per_s": side * side / (ms * 1e-3),
            "escaped": int((status == 0).sum()), "terminal": int((status == 1).sum()),
            "budget": int((status == 2).sum())}
-    # The flythrough frame end to end (offline/inflation.py:243-346): the same
-    # camera, 128x128 pixels with supersample 2 (the same ray count), host
-    # wall time of ray set-up, trace and shading to a float32 image.
-    from blackhorizon_b200.offline import OfflineSettings
-    from blackhorizon_b200.vaidya import render_layer_frame_device
-
-    fs = OfflineSettings(supersample=2, fov_degrees=70.0)
-    render_layer_frame_device(st, state[0], side // 2, side // 2, fs, "inward")
-    torch.cuda.synchronize()
-    t = time.perf_counter()
-    for _ in range(reps):
-        render_layer_frame_device(st, state[0], side // 2, side // 2, fs, "inward")
-    torch.cuda.synchronize()
-    out["frame_ms"] = (time.perf_counter() - t) * 1e3 / reps
     if with_cpu:
         from oracle import oracle
 
@@ -919,6 +863,127 @@ def cpu_baseline(state0, spin_h, S, seconds):
                       f"oracle/bh_oracle.c (float64) on {threads} threads, {dt:.1f} s"}
 
 
+def band_radius(band, mass: float, rtol: float) -> float:
+    """The float64 band radius a propagate call resolves to (M units): 'auto'
+    is 8 u M / rtol with u = 2^-24, as the library computes it."""
+    if band == "auto":
+        return 8.0 * 2.0 ** -24 * mass / rtol
+    return float(band)
+
+
+REF_PATH = os.path.join(ROOT, "baseline", "_ref")
+
+
+def _reference_modules():
+    """The reference package installed under baseline/_ref (pip --target),
+    imported unmodified."""
+    if REF_PATH not in sys.path:
+        sys.path.insert(0, REF_PATH)
+    import blackhorizon.geodesics as G
+    import blackhorizon.integrators as I
+    import blackhorizon.kerr as K
+
+    return G, I, K
+
+
+def _reference_propagate(task):
+    """The raw-throughput step in the reference's own NumPy code: S attempted
+    dormand_prince_step calls per ray, each followed by error_ratio and
+    step_factor with the tracer's accept/reject and step update
+    (tracer.py:109-120; the workload has no termination).  Per-ray spin uses
+    an array-valued KerrSpacetime.spin, which geodesic_rhs broadcasts.
+    Returns (seconds of the loop, final states)."""
+    s0, spin, S = task
+    G, I, K = _reference_modules()
+    st = object.__new__(K.KerrSpacetime)
+    st.mass = 1.0
+    st.spin = np.asarray(spin, dtype=np.float64)
+    y = np.array(s0, dtype=np.float64)
+    h = np.full(y.shape[0], 0.1)
+
+    def rhs(batch):
+        return G.geodesic_rhs(st, batch)
+
+    t = time.perf_counter()
+    with np.errstate(all="ignore"):
+        for _ in range(S):
+            y_new, err = I.dormand_prince_step(rhs, y, h)
+            ratio = I.error_ratio(y, y_new, err, 1e-8, 1e-10)
+            ok = ratio <= 1.0
+            y = np.where(ok[:, None], y_new, y)
+            h = np.clip(h * I.step_factor(ratio), 0.0, 2.0)
+    return time.perf_counter() - t, y
+
+
+def _reference_warm(_):
+    _reference_modules()
+    return os.getpid()
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def reference_numpy_baseline(s0, spin_h, seconds, rays_per_proc=4096):
+    """The reference's own NumPy path (installed unmodified under
+    baseline/_ref) on the first rays of the raw-throughput workload, timed on
+    this host: (i) one process, as the reference runs; (ii) one process per
+    host core, each on its own contiguous shard of rays_per_proc rays (rays
+    are independent, so per-ray results are the same).  The step count of the
+    sample is sized from a short probe to about `seconds` / 2 per leg; every
+    step does the same work, so the rate does not depend on it.  Returns
+    {"unavailable": why} when the reference cannot be imported."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+
+    try:
+        _reference_modules()
+    except Exception as exc:  # noqa: BLE001 - the reason goes into the JSON line
+        return {"unavailable": f"reference not importable from baseline/_ref: {exc!r}"}
+    procs = host_threads()
+    m = rays_per_proc
+    probe_steps = 10
+    dt, _ = _reference_propagate((s0[:m], spin_h[:m], probe_steps))
+    S = max(probe_steps, int(0.5 * seconds * probe_steps / max(dt, 1e-6)))
+    dt1, y_ref = _reference_propagate((s0[:m], spin_h[:m], S))
+    single = m * S / dt1
+    # The C port on the same rays and steps: the two must agree.
+    from oracle import oracle
+
+    y_port, _, _ = oracle.propagate(1.0, spin_h[:64], s0[:64], S, 1e-8, 1e-10,
+                                   nthreads=procs)
+    ok = np.all(np.isfinite(y_ref[:64]), axis=1)
+    port_rel = float(np.max(np.abs(y_port[ok] - y_ref[:64][ok]) /
+                            np.maximum(np.abs(y_ref[:64][ok]), 1.0)))
+    total = min(s0.shape[0], procs * m)
+    shards = [(s0[a:a + m], spin_h[a:a + m], S) for a in range(0, total, m)]
+    # Spawned workers (never forked from a process that holds a CUDA
+    # context), warmed up before the timed region.  A worker that cannot
+    # start raises BrokenProcessPool rather than being restarted.
+    with ProcessPoolExecutor(max_workers=procs, mp_context=mp.get_context("spawn")) as pool:
+        list(pool.map(_reference_warm, range(procs)))
+        t = time.perf_counter()
+        list(pool.map(_reference_propagate, shards))
+        dtp = time.perf_counter() - t
+    rays = sum(sh[0].shape[0] for sh in shards)
+    parallel = rays * S / dtp
+    return {"value": parallel, "unit": "ray-steps/s", "cores": procs, "kind": "reference",
+            "sample": f"first {rays} rays x {S} attempted DP5(4) steps of the same workload "
+                      f"({len(shards)} processes of {m} rays), the reference's NumPy "
+                      f"dormand_prince_step / error_ratio / step_factor loop (float64, "
+                      f"baseline/_ref, unmodified), {dtp:.1f} s",
+            "single_process": {"value": single, "rays": m, "steps": S, "seconds": dt1},
+            "cpu_model": cpu_model(),
+            "port_vs_reference_max_rel": port_rel}
+
+
 def run_reference(args):
     """The CPU restatement of the reference algorithm on this host's cores;
     rank 0 only."""
@@ -1028,37 +1093,14 @@ def profile_case(args):
         for _ in range(2):
             trace_tile(st, s0, esc, settings, radii, settings.rtol, settings.max_steps,
                        precision=prec, variant=args.variant)
-    elif args.profile_case == "viewer":
-        from blackhorizon_b200.offline import FlyCamera
-        from blackhorizon_b200.realtime import (BackgroundMode, QualityPreset, RenderSettings,
-                                                render_frame_device)
-        from blackhorizon_b200.workloads import REALTIME_FRAME as F
+    elif args.profile_case == "propagate":
+        from blackhorizon_b200.integrators import propagate
 
-        settings = RenderSettings(spin=F.spin, fov_degrees=F.fov,
-                                  background=BackgroundMode.STARFIELD).apply_preset(
-                                      QualityPreset(F.preset))
-        fly = FlyCamera.from_orbit(F.distance, F.inclination, 0.0)
+        state0, spins, _, _, _ = make_inputs(args.rays, 0, device)
+        band = args.f64_radius if args.f64_radius == "auto" else float(args.f64_radius)
         for _ in range(3):
-            render_frame_device(settings, fly, F.width, F.height, precision=prec)
-    elif args.profile_case == "emission":
-        from blackhorizon_b200.emission import (frame_tables, radiance_image,
-                                                static_observer_lapse)
-        from blackhorizon_b200.offline import FlyCamera, OfflineSettings, trace_frame
-        from blackhorizon_b200.post import develop
-        from blackhorizon_b200.workloads import OFFLINE_FRAME as F
-
-        settings = OfflineSettings(spin=F.spin, supersample=F.supersample,
-                                   max_steps=F.max_steps)
-        cam = FlyCamera.from_orbit(F.distance, F.inclination, F.azimuth)
-        st = KerrSpacetime(1.0, F.spin)
-        fr = trace_frame(cam, F.width, F.height, settings, precision=prec)
-        tables = frame_tables(st, settings, device)
-        lapse = float(static_observer_lapse(st, cam.position))
-        for _ in range(2):
-            hdr = radiance_image(st, fr.status, fr.escape_directions, fr.hit_positions,
-                                 fr.hit_momenta, F.width, F.height, settings, lapse,
-                                 tables=tables)
-            develop(hdr)
+            propagate(KerrSpacetime(1.0, 0.0), state0, args.dp5_steps, rtol=1e-8, atol=1e-10,
+                      precision=prec, spins=spins, variant=args.variant, f64_radius=band)
     else:
         C = DIFFERENTIABLE
         t = lambda x: torch.tensor(x, dtype=torch.float64, device=device)  # noqa: E731

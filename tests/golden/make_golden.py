@@ -1,12 +1,11 @@
 """Generate the golden fixtures under tests/golden/ from the reference itself.
 
-Run in a container where the reference project (MegaKruk/BlackHorizon) is
-importable; it is read from the path given by --reference (default: the
-read-only mount this build was developed against).  The fixtures are small
+Run where the reference project (MegaKruk/BlackHorizon) is importable; it is
+read from the checkout given by --reference (required).  The fixtures are small
 .npz files; MANIFEST.json records the command, the reference files' SHA-256
 and the shapes written, so a reader can regenerate and compare.
 
-    python tests/golden/make_golden.py --reference /root/reference
+    python tests/golden/make_golden.py --reference <path of the reference checkout>
 
 Every workload below is built with the reference's own functions
 (KerrSpacetime, null_momentum_from_velocity, build_state, PinholeCamera,
@@ -987,13 +986,14 @@ def gen_vaidya(ref, out):
     np.savez_compressed(os.path.join(out, "vaidya.npz"), **arrs)
 
 
-_REFERENCE_PATH = "/root/reference"
+_REFERENCE_PATH = ""  # set from --reference
 
 
 def main():
     global _REFERENCE_PATH
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=_REFERENCE_PATH)
+    ap.add_argument("--reference", required=True,
+                    help="path of the reference project checkout (MegaKruk/BlackHorizon)")
     ap.add_argument("--out", default=HERE)
     ap.add_argument("--procs", type=int, default=os.cpu_count() or 1)
     ap.add_argument("--skip-c3", action="store_true")
