@@ -48,6 +48,14 @@ class Tape:
     precision: str
 
 
+# Tape entries per ray of a first attempt when the caller gives no capacity:
+# a ray with more accepted steps than this makes the call trace again with
+# room for max_steps.  (A tape sized for max_steps from the start holds
+# n x max_steps step sizes, 5 GB for a 256x256 frame at 10000 steps, almost
+# all of it unused.)
+FIRST_TAPE_CAPACITY = 1024
+
+
 def trace_with_tape(spacetime: KerrSpacetime, state0: torch.Tensor, escape_radius: float,
                     max_steps: int = 20000, rtol: float = 1e-9, atol: float = 1e-12,
                     initial_step: float = 0.1, max_step: float = 2.0,
@@ -57,29 +65,39 @@ def trace_with_tape(spacetime: KerrSpacetime, state0: torch.Tensor, escape_radiu
                     timeout_s: float = 120.0):
     """trace_rays plus the tape of every ray's accepted steps.
 
+    ``capacity`` is the tape's length per ray.  Without one the tape starts
+    at FIRST_TAPE_CAPACITY entries and the call traces once more with
+    max_steps entries if a ray took more accepted steps than that.
+
     Returns (states, status, steps, Tape)."""
     s = state0.detach().to(torch.float64).contiguous()
     n = s.shape[0]
-    cap = int(capacity or max_steps)
+    cap = int(capacity) if capacity else min(int(max_steps), FIRST_TAPE_CAPACITY)
     lib = _lib.load()
     dev = s.device
     states = torch.empty_like(s)
     status = torch.empty(n, dtype=torch.int32, device=dev)
     steps = torch.empty(n, dtype=torch.int64, device=dev)
-    h_tape = torch.empty((n, cap), dtype=torch.float64, device=dev)
-    nck = (cap + checkpoint_every - 1) // checkpoint_every
-    ckpt = torch.empty((n, nck, 8), dtype=torch.float64, device=dev)
     ws = torch.empty(lib.bh_trace_workspace_bytes(), dtype=torch.uint8, device=dev)
     scene = _lib.Scene(spacetime.mass, spacetime.spin,
                        spacetime.capture_radius(capture_margin), float(escape_radius))
     cfg = make_config(max_steps, rtol, atol, initial_step, max_step, min_step, precision,
                       "aos", timeout_s, variant)
     stream = stream_handle()
-    _lib.check(lib.bh_trace_tape(cfg, scene, ptr(s), ptr(states), ptr(status), ptr(steps), n,
-                                 ptr(h_tape), ptr(ckpt), cap, int(checkpoint_every), ptr(ws),
-                                 stream), "trace_with_tape")
-    st = _lib.TraceStats()
-    _lib.check(lib.bh_trace_stats_read(ptr(ws), st, stream), "trace_with_tape")
+    while True:
+        h_tape = torch.empty((n, cap), dtype=torch.float64, device=dev)
+        nck = (cap + checkpoint_every - 1) // checkpoint_every
+        ckpt = torch.empty((n, nck, 8), dtype=torch.float64, device=dev)
+        _lib.check(lib.bh_trace_tape(cfg, scene, ptr(s), ptr(states), ptr(status), ptr(steps),
+                                     n, ptr(h_tape), ptr(ckpt), cap, int(checkpoint_every),
+                                     ptr(ws), stream), "trace_with_tape")
+        st = _lib.TraceStats()
+        rc = lib.bh_trace_stats_read(ptr(ws), st, stream)
+        if rc == _lib.BH_ERR_TAPE and not capacity and cap < int(max_steps):
+            cap = int(max_steps)
+            continue
+        _lib.check(rc, "trace_with_tape")
+        break
     tape = Tape(h_tape, ckpt, steps, cap, int(checkpoint_every), spacetime.mass,
                 spacetime.spin, precision)
     return states, status, steps, tape

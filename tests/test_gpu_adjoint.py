@@ -297,3 +297,23 @@ def test_c5_pixel_coordinate_gradients(cuda):
             assert err <= max(1e-5 * abs(rich), 1e-9), (i, which, g[i], d, rich)
             checked += 1
     assert checked == 24
+
+
+def test_tape_grows_when_a_ray_outruns_it(cuda, monkeypatch):
+    """Without a capacity the tape starts short and the trace runs again with
+    room for max_steps when a ray overflows it: the result equals a trace
+    with the full capacity from the start."""
+    from blackhorizon_b200 import adjoint as adj
+    from blackhorizon_b200.kerr import KerrSpacetime
+
+    st = KerrSpacetime(1.0, 0.7)
+    s0, _ = small_frame()
+    kw = dict(max_steps=5000, rtol=1e-9, capture_margin=0.01, checkpoint_every=16)
+    full = adj.trace_with_tape(st, s0, 100.0, capacity=5000, **kw)
+    monkeypatch.setattr(adj, "FIRST_TAPE_CAPACITY", 8)
+    grown = adj.trace_with_tape(st, s0, 100.0, **kw)
+    assert int(full[2].max()) > 8 and grown[3].capacity == 5000
+    assert torch.equal(full[0], grown[0]) and torch.equal(full[2], grown[2])
+    g = torch.ones_like(s0) * (full[1] == 2)[:, None]
+    a, b = adj.adjoint(full[3], g), adj.adjoint(grown[3], g)
+    assert torch.equal(a[0], b[0]) and torch.equal(a[1], b[1])
