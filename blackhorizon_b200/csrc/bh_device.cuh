@@ -538,24 +538,12 @@ __device__ __forceinline__ StageV<V> stage_at(const KerrV<V> &K, const WStateV<V
 // arithmetic to dormand_prince_step, which recomputes k1 every call.  The
 // embedded error is h times out.err.  The time component's sums are
 // accumulated as the stages are produced (it never feeds a stage input).
-// BH_F64_ROLLED = 1 gives the float64 lanes dp5_attempt_rolled (below).
-#ifndef BH_F64_ROLLED
-#define BH_F64_ROLLED 0
-#endif
-__device__ __forceinline__ void dp5_attempt_rolled(const KerrV<double> &K,
-                                                   const WStateV<double> &yw, double hw,
-                                                   const StageV<double> &k1,
-                                                   AttemptV<double> &out);
 template <class V>
 __device__ __forceinline__ void dp5_attempt(const KerrV<V> &K, const WStateV<V> &yw,
                                             V hw, const StageV<V> &k1,
                                             AttemptV<V> &out) {
     using namespace dp;
     using T = VT<V>;
-    if constexpr (std::is_same<V, double>::value && BH_F64_ROLLED != 0) {
-        dp5_attempt_rolled(K, yw, hw, k1, out);
-        return;
-    }
     V it = T::set(B1) * k1.thl;
     V et = T::set(E1) * k1.thl;
     const StageV<V> k2 = stage_at<V>(K, yw, hw, C2, T::set(A21) * k1.kx, T::set(A21) * k1.ky,
@@ -620,115 +608,6 @@ __device__ __forceinline__ void dp5_attempt(const KerrV<V> &K, const WStateV<V> 
     // Embedded error / h (e2 = 0): the exact parts p and -p_t cancel because
     // the weights e_i sum to zero.
     out.err[0] = T::fma(T::set(E7), s7.thl, et);
-    out.err[1] = BH_LIN6(kx, E1, k1, E3, k3, E4, k4, E5, k5, E6, k6, E7, s7);
-    out.err[2] = BH_LIN6(ky, E1, k1, E3, k3, E4, k4, E5, k5, E6, k6, E7, s7);
-    out.err[3] = BH_LIN6(kz, E1, k1, E3, k3, E4, k4, E5, k5, E6, k6, E7, s7);
-    out.err[4] = BH_LIN6(px, E1, k1, E3, k3, E4, k4, E5, k5, E6, k6, E7, s7);
-    out.err[5] = BH_LIN6(py, E1, k1, E3, k3, E4, k4, E5, k5, E6, k6, E7, s7);
-    out.err[6] = BH_LIN6(pz, E1, k1, E3, k3, E4, k4, E5, k5, E6, k6, E7, s7);
-}
-
-// The float64 lanes' attempt with one RHS call site instead of seven:
-// stage i = 2..7 takes its input from a static linear combination of the
-// earlier stages (one switch case per stage, so every stage derivative stays
-// in registers) and evaluates the RHS once per pass; stage 7 is the
-// first-same-as-last derivative at the fifth-order solution.  Every
-// operation is dp5_attempt's, in the same order, so results are
-// bit-identical; the kernel's code shrinks by six RHS copies.
-__device__ __forceinline__ void dp5_attempt_rolled(const KerrV<double> &K,
-                                                   const WStateV<double> &yw, double hw,
-                                                   const StageV<double> &k1,
-                                                   AttemptV<double> &out) {
-    using namespace dp;
-    using T = VT<double>;
-    StageV<double> k2, k3, k4, k5, k6, s7;
-    double it = B1 * k1.thl;
-    double et = E1 * k1.thl;
-    double r2n = 0.0;
-#pragma unroll 1
-    for (int i = 2; i <= 7; ++i) {
-        double c, sx, sy, sz, spx, spy, spz;
-        switch (i) {
-            case 2:
-                c = C2;
-                sx = A21 * k1.kx; sy = A21 * k1.ky; sz = A21 * k1.kz;
-                spx = A21 * k1.px; spy = A21 * k1.py; spz = A21 * k1.pz;
-                break;
-            case 3:
-                c = C3;
-                sx = BH_LIN2(kx, A31, k1, A32, k2); sy = BH_LIN2(ky, A31, k1, A32, k2);
-                sz = BH_LIN2(kz, A31, k1, A32, k2); spx = BH_LIN2(px, A31, k1, A32, k2);
-                spy = BH_LIN2(py, A31, k1, A32, k2); spz = BH_LIN2(pz, A31, k1, A32, k2);
-                break;
-            case 4:
-                c = C4;
-                sx = BH_LIN3(kx, A41, k1, A42, k2, A43, k3);
-                sy = BH_LIN3(ky, A41, k1, A42, k2, A43, k3);
-                sz = BH_LIN3(kz, A41, k1, A42, k2, A43, k3);
-                spx = BH_LIN3(px, A41, k1, A42, k2, A43, k3);
-                spy = BH_LIN3(py, A41, k1, A42, k2, A43, k3);
-                spz = BH_LIN3(pz, A41, k1, A42, k2, A43, k3);
-                break;
-            case 5:
-                c = C5;
-                sx = BH_LIN4(kx, A51, k1, A52, k2, A53, k3, A54, k4);
-                sy = BH_LIN4(ky, A51, k1, A52, k2, A53, k3, A54, k4);
-                sz = BH_LIN4(kz, A51, k1, A52, k2, A53, k3, A54, k4);
-                spx = BH_LIN4(px, A51, k1, A52, k2, A53, k3, A54, k4);
-                spy = BH_LIN4(py, A51, k1, A52, k2, A53, k3, A54, k4);
-                spz = BH_LIN4(pz, A51, k1, A52, k2, A53, k3, A54, k4);
-                break;
-            case 6:
-                c = C6;
-                sx = BH_LIN5(kx, A61, k1, A62, k2, A63, k3, A64, k4, A65, k5);
-                sy = BH_LIN5(ky, A61, k1, A62, k2, A63, k3, A64, k4, A65, k5);
-                sz = BH_LIN5(kz, A61, k1, A62, k2, A63, k3, A64, k4, A65, k5);
-                spx = BH_LIN5(px, A61, k1, A62, k2, A63, k3, A64, k4, A65, k5);
-                spy = BH_LIN5(py, A61, k1, A62, k2, A63, k3, A64, k4, A65, k5);
-                spz = BH_LIN5(pz, A61, k1, A62, k2, A63, k3, A64, k4, A65, k5);
-                break;
-            default:
-                // Fifth-order solution (b2 = b7 = 0): the increments, and the
-                // new state as the stage input of the FSAL evaluation.
-                c = 1.0;
-                out.it = it;
-                out.ix = BH_LIN5(kx, B1, k1, B3, k3, B4, k4, B5, k5, B6, k6);
-                out.iy = BH_LIN5(ky, B1, k1, B3, k3, B4, k4, B5, k5, B6, k6);
-                out.iz = BH_LIN5(kz, B1, k1, B3, k3, B4, k4, B5, k5, B6, k6);
-                sx = out.ix; sy = out.iy; sz = out.iz;
-                spx = BH_LIN5(px, B1, k1, B3, k3, B4, k4, B5, k5, B6, k6);
-                spy = BH_LIN5(py, B1, k1, B3, k3, B4, k4, B5, k5, B6, k6);
-                spz = BH_LIN5(pz, B1, k1, B3, k3, B4, k4, B5, k5, B6, k6);
-                break;
-        }
-        const double dpx = hw * spx, dpy = hw * spy, dpz = hw * spz;
-        const double X = fma(hw, fma(c, yw.px, sx), yw.x);
-        const double Y = fma(hw, fma(c, yw.py, sy), yw.y);
-        const double Z = fma(hw, fma(c, yw.pz, sz), yw.z);
-        const StageV<double> k = rhs_v<double>(K, X, Y, Z, yw.npt, yw.px + dpx, yw.py + dpy,
-                                               yw.pz + dpz, dpx, dpy, dpz, &r2n);
-        switch (i) {
-            case 2: k2 = k; break;
-            case 3: k3 = k; it = fma(B3, k3.thl, it); et = fma(E3, k3.thl, et); break;
-            case 4: k4 = k; it = fma(B4, k4.thl, it); et = fma(E4, k4.thl, et); break;
-            case 5: k5 = k; it = fma(B5, k5.thl, it); et = fma(E5, k5.thl, et); break;
-            case 6: k6 = k; it = fma(B6, k6.thl, it); et = fma(E6, k6.thl, et); break;
-            default:
-                s7 = k;
-                out.dpx = dpx; out.dpy = dpy; out.dpz = dpz;
-                out.ynw.t = fma(hw, yw.npt + it, yw.t);
-                out.ynw.x = X; out.ynw.y = Y; out.ynw.z = Z;
-                out.ynw.npt = yw.npt;
-                out.ynw.px = yw.px + dpx; out.ynw.py = yw.py + dpy; out.ynw.pz = yw.pz + dpz;
-                break;
-        }
-    }
-    out.r2n = r2n;
-    out.k7 = s7;
-    out.k7.kx = s7.kx - out.dpx;
-    out.k7.ky = s7.ky - out.dpy;
-    out.k7.kz = s7.kz - out.dpz;
-    out.err[0] = fma(E7, s7.thl, et);
     out.err[1] = BH_LIN6(kx, E1, k1, E3, k3, E4, k4, E5, k5, E6, k6, E7, s7);
     out.err[2] = BH_LIN6(ky, E1, k1, E3, k3, E4, k4, E5, k5, E6, k6, E7, s7);
     out.err[3] = BH_LIN6(kz, E1, k1, E3, k3, E4, k4, E5, k5, E6, k6, E7, s7);

@@ -211,36 +211,6 @@ __device__ __forceinline__ bool refine_hit(double m, double a, double r_in, doub
     return r >= r_in && r <= r_out;
 }
 
-// BH_TILE_OUTLINE = 1 calls the in-place refinement of the INLINE rounds and
-// the finalisation of a ray through out-of-line functions (scalar arguments):
-// both are rare per attempt, and inlined they enlarge the stepping loop.
-#ifndef BH_TILE_OUTLINE
-#define BH_TILE_OUTLINE 0
-#endif
-struct RefineOut {
-    RayState yc;
-    bool hit;
-};
-static __device__ __noinline__ RefineOut refine_hit_call(double m, double a, double r_in,
-                                                         double r_out, double t, double x,
-                                                         double y, double z, double pt,
-                                                         double px, double py, double pz,
-                                                         double h) {
-    RefineOut o;
-    o.hit = refine_hit(m, a, r_in, r_out, RayState{t, x, y, z, pt, px, py, pz}, h, o.yc);
-    return o;
-}
-
-// tile_finalize of a ray, out of line (hit: the crossing state of a disk hit).
-static __device__ __noinline__ void tile_finalize_call(TileArgs a, long long ray, double t,
-                                                       double x, double y, double z, double pt,
-                                                       double px, double py, double pz,
-                                                       int st, long long steps, bool has_hit,
-                                                       RayState hit) {
-    const RayState ys{t, x, y, z, pt, px, py, pz};
-    tile_finalize(a, ray, ys, st, steps, has_hit ? &hit : nullptr);
-}
-
 // INLINE = false: every crossing is parked for the refinement kernel, and
 // the misses come back as the next round's resumed rays.  INLINE = true
 // (the rounds that start with few resumed rays): crossings are refined in
@@ -289,12 +259,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) tile_kernel(const TileArgs args) 
 
     unsigned long long my_cross = 0, my_hits = 0;
     auto finish = [&](int l, const RayState &y, int st, const RayState *hit) {
-#if BH_TILE_OUTLINE
-        tile_finalize_call(args, ray[l], y.t, y.x, y.y, y.z, y.pt, y.px, y.py, y.pz, st,
-                           steps[l], hit != nullptr, hit ? *hit : y);
-#else
         tile_finalize(args, ray[l], y, st, steps[l], hit);
-#endif
         my_attempts += attempts[l];
         my_accepted += steps[l];
         if (attempts[l] > my_max_attempts) my_max_attempts = attempts[l];
@@ -390,18 +355,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) tile_kernel(const TileArgs args) 
                     RayState y1 = y0;
                     commit<V>(y1, yw, a, l, h[l]);
                     if (INLINE && disk && y0.z * y1.z < 0.0) {
-                        ++my_cross;
-#if BH_TILE_OUTLINE
-                        const RefineOut ro = refine_hit_call(
-                            args.mass, args.spin, args.disk_inner, args.disk_outer, y0.t, y0.x,
-                            y0.y, y0.z, y0.pt, y0.px, y0.py, y0.pz, h[l]);
-                        const RayState &yc = ro.yc;
-                        if (ro.hit) {
-#else
                         RayState yc;
+                        ++my_cross;
                         if (refine_hit(args.mass, args.spin, args.disk_inner, args.disk_outer,
                                        y0, h[l], yc)) {
-#endif
                             ++my_hits;
                             finish(l, y0, BH_RAY_DISK, &yc);
                             acc[l] = false;

@@ -298,13 +298,15 @@ __device__ __noinline__ BandStep band_attempt(double *p, double mass, double spi
 // until the queue drains (a fixed grid-stride split left a quarter of the
 // warp slots idle while the slowest warps finished).
 //
-// BAND (mixed lanes only): while one of the warp's rays lies between the
-// outer horizon and the band radius (args.f64_r2), the whole warp's attempt
-// runs in float64 (band_attempt, the float64 policy's step); outside it the
-// float stages run.  The test reads r^2 at each ray's current state from its
-// last derivative evaluation, and is warp-uniform, so the two paths never
-// diverge within a warp.  Inside the horizon the float stages run: the
-// reference's tracer captures such rays.
+// BAND (mixed lanes only): while one of the warp's rays lies between 1.01
+// times the outer horizon radius and the band radius (args.f64_r2), the whole
+// warp's attempt runs in float64 (band_attempt, the float64 policy's step);
+// outside it the float stages run.  The test reads r^2 at each ray's current
+// state from its last derivative evaluation, and is warp-uniform, so the two
+// paths never diverge within a warp; the rays that share a warp are the 64
+// (two per lane) of one claim, [64 k, 64 k + 64) of the launch.  Closer to
+// the horizon the float stages run: the reference's tracer captures such
+// rays.
 template <class V, int BLOCK, int MINB, bool PROJECT, bool BAND = false>
 __global__ void __launch_bounds__(BLOCK, MINB) propagate_kernel(const TraceArgs args) {
     using T = VT<V>;
@@ -362,10 +364,17 @@ __global__ void __launch_bounds__(BLOCK, MINB) propagate_kernel(const TraceArgs 
             // evaluation (BAND only).
             V r2c = T::set(0.0);
             StageV<V> k1 = first_stage_r2<V>(K, yw, BAND ? &r2c : nullptr);
-            float rp2[N];  // squared outer-horizon radius per lane (BAND)
+            // Squared lower edge of the band per lane (BAND): 1.01 r_+.  A
+            // past-directed ray that reaches the outer horizon approaches r_+
+            // only asymptotically in these coordinates (the ingoing chart does
+            // not cover the past horizon), so it sits just above r_+ for the
+            // rest of a no-termination run; the tracers capture it at
+            // r_+ (1 + margin), and below 1.01 r_+ the float stages run.
+            float rp2[N];
 #pragma unroll
             for (int l = 0; l < N; ++l) {
-                const double rp = mass[l] + ::sqrt(fmax(mass[l] * mass[l] - spin[l] * spin[l], 0.0));
+                const double rp =
+                    1.01 * (mass[l] + ::sqrt(fmax(mass[l] * mass[l] - spin[l] * spin[l], 0.0)));
                 rp2[l] = float(rp * rp);
             }
             const float band2 = float(args.f64_r2);

@@ -191,7 +191,7 @@ def propagate(spacetime, state0: Array, n_steps: int, rtol: float = 1e-8,
     Mixed policy: the stage arithmetic runs in float32 except in the float64
     band: while a ray of a warp lies between the outer horizon and
     ``f64_radius`` (units of M), the warp's attempt runs in float64 (with the
-    default launch shape).  The default ``"auto"`` puts the band's edge at
+    default launch shape; a warp holds rays [64 k, 64 k + 64) of the call).  The default ``"auto"`` puts the band's edge at
     8 u M / rtol (u = 2^-24), where float32 rounding of the curvature terms
     reaches the tolerance; 0 runs float32 stages everywhere.  Ignored by the
     float64 policy and, under ``"auto"``, by projecting calls.
@@ -298,9 +298,14 @@ def _propagate_streamed(spacetime, state0, n_steps, rtol, atol, initial_step, ma
     acc = torch.empty(n, dtype=torch.int64, device=dev)
     spin_d = None if spins is None else torch.empty(n, dtype=torch.float64, device=dev)
     k = max(1, min(int(chunks), n))
-    bounds = [(n * c // k, n * (c + 1) // k) for c in range(k)]
+    # Pieces start at multiples of 64 rays: a warp of the mixed propagator
+    # holds rays [64 j, 64 j + 64) of its launch and decides its float64 band
+    # for all of them, so aligned pieces give every ray the warp-mates, and
+    # hence the results, of the single launch.
+    cuts = [min(n, (n * c // k + 63) // 64 * 64) for c in range(k)] + [n]
+    bounds = [(a, b) for a, b in zip(cuts[:-1], cuts[1:]) if b > a]
     ws = [torch.empty(lib.bh_trace_workspace_bytes(), dtype=torch.uint8, device=dev)
-          for _ in range(k)]
+          for _ in bounds]
     cfg = make_config(1, rtol, atol, initial_step, max_step, 0.0, precision, "aos", timeout_s,
                       variant, 0, project_every,
                       f64_radius=_propagate_band(f64_radius, precision, project_every))
@@ -323,7 +328,7 @@ def _propagate_streamed(spacetime, state0, n_steps, rtol, atol, initial_step, ma
     for st in streams:
         main.wait_stream(st)
     stats = _lib.TraceStats()
-    for c in range(k):
+    for c in range(len(bounds)):
         part = _lib.TraceStats()
         _lib.check(lib.bh_trace_stats_read(ptr(ws[c]), part, stream_handle()), "propagate")
         stats.attempts += part.attempts

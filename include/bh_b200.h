@@ -98,7 +98,8 @@ typedef struct {
     int32_t reserved;      /* 0 */
     /* bh_propagate, BH_PRECISION_MIXED: radius (units of M) of the float64
      * band.  An attempt runs float64 stage arithmetic for every ray of a
-     * warp while one of them lies between the outer horizon and f64_radius;
+     * warp (rays [64 k, 64 k + 64) of the call) while one of them lies
+     * between 1.01 r_+ and f64_radius;
      * elsewhere the stages run in float32.  0 = no band; < 0 = 8 u M / rtol
      * (u = 2^-24), where the float32 rounding of the curvature terms, about
      * 4 u of their relative size 2 M / r, reaches the tolerance.  Must be 0
