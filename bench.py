@@ -5,9 +5,10 @@ Kerr-Schild sphere r = 30 M, directions uniform on the local sky, spin
 uniform in [-0.95, 0.95] per ray, past-directed null momenta; each step is
 2000 attempted DP5(4) steps per ray with per-ray error control (rtol 1e-8,
 atol 1e-10, h0 0.1, max_step 2) and no termination.  The product arm runs
-the mixed-precision kernel (float32 stage arithmetic, float64 state, error
-norm and step control); the plain float64 kernel runs on the same inputs and
-is reported beside it.  Synthetic data from seed 20260 (the reference's
+the mixed-precision kernel (float32 stage arithmetic with a float64 band near
+the hole, float64 state, error norm and step control); the plain float64
+kernel and the mixed kernel without the band run on the same inputs and are
+reported beside it.  Synthetic data from seed 20260 (the reference's
 benchmark has no dataset).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
@@ -20,7 +21,8 @@ its own 2^20 rays (weak scaling, no collective in the data path).
 
 ``--impl reference`` times the CPU restatement of the reference's algorithm
 (oracle/bh_oracle.c, all host cores) on a bounded sample of the same
-workload.
+workload.  The line's cpu_baseline is the reference's own NumPy code
+(installed under baseline/_ref) on the host's cores.
 """
 
 from __future__ import annotations
@@ -49,11 +51,11 @@ FLOPS_PER_RAY_STEP = 1336
 # out (2 x 8), accepted count (8).
 BYTES_PER_RAY = 176
 # DRAM bytes per ray of one propagate launch measured by ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum of a 2^21-ray, 200-step
-# launch of the default variants).  The state stays on chip between steps,
-# so the traffic grows with the ray count only; the benchmark scales it to
-# its own ray count.
-NCU_DRAM_BYTES_PER_RAY = {"mixed": 150.6, "fp64": 153.7}
+# (dram__bytes_read.sum + dram__bytes_write.sum of the default kernels on
+# 2^21 rays: mixed at 2000 steps, fp64 at 200).  The state stays on chip
+# between steps, so the traffic grows with the ray count only; the benchmark
+# scales it to its own ray count.
+NCU_DRAM_BYTES_PER_RAY = {"mixed": 156.0, "fp64": 153.7}
 
 METRIC = "ray-steps/s"
 
@@ -404,8 +406,8 @@ def run_ours(args):
                 "algorithmic_bytes": n * BYTES_PER_RAY,
                 "traffic": NCU_DRAM_BYTES_PER_RAY[prec] * n,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of a "
-                                  "2^21-ray 200-step launch, scaled by rays (independent "
-                                  "of the step count)",
+                                  "2^21-ray launch of the default kernel, scaled by rays "
+                                  "(independent of the step count)",
             },
             "gpu_launches": args.steps,
             "e2e": {
