@@ -260,23 +260,40 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args
 
 // One float64 DP5(4) attempt with the float64 policy's controller, for one
 // ray of a mixed thread: the float64 band of propagate_kernel.  p points at
-// the ray's float64 state in the block's state store (P doubles between
-// components); the state is updated there when the attempt is accepted.
-// The first-same-as-last derivative is evaluated afresh in float64 (the
-// float path keeps its own).  Not inlined: the band is the rare path, and
-// one out-of-line copy keeps the float loop's code compact.
+// the ray's float64 state in the block's state store and kp at its float64
+// first-same-as-last derivative (7 planes after the state's 8, P doubles
+// between components).  With have_k1 the stored derivative belongs to the
+// current state (the previous attempt was a band attempt too); otherwise it
+// is evaluated here.  The state and the derivative are updated there when the
+// attempt is accepted.  BH_BAND_INLINE = 0 keeps the band step out of line
+// (one copy, the rare path's code apart from the float loop's).
+#ifndef BH_BAND_INLINE
+#define BH_BAND_INLINE 0
+#endif
 struct BandStep {
     double h;       // the controller's next step size
     bool accepted;
 };
 template <int P>
-__device__ __noinline__ BandStep band_attempt(double *p, double mass, double spin, double h,
-                                              double rtol, double atol, double max_step) {
+#if BH_BAND_INLINE
+__device__ __forceinline__
+#else
+__device__ __noinline__
+#endif
+BandStep band_attempt(double *p, double *kp, bool have_k1, double mass, double spin, double h,
+                      double rtol, double atol, double max_step) {
     RayState y{p[0], p[P], p[2 * P], p[3 * P], p[4 * P], p[5 * P], p[6 * P], p[7 * P]};
     const KerrV<double> K = make_kerr<double>(mass, spin);
     WStateV<double> w;
     put_work<double>(w, 0, y);
-    const StageV<double> k1 = first_stage<double>(K, w);
+    StageV<double> k1;
+    if (have_k1) {
+        k1 = StageV<double>{kp[0], kp[P], kp[2 * P], kp[3 * P], kp[4 * P], kp[5 * P], kp[6 * P]};
+    } else {
+        k1 = first_stage<double>(K, w);
+        kp[0] = k1.kx; kp[P] = k1.ky; kp[2 * P] = k1.kz; kp[3 * P] = k1.thl;
+        kp[4 * P] = k1.px; kp[5 * P] = k1.py; kp[6 * P] = k1.pz;
+    }
     AttemptV<double> a;
     dp5_attempt<double>(K, w, h, k1, a);
     double ratio[1];
@@ -287,6 +304,9 @@ __device__ __noinline__ BandStep band_attempt(double *p, double mass, double spi
         commit<double>(y, w, a, 0, h);
         p[0] = y.t; p[P] = y.x; p[2 * P] = y.y; p[3 * P] = y.z;
         p[5 * P] = y.px; p[6 * P] = y.py; p[7 * P] = y.pz;
+        const StageV<double> &k7 = a.k7;
+        kp[0] = k7.kx; kp[P] = k7.ky; kp[2 * P] = k7.kz; kp[3 * P] = k7.thl;
+        kp[4 * P] = k7.px; kp[5 * P] = k7.py; kp[6 * P] = k7.pz;
     }
     return BandStep{next_step<true>(h, ratio[0], max_step), ok};
 }
@@ -378,6 +398,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) propagate_kernel(const TraceArgs 
                 rp2[l] = float(rp * rp);
             }
             const float band2 = float(args.f64_r2);
+            // Whether a lane's float64 derivative in shared memory belongs to
+            // its current state (BAND).
+            bool band_k1[N];
+#pragma unroll
+            for (int l = 0; l < N; ++l) band_k1[l] = false;
             long long k = 0;
             for (; k < args.max_attempts; ++k) {
                 bool in_band = false;
@@ -393,9 +418,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) propagate_kernel(const TraceArgs 
                 if (in_band) {
 #pragma unroll
                     for (int l = 0; l < N; ++l) {
+                        double *slot = ys.sh + l * BLOCK + threadIdx.x;
                         const BandStep b = band_attempt<N * BLOCK>(
-                            ys.sh + l * BLOCK + threadIdx.x, mass[l], spin[l], h[l], args.rtol,
-                            args.atol, args.max_step);
+                            slot, slot + 8 * N * BLOCK, band_k1[l], mass[l], spin[l], h[l],
+                            args.rtol, args.atol, args.max_step);
+                        band_k1[l] = true;
                         if (b.accepted) {
                             lam[l] += h[l];
                             ++acc[l];
@@ -423,6 +450,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) propagate_kernel(const TraceArgs 
                             ys.set(l, yl);
                             lam[l] += h[l];
                             ++acc[l];
+                            band_k1[l] = false;
                         }
                         h[l] = next_step<F64>(h[l], ratio[l], args.max_step);
                     }
@@ -529,7 +557,8 @@ static const void *kfn(bool propagate, size_t *smem) {
 static const void *kernel_for(bool propagate, int precision, int idx, bool project,
                               size_t *smem, bool band = false) {
     if (band && propagate && precision == BH_PRECISION_MIXED) {
-        *smem = StateStore<F2, 128>::shared_bytes();
+        // The state store plus 7 planes of float64 band derivatives.
+        *smem = StateStore<F2, 128>::shared_bytes() + size_t(7) * 2 * 128 * 8;
         return (const void *)propagate_kernel<F2, 128, 3, false, true>;
     }
     if (project) {
