@@ -69,8 +69,11 @@ __device__ __forceinline__ int tile_check(const TileArgs &a, const RayState &y,
     return -1;
 }
 
-// Writes every output of a finished ray.  hit: the refined crossing state of
-// a disk hit, else null.
+// Writes the per-ray outputs of a finished ray.  hit: the refined crossing
+// state of a disk hit, else null.  The hit buffers were zeroed before the
+// rounds, and the escape directions are computed after them from the final
+// states (escape_dir_kernel): both would otherwise be single-lane work inside
+// the stepping loop, where the rest of the warp waits.
 __device__ __forceinline__ void tile_finalize(const TileArgs &a, long long ray,
                                               const RayState &y, int st, long long steps,
                                               const RayState *hit) {
@@ -79,16 +82,26 @@ __device__ __forceinline__ void tile_finalize(const TileArgs &a, long long ray,
     a.steps[ray] = steps;
     // render.py:289-291
     a.saturated[ray] = (st == BH_RAY_MAX_STEPS || steps >= a.saturate_steps) ? 1 : 0;
-    double *hp = a.hit_pos + 3 * ray, *hm = a.hit_mom + 3 * ray, *ed = a.escape_dir + 3 * ray;
     if (hit) {
+        double *hp = a.hit_pos + 3 * ray, *hm = a.hit_mom + 3 * ray;
         hp[0] = hit->x; hp[1] = hit->y; hp[2] = hit->z;
         hm[0] = hit->px; hm[1] = hit->py; hm[2] = hit->pz;
-    } else {
-        hp[0] = hp[1] = hp[2] = 0.0;
-        hm[0] = hm[1] = hm[2] = 0.0;
     }
-    if (st == BH_RAY_ESCAPED) {
-        // render.py:164-181: dx = p - 2 H lp l, lp = -p_t + l.p, normalised.
+}
+
+// Escape directions of every finished ray, one thread per ray, from the final
+// states (render.py:164-181): dx = p - 2 H lp l, lp = -p_t + l.p, normalised;
+// zero for rays that did not escape.
+__global__ void __launch_bounds__(256) escape_dir_kernel(const TileArgs a) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n;
+         i += (long long)gridDim.x * blockDim.x) {
+        double *ed = a.escape_dir + 3 * i;
+        if (a.status[i] != BH_RAY_ESCAPED) {
+            ed[0] = ed[1] = ed[2] = 0.0;
+            continue;
+        }
+        RayState y;
+        load_state(a.states, a.n, a.layout, i, y);
         Geometry g;
         geometry_full(a.mass, a.spin, y.x, y.y, y.z, false, g);
         const double lp = -y.pt + ((g.l[0] * y.px + g.l[1] * y.py) + g.l[2] * y.pz);
@@ -96,8 +109,6 @@ __device__ __forceinline__ void tile_finalize(const TileArgs &a, long long ray,
         const double d0 = y.px - c * g.l[0], d1 = y.py - c * g.l[1], d2 = y.pz - c * g.l[2];
         const double nrm = ::sqrt((d0 * d0 + d1 * d1) + d2 * d2);
         ed[0] = d0 / nrm; ed[1] = d1 / nrm; ed[2] = d2 / nrm;
-    } else {
-        ed[0] = ed[1] = ed[2] = 0.0;
     }
 }
 
@@ -760,6 +771,13 @@ extern "C" int bh_trace_tile(const bh_trace_config *config, const bh_scene *scen
     a.saturated = saturated;
     int rc = tile_cuda(cudaMemsetAsync(base, 0, sizeof(TileWorkspace), s), "bh_trace_tile reset");
     if (rc != BH_OK) return rc;
+    // Rays that end off the disk report zero hit position and momentum.
+    rc = tile_cuda(cudaMemsetAsync(hit_positions, 0, (size_t)n * 3 * sizeof(double), s),
+                   "bh_trace_tile hit reset");
+    if (rc != BH_OK) return rc;
+    rc = tile_cuda(cudaMemsetAsync(hit_momenta, 0, (size_t)n * 3 * sizeof(double), s),
+                   "bh_trace_tile hit reset");
+    if (rc != BH_OK) return rc;
     const auto t0 = std::chrono::steady_clock::now();
     // Each round moves every resumed ray past at least one accepted step.
     // max_steps + 2 rounds bound the loop; past that a flush round finalises
@@ -806,6 +824,18 @@ extern "C" int bh_trace_tile(const bh_trace_config *config, const bh_scene *scen
             if (rc != BH_OK) return rc;
             a.resume = resume_sorted;
         }
+    }
+    {
+        int dev = 0, sms = 0;
+        rc = tile_cuda(cudaGetDevice(&dev), "bh_trace_tile device");
+        if (rc != BH_OK) return rc;
+        rc = tile_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev),
+                       "bh_trace_tile device");
+        if (rc != BH_OK) return rc;
+        const long long need = (n + 255) / 256;
+        escape_dir_kernel<<<(unsigned)(need < 8LL * sms ? need : 8LL * sms), 256, 0, s>>>(a);
+        rc = tile_cuda(cudaGetLastError(), "bh_trace_tile escape directions");
+        if (rc != BH_OK) return rc;
     }
     TileWorkspace hw;
     rc = tile_cuda(cudaMemcpyAsync(&hw, a.ws, sizeof(hw), cudaMemcpyDeviceToHost, s),

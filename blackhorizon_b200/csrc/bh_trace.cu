@@ -270,6 +270,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args
 #ifndef BH_BAND_INLINE
 #define BH_BAND_INLINE 0
 #endif
+// BH_BAND_INWARD = 1 (default): outside 4.5 M only inward-moving rays keep a
+// warp in the band (see propagate_kernel); 0 applies the band to every ray
+// in its radius range.
+#ifndef BH_BAND_INWARD
+#define BH_BAND_INWARD 1
+#endif
 struct BandStep {
     double h;       // the controller's next step size
     bool accepted;
@@ -319,8 +325,9 @@ BandStep band_attempt(double *p, double *kp, bool have_k1, double mass, double s
 // warp slots idle while the slowest warps finished).
 //
 // BAND (mixed lanes only): while one of the warp's rays lies between 1.01
-// times the outer horizon radius and the band radius (args.f64_r2), the whole
-// warp's attempt runs in float64 (band_attempt, the float64 policy's step);
+// times the outer horizon radius and the band radius (args.f64_r2), and is
+// moving inward or lies inside 4.5 M, the whole warp's attempt runs in
+// float64 (band_attempt, the float64 policy's step);
 // outside it the float stages run.  The test reads r^2 at each ray's current
 // state from its last derivative evaluation, and is warp-uniform, so the two
 // paths never diverge within a warp; the rays that share a warp are the 64
@@ -411,7 +418,28 @@ __global__ void __launch_bounds__(BLOCK, MINB) propagate_kernel(const TraceArgs 
 #pragma unroll
                     for (int l = 0; l < N; ++l) {
                         const float r2l = T::get(r2c, l);
-                        mine |= r2l > rp2[l] && r2l < band2;
+                        bool in = r2l > rp2[l] && r2l < band2;
+#if BH_BAND_INWARD
+                        // Outside 4.5 M (beyond every spherical photon orbit:
+                        // they lie at r <= 4 M) an outgoing ray has no radial
+                        // turning point left and escapes, so nothing amplifies
+                        // its float32 rounding later: only inward rays need
+                        // the band there.  dr/dlam has the sign of
+                        // x.v + z v_z a^2 / r^2, v = p + kappa_1.
+                        const float ml = float(mass[l]);
+                        if (in && r2l > 20.25f * ml * ml) {
+                            const float vx = T::get(yw.px, l) + T::get(k1.kx, l);
+                            const float vy = T::get(yw.py, l) + T::get(k1.ky, l);
+                            const float vz = T::get(yw.pz, l) + T::get(k1.kz, l);
+                            const float zl = T::get(yw.z, l);
+                            const float a2l = float(spin[l] * spin[l]);
+                            const float rdot = fmaf(T::get(yw.x, l), vx,
+                                                    fmaf(T::get(yw.y, l), vy,
+                                                         zl * vz * (1.0f + a2l / r2l)));
+                            in = rdot < 0.0f;
+                        }
+#endif
+                        mine |= in;
                     }
                     in_band = __any_sync(act, mine);
                 }
