@@ -265,28 +265,14 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args
 // between components).  With have_k1 the stored derivative belongs to the
 // current state (the previous attempt was a band attempt too); otherwise it
 // is evaluated here.  The state and the derivative are updated there when the
-// attempt is accepted.  BH_BAND_INLINE = 0 keeps the band step out of line
-// (one copy, the rare path's code apart from the float loop's).
-#ifndef BH_BAND_INLINE
-#define BH_BAND_INLINE 0
-#endif
-// BH_BAND_INWARD = 1 (default): outside 4.5 M only inward-moving rays keep a
-// warp in the band (see propagate_kernel); 0 applies the band to every ray
-// in its radius range.
-#ifndef BH_BAND_INWARD
-#define BH_BAND_INWARD 1
-#endif
+// attempt is accepted.  Out of line: one copy of the rare path's code, apart
+// from the float loop's (inlined, the headline kernel ran 6 % slower).
 struct BandStep {
     double h;       // the controller's next step size
     bool accepted;
 };
 template <int P>
-#if BH_BAND_INLINE
-__device__ __forceinline__
-#else
-__device__ __noinline__
-#endif
-BandStep band_attempt(double *p, double *kp, bool have_k1, double mass, double spin, double h,
+__device__ __noinline__ BandStep band_attempt(double *p, double *kp, bool have_k1, double mass, double spin, double h,
                       double rtol, double atol, double max_step) {
     RayState y{p[0], p[P], p[2 * P], p[3 * P], p[4 * P], p[5 * P], p[6 * P], p[7 * P]};
     const KerrV<double> K = make_kerr<double>(mass, spin);
@@ -325,10 +311,9 @@ BandStep band_attempt(double *p, double *kp, bool have_k1, double mass, double s
 // warp slots idle while the slowest warps finished).
 //
 // BAND (mixed lanes only): while one of the warp's rays lies between 1.01
-// times the outer horizon radius and the band radius (args.f64_r2), and is
-// moving inward or lies inside 4.5 M, the whole warp's attempt runs in
-// float64 (band_attempt, the float64 policy's step);
-// outside it the float stages run.  The test reads r^2 at each ray's current
+// times the outer horizon radius and the band radius (args.f64_r2), the
+// whole warp's attempt runs in float64 (band_attempt, the float64 policy's
+// step); outside it the float stages run.  The test reads r^2 at each ray's current
 // state from its last derivative evaluation, and is warp-uniform, so the two
 // paths never diverge within a warp; the rays that share a warp are the 64
 // (two per lane) of one claim, [64 k, 64 k + 64) of the launch.  Closer to
@@ -418,28 +403,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) propagate_kernel(const TraceArgs 
 #pragma unroll
                     for (int l = 0; l < N; ++l) {
                         const float r2l = T::get(r2c, l);
-                        bool in = r2l > rp2[l] && r2l < band2;
-#if BH_BAND_INWARD
-                        // Outside 4.5 M (beyond every spherical photon orbit:
-                        // they lie at r <= 4 M) an outgoing ray has no radial
-                        // turning point left and escapes, so nothing amplifies
-                        // its float32 rounding later: only inward rays need
-                        // the band there.  dr/dlam has the sign of
-                        // x.v + z v_z a^2 / r^2, v = p + kappa_1.
-                        const float ml = float(mass[l]);
-                        if (in && r2l > 20.25f * ml * ml) {
-                            const float vx = T::get(yw.px, l) + T::get(k1.kx, l);
-                            const float vy = T::get(yw.py, l) + T::get(k1.ky, l);
-                            const float vz = T::get(yw.pz, l) + T::get(k1.kz, l);
-                            const float zl = T::get(yw.z, l);
-                            const float a2l = float(spin[l] * spin[l]);
-                            const float rdot = fmaf(T::get(yw.x, l), vx,
-                                                    fmaf(T::get(yw.y, l), vy,
-                                                         zl * vz * (1.0f + a2l / r2l)));
-                            in = rdot < 0.0f;
-                        }
-#endif
-                        mine |= in;
+                        mine |= r2l > rp2[l] && r2l < band2;
                     }
                     in_band = __any_sync(act, mine);
                 }
