@@ -105,14 +105,16 @@ int bh_trace_with_tape(const bh_trace_config *config, const bh_scene *scene,
 // A ray parked at an accepted step whose z changed sign, for refinement.
 struct TileCrossing {
     double y0[8];        // state before the step
-    double y1[8];        // state after the step
+    double y1[8];        // state after the step; the refined crossing state once a hit
     double h;            // the step's size
     double h_next;       // controller step size after the step
     long long steps;     // accepted steps before the step
     long long attempts;  // attempts including the step
     long long ray;
+    int speculative;     // the ray went on in place past this crossing
+    int hit;             // set by the refinement for rays with speculative records
 };
-static_assert(sizeof(TileCrossing) == 168, "crossing record is 168 bytes");
+static_assert(sizeof(TileCrossing) == 176, "crossing record is 176 bytes");
 
 // A ray that continues after a crossing outside the disk.
 struct TileResume {
@@ -130,6 +132,8 @@ struct alignas(256) TileWorkspace {
     unsigned long long queue_head[2];
     unsigned long long n_cross[2];
     unsigned long long n_resume[2];
+    unsigned long long refine_head[2];  // chunks of 32 crossings claimed by the refinement
+    unsigned long long n_spec[2];       // speculative crossing records (may pass spec_cap)
     long long iterations;  // max attempts over finalised rays
     unsigned long long attempts, accepted, crossings, disk_hits;
     int timed_out;
@@ -149,7 +153,11 @@ struct TileArgs {
     double rtol, atol, initial_step, max_step;
     long long max_steps, max_attempts, saturate_steps;
     long long timeout_ns;
-    TileCrossing *cross;  // capacity n
+    TileCrossing *cross;  // capacity n: a parked ray stops, so one per ray and round
+    TileCrossing *spec;   // capacity spec_cap: crossings that the ray went on past
+    long long spec_cap;
+    unsigned long long *first_hit;  // per ray: fewest accepted steps of a refined hit
+    int8_t *has_spec;     // per ray: a speculative record exists
     TileResume *resume;   // capacity n
     double *states;
     int32_t *status;

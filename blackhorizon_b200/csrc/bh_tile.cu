@@ -12,27 +12,34 @@
 // Scheduling.  Refining a crossing costs about ten RK4 substeps; done inside
 // the tracing loop it would stall the other 31 lanes of the warp each time
 // one lane crosses, and crossings are frequent (most rays cross the plane at
-// least once).  So the tracer parks a crossing ray instead: it writes a
-// crossing record and its slot takes the next ray from the work queue.  A
-// second kernel refines all parked crossings in float64, one per thread, in
-// lock step; a hit finalises the ray, a miss writes a resume record, and the
-// second round of the tracer takes the resumed rays from its queue.  The
-// second round refines its crossings in place: it holds the minority of rays
-// that cross more than once (photon-ring orbits), whose tail is bound by the
-// latency of a lone ray's attempts, and parking them again would add one
-// latency-bound tail per crossing.  So a tile takes two rounds; the host
-// reads one counter per round.  (Claiming parked crossings from inside one
-// persistent launch instead, once its queue drains, was measured ten times
-// slower: every idle warp contends for the same claim counter.)
+// least once).  Two cases:
+//  - a crossing that the step's chord places clearly off the disk
+//    (clear_miss) needs no refinement: the reference's refinement would
+//    report a miss and the ray go on from the step's end, which it does in
+//    place.  On the offline renderer's default view that is a third of all
+//    crossings;
+//  - for the others the tracer parks the ray: it writes a crossing record
+//    and its slot takes the next ray from the work queue.  A second kernel
+//    refines all parked crossings in float64, one per thread, in lock step;
+//    a hit finalises the ray, and a miss (a crossing close to a disk edge)
+//    writes a resume record for the next round of the tracer.
+// Rounds that start with fewer than kInlineRefineBelow resumed rays refine
+// their crossings in place, which ends the rounds: such a round's time is
+// the latency of its longest ray, and parking again would add one such tail
+// per crossing.  The host reads one counter per round.  (Claiming parked
+// crossings from inside one persistent launch instead, once its queue
+// drains, was measured ten times slower: every idle warp contends for the
+// same claim counter.)
 //
 // Refinement.  The reference bisects the step fraction 40 times
 // (render.py:332-339): it ends on the dyadic cell (L, L + 2^-40) with L the
 // largest grid point k 2^-40 at which the substep is still on the starting
 // side, and takes the cell's midpoint.  Here an Illinois (modified regula
-// falsi) iteration brackets the root to a few cells, a short bisection over
-// the grid points left in the bracket finds the same L, and the crossing is
-// the same substep at (L + 1/2) 2^-40: the reference's point, from ~10 RK4
-// substeps instead of 41.
+// falsi) iteration converges on the root, the grid points on either side of
+// its estimate (and, should those not close the bracket, a bisection over the
+// grid points left in it) find the same L, and the crossing is the same
+// substep at (L + 1/2) 2^-40: the reference's point, from about 5 RK4
+// substeps instead of 41 (at most 7 on the offline renderer's default view).
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -181,11 +188,18 @@ __device__ __forceinline__ double crossing_fraction(const Rk4From &rk, const Ray
     if (same_side(1.0, f1)) return 1.0 - 0.5 * kCell;
     // Illinois on [lo, hi]: lo on z0's side, hi not; fa, fb the (possibly
     // halved) values used for interpolation.
-    double lo = 0.0, hi = 1.0, fa = z0, fb = f1;
+    double lo = 0.0, hi = 1.0, fa = z0, fb = f1, th = 0.5;
     int last = 0;
     for (int it = 0; it < 48 && hi - lo > 4.0 * kCell; ++it) {
-        double th = (lo * fb - hi * fa) / (fb - fa);
-        if (!(th > lo && th < hi)) th = 0.5 * (lo + hi);
+        th = (lo * fb - hi * fa) / (fb - fa);
+        if (!(th > lo && th < hi)) {
+            // The secant rounds onto an end of the bracket (or that end's
+            // value is exactly 0): the root lies within rounding of it.
+            // Falling back to the midpoint here, as plain Illinois does, cost
+            // the slowest crossing of a warp about 27 substeps instead of 6.
+            th = th <= lo ? lo : hi;
+            break;
+        }
         double f;
         if (same_side(th, f)) {
             lo = th; fa = f;
@@ -197,11 +211,23 @@ __device__ __forceinline__ double crossing_fraction(const Rk4From &rk, const Ray
             last = 1;
         }
     }
-    // The reference tests grid points only: bisect over the grid points
-    // still inside the bracket.  Grid point kl is at or below lo (on z0's
-    // side, as every point below the crossing is), kh at or above hi.
+    // The reference tests grid points only.  Grid point kl is at or below lo
+    // (on z0's side, as every point below the crossing is), kh at or above
+    // hi.  The two grid points on either side of the estimate th usually
+    // close the bracket; a bisection over the grid points still inside it
+    // finishes any other case.
     double kl = ::floor(lo * 0x1p40), kh = ::ceil(hi * 0x1p40);
     if (kh > 0x1p40) kh = 0x1p40;
+    double guess = ::floor(th * 0x1p40);
+    for (int p = 0; p < 2 && kh - kl > 1.0; ++p) {
+        const double km = ::fmin(::fmax(guess, kl + 1.0), kh - 1.0);
+        double f;
+        if (same_side(km * kCell, f)) {
+            kl = km; guess = km + 1.0;
+        } else {
+            kh = km; guess = km - 1.0;
+        }
+    }
     for (int it = 0; it < 48 && kh - kl > 1.0; ++it) {
         const double km = ::floor(0.5 * (kl + kh));
         double f;
@@ -222,6 +248,43 @@ __device__ __forceinline__ bool refine_hit(double m, double a, double r_in, doub
     return r >= r_in && r <= r_out;
 }
 
+// Where an accepted step whose z changes sign crosses the equatorial plane,
+// as far as its chord tells (render.py:268-281 refines the crossing and tests
+// its radius against the disk):
+//  - kClearMiss: certainly off the disk.  The reference's refinement would
+//    report a miss and the ray go on from the step's end (render.py:283-287),
+//    which the caller does in place;
+//  - kClearHit: certainly on the disk;
+//  - kNearEdge: close enough to an edge that only the refinement can tell.
+// The step's path lies within (4/27)(|h v0 - d| + |h v1 - d|) of its chord,
+// the bound for the cubic Hermite interpolant through the end points x0, x1
+// with end velocities v0, v1 (d = x1 - x0), and 1e-6 |d| more covers the
+// float32 velocities.  Twice that bound, carried into the plane through the
+// chord's slope, plus 4e-6 (1 + rho) for the float32 arithmetic here (about
+// 3e-7 rho), must keep the chord's crossing point clear of both disk
+// edges (rho_in, rho_out: the edges' cylindrical radii in the plane,
+// sqrt(r^2 + a^2)).  NaN anywhere gives kNearEdge.
+constexpr int kClearMiss = 0, kClearHit = 1, kNearEdge = 2;
+__device__ __forceinline__ int chord_crossing(const RayState &y0, const RayState &y1, float h,
+                                              float v0x, float v0y, float v0z, float v1x,
+                                              float v1y, float v1z, float rho_in,
+                                              float rho_out) {
+    const float dx = float(y1.x - y0.x), dy = float(y1.y - y0.y), dz = float(y1.z - y0.z);
+    const float ux = fmaf(h, v0x, -dx), uy = fmaf(h, v0y, -dy), uz = fmaf(h, v0z, -dz);
+    const float wx = fmaf(h, v1x, -dx), wy = fmaf(h, v1y, -dy), wz = fmaf(h, v1z, -dz);
+    const float dxy2 = fmaf(dx, dx, dy * dy);
+    const float dev = (4.0f / 27.0f) * (sqrtf(fmaf(ux, ux, fmaf(uy, uy, uz * uz))) +
+                                        sqrtf(fmaf(wx, wx, fmaf(wy, wy, wz * wz)))) +
+                      1e-6f * sqrtf(fmaf(dz, dz, dxy2));
+    const float ts = float(y0.z / (y0.z - y1.z));
+    const float px = fmaf(ts, dx, float(y0.x)), py = fmaf(ts, dy, float(y0.y));
+    const float rho = sqrtf(fmaf(px, px, py * py));
+    const float reach = 2.0f * dev * (1.0f + sqrtf(dxy2) / fabsf(dz)) + 4e-6f * (1.0f + rho);
+    if (rho - reach > rho_out || rho + reach < rho_in) return kClearMiss;
+    if (rho - reach >= rho_in && rho + reach <= rho_out) return kClearHit;
+    return kNearEdge;
+}
+
 // INLINE = false: every crossing is parked for the refinement kernel, and
 // the misses come back as the next round's resumed rays.  INLINE = true
 // (the rounds that start with few resumed rays): crossings are refined in
@@ -239,6 +302,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) tile_kernel(const TileArgs args) 
         ws->queue_head[par ^ 1] = 0;
         ws->n_cross[par ^ 1] = 0;
         ws->n_resume[par ^ 1] = 0;
+        ws->n_spec[par ^ 1] = 0;
+        // This round's refinement and settling claim their crossings from here.
+        ws->refine_head[par] = 0;
     }
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -246,6 +312,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) tile_kernel(const TileArgs args) 
     const long long n_in = args.round == 0 ? args.n : (long long)ws->n_resume[par];
     bool flush = args.flush != 0 || ws->timed_out != 0;
     const bool disk = args.disk_outer > 0.0;
+    const double a2 = args.spin * args.spin;
+    const float rho_in = float(::sqrt(fma(args.disk_inner, args.disk_inner, a2)));
+    const float rho_out = float(::sqrt(fma(args.disk_outer, args.disk_outer, a2)));
     const unsigned long long deadline = global_timer_ns() + (unsigned long long)args.timeout_ns;
     const bool has_deadline = args.timeout_ns > 0;
     const V rt = T::set(args.rtol), at = T::set(args.atol);
@@ -365,7 +434,23 @@ __global__ void __launch_bounds__(BLOCK, MINB) tile_kernel(const TileArgs args) 
                     const RayState y0 = ys.get(l);
                     RayState y1 = y0;
                     commit<V>(y1, yw, a, l, h[l]);
-                    if (INLINE && disk && y0.z * y1.z < 0.0) {
+                    const bool crosses = disk && y0.z * y1.z < 0.0;
+                    const int where =
+                        crosses ? chord_crossing(y0, y1, float(h[l]),
+                                                 float(y0.px) + float(T::get(k1.kx, l)),
+                                                 float(y0.py) + float(T::get(k1.ky, l)),
+                                                 float(y0.pz) + float(T::get(k1.kz, l)),
+                                                 float(y1.px) + float(T::get(a.k7.kx, l)),
+                                                 float(y1.py) + float(T::get(a.k7.ky, l)),
+                                                 float(y1.pz) + float(T::get(a.k7.kz, l)),
+                                                 rho_in, rho_out)
+                                : kClearMiss;
+                    if (crosses && where == kClearMiss) {
+                        // A miss decided by the chord: the ray goes on in place.
+                        ++my_cross;
+                    } else if (crosses && INLINE) {
+                        // The last rounds refine in place: a parked miss would
+                        // come back in yet another round.
                         RayState yc;
                         ++my_cross;
                         if (refine_hit(args.mass, args.spin, args.disk_inner, args.disk_outer,
@@ -375,10 +460,23 @@ __global__ void __launch_bounds__(BLOCK, MINB) tile_kernel(const TileArgs args) 
                             acc[l] = false;
                             continue;
                         }
-                    } else if (disk && y0.z * y1.z < 0.0) {
-                        // render.py:268-281: park for refinement.
-                        const unsigned long long k = atomicAdd(&ws->n_cross[par], 1ull);
-                        TileCrossing &c = args.cross[k];
+                    } else if (crosses) {
+                        // render.py:268-281: a record for the refinement.  Near a
+                        // disk edge the ray goes on in place, as after a miss,
+                        // and the refinement overwrites its outcome should the
+                        // crossing be a hit (refine_kernel, settle_kernel); else
+                        // the ray is parked and its slot takes the next ray.
+                        TileCrossing *rec = nullptr;
+                        bool go_on = false;
+                        if (where == kNearEdge) {
+                            const unsigned long long k = atomicAdd(&ws->n_spec[par], 1ull);
+                            if (k < (unsigned long long)args.spec_cap) {
+                                rec = &args.spec[k];
+                                go_on = true;
+                            }
+                        }
+                        if (!go_on) rec = &args.cross[atomicAdd(&ws->n_cross[par], 1ull)];
+                        TileCrossing &c = *rec;
                         c.y0[0] = y0.t; c.y0[1] = y0.x; c.y0[2] = y0.y; c.y0[3] = y0.z;
                         c.y0[4] = y0.pt; c.y0[5] = y0.px; c.y0[6] = y0.py; c.y0[7] = y0.pz;
                         c.y1[0] = y1.t; c.y1[1] = y1.x; c.y1[2] = y1.y; c.y1[3] = y1.z;
@@ -388,9 +486,15 @@ __global__ void __launch_bounds__(BLOCK, MINB) tile_kernel(const TileArgs args) 
                         c.steps = steps[l];
                         c.attempts = attempts[l];
                         c.ray = ray[l];
-                        ray[l] = -1;
-                        acc[l] = false;
-                        continue;
+                        c.speculative = go_on ? 1 : 0;
+                        c.hit = 0;
+                        if (go_on) {
+                            args.has_spec[ray[l]] = 1;
+                        } else {
+                            ray[l] = -1;
+                            acc[l] = false;
+                            continue;
+                        }
                     }
                     ys.set(l, y1);
                     ++steps[l];
@@ -438,28 +542,88 @@ __global__ void __launch_bounds__(BLOCK, MINB) tile_kernel(const TileArgs args) 
     }
 }
 
+// The crossing records of a round: the parked ones, then the speculative ones
+// (the index space of refine_kernel and settle_kernel).
+__device__ __forceinline__ long long crossing_count(const TileArgs &a, int par,
+                                                   long long *parked) {
+    const long long nc = (long long)a.ws->n_cross[par];
+    const unsigned long long ns = a.ws->n_spec[par];
+    *parked = nc;
+    return nc + (long long)(ns < (unsigned long long)a.spec_cap ? ns
+                                                                 : (unsigned long long)a.spec_cap);
+}
+
+__device__ __forceinline__ TileCrossing &crossing_at(const TileArgs &a, long long parked,
+                                                     long long i) {
+    return i < parked ? a.cross[i] : a.spec[i - parked];
+}
+
+// Appends resume records for the lanes with miss set (render.py:283-287: the
+// ray continues from the accepted state).  Every lane of the warp calls it.
+__device__ __forceinline__ void append_resumed(const TileArgs &a, int par, bool miss,
+                                               const TileCrossing *c) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const unsigned m = __ballot_sync(full, miss);
+    if (!m) return;
+    const int leader = __ffs(m) - 1;
+    unsigned long long b = 0;
+    if (lane == leader) b = atomicAdd(&a.ws->n_resume[par ^ 1], (unsigned long long)__popc(m));
+    b = __shfl_sync(full, b, leader);
+    if (miss) {
+        TileResume &r = a.resume[b + __popc(m & ((1u << lane) - 1u))];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) r.y[k] = c->y1[k];
+        r.h = c->h_next;
+        r.steps = c->steps + 1;
+        r.attempts = c->attempts;
+        r.ray = c->ray;
+    }
+}
+
+// Refines every crossing record of the round in float64, one per thread.  A
+// ray without speculative records has this one record: a hit finalises it and
+// a miss resumes it.  For a ray with speculative records (it went on past a
+// crossing near a disk edge) the record keeps its outcome, and the ray's
+// earliest hit is kept in first_hit; settle_kernel resolves those rays.
 __global__ void __launch_bounds__(128) refine_kernel(const TileArgs args) {
     TileWorkspace *ws = args.ws;
     const int par = args.round & 1;
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    const long long count = (long long)ws->n_cross[par];
-    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
-    const long long warp = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    long long parked = 0;
+    const long long count = crossing_count(args, par, &parked);
     unsigned long long my_cross = 0, my_hits = 0, my_attempts = 0, my_accepted = 0;
     long long my_max = 0;
-    for (long long base = warp * 32; base < count; base += warps * 32) {
+    // Warps claim 32 crossings at a time: a chunk's time is that of its
+    // slowest crossing (the iteration counts differ), so a fixed split
+    // would leave warps idle while others finish.
+    for (;;) {
+        unsigned long long chunk = 0;
+        if (lane == 0) chunk = atomicAdd(&ws->refine_head[par], 1ull);
+        chunk = __shfl_sync(full, chunk, 0);
+        const long long base = (long long)chunk * 32;
+        if (base >= count) break;
         const long long i = base + lane;
         bool miss = false;
-        TileCrossing c;
+        TileCrossing *cp = nullptr;
         if (i < count) {
-            c = args.cross[i];
+            cp = &crossing_at(args, parked, i);
+            TileCrossing &c = *cp;
             const RayState y0{c.y0[0], c.y0[1], c.y0[2], c.y0[3],
                               c.y0[4], c.y0[5], c.y0[6], c.y0[7]};
             RayState yc;
             ++my_cross;
-            if (refine_hit(args.mass, args.spin, args.disk_inner, args.disk_outer, y0, c.h,
-                           yc)) {
+            const bool hit = refine_hit(args.mass, args.spin, args.disk_inner, args.disk_outer,
+                                        y0, c.h, yc);
+            if (args.has_spec[c.ray]) {
+                c.hit = hit ? 1 : 0;
+                if (hit) {
+                    c.y1[0] = yc.t; c.y1[1] = yc.x; c.y1[2] = yc.y; c.y1[3] = yc.z;
+                    c.y1[4] = yc.pt; c.y1[5] = yc.px; c.y1[6] = yc.py; c.y1[7] = yc.pz;
+                    atomicMin(&args.first_hit[c.ray], (unsigned long long)c.steps);
+                }
+            } else if (hit) {
                 // render.py:278-281 and 283-286: DISK, state and steps as
                 // before the step.
                 tile_finalize(args, c.ray, y0, BH_RAY_DISK, c.steps, &yc);
@@ -471,23 +635,7 @@ __global__ void __launch_bounds__(128) refine_kernel(const TileArgs args) {
                 miss = true;
             }
         }
-        // Misses continue from the accepted state (render.py:283-287).
-        const unsigned m = __ballot_sync(full, miss);
-        if (m) {
-            const int leader = __ffs(m) - 1;
-            unsigned long long b = 0;
-            if (lane == leader) b = atomicAdd(&ws->n_resume[par ^ 1], (unsigned long long)__popc(m));
-            b = __shfl_sync(full, b, leader);
-            if (miss) {
-                TileResume &r = args.resume[b + __popc(m & ((1u << lane) - 1u))];
-#pragma unroll
-                for (int k = 0; k < 8; ++k) r.y[k] = c.y1[k];
-                r.h = c.h_next;
-                r.steps = c.steps + 1;
-                r.attempts = c.attempts;
-                r.ray = c.ray;
-            }
-        }
+        append_resumed(args, par, miss, cp);
     }
     for (int off = 16; off > 0; off >>= 1) {
         my_cross += __shfl_down_sync(full, my_cross, off);
@@ -499,6 +647,63 @@ __global__ void __launch_bounds__(128) refine_kernel(const TileArgs args) {
     }
     if (lane == 0 && my_cross) {
         atomicAdd(&ws->crossings, my_cross);
+        atomicAdd(&ws->disk_hits, my_hits);
+        atomicAdd(&ws->attempts, my_attempts);
+        atomicAdd(&ws->accepted, my_accepted);
+        atomicMax(&ws->iterations, my_max);
+    }
+}
+
+// Resolves the rays with speculative records after refine_kernel: the record
+// of the ray's earliest hit finalises it as DISK (over whatever its
+// continuation wrote: the reference stops at that crossing); with no hit, a
+// parked record's miss resumes the ray.  The attempt counters then include
+// the continuation's attempts past a crossing that proved a hit.
+__global__ void __launch_bounds__(128) settle_kernel(const TileArgs args) {
+    TileWorkspace *ws = args.ws;
+    const int par = args.round & 1;
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    long long parked = 0;
+    const long long count = crossing_count(args, par, &parked);
+    unsigned long long my_hits = 0, my_attempts = 0, my_accepted = 0;
+    long long my_max = 0;
+    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+    const long long warp = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    for (long long base = warp * 32; base < count; base += warps * 32) {
+        const long long i = base + lane;
+        bool miss = false;
+        const TileCrossing *cp = nullptr;
+        if (i < count) {
+            cp = &crossing_at(args, parked, i);
+            const TileCrossing &c = *cp;
+            if (args.has_spec[c.ray]) {
+                const unsigned long long first = args.first_hit[c.ray];
+                if (c.hit && (unsigned long long)c.steps == first) {
+                    const RayState y0{c.y0[0], c.y0[1], c.y0[2], c.y0[3],
+                                      c.y0[4], c.y0[5], c.y0[6], c.y0[7]};
+                    const RayState yc{c.y1[0], c.y1[1], c.y1[2], c.y1[3],
+                                      c.y1[4], c.y1[5], c.y1[6], c.y1[7]};
+                    tile_finalize(args, c.ray, y0, BH_RAY_DISK, c.steps, &yc);
+                    ++my_hits;
+                    my_attempts += c.attempts;
+                    my_accepted += c.steps;
+                    if (c.attempts > my_max) my_max = c.attempts;
+                } else if (!c.hit && !c.speculative && first == ~0ull) {
+                    miss = true;
+                }
+            }
+        }
+        append_resumed(args, par, miss, cp);
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        my_hits += __shfl_down_sync(full, my_hits, off);
+        my_attempts += __shfl_down_sync(full, my_attempts, off);
+        my_accepted += __shfl_down_sync(full, my_accepted, off);
+        const long long o = __shfl_down_sync(full, my_max, off);
+        my_max = o > my_max ? o : my_max;
+    }
+    if (lane == 0 && my_hits) {
         atomicAdd(&ws->disk_hits, my_hits);
         atomicAdd(&ws->attempts, my_attempts);
         atomicAdd(&ws->accepted, my_accepted);
@@ -537,12 +742,13 @@ static const void *tile_kernel_for(int precision, int idx, bool inl, size_t *sme
     }
 }
 
-// Measured on the offline renderer's 1280x800 supersample-2 frame: mixed
-// 37.9 ms with one float ray per thread at 128 x 3 (54.4 ms packed two per
-// thread: the parking and refill work does not pack); float64 36.3 ms at
-// 256 x 2 (37.4 ms at 128 x 3).
+// Measured on the offline renderer's 1280x800 supersample-2 frame (one
+// round): mixed 12.8 ms with one float ray per thread at 128 x 5 (96
+// registers), 13.2 ms at 128 x 4 and 256 x 2, 14.9 ms at 128 x 3, 18.8-21.7 ms
+// packed two per thread (the parking and refill work does not pack); float64
+// 30.6 ms at 256 x 2, 31.3 ms at 128 x 4, 32.2 ms at 128 x 3.
 int tile_default_variant(int precision) {
-    return precision == BH_PRECISION_MIXED ? 0 : 3;
+    return precision == BH_PRECISION_MIXED ? 2 : 3;
 }
 
 cudaError_t launch_tile(const TileArgs &args, int precision, int variant,
@@ -663,7 +869,11 @@ cudaError_t launch_refine(const TileArgs &args, cudaStream_t stream) {
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    refine_kernel<<<sms * 8, 128, 0, stream>>>(args);
+    int occ = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, refine_kernel, 128, 0);
+    if (e != cudaSuccess) return e;
+    refine_kernel<<<sms * (occ > 0 ? occ : 1), 128, 0, stream>>>(args);
+    settle_kernel<<<sms * 4, 128, 0, stream>>>(args);
     return cudaGetLastError();
 }
 
@@ -682,12 +892,23 @@ static int tile_cuda(cudaError_t e, const char *what) {
 
 using namespace bh;
 
-// Workspace: header, resume-sort counters, crossing records, and two
-// resume arrays (the second receives the reordered records).
+// Speculative crossing records a tile holds; past them a crossing near a disk
+// edge is parked like any other.  On the offline renderer's default view
+// about one ray in 1,600 records one.
+static long long spec_capacity(long long n) {
+    const long long c = n / 8 + 1024;
+    return c < n ? c : n;
+}
+
+// Workspace: header, resume-sort counters, parked and speculative crossing
+// records, two resume arrays (the second receives the reordered records),
+// each ray's first hit and speculative flag.
 extern "C" size_t bh_trace_tile_workspace_bytes(int64_t n) {
     if (n < 0) n = 0;
     return sizeof(TileWorkspace) + sizeof(TileResumeSort) +
-           (size_t)n * (sizeof(TileCrossing) + 2 * sizeof(TileResume));
+           (size_t)(n + spec_capacity(n)) * sizeof(TileCrossing) +
+           (size_t)n * (2 * sizeof(TileResume) + sizeof(unsigned long long)) +
+           (size_t)((n + 15) / 16 * 16);
 }
 
 extern "C" int bh_trace_tile(const bh_trace_config *config, const bh_scene *scene,
@@ -758,10 +979,12 @@ extern "C" int bh_trace_tile(const bh_trace_config *config, const bh_scene *scen
     TileResumeSort *resume_sort = reinterpret_cast<TileResumeSort *>(base + sizeof(TileWorkspace));
     a.cross = reinterpret_cast<TileCrossing *>(base + sizeof(TileWorkspace) +
                                                sizeof(TileResumeSort));
-    a.resume = reinterpret_cast<TileResume *>(base + sizeof(TileWorkspace) +
-                                              sizeof(TileResumeSort) +
-                                              (size_t)n * sizeof(TileCrossing));
+    a.spec_cap = spec_capacity(n);
+    a.spec = a.cross + n;
+    a.resume = reinterpret_cast<TileResume *>(a.spec + a.spec_cap);
     TileResume *resume_sorted = a.resume + n;
+    a.first_hit = reinterpret_cast<unsigned long long *>(resume_sorted + n);
+    a.has_spec = reinterpret_cast<int8_t *>(a.first_hit + n);
     a.states = states;
     a.status = status;
     a.steps = steps;
@@ -770,6 +993,11 @@ extern "C" int bh_trace_tile(const bh_trace_config *config, const bh_scene *scen
     a.escape_dir = escape_directions;
     a.saturated = saturated;
     int rc = tile_cuda(cudaMemsetAsync(base, 0, sizeof(TileWorkspace), s), "bh_trace_tile reset");
+    if (rc != BH_OK) return rc;
+    rc = tile_cuda(cudaMemsetAsync(a.first_hit, 0xff, (size_t)n * sizeof(unsigned long long), s),
+                   "bh_trace_tile reset");
+    if (rc != BH_OK) return rc;
+    rc = tile_cuda(cudaMemsetAsync(a.has_spec, 0, (size_t)n, s), "bh_trace_tile reset");
     if (rc != BH_OK) return rc;
     // Rays that end off the disk report zero hit position and momentum.
     rc = tile_cuda(cudaMemsetAsync(hit_positions, 0, (size_t)n * 3 * sizeof(double), s),

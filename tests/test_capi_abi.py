@@ -137,7 +137,13 @@ def test_trace_tile_argument_validation(bhlib):
     assert call(cfg, 2.3, 18.0, 0) == 0  # empty tile: nothing to do
     assert call(cfg, 2.3, 18.0, 4) == -5  # no workspace
     assert call(cfg, 2.3, 18.0, 4, C.c_void_p(0x10000), 100) == -5  # too small
-    assert bhlib.bh_trace_tile_workspace_bytes(10) == 256 + 1024 + 10 * (168 + 2 * 96)
+    # Header, resume-sort counters, n parked and min(n / 8 + 1024, n)
+    # speculative 176-byte crossing records, two 96-byte resume records, an
+    # 8-byte first hit and a 1-byte flag per ray (rounded up to 16 bytes).
+    for n in (10, 100_000):
+        spec = min(n // 8 + 1024, n)
+        assert bhlib.bh_trace_tile_workspace_bytes(n) == (
+            256 + 1024 + (n + spec) * 176 + n * (2 * 96 + 8) + (n + 15) // 16 * 16)
     # Config flags: BH_TRACE_INTERIOR only, and only with a stop radius > 0.
     cfg.flags = 2
     assert call(cfg, 2.3, 18.0, 4) == -1
