@@ -334,15 +334,17 @@ __global__ void __launch_bounds__(BLOCK, MINB) tile_kernel(const TileArgs args) 
     }
     StageV<V> k1 = first_stage<V>(K, yw);
     bool queue_open = true;
-    unsigned long long my_attempts = 0, my_accepted = 0;
-    long long my_max_attempts = 0;
-
-    unsigned long long my_cross = 0, my_hits = 0;
+    // Launch counters of this thread, in shared memory: they change once per
+    // ray, and in registers they cost the stepping loop five 64-bit values.
+    __shared__ unsigned long long cnt[5][BLOCK];  // attempts, accepted, max, crossings, hits
+#pragma unroll
+    for (int k = 0; k < 5; ++k) cnt[k][threadIdx.x] = 0;
     auto finish = [&](int l, const RayState &y, int st, const RayState *hit) {
         tile_finalize(args, ray[l], y, st, steps[l], hit);
-        my_attempts += attempts[l];
-        my_accepted += steps[l];
-        if (attempts[l] > my_max_attempts) my_max_attempts = attempts[l];
+        cnt[0][threadIdx.x] += attempts[l];
+        cnt[1][threadIdx.x] += steps[l];
+        if ((unsigned long long)attempts[l] > cnt[2][threadIdx.x])
+            cnt[2][threadIdx.x] = attempts[l];
         ray[l] = -1;
     };
 
@@ -447,15 +449,15 @@ __global__ void __launch_bounds__(BLOCK, MINB) tile_kernel(const TileArgs args) 
                                 : kClearMiss;
                     if (crosses && where == kClearMiss) {
                         // A miss decided by the chord: the ray goes on in place.
-                        ++my_cross;
+                        ++cnt[3][threadIdx.x];
                     } else if (crosses && INLINE) {
                         // The last rounds refine in place: a parked miss would
                         // come back in yet another round.
                         RayState yc;
-                        ++my_cross;
+                        ++cnt[3][threadIdx.x];
                         if (refine_hit(args.mass, args.spin, args.disk_inner, args.disk_outer,
                                        y0, h[l], yc)) {
-                            ++my_hits;
+                            ++cnt[4][threadIdx.x];
                             finish(l, y0, BH_RAY_DISK, &yc);
                             acc[l] = false;
                             continue;
@@ -523,6 +525,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) tile_kernel(const TileArgs args) 
             }
         }
     }
+    unsigned long long my_attempts = cnt[0][threadIdx.x], my_accepted = cnt[1][threadIdx.x];
+    long long my_max_attempts = (long long)cnt[2][threadIdx.x];
+    unsigned long long my_cross = cnt[3][threadIdx.x], my_hits = cnt[4][threadIdx.x];
     for (int off = 16; off > 0; off >>= 1) {
         my_attempts += __shfl_down_sync(full, my_attempts, off);
         my_accepted += __shfl_down_sync(full, my_accepted, off);

@@ -23,6 +23,19 @@
 
 namespace bh {
 
+// The scene of a ray slot: the launch's own for a state-array launch
+// (cam < 0), else that of the slot's camera.  A slot keeps only the camera's
+// index: four per-slot float64 values held in registers cost the stepping
+// loop spills.
+struct SlotScene {
+    double mass, spin, capture_radius, escape_radius;
+};
+__device__ __forceinline__ SlotScene slot_scene(const TraceArgs &a, int cam) {
+    if (cam < 0) return SlotScene{a.mass, a.spin, a.capture_radius, a.escape_radius};
+    const CameraDev &c = a.cameras[cam];
+    return SlotScene{c.mass, c.spin, c.capture_radius, c.escape_radius};
+}
+
 // PROJECT: every project_every controller iterations, each ray in flight is
 // projected onto the null constraint in float64 (project_null) and its FSAL
 // derivative recomputed; warp-uniform, so the warp pays one RHS per period.
@@ -43,26 +56,34 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args
 
     extern __shared__ double bh_state_smem[];
     StateStore<V, BLOCK> ys(bh_state_smem);
+    // Values that change once per ray live in shared memory, one column per
+    // thread: each slot's affine parameter and the thread's launch counters
+    // (attempts, accepted steps, most attempts of a ray).
+    __shared__ double lam_of[N][BLOCK];
+    __shared__ unsigned long long cnt[3][BLOCK];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) cnt[k][threadIdx.x] = 0;
     long long ray[N], steps[N], attempts[N];
+    int cam[N];  // the slot's camera (slot_scene)
     // r: Kerr-Schild radius of the slot's state, NaN while it lies clear of
     // both termination radii (settled_radius).
-    double h[N], mass[N], spin[N], rcap[N], resc[N], r[N], lam[N];
+    double h[N], r[N];
     WStateV<V> yw;
+    double mass0[N], spin0[N];
 #pragma unroll
     for (int l = 0; l < N; ++l) {
-        ray[l] = -1; steps[l] = 0; attempts[l] = 0;
-        h[l] = args.initial_step; mass[l] = 1.0; spin[l] = 0.0;
-        rcap[l] = 0.0; resc[l] = 0.0; r[l] = 0.0; lam[l] = 0.0;
+        ray[l] = -1; steps[l] = 0; attempts[l] = 0; cam[l] = -1;
+        h[l] = args.initial_step; r[l] = 0.0;
+        lam_of[l][threadIdx.x] = 0.0;
+        mass0[l] = 1.0; spin0[l] = 0.0;
         // A benign placeholder state for idle slots (finite, far from the hole).
         const RayState y0{0.0, 10.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0};
         ys.set(l, y0);
         put_work<V>(yw, l, y0);
     }
-    KerrV<V> K = make_kerr<V>(lanes_of<V>(mass), lanes_of<V>(spin));
+    KerrV<V> K = make_kerr<V>(lanes_of<V>(mass0), lanes_of<V>(spin0));
     StageV<V> k1 = first_stage<V>(K, yw);
     bool queue_open = true;
-    unsigned long long my_attempts = 0, my_accepted = 0;
-    long long my_max_attempts = 0;
 
     for (unsigned iter = 0;; ++iter) {
         // ---- warp-aggregated refill of the idle ray slots
@@ -94,21 +115,19 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args
                         RayState y0;
                         if (args.source == 0) {
                             load_state(args.state0, n, args.layout, idx, y0);
-                            mass[l] = args.mass; spin[l] = args.spin;
-                            rcap[l] = args.capture_radius; resc[l] = args.escape_radius;
+                            cam[l] = -1;
                         } else {
                             const int c = find_camera(args.cameras, args.ncameras, idx);
-                            const CameraDev &cam = args.cameras[c];
-                            camera_ray(cam, idx - cam.first_ray, y0);
-                            mass[l] = cam.mass; spin[l] = cam.spin;
-                            rcap[l] = cam.capture_radius; resc[l] = cam.escape_radius;
+                            camera_ray(args.cameras[c], idx - args.cameras[c].first_ray, y0);
+                            cam[l] = c;
                         }
+                        const SlotScene sc = slot_scene(args, cam[l]);
                         h[l] = args.initial_step;
-                        lam[l] = 0.0;
+                        lam_of[l][threadIdx.x] = 0.0;
                         steps[l] = 0;
                         attempts[l] = 0;
-                        r[l] = ks_radius(spin[l], y0);
-                        if (r[l] >= resc[l]) {
+                        r[l] = ks_radius(sc.spin, y0);
+                        if (r[l] >= sc.escape_radius) {
                             // tracer.py:95-99 rejects the whole call; count and skip.
                             atomicAdd(&ws->bad_rays, 1);
                             store_state(args.states, n, args.layout, idx, y0);
@@ -131,6 +150,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args
 #pragma unroll
         for (int l = 0; l < N; ++l) any_fresh |= fresh[l];
         if (any_fresh) {
+            double mass[N], spin[N];
+#pragma unroll
+            for (int l = 0; l < N; ++l) {
+                const SlotScene sc = slot_scene(args, cam[l]);
+                mass[l] = sc.mass; spin[l] = sc.spin;
+            }
             K = make_kerr<V>(lanes_of<V>(mass), lanes_of<V>(spin));
             const StageV<V> f = first_stage<V>(K, yw);
             take_stage(k1, f, fresh);
@@ -172,20 +197,22 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args
                         atomicExch(&ws->tape_overflow, 1);
                     }
                 }
+                const SlotScene sc = slot_scene(args, cam[l]);
                 if (acc[l]) {
                     commit<V>(yl, yw, a, l, h[l]);
                     ys.set(l, yl);
-                    lam[l] += h[l];
+                    lam_of[l][threadIdx.x] += h[l];
                     ++steps[l];
-                    r[l] = settled_radius(double(T::get(a.r2n, l)), rcap[l], resc[l], spin[l], yl);
+                    r[l] = settled_radius(double(T::get(a.r2n, l)), sc.capture_radius,
+                                          sc.escape_radius, sc.spin, yl);
                 }
                 h[l] = next_step<F64>(h[l], ratio[l], args.max_step);
 
                 const bool finite = all_finite(yl);
                 int st = BH_RAY_IN_FLIGHT;
                 if (!finite) st = BH_RAY_FAILED;
-                if (finite && r[l] <= rcap[l]) st = BH_RAY_CAPTURED;
-                if (finite && r[l] >= resc[l]) st = BH_RAY_ESCAPED;
+                if (finite && r[l] <= sc.capture_radius) st = BH_RAY_CAPTURED;
+                if (finite && r[l] >= sc.escape_radius) st = BH_RAY_ESCAPED;
                 const bool in_flight = st == BH_RAY_IN_FLIGHT;
                 if (in_flight && h[l] < args.min_step) st = BH_RAY_FAILED;
                 if (in_flight && steps[l] >= args.max_steps) st = BH_RAY_MAX_STEPS;
@@ -194,14 +221,15 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args
                 if (st != BH_RAY_IN_FLIGHT) {
                     // Returned states lie on the constraint too (p only: r
                     // and so the classification are unchanged).
-                    if constexpr (PROJECT) project_null(mass[l], spin[l], yl);
+                    if constexpr (PROJECT) project_null(sc.mass, sc.spin, yl);
                     store_state(args.states, n, args.layout, ray[l], yl);
                     args.status[ray[l]] = st;
                     args.steps[ray[l]] = steps[l];
-                    if (args.lam_io) args.lam_io[ray[l]] = lam[l];
-                    my_attempts += attempts[l];
-                    my_accepted += steps[l];
-                    if (attempts[l] > my_max_attempts) my_max_attempts = attempts[l];
+                    if (args.lam_io) args.lam_io[ray[l]] = lam_of[l][threadIdx.x];
+                    cnt[0][threadIdx.x] += attempts[l];
+                    cnt[1][threadIdx.x] += steps[l];
+                    if ((unsigned long long)attempts[l] > cnt[2][threadIdx.x])
+                        cnt[2][threadIdx.x] = attempts[l];
                     ray[l] = -1;
                 }
             }
@@ -214,7 +242,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args
                         proj[l] = ray[l] >= 0;
                         if (proj[l]) {
                             RayState yl = ys.get(l);
-                            project_null(mass[l], spin[l], yl);
+                            const SlotScene sc = slot_scene(args, cam[l]);
+                            project_null(sc.mass, sc.spin, yl);
                             ys.set(l, yl);
                             put_work<V>(yw, l, yl);
                         }
@@ -235,9 +264,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args
                     store_state(args.states, n, args.layout, ray[l], ys.get(l));
                     args.status[ray[l]] = BH_RAY_IN_FLIGHT;
                     args.steps[ray[l]] = steps[l];
-                    if (args.lam_io) args.lam_io[ray[l]] = lam[l];
-                    my_attempts += attempts[l];
-                    my_accepted += steps[l];
+                    if (args.lam_io) args.lam_io[ray[l]] = lam_of[l][threadIdx.x];
+                    cnt[0][threadIdx.x] += attempts[l];
+                    cnt[1][threadIdx.x] += steps[l];
                 }
                 if (lane == 0) atomicExch(&ws->timed_out, 1);
                 break;
@@ -245,6 +274,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args
         }
     }
     // ---- launch counters: one atomic per warp
+    unsigned long long my_attempts = cnt[0][threadIdx.x], my_accepted = cnt[1][threadIdx.x];
+    long long my_max_attempts = (long long)cnt[2][threadIdx.x];
     for (int off = 16; off > 0; off >>= 1) {
         my_attempts += __shfl_down_sync(full, my_attempts, off);
         my_accepted += __shfl_down_sync(full, my_accepted, off);

@@ -126,7 +126,7 @@ __device__ __forceinline__ V lanes_of(const double *v) {
 template <class V, int BLOCK>
 struct StateStore {
     static constexpr int N = VT<V>::N;
-    static constexpr bool kShared = sizeof(typename VT<V>::S) == 4;
+    static constexpr bool kShared = true;
     RayState reg[kShared ? 1 : N];
     double *sh;
     __device__ __forceinline__ explicit StateStore(double *smem) : sh(smem) {}
