@@ -701,6 +701,10 @@ int bh_trace_stats_read(const void *workspace, bh_trace_stats *out, void *stream
         set_error("escape_radius must exceed all initial radii (%d rays)", w.bad_rays);
         return BH_ERR_ESCAPE_RADIUS;
     }
+    if (w.bad_spins) {
+        set_error("Kerr bound violated: |spin| must be <= mass (%d rays)", w.bad_spins);
+        return BH_ERR_INVALID_ARGUMENT;
+    }
     if (w.timed_out) {
         set_error("trace deadline exceeded");
         return BH_ERR_TIMEOUT;

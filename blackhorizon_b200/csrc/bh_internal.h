@@ -19,6 +19,7 @@ struct alignas(256) TraceWorkspace {
     int timed_out;
     int bad_rays;
     int tape_overflow;  // rays with more accepted steps than the tape holds
+    int bad_spins;      // propagate: rays whose own spin breaks the Kerr bound
 };
 static_assert(sizeof(TraceWorkspace) == 256, "workspace header is 256 bytes");
 

@@ -395,6 +395,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) propagate_kernel(const TraceArgs 
                 ys.set(l, y0);
                 spin[l] = args.spin_of_ray ? args.spin_of_ray[src] : args.spin;
                 mass[l] = args.mass;
+                if (!(::fabs(spin[l]) <= mass[l])) {
+                    // A ray's own spin outside the Kerr bound: counted (the
+                    // stats read then fails the call) and traced at spin 0.
+                    if (valid[l]) atomicAdd(&ws->bad_spins, 1);
+                    spin[l] = 0.0;
+                }
                 h[l] = args.h_io[src];
                 lam[l] = args.lam_io ? args.lam_io[src] : 0.0;
                 acc[l] = 0;

@@ -297,13 +297,17 @@ int bh_trace_cameras_noalloc(const bh_trace_config *config,
 
 /* Copies the counters of the last launch on `workspace` to the host and
  * synchronises `stream`.  Returns BH_ERR_TIMEOUT / BH_ERR_ESCAPE_RADIUS when
- * the launch hit its deadline or met a ray outside its escape radius. */
+ * the launch hit its deadline or met a ray outside its escape radius, and
+ * BH_ERR_INVALID_ARGUMENT when a propagate launch met a ray whose own spin
+ * breaks the Kerr bound. */
 int bh_trace_stats_read(const void *workspace, bh_trace_stats *out,
                         void *stream);
 
 /* Adaptive propagation without termination: n_steps attempted DP5(4) steps
  * per ray with the accept/reject and step-size update of tracer.py:111-120.
- * spin_of_ray (n,) gives each ray its own spin when non-NULL.  states (n,8)
+ * spin_of_ray (n,) gives each ray its own spin when non-NULL; a ray whose spin
+ * breaks the Kerr bound is traced at spin 0 and makes bh_trace_stats_read
+ * return BH_ERR_INVALID_ARGUMENT.  states (n,8)
  * and h (n,) are updated in place; lam (n,), when non-NULL, accumulates the
  * affine parameter of the accepted steps in float64 (in/out); accepted (n,)
  * int64 receives accepted steps.  Uses the workspace counters like bh_trace. */

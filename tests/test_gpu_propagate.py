@@ -197,3 +197,15 @@ def test_streamed_from_host_memory_equals_device_path(cuda):
         assert got[4].attempts == ref[4].attempts and got[4].iterations == ref[4].iterations
     with pytest.raises(ValueError):
         propagate(st, state0.cpu(), 10, out=torch.empty(state0.shape, dtype=torch.float64))
+    # The kernel checks each ray's spin against the Kerr bound: one bad spin in
+    # either piece fails the streamed call, in both policies and in the
+    # resident path too.
+    for bad in (17, 49_999):
+        sp = spins.cpu().clone()
+        sp[bad] = 1.25
+        for precision in ("mixed", "fp64"):
+            with pytest.raises(ValueError, match="Kerr bound"):
+                propagate(st, state0.cpu().pin_memory(), 10, precision=precision,
+                          spins=sp.pin_memory(), out=torch.empty_like(host_s).pin_memory())
+            with pytest.raises(ValueError, match="Kerr bound"):
+                propagate(st, state0, 10, precision=precision, spins=sp.to(state0.device))
