@@ -133,6 +133,10 @@ _SIGNATURES = {
                                                 ctypes.POINTER(TraceStats), _P]),
     "bh_propagate": (ctypes.c_int, [ctypes.POINTER(TraceConfig), _D, _D, _P, _P, _P,
                                     _P, _P, _I64, _I64, _P, _P]),
+    "bh_propagate_ordered": (ctypes.c_int, [ctypes.POINTER(TraceConfig), _D, _D, _P, _P, _P,
+                                            _P, _P, _P, _I64, _I64, _P, _P]),
+    "bh_propagate_order_workspace_bytes": (_SZ, [_I64]),
+    "bh_propagate_order": (ctypes.c_int, [_P, _I32, _I64, _P, _P, _SZ, _P]),
     "bh_graph_trace_cameras": (ctypes.c_int, [ctypes.POINTER(TraceConfig), _I32, _I64, _P,
                                               _P, _P, _P, _SZ, ctypes.POINTER(_P)]),
     "bh_graph_launch": (ctypes.c_int, [_P, _P]),

@@ -705,6 +705,10 @@ int bh_trace_stats_read(const void *workspace, bh_trace_stats *out, void *stream
         set_error("Kerr bound violated: |spin| must be <= mass (%d rays)", w.bad_spins);
         return BH_ERR_INVALID_ARGUMENT;
     }
+    if (w.bad_order) {
+        set_error("order is not a permutation of [0, n) (%d entries out of range)", w.bad_order);
+        return BH_ERR_INVALID_ARGUMENT;
+    }
     if (w.timed_out) {
         set_error("trace deadline exceeded");
         return BH_ERR_TIMEOUT;
@@ -720,6 +724,14 @@ int bh_propagate(const bh_trace_config *config, double mass, double spin,
                  const double *spin_of_ray, double *states, double *h,
                  double *lam, int64_t *accepted, int64_t n, int64_t n_steps,
                  void *workspace, void *stream) {
+    return bh_propagate_ordered(config, mass, spin, spin_of_ray, states, h, lam, accepted,
+                                nullptr, n, n_steps, workspace, stream);
+}
+
+int bh_propagate_ordered(const bh_trace_config *config, double mass, double spin,
+                         const double *spin_of_ray, double *states, double *h, double *lam,
+                         int64_t *accepted, const int32_t *order, int64_t n, int64_t n_steps,
+                         void *workspace, void *stream) {
     int rc = config_ok(config);
     if (rc != BH_OK) return rc;
     if (config->f64_radius != 0.0 && config->project_every > 0)
@@ -752,6 +764,7 @@ int bh_propagate(const bh_trace_config *config, double mass, double spin,
     a.mass = mass;
     a.spin = spin;
     a.spin_of_ray = spin_of_ray;
+    a.order = order;
     a.h_io = h;
     a.lam_io = lam;
     a.steps = accepted;

@@ -20,6 +20,7 @@ struct alignas(256) TraceWorkspace {
     int bad_rays;
     int tape_overflow;  // rays with more accepted steps than the tape holds
     int bad_spins;      // propagate: rays whose own spin breaks the Kerr bound
+    int bad_order;      // propagate: order entries outside [0, n)
 };
 static_assert(sizeof(TraceWorkspace) == 256, "workspace header is 256 bytes");
 
@@ -45,6 +46,9 @@ struct TraceArgs {
     // single-scene parameters (source == 0)
     double mass, spin, capture_radius, escape_radius;
     const double *spin_of_ray;  // propagate only; may be null
+    // propagate: the ray at each launch position (bh_propagate_order); null
+    // takes the rays in their own order
+    const int32_t *order;
     // outputs
     double *states;
     int32_t *status;

@@ -1,0 +1,130 @@
+// bh_order.cu -- the order in which the mixed propagator takes its rays.
+//
+// The mixed propagator runs a warp's attempt in float64 while any of its 64
+// rays lies in the float64 band near the hole (propagate_kernel).  A warp of
+// rays taken in the caller's order mixes rays that approach the hole with
+// rays that leave it, so one ray in the band puts 63 others through float64
+// steps they do not need.  bh_propagate_order sorts the rays of each segment
+// of kOrderSegment consecutive rays by direction (inward first) and then by
+// impact parameter |x × p| / |p|.  Rays that pass the hole alike then share
+// warps, and the band's time concentrates in fewer warps: on the
+// raw-throughput workload (a CPU restatement of the kernel's arithmetic with
+// 64-ray warps, 16,384 rays) the share of warp-attempts in float64 fell from
+// 5.5 % to 1.4 %, against 1.3 % of ray-attempts, with the same endpoint
+// errors.  Segments keep the order local: a caller that streams a batch in
+// pieces starting at multiples of kOrderSegment gets the warps, and so the
+// results, of the single launch.
+//
+// The sort is CUB's stable radix sort (cub::DeviceRadixSort from the CUDA
+// toolkit) of 64-bit keys: segment, outward flag, impact parameter as float32
+// bits.  Equal keys keep the caller's order, so the order is deterministic.
+#include <cstdint>
+
+#include <cub/device/device_radix_sort.cuh>
+
+#include "bh_trace_common.cuh"
+
+namespace bh {
+
+constexpr int kOrderSegmentLog2 = 14;  // 16,384 rays
+
+__global__ void __launch_bounds__(256) order_keys_kernel(const double *states, int layout,
+                                                         long long n, unsigned long long *keys,
+                                                         int32_t *idx) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        RayState y;
+        load_state(states, n, layout, i, y);
+        const double cx = y.y * y.pz - y.z * y.py, cy = y.z * y.px - y.x * y.pz,
+                     cz = y.x * y.py - y.y * y.px;
+        const double pn = ::sqrt(y.px * y.px + y.py * y.py + y.pz * y.pz);
+        const float b = float(::sqrt(cx * cx + cy * cy + cz * cz) / pn);
+        const bool outward = !(y.x * y.px + y.y * y.py + y.z * y.pz < 0.0);
+        // b >= 0: its float32 bits order as unsigned integers; NaN goes last.
+        const unsigned bits = b >= 0.0f ? __float_as_uint(b) : 0xffffffffu;
+        keys[i] = ((unsigned long long)(i >> kOrderSegmentLog2) << 33) |
+                  ((unsigned long long)(outward ? 1 : 0) << 32) | bits;
+        idx[i] = (int32_t)i;
+    }
+}
+
+static size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+
+static int end_bit_for(long long n) {
+    int seg_bits = 0;
+    while (seg_bits < 31 && ((n - 1) >> kOrderSegmentLog2) >> seg_bits) ++seg_bits;
+    return 33 + seg_bits;
+}
+
+static size_t sort_temp_bytes(long long n) {
+    size_t bytes = 0;
+    if (n <= 0) return 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const unsigned long long *)nullptr,
+                                    (unsigned long long *)nullptr, (const int32_t *)nullptr,
+                                    (int32_t *)nullptr, (int)n, 0, end_bit_for(n));
+    return bytes;
+}
+
+}  // namespace bh
+
+using namespace bh;
+
+extern "C" size_t bh_propagate_order_workspace_bytes(int64_t n) {
+    if (n <= 0) return 256;
+    if (n > INT32_MAX) return 0;
+    return align256((size_t)n * 8) * 2 + align256((size_t)n * 4) + align256(sort_temp_bytes(n));
+}
+
+extern "C" int bh_propagate_order(const double *states, int32_t layout, int64_t n,
+                                  int32_t *order, void *workspace, size_t workspace_bytes,
+                                  void *stream) {
+    if (layout != BH_LAYOUT_AOS && layout != BH_LAYOUT_SOA) {
+        set_error("layout must be BH_LAYOUT_AOS or BH_LAYOUT_SOA");
+        return BH_ERR_INVALID_ARGUMENT;
+    }
+    if (n < 0 || n > INT32_MAX) {
+        set_error("n must be in [0, 2^31 - 1]");
+        return BH_ERR_INVALID_ARGUMENT;
+    }
+    if (n == 0) return BH_OK;
+    if (!states || !order) {
+        set_error("NULL pointer argument");
+        return BH_ERR_INVALID_ARGUMENT;
+    }
+    if (layout == BH_LAYOUT_AOS && (reinterpret_cast<uintptr_t>(states) & 15u)) {
+        set_error("state buffers must be 16-byte aligned");
+        return BH_ERR_INVALID_ARGUMENT;
+    }
+    if (!workspace || (reinterpret_cast<uintptr_t>(workspace) & 255u) ||
+        workspace_bytes < bh_propagate_order_workspace_bytes(n)) {
+        set_error("workspace must be 256-byte aligned and hold bh_propagate_order_workspace_bytes(n)");
+        return BH_ERR_WORKSPACE;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    char *base = static_cast<char *>(workspace);
+    unsigned long long *keys = reinterpret_cast<unsigned long long *>(base);
+    unsigned long long *keys_out =
+        reinterpret_cast<unsigned long long *>(base + align256((size_t)n * 8));
+    int32_t *idx = reinterpret_cast<int32_t *>(base + 2 * align256((size_t)n * 8));
+    void *temp = base + 2 * align256((size_t)n * 8) + align256((size_t)n * 4);
+    size_t temp_bytes = sort_temp_bytes(n);
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) {
+        set_error("bh_propagate_order: %s", cudaGetErrorString(e));
+        return BH_ERR_CUDA;
+    }
+    const long long need = (n + 255) / 256;
+    order_keys_kernel<<<(unsigned)(need < 8LL * sms ? need : 8LL * sms), 256, 0, s>>>(
+        states, layout, n, keys, idx);
+    e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys, keys_out, idx, order, (int)n,
+                                            0, end_bit_for(n), s);
+    if (e != cudaSuccess) {
+        set_error("bh_propagate_order: %s", cudaGetErrorString(e));
+        return BH_ERR_CUDA;
+    }
+    return BH_OK;
+}

@@ -381,7 +381,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) propagate_kernel(const TraceArgs 
         const unsigned act = __ballot_sync(full, g < groups);
         if (g < groups) {
             double h[N], lam[N], spin[N], mass[N];
-            long long acc[N];
+            long long acc[N], src[N];
             bool valid[N];
 #pragma unroll
             for (int l = 0; l < N; ++l) {
@@ -389,11 +389,22 @@ __global__ void __launch_bounds__(BLOCK, MINB) propagate_kernel(const TraceArgs 
                 valid[l] = i < n;
                 // A missing last ray repeats the group's first ray; its results
                 // are not stored.
-                const long long src = valid[l] ? i : g * N;
+                src[l] = valid[l] ? i : g * N;
+                if (args.order) {
+                    const long long o = args.order[src[l]];
+                    if (o < 0 || o >= n) {
+                        // Not a permutation: counted (the stats read fails the
+                        // call), and the position's own ray is traced instead.
+                        if (valid[l]) atomicAdd(&ws->bad_order, 1);
+                        valid[l] = false;
+                    } else {
+                        src[l] = o;
+                    }
+                }
                 RayState y0;
-                load_state(args.state0, n, args.layout, src, y0);
+                load_state(args.state0, n, args.layout, src[l], y0);
                 ys.set(l, y0);
-                spin[l] = args.spin_of_ray ? args.spin_of_ray[src] : args.spin;
+                spin[l] = args.spin_of_ray ? args.spin_of_ray[src[l]] : args.spin;
                 mass[l] = args.mass;
                 if (!(::fabs(spin[l]) <= mass[l])) {
                     // A ray's own spin outside the Kerr bound: counted (the
@@ -401,8 +412,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) propagate_kernel(const TraceArgs 
                     if (valid[l]) atomicAdd(&ws->bad_spins, 1);
                     spin[l] = 0.0;
                 }
-                h[l] = args.h_io[src];
-                lam[l] = args.lam_io ? args.lam_io[src] : 0.0;
+                h[l] = args.h_io[src[l]];
+                lam[l] = args.lam_io ? args.lam_io[src[l]] : 0.0;
                 acc[l] = 0;
             }
             const KerrV<V> K = make_kerr<V>(lanes_of<V>(mass), lanes_of<V>(spin));
@@ -519,7 +530,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) propagate_kernel(const TraceArgs 
 #pragma unroll
             for (int l = 0; l < N; ++l) {
                 if (!valid[l]) continue;
-                const long long i = g * N + l;
+                const long long i = src[l];
                 RayState yl = ys.get(l);
                 if constexpr (PROJECT) project_null(mass[l], spin[l], yl);
                 store_state(args.states, n, args.layout, i, yl);

@@ -184,17 +184,24 @@ def propagate(spacetime, state0: Array, n_steps: int, rtol: float = 1e-8,
               h0: Array | None = None, layout: str = "aos",
               timeout_s: float = 0.0, variant: int = -1, workspace=None,
               in_place: bool = False, project_every: int = 0, out=None,
-              chunks: int = 2, f64_radius: float | str = "auto"):
+              chunks: int = 2, f64_radius: float | str = "auto", order_rays=None):
     """n_steps attempted DP5(4) steps per ray with per-ray accept/reject and
     step update (tracer.py:111-120), no termination.
 
     Mixed policy: the stage arithmetic runs in float32 except in the float64
     band: while a ray of a warp lies between the outer horizon and
     ``f64_radius`` (units of M), the warp's attempt runs in float64 (with the
-    default launch shape; a warp holds rays [64 k, 64 k + 64) of the call).  The default ``"auto"`` puts the band's edge at
+    default launch shape).  The default ``"auto"`` puts the band's edge at
     8 u M / rtol (u = 2^-24), where float32 rounding of the curvature terms
     reaches the tolerance; 0 runs float32 stages everywhere.  Ignored by the
     float64 policy and, under ``"auto"``, by projecting calls.
+
+    ``order_rays`` (default: on whenever the band is): the launch takes the
+    rays of each segment of ORDER_SEGMENT consecutive rays inward-moving
+    first, by impact parameter (bh_propagate_order), so that rays passing the
+    hole alike share warps and fewer warps need the band; results come back
+    in the caller's order.  Off, a warp holds rays [64 k, 64 k + 64) of the
+    call.
 
     Returns (states, h, lam, accepted, stats): ``lam`` is the affine
     parameter each ray advanced (sum of its accepted step sizes, float64).
@@ -218,7 +225,7 @@ def propagate(spacetime, state0: Array, n_steps: int, rtol: float = 1e-8,
                              "nor in_place")
         return _propagate_streamed(spacetime, state0, n_steps, rtol, atol, initial_step,
                                    max_step, precision, spins, timeout_s, variant,
-                                   project_every, out, chunks, f64_radius)
+                                   project_every, out, chunks, f64_radius, order_rays)
     s, host = to_device_f64(state0, "state0")
     n = s.shape[0] if layout == "aos" else s.shape[-1]
     if layout == "aos" and (s.dim() != 2 or s.shape[1] != 8):
@@ -250,18 +257,41 @@ def propagate(spacetime, state0: Array, n_steps: int, rtol: float = 1e-8,
                                      initial_step)["variant"]
     ws = workspace if workspace is not None else torch.empty(
         lib.bh_trace_workspace_bytes(), dtype=torch.uint8, device=s.device)
+    band = _propagate_band(f64_radius, precision, project_every)
     cfg = make_config(1, rtol, atol, initial_step, max_step, 0.0, precision,
-                      layout, timeout_s, variant, 0, project_every,
-                      f64_radius=_propagate_band(f64_radius, precision, project_every))
+                      layout, timeout_s, variant, 0, project_every, f64_radius=band)
     stream = stream_handle()
-    _lib.check(lib.bh_propagate(cfg, float(spacetime.mass), float(spacetime.spin),
-                                ptr(spin_t), ptr(states), ptr(h), ptr(lam), ptr(acc), n,
-                                int(n_steps), ptr(ws), stream), "propagate")
+    order = _ray_order(lib, states, layout, n, order_rays, band) if n else None
+    _lib.check(lib.bh_propagate_ordered(cfg, float(spacetime.mass), float(spacetime.spin),
+                                        ptr(spin_t), ptr(states), ptr(h), ptr(lam), ptr(acc),
+                                        ptr(order), n, int(n_steps), ptr(ws), stream),
+               "propagate")
     stats = _lib.TraceStats()
     _lib.check(lib.bh_trace_stats_read(ptr(ws), stats, stream), "propagate")
     return (out_like(states, host, state0), out_like(h, host, state0),
             out_like(lam, host, state0),
             acc.cpu().numpy() if host is not None else acc, stats)
+
+
+# Rays per segment of bh_propagate_order (include/bh_b200.h): the launch order
+# stays within each segment.
+ORDER_SEGMENT = 16384
+
+
+def _ray_order(lib, states, layout: str, n: int, order_rays, band):
+    """The launch order of a propagate call's rays (an int32 device tensor),
+    or None for the rays' own order.  order_rays None orders whenever the
+    float64 band is on."""
+    if order_rays is None:
+        order_rays = band != 0.0
+    if not order_rays:
+        return None
+    order = torch.empty(n, dtype=torch.int32, device=states.device)
+    ws = torch.empty(lib.bh_propagate_order_workspace_bytes(n), dtype=torch.uint8,
+                     device=states.device)
+    _lib.check(lib.bh_propagate_order(ptr(states), _lib.LAYOUT[layout], n, ptr(order), ptr(ws),
+                                      ws.numel(), stream_handle()), "propagate order")
+    return order
 
 
 def _propagate_band(f64_radius, precision: str, project_every: int):
@@ -274,7 +304,7 @@ def _propagate_band(f64_radius, precision: str, project_every: int):
 
 def _propagate_streamed(spacetime, state0, n_steps, rtol, atol, initial_step, max_step,
                         precision, spins, timeout_s, variant, project_every, out, chunks,
-                        f64_radius="auto"):
+                        f64_radius="auto", order_rays=None):
     def pinned_f64(t, name, shape):
         if not (torch.is_tensor(t) and not t.is_cuda and t.is_pinned()
                 and t.dtype == torch.float64 and t.is_contiguous() and tuple(t.shape) == shape):
@@ -299,17 +329,19 @@ def _propagate_streamed(spacetime, state0, n_steps, rtol, atol, initial_step, ma
     acc = torch.empty(n, dtype=torch.int64, device=dev)
     spin_d = None if spins is None else torch.empty(n, dtype=torch.float64, device=dev)
     k = max(1, min(int(chunks), n))
-    # Pieces start at multiples of 64 rays: a warp of the mixed propagator
-    # holds rays [64 j, 64 j + 64) of its launch and decides its float64 band
-    # for all of them, so aligned pieces give every ray the warp-mates, and
-    # hence the results, of the single launch.
-    cuts = [min(n, (n * c // k + 63) // 64 * 64) for c in range(k)] + [n]
+    band = _propagate_band(f64_radius, precision, project_every)
+    ordered = (band != 0.0) if order_rays is None else bool(order_rays)
+    # A warp of the mixed propagator decides its float64 band for its 64 rays:
+    # pieces that start at multiples of 64 rays (of ORDER_SEGMENT rays when the
+    # launch orders its rays within such segments) give every ray the
+    # warp-mates, and hence the results, of the single launch.
+    align = ORDER_SEGMENT if ordered else 64
+    cuts = [min(n, (n * c // k + align - 1) // align * align) for c in range(k)] + [n]
     bounds = [(a, b) for a, b in zip(cuts[:-1], cuts[1:]) if b > a]
     ws = [torch.empty(lib.bh_trace_workspace_bytes(), dtype=torch.uint8, device=dev)
           for _ in bounds]
     cfg = make_config(1, rtol, atol, initial_step, max_step, 0.0, precision, "aos", timeout_s,
-                      variant, 0, project_every,
-                      f64_radius=_propagate_band(f64_radius, precision, project_every))
+                      variant, 0, project_every, f64_radius=band)
     main = torch.cuda.current_stream(dev)
     streams = [torch.cuda.Stream(dev), torch.cuda.Stream(dev)]
     for st in streams:
@@ -320,11 +352,14 @@ def _propagate_streamed(spacetime, state0, n_steps, rtol, atol, initial_step, ma
             states[a:b].copy_(state0[a:b], non_blocking=True)
             if spin_d is not None:
                 spin_d[a:b].copy_(spins[a:b], non_blocking=True)
-            _lib.check(lib.bh_propagate(cfg, float(spacetime.mass), float(spacetime.spin),
-                                        ptr(None if spin_d is None else spin_d[a:b]),
-                                        ptr(states[a:b]), ptr(h[a:b]), ptr(lam[a:b]),
-                                        ptr(acc[a:b]), b - a, int(n_steps), ptr(ws[c]),
-                                        st.cuda_stream), "propagate")
+            order = _ray_order(lib, states[a:b], "aos", b - a, ordered, band)
+            _lib.check(lib.bh_propagate_ordered(cfg, float(spacetime.mass),
+                                                float(spacetime.spin),
+                                                ptr(None if spin_d is None else spin_d[a:b]),
+                                                ptr(states[a:b]), ptr(h[a:b]), ptr(lam[a:b]),
+                                                ptr(acc[a:b]), ptr(order), b - a,
+                                                int(n_steps), ptr(ws[c]), st.cuda_stream),
+                       "propagate")
             out[a:b].copy_(states[a:b], non_blocking=True)
     for st in streams:
         main.wait_stream(st)

@@ -24,7 +24,7 @@
 extern "C" {
 #endif
 
-#define BH_ABI_VERSION 4
+#define BH_ABI_VERSION 5
 
 typedef enum {
     BH_OK = 0,
@@ -315,6 +315,33 @@ int bh_propagate(const bh_trace_config *config, double mass, double spin,
                  const double *spin_of_ray, double *states, double *h,
                  double *lam, int64_t *accepted, int64_t n, int64_t n_steps,
                  void *workspace, void *stream);
+
+/* bh_propagate with the rays taken in the order `order` (n,) int32: launch
+ * position i holds ray order[i], and every per-ray array stays indexed by
+ * ray.  NULL takes the rays in their own order (bh_propagate).  Entries
+ * outside [0, n) are not traced and make bh_trace_stats_read return
+ * BH_ERR_INVALID_ARGUMENT.  The mixed propagator decides its float64 band per
+ * warp of 64 launch positions; bh_propagate_order's order groups rays that
+ * pass the hole alike, so fewer warps need the band.  No counterpart in the
+ * reference, which steps every ray on its own. */
+int bh_propagate_ordered(const bh_trace_config *config, double mass, double spin,
+                         const double *spin_of_ray, double *states, double *h,
+                         double *lam, int64_t *accepted, const int32_t *order,
+                         int64_t n, int64_t n_steps, void *workspace, void *stream);
+
+/* Device workspace bh_propagate_order needs for n rays (256-byte aligned);
+ * 0 for n > 2^31 - 1. */
+size_t bh_propagate_order_workspace_bytes(int64_t n);
+
+/* Writes into order (n,) int32, on the device, the order in which
+ * bh_propagate_ordered should take the rays of states (layout AOS (n,8) or
+ * SOA (8,n)): within each segment of 16,384 consecutive rays, inward-moving
+ * rays first (x.p < 0), each group by impact parameter |x × p| / |p|; equal
+ * keys keep their order.  Deterministic.  A batch streamed in pieces that
+ * start at multiples of 16,384 rays gets, piece by piece, the order and
+ * hence the results of the single launch. */
+int bh_propagate_order(const double *states, int32_t layout, int64_t n, int32_t *order,
+                       void *workspace, size_t workspace_bytes, void *stream);
 
 /* ------------------------------------------------------------ adjoint */
 

@@ -65,7 +65,7 @@ def test_struct_layouts_match_header(tmp_path):
 
 
 def test_status_strings(bhlib):
-    assert bhlib.bh_abi_version() == 4
+    assert bhlib.bh_abi_version() == 5
     assert bhlib.bh_status_string(0) == b"ok"
     assert b"escape_radius" in bhlib.bh_status_string(-4)
     assert bhlib.bh_trace_workspace_bytes() == 256
@@ -204,3 +204,23 @@ def test_check_maps_status_to_reference_exceptions(bhlib):
         _lib.check(-4)
     with pytest.raises(RuntimeError):
         _lib.check(-3)
+
+
+def test_propagate_order_argument_validation(bhlib):
+    """bh_propagate_order checks its layout, size, pointers and workspace
+    before any CUDA call; its workspace covers two 64-bit key arrays, an int32
+    index array and the sort's temporary storage."""
+    import ctypes as C
+
+    fake = C.c_void_p(0x10000)  # never dereferenced: validation fails first
+    assert bhlib.bh_propagate_order(fake, 2, 4, fake, None, 0, None) == -1
+    assert b"layout" in bhlib.bh_last_error()
+    assert bhlib.bh_propagate_order(fake, 0, -1, fake, None, 0, None) == -1
+    assert bhlib.bh_propagate_order(fake, 0, 0, fake, None, 0, None) == 0
+    assert bhlib.bh_propagate_order(None, 0, 4, fake, None, 0, None) == -1
+    assert bhlib.bh_propagate_order(fake, 0, 4, fake, None, 0, None) == -5
+    need = bhlib.bh_propagate_order_workspace_bytes(100_000)
+    assert need % 256 == 0 and need >= 100_000 * (8 + 8 + 4)
+    assert bhlib.bh_propagate_order(fake, 0, 100_000, fake, fake, need - 1, None) == -5
+    assert bhlib.bh_propagate_order_workspace_bytes(1 << 31) == 0
+

@@ -15,7 +15,9 @@ different affine parameter.  Accuracy is therefore measured at equal affine
 parameter: the oracle integrates each ray to the lambda the kernel reached,
 at rtol 1e-12 (the reference's DP5(4) and controller, last step cut to land
 on lambda).  The headline bar, on the first 16,384 rays, holds the default
-mixed path (float64 band inside 8 u M / rtol) to the float64 kernel: the
+mixed path (float64 band inside 8 u M / rtol, the rays of each 16,384-ray
+segment launched inward-moving first by impact parameter) to the float64
+kernel: the
 fraction of rays within 1e-6 no more than 0.5 points below float64's, the
 99th percentile within 1e-6, and every ray within max(1e-6, 50 x its float64
 error).  Float32 stages everywhere (no band) are held to median 1e-6, 90th
@@ -209,3 +211,77 @@ def test_streamed_from_host_memory_equals_device_path(cuda):
                           spins=sp.pin_memory(), out=torch.empty_like(host_s).pin_memory())
             with pytest.raises(ValueError, match="Kerr bound"):
                 propagate(st, state0, 10, precision=precision, spins=sp.to(state0.device))
+
+
+def test_ray_order_is_a_permutation_within_segments(cuda):
+    """bh_propagate_order: a permutation of the rays that stays within each
+    segment of ORDER_SEGMENT rays and, inside one, puts inward-moving rays
+    first, each group by impact parameter |x × p| / |p| (float32 keys)."""
+    from blackhorizon_b200 import _lib
+    from blackhorizon_b200.integrators import ORDER_SEGMENT, _ray_order
+
+    n = 3 * ORDER_SEGMENT + 1000
+    state0, _, _ = c2_rays(n)
+    order = _ray_order(_lib.load(), state0, "aos", n, True, 0.0).cpu().numpy()
+    assert np.array_equal(np.sort(order), np.arange(n))
+    seg = np.arange(n) // ORDER_SEGMENT
+    assert np.array_equal(order // ORDER_SEGMENT, seg)
+    s = state0.cpu().numpy()
+    x, p = s[:, 1:4], s[:, 5:8]
+    b = np.linalg.norm(np.cross(x, p), axis=1) / np.linalg.norm(p, axis=1)
+    outward = ~((x * p).sum(axis=1) < 0.0)
+    for k in range(int(seg.max()) + 1):
+        o = order[seg == k]
+        assert np.all(np.diff(outward[o].astype(int)) >= 0)
+        for flag in (False, True):
+            bo = b[o[outward[o] == flag]]
+            # Keys are float32 of a float64 expression: allow its rounding.
+            assert np.all(np.diff(bo) >= -1e-6 * np.maximum(bo[1:], 1.0))
+    # The same order again (deterministic).
+    again = _ray_order(_lib.load(), state0, "aos", n, True, 0.0).cpu().numpy()
+    assert np.array_equal(order, again)
+
+
+def test_ray_order_leaves_float64_results_unchanged(cuda):
+    """The float64 policy has no band, so each ray's steps do not depend on its
+    warp-mates: the ordered launch returns the unordered one's results bit for
+    bit, every array in the caller's order."""
+    from blackhorizon_b200 import propagate
+    from blackhorizon_b200.kerr import KerrSpacetime
+
+    n = 20_000
+    state0, spins, _ = c2_rays(n)
+    st = KerrSpacetime(1.0, 0.0)
+    a = propagate(st, state0, 300, precision="fp64", spins=spins, order_rays=True)
+    b = propagate(st, state0, 300, precision="fp64", spins=spins, order_rays=False)
+    for k in range(4):
+        assert torch.equal(a[k], b[k])
+    assert a[4].attempts == b[4].attempts == n * 300
+
+
+def test_ordered_launch_rejects_a_bad_order(cuda):
+    """An order entry outside [0, n) is not traced, and the stats read fails
+    the call with ValueError."""
+    from blackhorizon_b200 import _lib
+    from blackhorizon_b200.backend import stream_handle
+    from blackhorizon_b200.integrators import make_config
+
+    lib = _lib.load()
+    n = 4096
+    state0, spins, _ = c2_rays(n)
+    work = state0.clone()
+    h = torch.full((n,), 0.1, dtype=torch.float64, device="cuda")
+    lam = torch.zeros(n, dtype=torch.float64, device="cuda")
+    acc = torch.empty(n, dtype=torch.int64, device="cuda")
+    ws = torch.empty(lib.bh_trace_workspace_bytes(), dtype=torch.uint8, device="cuda")
+    order = torch.arange(n, dtype=torch.int32, device="cuda")
+    order[77] = n + 5
+    cfg = make_config(1, 1e-8, 1e-10, 0.1, 2.0, 0.0, "mixed", f64_radius="auto")
+    _lib.check(lib.bh_propagate_ordered(cfg, 1.0, 0.0, spins.data_ptr(), work.data_ptr(),
+                                        h.data_ptr(), lam.data_ptr(), acc.data_ptr(),
+                                        order.data_ptr(), n, 10, ws.data_ptr(),
+                                        stream_handle()))
+    st = _lib.TraceStats()
+    with pytest.raises(ValueError, match="permutation"):
+        _lib.check(lib.bh_trace_stats_read(ws.data_ptr(), st, stream_handle()))
+
