@@ -278,20 +278,39 @@ def propagate(spacetime, state0: Array, n_steps: int, rtol: float = 1e-8,
 ORDER_SEGMENT = 16384
 
 
-def _ray_order(lib, states, layout: str, n: int, order_rays, band):
+def _ray_order(lib, states, layout: str, n: int, order_rays, band, buffers=None):
     """The launch order of a propagate call's rays (an int32 device tensor),
     or None for the rays' own order.  order_rays None orders whenever the
-    float64 band is on."""
+    float64 band is on.  buffers: (order, workspace) allocated by the caller
+    (_order_buffers), else allocated here on the current stream."""
     if order_rays is None:
         order_rays = band != 0.0
     if not order_rays:
         return None
-    order = torch.empty(n, dtype=torch.int32, device=states.device)
-    ws = torch.empty(lib.bh_propagate_order_workspace_bytes(n), dtype=torch.uint8,
-                     device=states.device)
+    order, ws = buffers if buffers is not None else _order_buffers(lib, n, states.device)
     _lib.check(lib.bh_propagate_order(ptr(states), _lib.LAYOUT[layout], n, ptr(order), ptr(ws),
                                       ws.numel(), stream_handle()), "propagate order")
     return order
+
+
+def _order_buffers(lib, n: int, device):
+    """An order array and bh_propagate_order's workspace for n rays."""
+    return (torch.empty(n, dtype=torch.int32, device=device),
+            torch.empty(lib.bh_propagate_order_workspace_bytes(n), dtype=torch.uint8,
+                        device=device))
+
+
+# Two side streams per device for the streamed path, kept for the process: the
+# caching allocator keeps freed blocks per stream, and streams made afresh on
+# every call kept missing that cache.
+_SIDE_STREAMS: dict = {}
+
+
+def _side_streams(dev):
+    key = dev.index if dev.index is not None else torch.cuda.current_device()
+    if key not in _SIDE_STREAMS:
+        _SIDE_STREAMS[key] = [torch.cuda.Stream(dev), torch.cuda.Stream(dev)]
+    return _SIDE_STREAMS[key]
 
 
 def _propagate_band(f64_radius, precision: str, project_every: int):
@@ -343,16 +362,22 @@ def _propagate_streamed(spacetime, state0, n_steps, rtol, atol, initial_step, ma
     cfg = make_config(1, rtol, atol, initial_step, max_step, 0.0, precision, "aos", timeout_s,
                       variant, 0, project_every, f64_radius=band)
     main = torch.cuda.current_stream(dev)
-    streams = [torch.cuda.Stream(dev), torch.cuda.Stream(dev)]
+    # Every buffer is allocated on the caller's stream before the pieces are
+    # enqueued.  An allocation inside a side stream's context could miss the
+    # allocator's cache and stall the host in the middle of the pipeline (one
+    # call in about ten stalled 16 ms so).  They stay alive until the side
+    # streams' work is done (the stats reads below synchronise).
+    order_bufs = [_order_buffers(lib, b - a, dev) if ordered else None for a, b in bounds]
+    streams = _side_streams(dev)
     for st in streams:
-        st.wait_stream(main)  # h and lam are initialised on the main stream
+        st.wait_stream(main)  # h, lam and the buffers come from the main stream
     for c, (a, b) in enumerate(bounds):
         st = streams[c % 2]
         with torch.cuda.stream(st):
             states[a:b].copy_(state0[a:b], non_blocking=True)
             if spin_d is not None:
                 spin_d[a:b].copy_(spins[a:b], non_blocking=True)
-            order = _ray_order(lib, states[a:b], "aos", b - a, ordered, band)
+            order = _ray_order(lib, states[a:b], "aos", b - a, ordered, band, order_bufs[c])
             _lib.check(lib.bh_propagate_ordered(cfg, float(spacetime.mass),
                                                 float(spacetime.spin),
                                                 ptr(None if spin_d is None else spin_d[a:b]),
