@@ -334,6 +334,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) tile_kernel(const TileArgs args) 
     }
     StageV<V> k1 = first_stage<V>(K, yw);
     bool queue_open = true;
+    int refill_waited = 0;  // iterations the warp's idle slots have waited
     // Launch counters of this thread, in shared memory: they change once per
     // ray, and in registers they cost the stepping loop five 64-bit values.
     __shared__ unsigned long long cnt[5][BLOCK];  // attempts, accepted, max, crossings, hits
@@ -360,7 +361,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) tile_kernel(const TileArgs args) 
         bool fresh[N];
 #pragma unroll
         for (int l = 0; l < N; ++l) fresh[l] = false;
-        if (total) {
+        // A refill costs the warp one first-stage evaluation however many slots
+        // it fills, so idle slots wait for company: at least a batch of
+        // them, or a number of iterations (bh_trace_common.cuh).
+        const bool do_refill =
+            total && (total >= BH_TILE_REFILL_BATCH || refill_waited >= BH_TILE_REFILL_WAIT);
+        refill_waited = total && !do_refill ? refill_waited + 1 : 0;
+        if (do_refill) {
             unsigned any = 0;
 #pragma unroll
             for (int l = 0; l < N; ++l) any |= mask[l];

@@ -84,6 +84,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args
     KerrV<V> K = make_kerr<V>(lanes_of<V>(mass0), lanes_of<V>(spin0));
     StageV<V> k1 = first_stage<V>(K, yw);
     bool queue_open = true;
+    int refill_waited = 0;  // iterations the warp's idle slots have waited
 
     for (unsigned iter = 0;; ++iter) {
         // ---- warp-aggregated refill of the idle ray slots
@@ -97,7 +98,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args
         bool fresh[N];
 #pragma unroll
         for (int l = 0; l < N; ++l) fresh[l] = false;
-        if (total) {
+        // Idle slots wait for company (bh_trace_common.cuh): a refill costs
+        // the warp one first-stage evaluation however many slots it fills.
+        const bool do_refill =
+            total && (total >= BH_TRACE_REFILL_BATCH || refill_waited >= BH_TRACE_REFILL_WAIT);
+        refill_waited = total && !do_refill ? refill_waited + 1 : 0;
+        if (do_refill) {
             unsigned any = 0;
 #pragma unroll
             for (int l = 0; l < N; ++l) any |= mask[l];
@@ -163,7 +169,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const TraceArgs args
         bool active = false;
 #pragma unroll
         for (int l = 0; l < N; ++l) active |= ray[l] >= 0;
-        if (!__any_sync(full, active)) break;
+        // Idle slots that wait for a refill batch keep the warp in the loop
+        // while the queue is open.
+        if (!__any_sync(full, active || queue_open)) break;
 
         if (active) {
             // ---- one controller iteration for every slot (tracer.py:109-149)
