@@ -56,13 +56,14 @@ static int end_bit_for(long long n) {
     return 33 + seg_bits;
 }
 
-static size_t sort_temp_bytes(long long n) {
-    size_t bytes = 0;
-    if (n <= 0) return 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const unsigned long long *)nullptr,
-                                    (unsigned long long *)nullptr, (const int32_t *)nullptr,
-                                    (int32_t *)nullptr, (int)n, 0, end_bit_for(n));
-    return bytes;
+// The sort's temporary storage for n keys; false when CUB cannot size it.
+static bool sort_temp_bytes(long long n, size_t *bytes) {
+    *bytes = 0;
+    if (n <= 0) return true;
+    return cub::DeviceRadixSort::SortPairs(nullptr, *bytes, (const unsigned long long *)nullptr,
+                                           (unsigned long long *)nullptr,
+                                           (const int32_t *)nullptr, (int32_t *)nullptr, (int)n,
+                                           0, end_bit_for(n)) == cudaSuccess;
 }
 
 }  // namespace bh
@@ -71,8 +72,9 @@ using namespace bh;
 
 extern "C" size_t bh_propagate_order_workspace_bytes(int64_t n) {
     if (n <= 0) return 256;
-    if (n > INT32_MAX) return 0;
-    return align256((size_t)n * 8) * 2 + align256((size_t)n * 4) + align256(sort_temp_bytes(n));
+    size_t temp = 0;
+    if (n > INT32_MAX || !sort_temp_bytes(n, &temp)) return 0;
+    return align256((size_t)n * 8) * 2 + align256((size_t)n * 4) + align256(temp);
 }
 
 extern "C" int bh_propagate_order(const double *states, int32_t layout, int64_t n,
@@ -95,8 +97,17 @@ extern "C" int bh_propagate_order(const double *states, int32_t layout, int64_t 
         set_error("state buffers must be 16-byte aligned");
         return BH_ERR_INVALID_ARGUMENT;
     }
-    if (!workspace || (reinterpret_cast<uintptr_t>(workspace) & 255u) ||
-        workspace_bytes < bh_propagate_order_workspace_bytes(n)) {
+    if (!workspace || (reinterpret_cast<uintptr_t>(workspace) & 255u)) {
+        set_error("workspace must be 256-byte aligned and hold bh_propagate_order_workspace_bytes(n)");
+        return BH_ERR_WORKSPACE;
+    }
+    // Sizing the sort asks CUDA for the device's properties.
+    const size_t ws_need = bh_propagate_order_workspace_bytes(n);
+    if (ws_need == 0) {
+        set_error("bh_propagate_order: the sort's temporary storage could not be sized");
+        return BH_ERR_CUDA;
+    }
+    if (workspace_bytes < ws_need) {
         set_error("workspace must be 256-byte aligned and hold bh_propagate_order_workspace_bytes(n)");
         return BH_ERR_WORKSPACE;
     }
@@ -107,7 +118,8 @@ extern "C" int bh_propagate_order(const double *states, int32_t layout, int64_t 
         reinterpret_cast<unsigned long long *>(base + align256((size_t)n * 8));
     int32_t *idx = reinterpret_cast<int32_t *>(base + 2 * align256((size_t)n * 8));
     void *temp = base + 2 * align256((size_t)n * 8) + align256((size_t)n * 4);
-    size_t temp_bytes = sort_temp_bytes(n);
+    size_t temp_bytes = 0;
+    sort_temp_bytes(n, &temp_bytes);
     int dev = 0, sms = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

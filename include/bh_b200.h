@@ -330,7 +330,7 @@ int bh_propagate_ordered(const bh_trace_config *config, double mass, double spin
                          int64_t n, int64_t n_steps, void *workspace, void *stream);
 
 /* Device workspace bh_propagate_order needs for n rays (256-byte aligned);
- * 0 for n > 2^31 - 1. */
+ * 0 for n > 2^31 - 1, or when the sort's temporary storage cannot be sized. */
 size_t bh_propagate_order_workspace_bytes(int64_t n);
 
 /* Writes into order (n,) int32, on the device, the order in which

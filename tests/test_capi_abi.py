@@ -208,8 +208,8 @@ def test_check_maps_status_to_reference_exceptions(bhlib):
 
 def test_propagate_order_argument_validation(bhlib):
     """bh_propagate_order checks its layout, size, pointers and workspace
-    before any CUDA call; its workspace covers two 64-bit key arrays, an int32
-    index array and the sort's temporary storage."""
+    alignment before any CUDA call; its workspace covers two 64-bit key
+    arrays, an int32 index array and the sort's temporary storage."""
     import ctypes as C
 
     fake = C.c_void_p(0x10000)  # never dereferenced: validation fails first
@@ -219,8 +219,11 @@ def test_propagate_order_argument_validation(bhlib):
     assert bhlib.bh_propagate_order(fake, 0, 0, fake, None, 0, None) == 0
     assert bhlib.bh_propagate_order(None, 0, 4, fake, None, 0, None) == -1
     assert bhlib.bh_propagate_order(fake, 0, 4, fake, None, 0, None) == -5
+    assert bhlib.bh_propagate_order(fake, 0, 4, fake, C.c_void_p(0x10010), 1 << 20, None) == -5
+    # Sizing the sort needs a CUDA device; without one the size is 0.
     need = bhlib.bh_propagate_order_workspace_bytes(100_000)
-    assert need % 256 == 0 and need >= 100_000 * (8 + 8 + 4)
-    assert bhlib.bh_propagate_order(fake, 0, 100_000, fake, fake, need - 1, None) == -5
+    if need:
+        assert need % 256 == 0 and need >= 100_000 * (8 + 8 + 4)
+        assert bhlib.bh_propagate_order(fake, 0, 100_000, fake, fake, need - 1, None) == -5
     assert bhlib.bh_propagate_order_workspace_bytes(1 << 31) == 0
 
