@@ -755,10 +755,11 @@ static const void *tile_kernel_for(int precision, int idx, bool inl, size_t *sme
 }
 
 // Measured on the offline renderer's 1280x800 supersample-2 frame (one
-// round): mixed 12.8 ms with one float ray per thread at 128 x 5 (96
-// registers), 13.2 ms at 128 x 4 and 256 x 2, 14.9 ms at 128 x 3, 18.8-21.7 ms
-// packed two per thread (the parking and refill work does not pack); float64
-// 30.6 ms at 256 x 2, 31.3 ms at 128 x 4, 32.2 ms at 128 x 3.
+// round, refill batching): mixed 11.8 ms with one float ray per thread at
+// 128 x 5 (96 registers), 12.3-12.4 ms at 128 x 3, 128 x 4 and 256 x 2,
+// 14.5-16.3 ms packed two per thread (the parking and refill work does not
+// pack); float64 24.9 ms at 256 x 2, 25.4 ms at 128 x 4, 26.4 ms at 128 x 3,
+// 30.0 ms at 128 x 2.
 int tile_default_variant(int precision) {
     return precision == BH_PRECISION_MIXED ? 2 : 3;
 }
