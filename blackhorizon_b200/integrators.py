@@ -200,8 +200,9 @@ def propagate(spacetime, state0: Array, n_steps: int, rtol: float = 1e-8,
     rays of each segment of ORDER_SEGMENT consecutive rays inward-moving
     first, by impact parameter (bh_propagate_order), so that rays passing the
     hole alike share warps and fewer warps need the band; results come back
-    in the caller's order.  Off, a warp holds rays [64 k, 64 k + 64) of the
-    call.
+    in the caller's order.  Off (and for launches of more than 2^31 - 1
+    rays, whose indices the order cannot hold), a warp holds rays
+    [64 k, 64 k + 64) of the call.
 
     Returns (states, h, lam, accepted, stats): ``lam`` is the affine
     parameter each ray advanced (sum of its accepted step sizes, float64).
@@ -287,7 +288,8 @@ def _ray_order(lib, states, layout: str, n: int, order_rays, band, buffers=None)
     (_order_buffers), else allocated here on the current stream."""
     if order_rays is None:
         order_rays = band != 0.0
-    if not order_rays:
+    # The order holds int32 ray indices: larger launches take the rays as given.
+    if not order_rays or n > _INT32_MAX:
         return None
     order, ws = buffers if buffers is not None else _order_buffers(lib, n, states.device)
     _lib.check(lib.bh_propagate_order(ptr(states), _lib.LAYOUT[layout], n, ptr(order), ptr(ws),
@@ -295,8 +297,14 @@ def _ray_order(lib, states, layout: str, n: int, order_rays, band, buffers=None)
     return order
 
 
+_INT32_MAX = 2**31 - 1
+
+
 def _order_buffers(lib, n: int, device):
-    """An order array and bh_propagate_order's workspace for n rays."""
+    """An order array and bh_propagate_order's workspace for n rays (None
+    beyond the int32 range, where the launch takes the rays as given)."""
+    if n > _INT32_MAX:
+        return None
     return (torch.empty(n, dtype=torch.int32, device=device),
             torch.empty(lib.bh_propagate_order_workspace_bytes(n), dtype=torch.uint8,
                         device=device))
