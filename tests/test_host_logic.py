@@ -207,3 +207,23 @@ def test_camera_paths_match_reference():
         CameraPath([])
     with pytest.raises(ValueError):
         CameraPath([keys[1], keys[0]])
+
+
+def test_streamed_pieces_cover_the_batch_at_aligned_starts():
+    """The streamed propagate's pieces: contiguous, covering [0, n), each
+    starting at a multiple of the alignment (64 rays, or the ray order's
+    16,384-ray segment); with three or more pieces the first and the last hold
+    about n/16 rays."""
+    from blackhorizon_b200.integrators import ORDER_SEGMENT, _pieces
+
+    for n in (1, 63, 64, 1000, 50_000, 1 << 20, 3 * ORDER_SEGMENT + 5):
+        for k in (1, 2, 3, 4, 7):
+            for align in (64, ORDER_SEGMENT):
+                b = _pieces(n, k, align)
+                assert b[0][0] == 0 and b[-1][1] == n
+                assert all(x[1] == y[0] for x, y in zip(b, b[1:]))
+                assert all(a < e for a, e in b)
+                assert all(a % align == 0 for a, _ in b)
+                assert len(b) <= k
+    b = _pieces(1 << 20, 3, ORDER_SEGMENT)
+    assert [e - a for a, e in b] == [65536, 917504, 65536]
