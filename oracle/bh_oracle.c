@@ -1,8 +1,8 @@
 /*
  * bh_oracle.c -- CPU restatement of BlackHorizon's geodesic hot path.
  *
- * TEST INFRASTRUCTURE ONLY: the checker for the CUDA library, never part of
- * the product.  Compile with -ffp-contract=off and without -ffast-math so each
+ * TEST INFRASTRUCTURE ONLY: the oracle that the CUDA library's results are
+ * checked against, never part of the product.  Compile with -ffp-contract=off and without -ffast-math so each
  * expression rounds exactly like the NumPy expression it restates.  The
  * association order of every sum and product below follows the reference
  * expression left to right; NumPy reduces a 3-element axis sequentially and an

@@ -1,8 +1,8 @@
 """ctypes front end of the CPU oracle (``oracle/bh_oracle.c``).
 
 TEST INFRASTRUCTURE ONLY.  The parity tests, ``__graft_entry__.smoke()`` and
-the CPU-baseline leg of ``bench.py`` use this module as the checker for the
-CUDA library; the product package ``blackhorizon_b200`` never imports it.
+the CPU-baseline leg of ``bench.py`` check the CUDA library's results against
+this oracle; the product package ``blackhorizon_b200`` never imports it.
 
 Each wrapper names the reference function (MegaKruk/BlackHorizon, path within
 that project) whose behaviour the C restatement follows.
