@@ -5,7 +5,7 @@
 Compiles every .cu under blackhorizon_b200/csrc with
 ``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3`` and links one shared
 library with the CUDA runtime linked statically, so the library only needs
-the driver at run time.  ``-Xptxas -v`` output (registers, spills, shared
+the CUDA driver at run time.  ``-Xptxas -v`` output (registers, spills, shared
 memory per kernel) is written to blackhorizon_b200/_build/ptxas.log.
 """
 
