@@ -118,17 +118,23 @@ struct VaidyaGeo {
     double h, l[3], hs, ht, r;
 };
 
-// vaidya.py:285-325 (geometry_t).
+// vaidya.py:285-325 (geometry_t).  hint (may be null): the table bracket of
+// the ray's previous evaluation, or -1; the search for v starts there (the
+// same bracket as the bisection's) and the hint takes v's bracket.  A ray's v
+// moves little between evaluations, so the search costs a load or two instead
+// of a bisection's chain of dependent loads.
 __device__ __forceinline__ void vd_geometry(const VaidyaDev &d, double t, double x, double y,
-                                            double z, VaidyaGeo &g) {
+                                            double z, VaidyaGeo &g, long long *hint = nullptr) {
     const double r = np_max(::sqrt((x * x + y * y) + z * z), 1e-9);
     g.r = r;
     g.l[0] = x / r; g.l[1] = y / r; g.l[2] = z / r;
     const double v = t + r, eps = 1e-4;
     // The five mass samples of the central differences need the v-dependent
     // parts at three times only, and v +- eps lie in or next to v's bracket.
-    long long lo = 0;
-    const VdMassAt a0 = vd_mass_at(d, v, &lo, false);
+    const bool near = hint && *hint >= 0;
+    long long lo = near ? *hint : 0;
+    const VdMassAt a0 = vd_mass_at(d, v, &lo, near);
+    if (hint) *hint = lo;
     long long lo_p = lo, lo_m = lo;
     const VdMassAt ap = vd_mass_at(d, v + eps, &lo_p, true);
     const VdMassAt am = vd_mass_at(d, v - eps, &lo_m, true);
@@ -144,9 +150,10 @@ __device__ __forceinline__ void vd_geometry(const VaidyaDev &d, double t, double
 }
 
 // vaidya.py:356-394 (vaidya_geodesic_rhs).
-__device__ __forceinline__ RayState vd_rhs(const VaidyaDev &d, const RayState &y) {
+__device__ __forceinline__ RayState vd_rhs(const VaidyaDev &d, const RayState &y,
+                                           long long *hint = nullptr) {
     VaidyaGeo g;
-    vd_geometry(d, y.t, y.x, y.y, y.z, g);
+    vd_geometry(d, y.t, y.x, y.y, y.z, g, hint);
     const double l_dot_p = (g.l[0] * y.px + g.l[1] * y.py) + g.l[2] * y.pz;
     const double lp = -y.pt + l_dot_p;
     const double lp2 = lp * lp;
@@ -170,11 +177,12 @@ __device__ __forceinline__ RayState vd_axpy(const RayState &y, double a, const R
 }
 
 // rk4_step (integrators.py:57-73) with the surrogate's RHS, all float64.
-__device__ __forceinline__ void vd_rk4(const VaidyaDev &d, RayState &y, double h) {
-    const RayState k1 = vd_rhs(d, y);
-    const RayState k2 = vd_rhs(d, vd_axpy(y, 0.5 * h, k1));
-    const RayState k3 = vd_rhs(d, vd_axpy(y, 0.5 * h, k2));
-    const RayState k4 = vd_rhs(d, vd_axpy(y, h, k3));
+__device__ __forceinline__ void vd_rk4(const VaidyaDev &d, RayState &y, double h,
+                                       long long *hint = nullptr) {
+    const RayState k1 = vd_rhs(d, y, hint);
+    const RayState k2 = vd_rhs(d, vd_axpy(y, 0.5 * h, k1), hint);
+    const RayState k3 = vd_rhs(d, vd_axpy(y, 0.5 * h, k2), hint);
+    const RayState k4 = vd_rhs(d, vd_axpy(y, h, k3), hint);
     const double h6 = h / 6.0;
     y.t += h6 * (k1.t + 2.0 * k2.t + 2.0 * k3.t + k4.t);
     y.x += h6 * (k1.x + 2.0 * k2.x + 2.0 * k3.x + k4.x);
@@ -255,6 +263,7 @@ __global__ void __launch_bounds__(128) vd_trace_kernel(const VaidyaTraceArgs a) 
     const unsigned lt_mask = (1u << lane) - 1u;
     const long long n = a.n;
     long long ray = -1, it = 0;
+    long long vlo = -1;  // the ray's last table bracket (vd_geometry)
     RayState y{0.0, 10.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0};
     bool queue_open = true;
     unsigned long long my_steps = 0;
@@ -281,6 +290,7 @@ __global__ void __launch_bounds__(128) vd_trace_kernel(const VaidyaTraceArgs a) 
                     load_state(a.state0, n, BH_LAYOUT_AOS, idx, y);
                     ray = idx;
                     it = 0;
+                    vlo = -1;
                     double *e = a.escape_dir + 3 * idx;
                     e[0] = e[1] = e[2] = 0.0;
                     a.end_mass[idx] = 0.0;
@@ -322,7 +332,7 @@ __global__ void __launch_bounds__(128) vd_trace_kernel(const VaidyaTraceArgs a) 
             }
         }
         if (!step) continue;
-        vd_rk4(a.d, y, h);
+        vd_rk4(a.d, y, h, &vlo);
         ++it;
     }
     for (int off = 16; off > 0; off >>= 1) {
