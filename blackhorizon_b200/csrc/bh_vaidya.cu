@@ -23,6 +23,7 @@ namespace bh {
 struct VaidyaDev {
     double mass, charge, q2, tail_mass, tail_start, tail_power, shell_start_v, shell_width,
         mass_cap;
+    double tail_unit;  // tail_start / tail_start, rounded on the host
     const double *sv, *sr, *sm2;
     long long n;
 };
@@ -31,7 +32,8 @@ struct VaidyaDev {
 // values at nodes, slope (x - x_j) + y_j between.  vd_locate finds the
 // bracket xp[lo] <= x < xp[lo + 1] of an interior x (xp[0] <= x <
 // xp[n - 1]); vd_locate_near finds it from the bracket of a nearby point,
-// the same index the bisection gives.
+// the same index the bisection gives.  vd_interp_slope evaluates the bracket
+// with its slope from vd_slope.
 __device__ __forceinline__ long long vd_locate(double x, const double *xp, long long n) {
     long long lo = 0, hi = n - 1;
     while (hi - lo > 1) {  // xp[lo] <= x < xp[hi]
@@ -49,35 +51,41 @@ __device__ __forceinline__ long long vd_locate_near(double x, long long lo, cons
     }
     return vd_locate(x, xp, n);
 }
-__device__ __forceinline__ double vd_interp_in(double x, long long lo, const double *xp,
-                                               const double *fp) {
-    if (xp[lo] == x) return fp[lo];
-    const double slope = __ddiv_rn(__dsub_rn(fp[lo + 1], fp[lo]), __dsub_rn(xp[lo + 1], xp[lo]));
-    return __dadd_rn(__dmul_rn(slope, __dsub_rn(x, xp[lo])), fp[lo]);
+__device__ __forceinline__ double vd_slope(long long lo, const double *xp, const double *fp) {
+    return __ddiv_rn(__dsub_rn(fp[lo + 1], fp[lo]), __dsub_rn(xp[lo + 1], xp[lo]));
 }
-__device__ __forceinline__ double vd_interp(double x, const double *xp, const double *fp,
-                                            long long n) {
-    if (x != x) return x;
-    if (x < xp[0]) return fp[0];
-    if (x >= xp[n - 1]) return fp[n - 1];
-    return vd_interp_in(x, vd_locate(x, xp, n), xp, fp);
+__device__ __forceinline__ double vd_interp_slope(double x, long long lo, const double *xp,
+                                                  const double *fp, double slope) {
+    if (xp[lo] == x) return fp[lo];
+    return __dadd_rn(__dmul_rn(slope, __dsub_rn(x, xp[lo])), fp[lo]);
 }
 
 // vaidya.py:153-159: m1(v) = M - dm (v_tail / max(v, v_tail))^(p - 1).
+// Before the tail (v <= v_tail) the base is v_tail / v_tail, the same
+// correctly rounded quotient on the host, and it is 1 for a finite positive
+// v_tail; pow(1, y) = 1 for every y (C99 F.9.4.4, as CUDA's pow).  The values
+// are the reference's without the division or the pow, which the
+// flythrough's rays (v below v_tail) never need.
 __device__ __forceinline__ double vd_m1(const VaidyaDev &d, double v) {
-    const double vs = np_max(v, d.tail_start);
-    return d.mass - d.tail_mass * ::pow(d.tail_start / vs, d.tail_power - 1.0);
+    const double base = v <= d.tail_start ? d.tail_unit : d.tail_start / np_max(v, d.tail_start);
+    return d.mass - d.tail_mass * (base == 1.0 ? 1.0 : ::pow(base, d.tail_power - 1.0));
 }
 
 // The v-dependent parts of m(v, r) (vaidya.py:244-269): the Price-tail mass
 // m1(v), the shell radius R(v) and the inflated excess, clipped.  The two
-// table columns share one bracket; *lo carries it to a nearby v (hint >= 0)
-// and returns this v's bracket (unchanged for v outside the table).
+// table columns share one bracket.  VdBracket carries a bracket and its two
+// slopes to a nearby v: the search starts there (the bisection's bracket all
+// the same) and the slopes, a function of the bracket alone, are reused while
+// it holds.  It takes v's bracket (unchanged for v outside the table); lo = -1
+// before the first look-up.
 struct VdMassAt {
     double m1, shell_r, inc;
 };
-__device__ __forceinline__ VdMassAt vd_mass_at(const VaidyaDev &d, double v, long long *lo,
-                                               bool hint) {
+struct VdBracket {
+    long long lo;
+    double k_r, k_m2;
+};
+__device__ __forceinline__ VdMassAt vd_mass_at(const VaidyaDev &d, double v, VdBracket *b) {
     VdMassAt o;
     double m2;
     if (v != v) {
@@ -90,10 +98,15 @@ __device__ __forceinline__ VdMassAt vd_mass_at(const VaidyaDev &d, double v, lon
         o.shell_r = d.sr[d.n - 1];
         m2 = d.sm2[d.n - 1];
     } else {
-        const long long j = hint ? vd_locate_near(v, *lo, d.sv, d.n) : vd_locate(v, d.sv, d.n);
-        *lo = j;
-        o.shell_r = vd_interp_in(v, j, d.sv, d.sr);
-        m2 = vd_interp_in(v, j, d.sv, d.sm2);
+        const long long j =
+            b->lo >= 0 ? vd_locate_near(v, b->lo, d.sv, d.n) : vd_locate(v, d.sv, d.n);
+        if (j != b->lo) {
+            b->lo = j;
+            b->k_r = vd_slope(j, d.sv, d.sr);
+            b->k_m2 = vd_slope(j, d.sv, d.sm2);
+        }
+        o.shell_r = vd_interp_slope(v, j, d.sv, d.sr, b->k_r);
+        m2 = vd_interp_slope(v, j, d.sv, d.sm2, b->k_m2);
     }
     o.m1 = vd_m1(d, v);
     o.inc = 0.0;
@@ -101,43 +114,46 @@ __device__ __forceinline__ VdMassAt vd_mass_at(const VaidyaDev &d, double v, lon
     return o;
 }
 
-// m(v, r) from the v-dependent parts: the blend across the shell width.
+// m(v, r) from the v-dependent parts: the blend across the shell width w.
+// Correctly rounded division is monotone, so R - r >= w gives a quotient >= 1
+// and R - r <= -w one <= -1: the clip's 1 and 0, taken without the division.
 __device__ __forceinline__ double vd_mass_r(const VaidyaDev &d, const VdMassAt &a, double r) {
-    const double t = np_min(np_max((a.shell_r - r) / d.shell_width + 0.5, 0.0), 1.0);
+    const double dr = a.shell_r - r;
+    const double t = dr >= d.shell_width    ? 1.0
+                     : dr <= -d.shell_width ? 0.0
+                                            : np_min(np_max(dr / d.shell_width + 0.5, 0.0), 1.0);
     const double blend = t * t * (3.0 - 2.0 * t);
     return a.m1 + blend * a.inc;
 }
 
 // vaidya.py:244-269: m(v, r).
 __device__ __forceinline__ double vd_mass(const VaidyaDev &d, double v, double r) {
-    long long lo = 0;
-    return vd_mass_r(d, vd_mass_at(d, v, &lo, false), r);
+    VdBracket b{-1, 0.0, 0.0};
+    return vd_mass_r(d, vd_mass_at(d, v, &b), r);
 }
 
 struct VaidyaGeo {
     double h, l[3], hs, ht, r;
 };
 
-// vaidya.py:285-325 (geometry_t).  hint (may be null): the table bracket of
-// the ray's previous evaluation, or -1; the search for v starts there (the
-// same bracket as the bisection's) and the hint takes v's bracket.  A ray's v
-// moves little between evaluations, so the search costs a load or two instead
-// of a bisection's chain of dependent loads.
+// vaidya.py:285-325 (geometry_t).  hint (may be null): the ray's bracket from
+// its previous evaluation (VdBracket), which takes v's.  A ray's v moves little
+// between evaluations, so the search costs a load or two instead of a
+// bisection's chain of dependent loads, and the slopes seldom change.
 __device__ __forceinline__ void vd_geometry(const VaidyaDev &d, double t, double x, double y,
-                                            double z, VaidyaGeo &g, long long *hint = nullptr) {
+                                            double z, VaidyaGeo &g, VdBracket *hint = nullptr) {
     const double r = np_max(::sqrt((x * x + y * y) + z * z), 1e-9);
     g.r = r;
     g.l[0] = x / r; g.l[1] = y / r; g.l[2] = z / r;
     const double v = t + r, eps = 1e-4;
     // The five mass samples of the central differences need the v-dependent
     // parts at three times only, and v +- eps lie in or next to v's bracket.
-    const bool near = hint && *hint >= 0;
-    long long lo = near ? *hint : 0;
-    const VdMassAt a0 = vd_mass_at(d, v, &lo, near);
-    if (hint) *hint = lo;
-    long long lo_p = lo, lo_m = lo;
-    const VdMassAt ap = vd_mass_at(d, v + eps, &lo_p, true);
-    const VdMassAt am = vd_mass_at(d, v - eps, &lo_m, true);
+    VdBracket b = hint ? *hint : VdBracket{-1, 0.0, 0.0};
+    const VdMassAt a0 = vd_mass_at(d, v, &b);
+    if (hint) *hint = b;
+    VdBracket b_p = b, b_m = b;
+    const VdMassAt ap = vd_mass_at(d, v + eps, &b_p);
+    const VdMassAt am = vd_mass_at(d, v - eps, &b_m);
     const double m0 = vd_mass_r(d, a0, r);
     const double m_v = (vd_mass_r(d, ap, r) - vd_mass_r(d, am, r)) / (2.0 * eps);
     const double m_r = (vd_mass_r(d, a0, r + eps) - vd_mass_r(d, a0, r - eps)) / (2.0 * eps);
@@ -151,7 +167,7 @@ __device__ __forceinline__ void vd_geometry(const VaidyaDev &d, double t, double
 
 // vaidya.py:356-394 (vaidya_geodesic_rhs).
 __device__ __forceinline__ RayState vd_rhs(const VaidyaDev &d, const RayState &y,
-                                           long long *hint = nullptr) {
+                                           VdBracket *hint = nullptr) {
     VaidyaGeo g;
     vd_geometry(d, y.t, y.x, y.y, y.z, g, hint);
     const double l_dot_p = (g.l[0] * y.px + g.l[1] * y.py) + g.l[2] * y.pz;
@@ -178,7 +194,7 @@ __device__ __forceinline__ RayState vd_axpy(const RayState &y, double a, const R
 
 // rk4_step (integrators.py:57-73) with the surrogate's RHS, all float64.
 __device__ __forceinline__ void vd_rk4(const VaidyaDev &d, RayState &y, double h,
-                                       long long *hint = nullptr) {
+                                       VdBracket *hint = nullptr) {
     const RayState k1 = vd_rhs(d, y, hint);
     const RayState k2 = vd_rhs(d, vd_axpy(y, 0.5 * h, k1), hint);
     const RayState k3 = vd_rhs(d, vd_axpy(y, 0.5 * h, k2), hint);
@@ -263,7 +279,7 @@ __global__ void __launch_bounds__(128) vd_trace_kernel(const VaidyaTraceArgs a) 
     const unsigned lt_mask = (1u << lane) - 1u;
     const long long n = a.n;
     long long ray = -1, it = 0;
-    long long vlo = -1;  // the ray's last table bracket (vd_geometry)
+    VdBracket vb{-1, 0.0, 0.0};  // the ray's last table bracket (vd_geometry)
     RayState y{0.0, 10.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0};
     bool queue_open = true;
     unsigned long long my_steps = 0;
@@ -290,7 +306,7 @@ __global__ void __launch_bounds__(128) vd_trace_kernel(const VaidyaTraceArgs a) 
                     load_state(a.state0, n, BH_LAYOUT_AOS, idx, y);
                     ray = idx;
                     it = 0;
-                    vlo = -1;
+                    vb.lo = -1;
                     double *e = a.escape_dir + 3 * idx;
                     e[0] = e[1] = e[2] = 0.0;
                     a.end_mass[idx] = 0.0;
@@ -332,7 +348,7 @@ __global__ void __launch_bounds__(128) vd_trace_kernel(const VaidyaTraceArgs a) 
             }
         }
         if (!step) continue;
-        vd_rk4(a.d, y, h, &vlo);
+        vd_rk4(a.d, y, h, &vb);
         ++it;
     }
     for (int off = 16; off > 0; off >>= 1) {
@@ -371,6 +387,7 @@ static int vd_dev(const bh_vaidya *s, VaidyaDev &d) {
     d.q2 = std::pow(s->charge, 2.0);
     d.tail_mass = s->tail_mass;
     d.tail_start = s->tail_start;
+    d.tail_unit = s->tail_start / s->tail_start;
     d.tail_power = s->tail_power;
     d.shell_start_v = s->shell_start_v;
     d.shell_width = s->shell_width;
