@@ -192,22 +192,38 @@ __device__ __forceinline__ RayState vd_axpy(const RayState &y, double a, const R
                     y.pt + a * k.pt, y.px + a * k.px, y.py + a * k.py, y.pz + a * k.pz};
 }
 
-// rk4_step (integrators.py:57-73) with the surrogate's RHS, all float64.
+// rk4_step (integrators.py:57-73) with the surrogate's RHS, all float64.  The
+// four stages run as a loop over one copy of the RHS, whose inlined code
+// would otherwise be four times the instruction cache's worth; the stage
+// offsets (h/2, h/2, h) and the weighted sum ((k1 + 2 k2) + 2 k3) + k4 are
+// the same operations in the same order, though the compiler may fuse other
+// multiply-adds than in the unrolled form (last-place differences; the
+// reference, in NumPy, fuses none).
 __device__ __forceinline__ void vd_rk4(const VaidyaDev &d, RayState &y, double h,
                                        VdBracket *hint = nullptr) {
-    const RayState k1 = vd_rhs(d, y, hint);
-    const RayState k2 = vd_rhs(d, vd_axpy(y, 0.5 * h, k1), hint);
-    const RayState k3 = vd_rhs(d, vd_axpy(y, 0.5 * h, k2), hint);
-    const RayState k4 = vd_rhs(d, vd_axpy(y, h, k3), hint);
+    RayState k = y, acc = y;
+#pragma unroll 1
+    for (int s = 0; s < 4; ++s) {
+        const RayState in = s == 0 ? y : vd_axpy(y, s == 3 ? h : 0.5 * h, k);
+        k = vd_rhs(d, in, hint);
+        if (s == 0) {
+            acc = k;
+        } else {
+            const double w = s == 3 ? 1.0 : 2.0;
+            acc = RayState{acc.t + w * k.t,   acc.x + w * k.x,   acc.y + w * k.y,
+                           acc.z + w * k.z,   acc.pt + w * k.pt, acc.px + w * k.px,
+                           acc.py + w * k.py, acc.pz + w * k.pz};
+        }
+    }
     const double h6 = h / 6.0;
-    y.t += h6 * (k1.t + 2.0 * k2.t + 2.0 * k3.t + k4.t);
-    y.x += h6 * (k1.x + 2.0 * k2.x + 2.0 * k3.x + k4.x);
-    y.y += h6 * (k1.y + 2.0 * k2.y + 2.0 * k3.y + k4.y);
-    y.z += h6 * (k1.z + 2.0 * k2.z + 2.0 * k3.z + k4.z);
-    y.pt += h6 * (k1.pt + 2.0 * k2.pt + 2.0 * k3.pt + k4.pt);
-    y.px += h6 * (k1.px + 2.0 * k2.px + 2.0 * k3.px + k4.px);
-    y.py += h6 * (k1.py + 2.0 * k2.py + 2.0 * k3.py + k4.py);
-    y.pz += h6 * (k1.pz + 2.0 * k2.pz + 2.0 * k3.pz + k4.pz);
+    y.t += h6 * acc.t;
+    y.x += h6 * acc.x;
+    y.y += h6 * acc.y;
+    y.z += h6 * acc.z;
+    y.pt += h6 * acc.pt;
+    y.px += h6 * acc.px;
+    y.py += h6 * acc.py;
+    y.pz += h6 * acc.pz;
 }
 
 __device__ __forceinline__ long long vd_tid() {
