@@ -78,7 +78,7 @@ def parse():
     ap.add_argument("--no-workloads", action="store_true",
                     help="skip the full-HD frame, the 64-camera batch and the adjoint")
     ap.add_argument("--profile-case",
-                    choices=("trace", "propagate", "adjoint", "tile", "realtime"),
+                    choices=("trace", "propagate", "adjoint", "tile", "realtime", "inflation"),
                     default=None,
                     help="run one small untimed case of that kernel (for ncu captures): "
                          "trace = the 1920x1080 frame (2 warm-up launches, then 1); "
@@ -86,6 +86,7 @@ def parse():
                          "tape (1 warm-up sweep, then 1); tile = the offline frame at "
                          "640x400 supersample 2 (1,024,000 rays), first pass only, twice; "
                          "realtime = the 1280x720 real-time frame, three launches; "
+                         "inflation = the 256x256 mass-inflation tile, three launches; "
                          "propagate = the raw-throughput workload at --rays rays and "
                          "--dp5-steps steps, three launches")
     return ap.parse_args()
@@ -683,19 +684,18 @@ def realtime_workload(device, with_cpu=True, warmup=2, reps=5, cpu_stride=8):
     return out
 
 
-def inflation_workload(device, with_cpu=True, warmup=1, reps=3, side=256, cpu_stride=4):
-    """The mass-inflation renderer's tracing (offline/inflation.py:165-240):
-    a rain observer at r = 1.3 M, v = 6 in the flythrough surrogate (q = 0.9,
-    Ori shell launched at v = 6, R = 1.2) looking inward (toward the
-    layer), side x side tetrad rays, fixed RK4 through the time-dependent
-    geometry."""
+def inflation_tile_inputs(device, side=256):
+    """The mass-inflation tile's rays: a rain observer at r = 1.3 M, v = 6 in
+    the flythrough surrogate (q = 0.9, Ori shell launched at v = 6, R = 1.2)
+    looking inward (toward the layer), side x side tetrad rays over a 70 deg
+    field.  Returns (spacetime, host states, device states, escape radius,
+    stop radius)."""
     import math as _m
 
     import torch
 
     from blackhorizon_b200.frames import build_tetrad, tetrad_ray_momenta
-    from blackhorizon_b200.vaidya import (ChargedVaidyaSpacetime, camera_four_velocity,
-                                          rain_state, trace_vaidya_tile)
+    from blackhorizon_b200.vaidya import ChargedVaidyaSpacetime, camera_four_velocity, rain_state
 
     st = ChargedVaidyaSpacetime(charge=0.9, shell_start_v=6.0, shell_start_radius=1.2)
     state = rain_state(st, np.array([1.3, 0.0, 0.0]), 6.0)
@@ -710,8 +710,17 @@ def inflation_workload(device, with_cpu=True, warmup=1, reps=3, side=256, cpu_st
     local /= np.linalg.norm(local, axis=-1, keepdims=True)
     mom = tetrad_ray_momenta(st.frozen(6.0), pos, tet, local)
     s0 = np.concatenate([np.full((side * side, 1), 6.0), np.tile(pos, (side * side, 1)), mom], 1)
-    s0d = torch.as_tensor(s0, device=device)
-    esc, stop = max(12.0, 2.5 * 1.3), st.inner_horizon_radius * 1.001
+    return st, s0, torch.as_tensor(s0, device=device), max(12.0, 2.5 * 1.3), \
+        st.inner_horizon_radius * 1.001
+
+
+def inflation_workload(device, with_cpu=True, warmup=1, reps=3, side=256, cpu_stride=4):
+    """The mass-inflation renderer's tracing (offline/inflation.py:165-240)
+    over inflation_tile_inputs' rays: fixed RK4 through the time-dependent
+    geometry."""
+    from blackhorizon_b200.vaidya import trace_vaidya_tile
+
+    st, s0, s0d, esc, stop = inflation_tile_inputs(device, side)
     run = lambda: trace_vaidya_tile(st, s0d, esc, stop)  # noqa: E731
     for _ in range(warmup):
         status, _, _, _ = run()
@@ -1110,6 +1119,12 @@ def profile_case(args):
         for _ in range(2):
             trace_tile(st, s0, esc, settings, radii, settings.rtol, settings.max_steps,
                        precision=prec, variant=args.variant)
+    elif args.profile_case == "inflation":
+        from blackhorizon_b200.vaidya import trace_vaidya_tile
+
+        st, _, s0d, esc, stop = inflation_tile_inputs(device)
+        for _ in range(3):
+            trace_vaidya_tile(st, s0d, esc, stop)
     elif args.profile_case == "propagate":
         from blackhorizon_b200.integrators import propagate
 
