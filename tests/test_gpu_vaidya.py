@@ -79,6 +79,43 @@ def _hamiltonian(st, s):
     return 0.5 * (-p_t ** 2 + np.sum(p_s * p_s, axis=-1)) - geo.h * lp ** 2
 
 
+def test_mass_function_exact_branches(cuda):
+    """m(v, r) (vaidya.py:153-269) where the device skips work:
+    - before the tail (v <= v_tail, v_tail itself included) the power's base is
+      v_tail / v_tail and pow(1, y) = 1, so m1 = M - dm exactly, as the
+      reference's float64 gives;
+    - where the shell blend's clip saturates (|R(v) - r| >= w), m is m1 (outside
+      the shell) or m1 + the clipped excess (inside) with no division.
+    Checked against a NumPy restatement on the library's own shell table:
+    exact where no power runs, within 1 ulp where one does (libm and CUDA may
+    round pow differently) and inside the shell (the sum m1 + 1.0 x excess may
+    be fused)."""
+    from blackhorizon_b200.vaidya import ChargedVaidyaSpacetime
+
+    rng = np.random.default_rng(7)
+    st = ChargedVaidyaSpacetime(charge=0.9)  # shell launched at v = 14, after the tail start
+    v = np.concatenate([rng.uniform(0.0, st.tail_start, 500), [st.tail_start, 0.0]])
+    r = rng.uniform(0.3, 30.0, v.size)
+    np.testing.assert_array_equal(st.mass_function(v, r), st.mass - st.tail_mass)
+    v_tail = rng.uniform(st.tail_start, 14.0, 500)
+    m1 = st.mass - st.tail_mass * (st.tail_start / v_tail) ** (st.tail_power - 1.0)
+    np.testing.assert_array_max_ulp(st.mass_function(v_tail, np.full(500, 5.0)), m1, maxulp=1)
+
+    fly = ChargedVaidyaSpacetime(charge=0.9, shell_start_v=6.0, shell_start_radius=1.2)
+    vs = rng.uniform(6.0, 11.0, 400)
+    shell_r = np.interp(vs, fly._shell_v, fly._shell_r)
+    m2 = np.interp(vs, fly._shell_v, fly._shell_m2)
+    inc = np.minimum(np.maximum(m2 - (fly.mass - fly.tail_mass), 0.0), fly.mass_cap)
+    gap = fly.shell_width * rng.uniform(1.5, 3.0, vs.size)
+    outside = fly.mass_function(vs, shell_r + gap)
+    np.testing.assert_array_equal(outside, fly.mass - fly.tail_mass)
+    inside_r = shell_r - gap
+    ok = inside_r > 0.05
+    inside = fly.mass_function(vs[ok], inside_r[ok])
+    np.testing.assert_array_max_ulp(inside, (fly.mass - fly.tail_mass) + inc[ok], maxulp=1)
+    assert (inc[ok] > 0).any()
+
+
 def test_reference_physics_anchors(cuda):
     """tests/test_vaidya.py:32-172 through the b200 surrogate."""
     from blackhorizon_b200.vaidya import ChargedVaidyaSpacetime, vaidya_geodesic_rhs, vaidya_rk4
