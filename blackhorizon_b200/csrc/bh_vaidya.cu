@@ -133,18 +133,24 @@ __device__ __forceinline__ double vd_mass(const VaidyaDev &d, double v, double r
 }
 
 struct VaidyaGeo {
-    double h, l[3], hs, ht, r;
+    double h, l[3], hs, ht, r, ir;
 };
 
-// vaidya.py:285-325 (geometry_t).  hint (may be null): the ray's bracket from
+// vaidya.py:285-325 (geometry_t).  The reference's twelve quotients by r, r^2,
+// r^3 and 2 eps (here and in vd_rhs) are products with one reciprocal 1 / r:
+// each differs from the quotient by an ulp or two, and float64 division is
+// the dearest operation of the RHS (the flythrough tile takes half the time;
+// its statuses are unchanged).  hint (may be null): the ray's bracket from
 // its previous evaluation (VdBracket), which takes v's.  A ray's v moves little
 // between evaluations, so the search costs a load or two instead of a
 // bisection's chain of dependent loads, and the slopes seldom change.
 __device__ __forceinline__ void vd_geometry(const VaidyaDev &d, double t, double x, double y,
                                             double z, VaidyaGeo &g, VdBracket *hint = nullptr) {
     const double r = np_max(::sqrt((x * x + y * y) + z * z), 1e-9);
+    const double ir = 1.0 / r;
     g.r = r;
-    g.l[0] = x / r; g.l[1] = y / r; g.l[2] = z / r;
+    g.ir = ir;
+    g.l[0] = x * ir; g.l[1] = y * ir; g.l[2] = z * ir;
     const double v = t + r, eps = 1e-4;
     // The five mass samples of the central differences need the v-dependent
     // parts at three times only, and v +- eps lie in or next to v's bracket.
@@ -155,12 +161,13 @@ __device__ __forceinline__ void vd_geometry(const VaidyaDev &d, double t, double
     const VdMassAt ap = vd_mass_at(d, v + eps, &b_p);
     const VdMassAt am = vd_mass_at(d, v - eps, &b_m);
     const double m0 = vd_mass_r(d, a0, r);
-    const double m_v = (vd_mass_r(d, ap, r) - vd_mass_r(d, am, r)) / (2.0 * eps);
-    const double m_r = (vd_mass_r(d, a0, r + eps) - vd_mass_r(d, a0, r - eps)) / (2.0 * eps);
-    const double r2 = r * r;
-    g.h = m0 / r - d.q2 / (2.0 * r2);
-    const double h_v = m_v / r;
-    const double h_r = m_r / r - m0 / r2 + d.q2 / (r2 * r);
+    const double i2e = 1.0 / (2.0 * eps);
+    const double m_v = (vd_mass_r(d, ap, r) - vd_mass_r(d, am, r)) * i2e;
+    const double m_r = (vd_mass_r(d, a0, r + eps) - vd_mass_r(d, a0, r - eps)) * i2e;
+    const double ir2 = ir * ir;
+    g.h = m0 * ir - 0.5 * d.q2 * ir2;
+    const double h_v = m_v * ir;
+    const double h_r = m_r * ir - m0 * ir2 + d.q2 * ir2 * ir;
     g.hs = h_v + h_r;
     g.ht = h_v;
 }
@@ -174,7 +181,7 @@ __device__ __forceinline__ RayState vd_rhs(const VaidyaDev &d, const RayState &y
     const double lp = -y.pt + l_dot_p;
     const double lp2 = lp * lp;
     const double c = 2.0 * g.h * lp;
-    const double k = c / g.r;
+    const double k = c * g.ir;
     RayState o;
     o.t = -y.pt + c;
     o.x = y.px - c * g.l[0];
