@@ -137,17 +137,18 @@ struct VaidyaGeo {
 };
 
 // vaidya.py:285-325 (geometry_t).  The reference's twelve quotients by r, r^2,
-// r^3 and 2 eps (here and in vd_rhs) are products with one reciprocal 1 / r:
-// each differs from the quotient by an ulp or two, and float64 division is
-// the dearest operation of the RHS (the flythrough tile takes half the time;
-// its statuses are unchanged).  hint (may be null): the ray's bracket from
+// r^3 and 2 eps (here and in vd_rhs) are products with one reciprocal 1 / r
+// (rcp_f64: the MUFU seed and two Newton steps): each differs from the
+// quotient by an ulp or two, and float64 division is the dearest operation of
+// the RHS (the flythrough tile takes half the time; its statuses are
+// unchanged).  hint (may be null): the ray's bracket from
 // its previous evaluation (VdBracket), which takes v's.  A ray's v moves little
 // between evaluations, so the search costs a load or two instead of a
 // bisection's chain of dependent loads, and the slopes seldom change.
 __device__ __forceinline__ void vd_geometry(const VaidyaDev &d, double t, double x, double y,
                                             double z, VaidyaGeo &g, VdBracket *hint = nullptr) {
     const double r = np_max(::sqrt((x * x + y * y) + z * z), 1e-9);
-    const double ir = 1.0 / r;
+    const double ir = rcp_f64(r);  // r >= 1e-9: within 2 ulp of 1 / r, no slow path
     g.r = r;
     g.ir = ir;
     g.l[0] = x * ir; g.l[1] = y * ir; g.l[2] = z * ir;
